@@ -1,0 +1,671 @@
+// C ABI of libacfd_gpu (include/acfd.h): case life cycle, host <-> device
+// coherence, and the schedule of one fluid time step
+// (EvolveFluidDynamics -> DiscretizeTime -> RungeKutta2/3 -> LLLU +
+// TreatBoundary, fluid_dynamics.c:55-148, boundary_treatment.c:28-65).
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "acfd_internal.cuh"
+
+namespace acfd {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+int cuda_status(cudaError_t e, const char *what)
+{
+    set_error("%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+    return (e == cudaErrorMemoryAllocation) ? ACFD_ERR_NOMEM : ACFD_ERR_CUDA;
+}
+
+int launch_stage_exact(const Grid &, const ModelParams &, const StageArgs &, int, bool, cudaStream_t);
+int launch_stage_fast(const Grid &, const ModelParams &, const StageArgs &, int, bool, cudaStream_t);
+int launch_stage_fp32(const Grid &, const ModelParams &, const StageArgs &, int, bool, cudaStream_t);
+int launch_weno_batch_exact(int, const double *, double *, int, cudaStream_t);
+int launch_weno_batch_fast(int, const double *, double *, int, cudaStream_t);
+int launch_weno_batch_fp32(int, const double *, double *, int, cudaStream_t);
+int launch_fhat_batch_exact(const ModelParams &, int, const double *, double *, int, cudaStream_t);
+int launch_fhat_batch_fast(const ModelParams &, int, const double *, double *, int, cudaStream_t);
+int launch_fhat_batch_fp32(const ModelParams &, int, const double *, double *, int, cudaStream_t);
+
+// IB (ib.cu)
+struct IbState;
+int ib_create(IbState **out);
+void ib_destroy(IbState *ib);
+int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, cudaStream_t st);
+int ib_count(const IbState *ib);
+int ib_compute_geometric_field(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partition_t &part,
+                               double *U, int *flags, cudaStream_t st);
+int ib_treat(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partition_t &part, double *U,
+             int *flags, int tn, cudaStream_t st);
+int ib_check(IbState *ib, cudaStream_t st);
+
+__global__ void set_scalar(double *p, double v)
+{
+    *p = v;
+}
+
+}  // namespace acfd
+
+using namespace acfd;
+
+struct acfd_case {
+    acfd_partition_t part;
+    acfd_model_t model;
+    Grid grid;
+    ModelParams mp;
+    int device = 0;
+    int mode = ACFD_FP64;
+    double *U = nullptr;       // [3][5][nn]
+    int *flags = nullptr;      // [4][nn]
+    double *d_dt = nullptr;    // device scalar dt of the current step
+    double *cfl_part = nullptr;
+    double *cfl_out = nullptr;
+    double *h_cfl = nullptr;   // pinned
+    acfd_node_t *staging = nullptr;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::vector<std::vector<FaceBox>> bc_groups;  // ordered, each group independent inside
+    IbState *ib = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_mode = -1;
+};
+
+namespace {
+
+bool viscous(const acfd_case *cs)
+{
+    return cs->model.refMu > 0.0;
+}
+
+double *level(acfd_case *cs, int l)
+{
+    return cs->U + (long long)l * kVars * cs->grid.nn;
+}
+
+// ordered ghost-fill plan: layer r = 0..max(ng), faces W,E,S,N,F,B; the two
+// faces normal to one axis never read each other's box, so they form one
+// launch (boundary_treatment.c:51-63)
+void build_bc_plan(acfd_case *cs)
+{
+    const acfd_partition_t &p = cs->part;
+    const int R = std::max(p.ng[0], std::max(p.ng[1], p.ng[2]));
+    cs->bc_groups.clear();
+    for (int r = 0; r <= R; ++r) {
+        for (int axis = 0; axis < 3; ++axis) {
+            std::vector<FaceBox> group;
+            for (int side = 0; side < 2; ++side) {
+                const int face = 1 + 2 * axis + side;
+                FaceBox b;
+                b.face = face;
+                b.r = r;
+                bool empty = false;
+                for (int s = 0; s < 3; ++s) {
+                    const int N = p.N[face][s];
+                    const int w = std::min(r, p.ng[s]);
+                    b.box[s][0] = p.ns[face][s][0] + w * (N - !N);
+                    b.box[s][1] = p.ns[face][s][1] + w * (N + !N) - (p.ng[s] < r) * (!!N);
+                    if (b.box[s][0] >= b.box[s][1]) {
+                        empty = true;
+                    }
+                }
+                // periodic boundary planes (r == 0) need no treatment
+                if (!empty && !(r == 0 && p.typeBC[face] == 4)) {
+                    group.push_back(b);
+                }
+            }
+            if (!group.empty()) {
+                cs->bc_groups.push_back(group);
+            }
+        }
+    }
+}
+
+int treat_boundary(acfd_case *cs, int tn)
+{
+    if (cs->ib && ib_count(cs->ib) > 0) {
+        int st = ib_treat(cs->ib, cs->grid, cs->mp, cs->part, cs->U, cs->flags, tn, cs->stream);
+        if (st != ACFD_OK) {
+            return st;
+        }
+    }
+    double *U = level(cs, tn);
+    for (const auto &grp : cs->bc_groups) {
+        int st = launch_domain_boundary(cs->grid, cs->mp, cs->part, grp.data(), (int)grp.size(), U, cs->stream);
+        if (st != ACFD_OK) {
+            return st;
+        }
+    }
+    return ACFD_OK;
+}
+
+int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int tn, int tm, int p)
+{
+    StageArgs a;
+    a.Uo = level(cs, to);
+    a.Un = level(cs, tn);
+    a.Um = level(cs, tm);
+    a.did = cs->flags;
+    a.dt = cs->d_dt;
+    a.dt_scale = dt_scale;
+    a.coeA = coeA;
+    a.coeB = coeB;
+    a.accumulate = 0;
+    if (p == ACFD_PHI) {
+        return launch_stage_phi(cs->grid, cs->mp, a, cs->stream);
+    }
+    int s0 = p, s1 = p + 1;
+    if (p == ACFD_DIMS) {
+        s0 = 0;
+        s1 = 3;
+    }
+    const bool visc = viscous(cs);
+    for (int s = s0; s < s1; ++s) {
+        a.accumulate = (cs->model.multidim == 1 && s != 0) ? 1 : 0;
+        int st;
+        switch (cs->mode) {
+            case ACFD_FP64_EXACT: st = launch_stage_exact(cs->grid, cs->mp, a, s, visc, cs->stream); break;
+            case ACFD_FP64: st = launch_stage_fast(cs->grid, cs->mp, a, s, visc, cs->stream); break;
+            default: st = launch_stage_fp32(cs->grid, cs->mp, a, s, visc, cs->stream); break;
+        }
+        if (st != ACFD_OK) {
+            return st;
+        }
+    }
+    return ACFD_OK;
+}
+
+#define TRY(x)                      \
+    do {                            \
+        int st__ = (x);             \
+        if (st__ != ACFD_OK) return st__; \
+    } while (0)
+
+// DiscretizeTime (fluid_dynamics.c:121-148) with dt = dt_scale * step dt
+int discretize(acfd_case *cs, double dt_scale, int s)
+{
+    if (cs->model.tScheme == 0) {
+        TRY(stage(cs, dt_scale, 0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN, s));
+        TRY(treat_boundary(cs, ACFD_TN));
+        TRY(stage(cs, dt_scale, 1.0 / 2.0, 1.0 / 2.0, ACFD_TO, ACFD_TN, ACFD_TO, s));
+        TRY(treat_boundary(cs, ACFD_TO));
+        return ACFD_OK;
+    }
+    TRY(stage(cs, dt_scale, 0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN, s));
+    TRY(treat_boundary(cs, ACFD_TN));
+    TRY(stage(cs, dt_scale, 3.0 / 4.0, 1.0 / 4.0, ACFD_TO, ACFD_TN, ACFD_TM, s));
+    TRY(treat_boundary(cs, ACFD_TM));
+    TRY(stage(cs, dt_scale, 1.0 / 3.0, 2.0 / 3.0, ACFD_TO, ACFD_TM, ACFD_TO, s));
+    TRY(treat_boundary(cs, ACFD_TO));
+    return ACFD_OK;
+}
+
+// EvolveFluidDynamics (fluid_dynamics.c:55-116); the step dt is in d_dt
+int evolve(acfd_case *cs)
+{
+    static const int kOrder[9][6] = {
+        {2, 1, 0, 0, 1, 2}, {2, 1, 1, 2, -1, -1}, {2, 0, 0, 2, -1, -1}, {1, 0, 0, 1, -1, -1},
+        {-1, -1, -1, -1, -1, -1}, {2, 2, -1, -1, -1, -1}, {-1, -1, -1, -1, -1, -1},
+        {1, 1, -1, -1, -1, -1}, {0, 0, -1, -1, -1, -1}};
+    if (cs->model.sState != 0) {
+        TRY(discretize(cs, 0.5, ACFD_PHI));
+    }
+    if (cs->model.multidim == 0) {
+        const int c = cs->part.collapse;
+        if (c >= 0 && c < 9) {
+            for (int n = 0; n < 6 && kOrder[c][n] >= 0; ++n) {
+                TRY(discretize(cs, 0.5, kOrder[c][n]));
+            }
+        }
+    } else if (cs->model.multidim == 1) {
+        TRY(discretize(cs, 0.5, ACFD_DIMS));
+        TRY(discretize(cs, 0.5, ACFD_DIMS));
+    }
+    if (cs->model.sState != 0) {
+        TRY(discretize(cs, 0.5, ACFD_PHI));
+    }
+    return ACFD_OK;
+}
+
+int set_dt(acfd_case *cs, double dt)
+{
+    set_scalar<<<1, 1, 0, cs->stream>>>(cs->d_dt, dt);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "set_scalar launch");
+}
+
+void release_graph(acfd_case *cs)
+{
+    if (cs->graph_exec) {
+        cudaGraphExecDestroy(cs->graph_exec);
+        cs->graph_exec = nullptr;
+    }
+    if (cs->graph) {
+        cudaGraphDestroy(cs->graph);
+        cs->graph = nullptr;
+    }
+    cs->graph_mode = -1;
+}
+
+int check_case(const acfd_case *cs)
+{
+    if (!cs) {
+        set_error("null case handle");
+        return ACFD_ERR_ARG;
+    }
+    return ACFD_OK;
+}
+
+int ensure_staging(acfd_case *cs)
+{
+    if (cs->staging) {
+        return ACFD_OK;
+    }
+    const size_t total = (size_t)cs->grid.n[0] * cs->grid.n[1] * cs->grid.n[2];
+    ACFD_CUDA(cudaMalloc(&cs->staging, total * sizeof(acfd_node_t)));
+    return ACFD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int acfd_abi_version(void)
+{
+    return ACFD_ABI_VERSION;
+}
+
+int acfd_last_error(char *buf, size_t len)
+{
+    if (!buf || len == 0) {
+        return ACFD_ERR_ARG;
+    }
+    snprintf(buf, len, "%s", g_err);
+    return ACFD_OK;
+}
+
+int acfd_init(const acfd_partition_t *part, const acfd_model_t *model, acfd_case_t **out)
+{
+    if (!part || !model || !out) {
+        set_error("acfd_init: null argument");
+        return ACFD_ERR_ARG;
+    }
+    *out = nullptr;
+    for (int s = 0; s < 3; ++s) {
+        if (part->n[s] < 3 || part->ns[0][s][0] < 0 || part->ns[0][s][1] > part->n[s]) {
+            set_error("acfd_init: invalid node counts/ranges on axis %d", s);
+            return ACFD_ERR_ARG;
+        }
+    }
+    if (model->sScheme != 0 && model->sScheme != 1) {
+        set_error("acfd_init: sScheme %d not supported", model->sScheme);
+        return ACFD_ERR_ARG;
+    }
+    if (model->tScheme != 0 && model->tScheme != 1) {
+        set_error("acfd_init: tScheme %d not supported", model->tScheme);
+        return ACFD_ERR_ARG;
+    }
+    acfd_case *cs = new acfd_case();
+    cs->part = *part;
+    cs->model = *model;
+    ACFD_CUDA(cudaGetDevice(&cs->device));
+    Grid &g = cs->grid;
+    for (int s = 0; s < 3; ++s) {
+        g.n[s] = part->n[s];
+        g.lo[s] = part->ns[0][s][0];
+        g.hi[s] = part->ns[0][s][1];
+        g.dd[s] = part->dd[s];
+    }
+    g.pitch = (part->n[0] + 7) & ~7;
+    g.nn = (long long)g.pitch * g.n[1] * g.n[2];
+    ModelParams &m = cs->mp;
+    m.gamma = model->gamma;
+    m.gasR = model->gasR;
+    m.cv = model->cv;
+    m.refMu = model->refMu;
+    m.refT = model->refT;
+    for (int s = 0; s < 3; ++s) m.g[s] = model->g[s];
+    m.sScheme = model->sScheme;
+    m.jacobMean = model->jacobMean;
+    m.fluxSplit = model->fluxSplit;
+    m.multidim = model->multidim;
+    m.sState = model->sState;
+    m.ibmLayer = model->ibmLayer;
+    int st = ACFD_OK;
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&cs->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        st = cuda_status(e, "cudaStreamCreate");
+        delete cs;
+        return st;
+    }
+    cs->own_stream = true;
+    const size_t ubytes = sizeof(double) * kLevels * kVars * (size_t)g.nn;
+    const size_t fbytes = sizeof(int) * 4 * (size_t)g.nn;
+    if ((e = cudaMalloc(&cs->U, ubytes)) != cudaSuccess ||
+        (e = cudaMalloc(&cs->flags, fbytes)) != cudaSuccess ||
+        (e = cudaMalloc(&cs->d_dt, sizeof(double))) != cudaSuccess ||
+        (e = cudaMalloc(&cs->cfl_part, sizeof(double) * 3 * kCflBlocks)) != cudaSuccess ||
+        (e = cudaMalloc(&cs->cfl_out, sizeof(double) * 3)) != cudaSuccess ||
+        (e = cudaMallocHost(&cs->h_cfl, sizeof(double) * 3)) != cudaSuccess) {
+        st = cuda_status(e, "acfd_init allocation");
+        acfd_finalize(cs);
+        return st;
+    }
+    // padding and never-written nodes: flags -1 (outside PIN), U zero
+    cudaMemsetAsync(cs->U, 0, ubytes, cs->stream);
+    cudaMemsetAsync(cs->flags, 0xff, fbytes, cs->stream);
+    if ((st = ib_create(&cs->ib)) != ACFD_OK) {
+        acfd_finalize(cs);
+        return st;
+    }
+    build_bc_plan(cs);
+    if ((e = cudaStreamSynchronize(cs->stream)) != cudaSuccess) {
+        st = cuda_status(e, "acfd_init");
+        acfd_finalize(cs);
+        return st;
+    }
+    *out = cs;
+    return ACFD_OK;
+}
+
+int acfd_finalize(acfd_case_t *cs)
+{
+    if (!cs) {
+        return ACFD_OK;
+    }
+    if (cs->stream) {
+        cudaStreamSynchronize(cs->stream);
+    }
+    release_graph(cs);
+    if (cs->ib) ib_destroy(cs->ib);
+    cudaFree(cs->U);
+    cudaFree(cs->flags);
+    cudaFree(cs->d_dt);
+    cudaFree(cs->cfl_part);
+    cudaFree(cs->cfl_out);
+    cudaFree(cs->staging);
+    if (cs->h_cfl) cudaFreeHost(cs->h_cfl);
+    if (cs->own_stream && cs->stream) cudaStreamDestroy(cs->stream);
+    delete cs;
+    return ACFD_OK;
+}
+
+int acfd_set_stream(acfd_case_t *cs, void *stream)
+{
+    TRY(check_case(cs));
+    ACFD_CUDA(cudaStreamSynchronize(cs->stream));
+    if (cs->own_stream) {
+        cudaStreamDestroy(cs->stream);
+        cs->own_stream = false;
+    }
+    if (stream) {
+        cs->stream = (cudaStream_t)stream;
+    } else {
+        ACFD_CUDA(cudaStreamCreateWithFlags(&cs->stream, cudaStreamNonBlocking));
+        cs->own_stream = true;
+    }
+    release_graph(cs);
+    return ACFD_OK;
+}
+
+int acfd_set_precision(acfd_case_t *cs, int mode)
+{
+    TRY(check_case(cs));
+    if (mode < ACFD_FP64_EXACT || mode > ACFD_FP32_HYBRID) {
+        set_error("acfd_set_precision: unknown mode %d", mode);
+        return ACFD_ERR_ARG;
+    }
+    if (mode == ACFD_FP32_HYBRID) {
+        set_error("acfd_set_precision: the hybrid form needs a loaded sensor");
+        return ACFD_ERR_STATE;
+    }
+    if (mode != cs->mode) {
+        release_graph(cs);
+    }
+    cs->mode = mode;
+    return ACFD_OK;
+}
+
+int acfd_sync_to_device(acfd_case_t *cs, const acfd_node_t *node, unsigned mask)
+{
+    TRY(check_case(cs));
+    if (!node) {
+        set_error("acfd_sync_to_device: null node array");
+        return ACFD_ERR_ARG;
+    }
+    TRY(ensure_staging(cs));
+    const size_t total = (size_t)cs->grid.n[0] * cs->grid.n[1] * cs->grid.n[2];
+    ACFD_CUDA(cudaMemcpyAsync(cs->staging, node, total * sizeof(acfd_node_t), cudaMemcpyHostToDevice, cs->stream));
+    TRY(launch_scatter_nodes(cs->grid, cs->staging, cs->U, cs->flags, mask, cs->stream));
+    ACFD_CUDA(cudaStreamSynchronize(cs->stream));
+    return ACFD_OK;
+}
+
+int acfd_sync_to_host(acfd_case_t *cs, acfd_node_t *node, unsigned mask)
+{
+    TRY(check_case(cs));
+    if (!node) {
+        set_error("acfd_sync_to_host: null node array");
+        return ACFD_ERR_ARG;
+    }
+    TRY(ensure_staging(cs));
+    const size_t total = (size_t)cs->grid.n[0] * cs->grid.n[1] * cs->grid.n[2];
+    // keep host members that are not selected: start from the host copy
+    if ((mask & ACFD_SYNC_ALL) != ACFD_SYNC_ALL) {
+        ACFD_CUDA(cudaMemcpyAsync(cs->staging, node, total * sizeof(acfd_node_t), cudaMemcpyHostToDevice,
+                                  cs->stream));
+    }
+    TRY(launch_gather_nodes(cs->grid, cs->U, cs->flags, cs->staging, mask, cs->stream));
+    ACFD_CUDA(cudaMemcpyAsync(node, cs->staging, total * sizeof(acfd_node_t), cudaMemcpyDeviceToHost, cs->stream));
+    ACFD_CUDA(cudaStreamSynchronize(cs->stream));
+    return ib_check(cs->ib, cs->stream);
+}
+
+int acfd_device_state(acfd_case_t *cs, double **U, int **flags, int *pitch, size_t *plane)
+{
+    TRY(check_case(cs));
+    if (U) *U = cs->U;
+    if (flags) *flags = cs->flags;
+    if (pitch) *pitch = cs->grid.pitch;
+    if (plane) *plane = (size_t)cs->grid.nn;
+    return ACFD_OK;
+}
+
+int acfd_cfl(acfd_case_t *cs, double vmax[3])
+{
+    TRY(check_case(cs));
+    if (!vmax) {
+        set_error("acfd_cfl: null output");
+        return ACFD_ERR_ARG;
+    }
+    TRY(launch_cfl(cs->grid, cs->mp, cs->U, cs->flags, cs->cfl_part, cs->cfl_out, cs->stream));
+    ACFD_CUDA(cudaMemcpyAsync(cs->h_cfl, cs->cfl_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, cs->stream));
+    ACFD_CUDA(cudaStreamSynchronize(cs->stream));
+    for (int s = 0; s < 3; ++s) {
+        vmax[s] = cs->h_cfl[s];
+    }
+    return ib_check(cs->ib, cs->stream);
+}
+
+int acfd_evolve_fluid(acfd_case_t *cs, double dt)
+{
+    TRY(check_case(cs));
+    TRY(set_dt(cs, dt));
+    TRY(evolve(cs));
+    return ACFD_OK;
+}
+
+int acfd_evolve_fluid_graph(acfd_case_t *cs, double dt)
+{
+    TRY(check_case(cs));
+    TRY(set_dt(cs, dt));
+    if (!cs->graph_exec || cs->graph_mode != cs->mode) {
+        release_graph(cs);
+        ACFD_CUDA(cudaStreamBeginCapture(cs->stream, cudaStreamCaptureModeThreadLocal));
+        int st = evolve(cs);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(cs->stream, &graph);
+        if (st != ACFD_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        if (e != cudaSuccess) {
+            return cuda_status(e, "cudaStreamEndCapture");
+        }
+        cs->graph = graph;
+        ACFD_CUDA(cudaGraphInstantiate(&cs->graph_exec, cs->graph, 0));
+        cs->graph_mode = cs->mode;
+    }
+    ACFD_CUDA(cudaGraphLaunch(cs->graph_exec, cs->stream));
+    return ACFD_OK;
+}
+
+int acfd_discretize_time(acfd_case_t *cs, double dt, int s)
+{
+    TRY(check_case(cs));
+    if (s < 0 || s > ACFD_PHI) {
+        set_error("acfd_discretize_time: operator %d", s);
+        return ACFD_ERR_ARG;
+    }
+    TRY(set_dt(cs, dt));
+    return discretize(cs, 1.0, s);
+}
+
+int acfd_lllu(acfd_case_t *cs, double dt, double coeA, double coeB, int to, int tn, int tm, int s)
+{
+    TRY(check_case(cs));
+    if (to < 0 || to > 2 || tn < 0 || tn > 2 || tm < 0 || tm > 2 || s < 0 || s > ACFD_PHI || tn == tm) {
+        set_error("acfd_lllu: bad levels/operator");
+        return ACFD_ERR_ARG;
+    }
+    TRY(set_dt(cs, dt));
+    return stage(cs, 1.0, coeA, coeB, to, tn, tm, s);
+}
+
+int acfd_treat_boundary(acfd_case_t *cs, int tn)
+{
+    TRY(check_case(cs));
+    if (tn < 0 || tn > 2) {
+        set_error("acfd_treat_boundary: level %d", tn);
+        return ACFD_ERR_ARG;
+    }
+    return treat_boundary(cs, tn);
+}
+
+int acfd_geo_upload(acfd_case_t *cs, const acfd_polyhedron_t *poly, int totN)
+{
+    TRY(check_case(cs));
+    if (totN < 0 || (totN > 0 && !poly)) {
+        set_error("acfd_geo_upload: bad body list");
+        return ACFD_ERR_ARG;
+    }
+    TRY(ib_upload(cs->ib, poly, totN, cs->stream));
+    release_graph(cs);
+    return ACFD_OK;
+}
+
+int acfd_compute_geometric_field(acfd_case_t *cs)
+{
+    TRY(check_case(cs));
+    return ib_compute_geometric_field(cs->ib, cs->grid, cs->mp, cs->part, cs->U, cs->flags, cs->stream);
+}
+
+int acfd_treat_ib(acfd_case_t *cs, int tn)
+{
+    TRY(check_case(cs));
+    if (tn < 0 || tn > 2) {
+        set_error("acfd_treat_ib: level %d", tn);
+        return ACFD_ERR_ARG;
+    }
+    return ib_treat(cs->ib, cs->grid, cs->mp, cs->part, cs->U, cs->flags, tn, cs->stream);
+}
+
+static ModelParams params_of(const acfd_model_t *model)
+{
+    ModelParams m;
+    memset(&m, 0, sizeof(m));
+    m.gamma = model->gamma;
+    m.gasR = model->gasR;
+    m.cv = model->cv;
+    m.refMu = model->refMu;
+    m.refT = model->refT;
+    m.sScheme = model->sScheme;
+    m.jacobMean = model->jacobMean;
+    m.fluxSplit = model->fluxSplit;
+    m.multidim = model->multidim;
+    m.ibmLayer = model->ibmLayer;
+    return m;
+}
+
+int acfd_weno_batch(int scheme, int mode, const double *F, double *Fhat, int count)
+{
+    if (!F || !Fhat || count < 0 || (scheme != 0 && scheme != 1)) {
+        set_error("acfd_weno_batch: bad arguments");
+        return ACFD_ERR_ARG;
+    }
+    double *dF = nullptr, *dO = nullptr;
+    ACFD_CUDA(cudaMalloc(&dF, sizeof(double) * 25 * (size_t)(count ? count : 1)));
+    cudaError_t e = cudaMalloc(&dO, sizeof(double) * 5 * (size_t)(count ? count : 1));
+    if (e != cudaSuccess) {
+        cudaFree(dF);
+        return cuda_status(e, "cudaMalloc");
+    }
+    int st = ACFD_OK;
+    if ((e = cudaMemcpy(dF, F, sizeof(double) * 25 * (size_t)count, cudaMemcpyHostToDevice)) != cudaSuccess) {
+        st = cuda_status(e, "cudaMemcpy");
+    }
+    if (st == ACFD_OK) {
+        st = (mode == ACFD_FP64_EXACT) ? launch_weno_batch_exact(scheme, dF, dO, count, 0)
+             : (mode == ACFD_FP64)     ? launch_weno_batch_fast(scheme, dF, dO, count, 0)
+                                       : launch_weno_batch_fp32(scheme, dF, dO, count, 0);
+    }
+    if (st == ACFD_OK && (e = cudaMemcpy(Fhat, dO, sizeof(double) * 5 * (size_t)count, cudaMemcpyDeviceToHost)) != cudaSuccess) {
+        st = cuda_status(e, "cudaMemcpy");
+    }
+    cudaFree(dF);
+    cudaFree(dO);
+    return st;
+}
+
+int acfd_fhat_batch(const acfd_model_t *model, int s, int mode, const double *Ust, double *Fhat, int count)
+{
+    if (!model || !Ust || !Fhat || count < 0 || s < 0 || s > 2) {
+        set_error("acfd_fhat_batch: bad arguments");
+        return ACFD_ERR_ARG;
+    }
+    const ModelParams m = params_of(model);
+    double *dU = nullptr, *dO = nullptr;
+    ACFD_CUDA(cudaMalloc(&dU, sizeof(double) * 30 * (size_t)(count ? count : 1)));
+    cudaError_t e = cudaMalloc(&dO, sizeof(double) * 5 * (size_t)(count ? count : 1));
+    if (e != cudaSuccess) {
+        cudaFree(dU);
+        return cuda_status(e, "cudaMalloc");
+    }
+    int st = ACFD_OK;
+    if ((e = cudaMemcpy(dU, Ust, sizeof(double) * 30 * (size_t)count, cudaMemcpyHostToDevice)) != cudaSuccess) {
+        st = cuda_status(e, "cudaMemcpy");
+    }
+    if (st == ACFD_OK) {
+        st = (mode == ACFD_FP64_EXACT) ? launch_fhat_batch_exact(m, s, dU, dO, count, 0)
+             : (mode == ACFD_FP64)     ? launch_fhat_batch_fast(m, s, dU, dO, count, 0)
+                                       : launch_fhat_batch_fp32(m, s, dU, dO, count, 0);
+    }
+    if (st == ACFD_OK && (e = cudaMemcpy(Fhat, dO, sizeof(double) * 5 * (size_t)count, cudaMemcpyDeviceToHost)) != cudaSuccess) {
+        st = cuda_status(e, "cudaMemcpy");
+    }
+    cudaFree(dU);
+    cudaFree(dO);
+    return st;
+}
+
+}  // extern "C"

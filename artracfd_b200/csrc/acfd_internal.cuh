@@ -1,0 +1,102 @@
+// Internal declarations of libacfd_gpu (not part of the C ABI).
+//
+// Device layout of one case ("structure of arrays", FP64 state):
+//   U[level][var][node]   level in {TO,TN,TM}, var in rho,rho*u,rho*v,rho*w,rho*eT
+//   node = (k * n[Y] + j) * pitch + i        pitch = n[X] rounded up to 8 doubles
+//   did, fid, lid, gst    int32 planes with the same node index
+// so that each variable of each level is a 3D array whose x-rows start on a
+// 64-byte boundary and whose accesses along x are fully coalesced.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "acfd.h"
+
+namespace acfd {
+
+constexpr int kLevels = 3;
+constexpr int kVars = 5;
+
+// Everything a stage kernel needs about the grid and the model, passed by
+// value (fits in kernel parameter space).
+struct Grid {
+    int n[3];         // nodes per dimension (with ghosts)
+    int pitch;        // padded x extent
+    long long nn;     // nodes per plane = n[Z]*n[Y]*pitch
+    int lo[3], hi[3]; // PIN range [lo, hi)
+    double dd[3];     // reciprocal mesh sizes
+};
+
+struct ModelParams {
+    double gamma, gasR, cv, refMu, refT;
+    double g[3];
+    int sScheme, jacobMean, fluxSplit, multidim, sState, ibmLayer;
+};
+
+// Arguments of one LLLU stage.
+struct StageArgs {
+    const double *Uo;     // level to (read at the node itself)
+    const double *Un;     // level tn (stencil level)
+    double *Um;           // level tm (written; may alias Uo)
+    const int *did;
+    const double *dt;     // device scalar: step dt
+    double dt_scale;      // this sweep uses dt_scale * (*dt) (0.5 for Strang halves)
+    double coeA, coeB;
+    int accumulate;       // operator-by-operator Y/Z: Um += coeB*r*Phi
+};
+
+// ---------------------------------------------------------------------------
+// error state (per host thread)
+// ---------------------------------------------------------------------------
+void set_error(const char *fmt, ...);
+int cuda_status(cudaError_t e, const char *what);
+
+#define ACFD_CUDA(call)                                           \
+    do {                                                          \
+        cudaError_t e__ = (call);                                 \
+        if (e__ != cudaSuccess) return acfd::cuda_status(e__, #call); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// kernel launchers (one translation unit per arithmetic form)
+// ---------------------------------------------------------------------------
+// FP64, reference operation order, compiled with --fmad=false
+int launch_stage_exact(const Grid &g, const ModelParams &m, const StageArgs &a, int s,
+                       bool viscous, cudaStream_t st);
+// FP64, reassociated with FMA
+int launch_stage_fast(const Grid &g, const ModelParams &m, const StageArgs &a, int s,
+                      bool viscous, cudaStream_t st);
+// FP32 stencil arithmetic with FP64 accumulation
+int launch_stage_fp32(const Grid &g, const ModelParams &m, const StageArgs &a, int s,
+                      bool viscous, cudaStream_t st);
+// gravity source stage
+int launch_stage_phi(const Grid &g, const ModelParams &m, const StageArgs &a, cudaStream_t st);
+
+// per-point twins
+int launch_weno_batch(int scheme, int mode, const double *F, double *Fhat, int count,
+                      cudaStream_t st);
+int launch_fhat_batch(const ModelParams &m, int s, int mode, const double *U, double *F,
+                      int count, cudaStream_t st);
+
+// domain ghost fill: one launch per group of independent face boxes
+struct FaceBox {
+    int box[3][2];
+    int face;  // 1..6
+    int r;     // layer
+};
+int launch_domain_boundary(const Grid &g, const ModelParams &m, const acfd_partition_t &part,
+                           const FaceBox *boxes, int nbox, double *U, cudaStream_t st);
+
+// CFL wave-speed maximum: partials (>= kCflBlocks*3 doubles) then out[3]
+constexpr int kCflBlocks = 296;
+int launch_cfl(const Grid &g, const ModelParams &m, const double *U, const int *did,
+               double *partials, double *out, cudaStream_t st);
+
+// layout conversion between the reference node records and the device planes
+int launch_scatter_nodes(const Grid &g, const acfd_node_t *staged, double *U, int *flags,
+                         unsigned mask, cudaStream_t st);
+int launch_gather_nodes(const Grid &g, const double *U, const int *flags, acfd_node_t *staged,
+                        unsigned mask, cudaStream_t st);
+
+}  // namespace acfd

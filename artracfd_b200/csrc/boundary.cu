@@ -1,0 +1,397 @@
+// Domain ghost-node fill (boundary_treatment.c:28-192), CFL wave-speed
+// maximum (solve.c:108-153), gravity source stage (source_term.c:21-39) and
+// the reference-layout <-> device-layout conversion.
+//
+// Compiled with --fmad=false: the primitive/conservative maps and the
+// method-of-images arithmetic are evaluated in the reference's order, so the
+// filled ghost values are bitwise those of the reference.
+#include <cstdio>
+
+#include "acfd_internal.cuh"
+
+namespace acfd {
+
+namespace {
+
+__device__ __forceinline__ long long node_of(const Grid &g, int i, int j, int k)
+{
+    return ((long long)k * g.n[1] + j) * g.pitch + i;
+}
+
+__device__ __forceinline__ void load5(const double *U, long long nn, long long id, double u[5])
+{
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        u[v] = U[v * nn + id];
+    }
+}
+
+__device__ __forceinline__ void store5(double *U, long long nn, long long id, const double u[5])
+{
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        U[v * nn + id] = u[v];
+    }
+}
+
+// MapPrimitive / MapConservative (cfd_commons.c:296-322)
+__device__ __forceinline__ void to_primitive(double gamma, double gasR, const double U[5], double Uo[6])
+{
+    Uo[0] = U[0];
+    Uo[1] = U[1] / U[0];
+    Uo[2] = U[2] / U[0];
+    Uo[3] = U[3] / U[0];
+    Uo[4] = (U[4] - 0.5 * (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / U[0]) * (gamma - 1.0);
+    Uo[5] = Uo[4] / (Uo[0] * gasR);
+}
+
+__device__ __forceinline__ void to_conservative(double gamma, const double Uo[6], double U[5])
+{
+    U[0] = Uo[0];
+    U[1] = Uo[0] * Uo[1];
+    U[2] = Uo[0] * Uo[2];
+    U[3] = Uo[0] * Uo[3];
+    U[4] = 0.5 * Uo[0] * (Uo[1] * Uo[1] + Uo[2] * Uo[2] + Uo[3] * Uo[3]) + Uo[4] / (gamma - 1.0);
+}
+
+struct FaceJob {
+    int lo[3];
+    int ext[3];
+    int N[3];
+    int LN[3];
+    int type;
+    int r;
+    long long count;
+    double given[6];
+};
+
+struct FaceJobs {
+    FaceJob job[2];
+    int njob;
+};
+
+__global__ void domain_fill(Grid g, ModelParams mp, FaceJobs jobs, double *U)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int q = 0;
+    if (t >= jobs.job[0].count) {
+        t -= jobs.job[0].count;
+        q = 1;
+        if (jobs.njob < 2 || t >= jobs.job[1].count) {
+            return;
+        }
+    }
+    const FaceJob &J = jobs.job[q];
+    const int i = J.lo[0] + (int)(t % J.ext[0]);
+    const long long rest = t / J.ext[0];
+    const int j = J.lo[1] + (int)(rest % J.ext[1]);
+    const int k = J.lo[2] + (int)(rest / J.ext[1]);
+    const long long nn = g.nn;
+    const long long id = node_of(g, i, j, k);
+    const int *N = J.N;
+    const int r = J.r;
+    double Ut[5];
+    if (r != 0) {
+        // ghost layer r
+        if (J.type == 2 || J.type == 3) {
+            double UO[5], UI[5], UoO[6], UoI[6], UoG[6];
+            load5(U, nn, node_of(g, i - r * N[0], j - r * N[1], k - r * N[2]), UO);
+            load5(U, nn, node_of(g, i - 2 * r * N[0], j - 2 * r * N[1], k - 2 * r * N[2]), UI);
+            to_primitive(mp.gamma, mp.gasR, UO, UoO);
+            to_primitive(mp.gamma, mp.gasR, UI, UoI);
+            // method of images (immersed_boundary.c:341-356)
+            UoG[1] = UoO[1] + UoO[1] - UoI[1];
+            UoG[2] = UoO[2] + UoO[2] - UoI[2];
+            UoG[3] = UoO[3] + UoO[3] - UoI[3];
+            UoG[4] = UoI[4];
+            UoG[5] = UoI[5];
+            UoG[0] = UoG[4] / (UoG[5] * mp.gasR);
+            to_conservative(mp.gamma, UoG, Ut);
+        } else if (J.type == 4) {
+            load5(U, nn, node_of(g, i - J.LN[0], j - J.LN[1], k - J.LN[2]), Ut);
+        } else {
+            load5(U, nn, node_of(g, i - N[0], j - N[1], k - N[2]), Ut);
+        }
+        store5(U, nn, id, Ut);
+        return;
+    }
+    // physical boundary node
+    switch (J.type) {
+        case 0:  // inflow
+            to_conservative(mp.gamma, J.given, Ut);
+            break;
+        case 1:  // outflow
+            load5(U, nn, node_of(g, i - N[0], j - N[1], k - N[2]), Ut);
+            break;
+        case 2:  // slip wall
+        case 3: {  // no-slip wall
+            double Uh[5], Uoh[6], UoO[6];
+            load5(U, nn, node_of(g, i - N[0], j - N[1], k - N[2]), Uh);
+            to_primitive(mp.gamma, mp.gasR, Uh, Uoh);
+            if (J.type == 2) {
+                UoO[1] = (double)(!N[0]) * Uoh[1];
+                UoO[2] = (double)(!N[1]) * Uoh[2];
+                UoO[3] = (double)(!N[2]) * Uoh[3];
+            } else {
+                UoO[1] = 0.0;
+                UoO[2] = 0.0;
+                UoO[3] = 0.0;
+            }
+            UoO[4] = Uoh[4];
+            UoO[5] = (0.0 > J.given[5]) ? Uoh[5] : J.given[5];
+            UoO[0] = UoO[4] / (UoO[5] * mp.gasR);
+            to_conservative(mp.gamma, UoO, Ut);
+            break;
+        }
+        default:  // periodic: the boundary plane is computed like an interior node
+            return;
+    }
+    store5(U, nn, id, Ut);
+}
+
+// CFL: per-direction max of |u_s| + sqrt(gamma*gasR*T) over PIN nodes with
+// did == 0 (the max is order independent, so the result is the reference's)
+__device__ __forceinline__ double vmax_of(double a, double b)
+{
+    return (a < b) ? b : a;  // NaN in b never replaces a, as in solve.c:145
+}
+
+__global__ void cfl_partial(Grid g, ModelParams mp, const double *U, const int *did, double *part)
+{
+    const int Lx = g.hi[0] - g.lo[0], Ly = g.hi[1] - g.lo[1], Lz = g.hi[2] - g.lo[2];
+    const long long total = (long long)Lx * Ly * Lz;
+    double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = g.lo[0] + (int)(t % Lx);
+        const long long rest = t / Lx;
+        const int j = g.lo[1] + (int)(rest % Ly);
+        const int k = g.lo[2] + (int)(rest / Ly);
+        const long long id = node_of(g, i, j, k);
+        if (did[id] != 0) {
+            continue;
+        }
+        double Uc[5], Uo[6];
+        load5(U, g.nn, id, Uc);
+        to_primitive(mp.gamma, mp.gasR, Uc, Uo);
+        const double c = sqrt(mp.gamma * mp.gasR * Uo[5]);
+        m0 = vmax_of(m0, fabs(Uo[1]) + c);
+        m1 = vmax_of(m1, fabs(Uo[2]) + c);
+        m2 = vmax_of(m2, fabs(Uo[3]) + c);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        m0 = vmax_of(m0, __shfl_xor_sync(0xffffffffu, m0, o));
+        m1 = vmax_of(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+        m2 = vmax_of(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+    }
+    __shared__ double sm[3][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        sm[0][warp] = m0;
+        sm[1][warp] = m1;
+        sm[2][warp] = m2;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double m = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            m = vmax_of(m, sm[threadIdx.x][w]);
+        }
+        part[3 * blockIdx.x + threadIdx.x] = m;
+    }
+}
+
+__global__ void cfl_final(const double *part, int nblocks, double *out)
+{
+    const int s = threadIdx.x;
+    if (s < 3) {
+        double m = 0.0;
+        for (int b = 0; b < nblocks; ++b) {
+            m = vmax_of(m, part[3 * b + s]);
+        }
+        out[s] = m;
+    }
+}
+
+// gravity source stage: LLLU with p = PHI (fluid_dynamics.c:177-214)
+__global__ void stage_phi(Grid g, ModelParams mp, StageArgs a)
+{
+    const int Lx = g.hi[0] - g.lo[0], Ly = g.hi[1] - g.lo[1], Lz = g.hi[2] - g.lo[2];
+    const long long total = (long long)Lx * Ly * Lz;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) {
+        return;
+    }
+    const int i = g.lo[0] + (int)(t % Lx);
+    const long long rest = t / Lx;
+    const int j = g.lo[1] + (int)(rest % Ly);
+    const int k = g.lo[2] + (int)(rest / Ly);
+    const long long id = node_of(g, i, j, k);
+    if (a.did[id] != 0) {
+        return;
+    }
+    const double dt = a.dt_scale * a.dt[0];
+    double Phi[5];
+    if (mp.sState == 0) {
+        for (int v = 0; v < 5; ++v) Phi[v] = 0.0;
+    } else {
+        double Un[5];
+        load5(a.Un, g.nn, id, Un);
+        const double V[3] = {Un[1] / Un[0], Un[2] / Un[0], Un[3] / Un[0]};
+        const double fb[3] = {Un[0] * mp.g[0], Un[0] * mp.g[1], Un[0] * mp.g[2]};
+        Phi[0] = 0.0;
+        Phi[1] = fb[0];
+        Phi[2] = fb[1];
+        Phi[3] = fb[2];
+        Phi[4] = fb[0] * V[0] + fb[1] * V[1] + fb[2] * V[2];
+    }
+    for (int v = 0; v < 5; ++v) {
+        const long long q = v * g.nn + id;
+        a.Um[q] = a.coeA * a.Uo[q] + a.coeB * (a.Un[q] + dt * Phi[v]);
+    }
+}
+
+// reference node records (AoS, 136 B) <-> device planes
+__global__ void scatter_nodes(Grid g, const acfd_node_t *staged, double *U, int *flags, unsigned mask)
+{
+    const long long total = (long long)g.n[0] * g.n[1] * g.n[2];
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) {
+        return;
+    }
+    const int i = (int)(t % g.n[0]);
+    const long long rest = t / g.n[0];
+    const int j = (int)(rest % g.n[1]);
+    const int k = (int)(rest / g.n[1]);
+    const long long id = node_of(g, i, j, k);
+    const acfd_node_t &nd = staged[t];
+    for (int l = 0; l < kLevels; ++l) {
+        if (mask & (1u << l)) {
+            for (int v = 0; v < kVars; ++v) {
+                U[((long long)l * kVars + v) * g.nn + id] = nd.U[l][v];
+            }
+        }
+    }
+    if (mask & ACFD_SYNC_FLAGS) {
+        flags[id] = nd.did;
+        flags[g.nn + id] = nd.fid;
+        flags[2 * g.nn + id] = nd.lid;
+        flags[3 * g.nn + id] = nd.gst;
+    }
+}
+
+__global__ void gather_nodes(Grid g, const double *U, const int *flags, acfd_node_t *staged, unsigned mask)
+{
+    const long long total = (long long)g.n[0] * g.n[1] * g.n[2];
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) {
+        return;
+    }
+    const int i = (int)(t % g.n[0]);
+    const long long rest = t / g.n[0];
+    const int j = (int)(rest % g.n[1]);
+    const int k = (int)(rest / g.n[1]);
+    const long long id = node_of(g, i, j, k);
+    acfd_node_t &nd = staged[t];
+    for (int l = 0; l < kLevels; ++l) {
+        if (mask & (1u << l)) {
+            for (int v = 0; v < kVars; ++v) {
+                nd.U[l][v] = U[((long long)l * kVars + v) * g.nn + id];
+            }
+        }
+    }
+    if (mask & ACFD_SYNC_FLAGS) {
+        nd.did = flags[id];
+        nd.fid = flags[g.nn + id];
+        nd.lid = flags[2 * g.nn + id];
+        nd.gst = flags[3 * g.nn + id];
+    }
+}
+
+unsigned blocks_for(long long n, int bs)
+{
+    return (unsigned)((n + bs - 1) / bs);
+}
+
+}  // namespace
+
+int launch_domain_boundary(const Grid &g, const ModelParams &m, const acfd_partition_t &part,
+                           const FaceBox *boxes, int nbox, double *U, cudaStream_t st)
+{
+    if (nbox < 1 || nbox > 2) {
+        set_error("domain boundary group of %d faces", nbox);
+        return ACFD_ERR_ARG;
+    }
+    FaceJobs jobs;
+    jobs.njob = nbox;
+    long long total = 0;
+    for (int q = 0; q < nbox; ++q) {
+        FaceJob &J = jobs.job[q];
+        const FaceBox &b = boxes[q];
+        const int p = b.face;
+        for (int s = 0; s < 3; ++s) {
+            J.lo[s] = b.box[s][0];
+            J.ext[s] = b.box[s][1] - b.box[s][0];
+            J.N[s] = part.N[p][s];
+            J.LN[s] = part.m[s] * part.N[p][s];
+        }
+        J.type = part.typeBC[p];
+        J.r = b.r;
+        J.count = (long long)J.ext[0] * J.ext[1] * J.ext[2];
+        for (int v = 0; v < 6; ++v) {
+            J.given[v] = part.varBC[p][v];
+        }
+        total += J.count;
+    }
+    if (nbox == 1) {
+        jobs.job[1] = jobs.job[0];
+        jobs.job[1].count = 0;
+    }
+    if (total == 0) {
+        return ACFD_OK;
+    }
+    domain_fill<<<blocks_for(total, 256), 256, 0, st>>>(g, m, jobs, U);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "domain_fill launch");
+}
+
+int launch_cfl(const Grid &g, const ModelParams &m, const double *U, const int *did, double *partials,
+               double *out, cudaStream_t st)
+{
+    cfl_partial<<<kCflBlocks, 256, 0, st>>>(g, m, U, did, partials);
+    cfl_final<<<1, 32, 0, st>>>(partials, kCflBlocks, out);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "cfl launch");
+}
+
+int launch_stage_phi(const Grid &g, const ModelParams &m, const StageArgs &a, cudaStream_t st)
+{
+    const long long total = (long long)(g.hi[0] - g.lo[0]) * (g.hi[1] - g.lo[1]) * (g.hi[2] - g.lo[2]);
+    if (total <= 0) {
+        return ACFD_OK;
+    }
+    stage_phi<<<blocks_for(total, 256), 256, 0, st>>>(g, m, a);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "stage_phi launch");
+}
+
+int launch_scatter_nodes(const Grid &g, const acfd_node_t *staged, double *U, int *flags, unsigned mask,
+                         cudaStream_t st)
+{
+    const long long total = (long long)g.n[0] * g.n[1] * g.n[2];
+    scatter_nodes<<<blocks_for(total, 256), 256, 0, st>>>(g, staged, U, flags, mask);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "scatter_nodes launch");
+}
+
+int launch_gather_nodes(const Grid &g, const double *U, const int *flags, acfd_node_t *staged, unsigned mask,
+                        cudaStream_t st)
+{
+    const long long total = (long long)g.n[0] * g.n[1] * g.n[2];
+    gather_nodes<<<blocks_for(total, 256), 256, 0, st>>>(g, U, flags, staged, mask);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "gather_nodes launch");
+}
+
+}  // namespace acfd

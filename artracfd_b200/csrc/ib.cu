@@ -1,0 +1,868 @@
+// Immersed boundaries on the device: node mapping (ComputeGeometricField,
+// immersed_boundary.c:65-264, with the point-in-polyhedron test of
+// computational_geometry.c:463-783) and the ghost-node reconstruction
+// (TreatImmersedBoundary, immersed_boundary.c:270-487).
+//
+// Compiled with --fmad=false and written in the reference's evaluation
+// order: node flags (did, fid, lid, gst), image-point node indices and IDW
+// stencils are bit-exact, ghost values bitwise up to the order-free parts.
+//
+// Parallel structure:
+//  * domain mapping: one launch per body in body order (first body wins, as
+//    the reference's body loop); a block stages the body's facets
+//    (v0, e01, e02 per facet) in shared memory and each thread scans them for
+//    its node;
+//  * interfacial field: newly uncovered nodes are marked first, so that the
+//    reconstruction reads only nodes that stay fluid (the reference's TYPEF
+//    selection) and never a value written in the same pass;
+//  * ghost layers: one launch per layer over all bodies' boxes (layer r reads
+//    fluid nodes or layer r-1 only; bodies do not read each other).
+#include <algorithm>
+#include <cfloat>
+#include <vector>
+
+#include "acfd_internal.cuh"
+
+namespace acfd {
+
+struct DevBody {
+    int faceN, edgeN, vertN, state;
+    double r, O[3], V[3], W[3], T, cf;
+    double box[3][2];
+    const int *f;
+    const double *Nf;
+    const int *e;
+    const double *Ne;
+    const double *v;
+    const double *Nv;
+    const double *tri;  // faceN x 9: v0, e01, e02
+};
+
+struct IbState {
+    std::vector<DevBody> host;
+    DevBody *dev = nullptr;
+    std::vector<void *> buffers;
+    unsigned char *joined = nullptr;
+    long long joined_n = 0;
+    int *status = nullptr;  // device error word
+    int count = 0;
+};
+
+namespace {
+
+constexpr int kIbR = 2;  // IDW search radius of the reconstruction (immersed_boundary.c:27)
+constexpr int kTypeD = -1, kTypeF = -2;
+
+struct IbGrid {
+    Grid g;
+    int ng[3];
+    double dmin[3];  // domain minimum
+    double d[3];
+    double tinyL;
+    int gl;
+    int ibmLayer;
+    int pathSep[4];
+    int path[30][3];
+};
+
+__device__ __forceinline__ long long node_of(const Grid &g, int i, int j, int k)
+{
+    return ((long long)k * g.n[1] + j) * g.pitch + i;
+}
+
+__device__ __forceinline__ double dot3(const double *a, const double *b)
+{
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+__device__ __forceinline__ double dist2(const double *a, const double *b)
+{
+    const double v[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+    return dot3(v, v);
+}
+
+__device__ __forceinline__ bool in_pin(const Grid &g, int k, int j, int i)
+{
+    return (g.lo[2] <= k) && (g.hi[2] > k) && (g.lo[1] <= j) && (g.hi[1] > j) && (g.lo[0] <= i) && (g.hi[0] > i);
+}
+
+__device__ __forceinline__ int map_node(double s, double smin, double dds, int ng)
+{
+    return (int)((s - smin) * dds + 0.5) + ng;
+}
+
+__device__ __forceinline__ double map_point(int n, double smin, double ds, int ng)
+{
+    return smin + (n - ng) * ds;
+}
+
+__device__ __forceinline__ void node_point(const IbGrid &G, int k, int j, int i, double p[3])
+{
+    p[0] = map_point(i, G.dmin[0], G.d[0], G.ng[0]);
+    p[1] = map_point(j, G.dmin[1], G.d[1], G.ng[1]);
+    p[2] = map_point(k, G.dmin[2], G.d[2], G.ng[2]);
+}
+
+__host__ __device__ inline int confine(int n, int lo, int hi)
+{
+    const int a = (lo > n) ? lo : n;
+    return (hi - 1 < a) ? hi - 1 : a;
+}
+
+__device__ __forceinline__ void to_primitive(double gamma, double gasR, const double U[5], double Uo[6])
+{
+    Uo[0] = U[0];
+    Uo[1] = U[1] / U[0];
+    Uo[2] = U[2] / U[0];
+    Uo[3] = U[3] / U[0];
+    Uo[4] = (U[4] - 0.5 * (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / U[0]) * (gamma - 1.0);
+    Uo[5] = Uo[4] / (Uo[0] * gasR);
+}
+
+__device__ __forceinline__ void to_conservative(double gamma, const double Uo[6], double U[5])
+{
+    U[0] = Uo[0];
+    U[1] = Uo[0] * Uo[1];
+    U[2] = Uo[0] * Uo[2];
+    U[3] = Uo[0] * Uo[3];
+    U[4] = 0.5 * Uo[0] * (Uo[1] * Uo[1] + Uo[2] * Uo[2] + Uo[3] * Uo[3]) + Uo[4] / (gamma - 1.0);
+}
+
+// Eberly's point-triangle distance (computational_geometry.c:511-688)
+__device__ double point_triangle(const double p[3], const double v0[3], const double e01[3], const double e02[3],
+                                 double para[3])
+{
+    const double D[3] = {v0[0] - p[0], v0[1] - p[1], v0[2] - p[2]};
+    const double a = dot3(e01, e01), b = dot3(e01, e02), c = dot3(e02, e02);
+    const double d = dot3(e01, D), e = dot3(e02, D), f = dot3(D, D);
+    const double det = a * c - b * b;
+    double s = b * e - c * d;
+    double t = b * d - a * e;
+    double q;
+    if (s + t <= det) {
+        if (s < 0.0) {
+            if (t < 0.0) {
+                if (d < 0.0) {
+                    t = 0.0;
+                    if (-d >= a) { s = 1.0; q = a + 2.0 * d + f; }
+                    else { s = -d / a; q = d * s + f; }
+                } else {
+                    s = 0.0;
+                    if (e >= 0.0) { t = 0.0; q = f; }
+                    else if (-e >= c) { t = 1.0; q = c + 2.0 * e + f; }
+                    else { t = -e / c; q = e * t + f; }
+                }
+            } else {
+                s = 0.0;
+                if (e >= 0.0) { t = 0.0; q = f; }
+                else if (-e >= c) { t = 1.0; q = c + 2.0 * e + f; }
+                else { t = -e / c; q = e * t + f; }
+            }
+        } else if (t < 0.0) {
+            t = 0.0;
+            if (d >= 0.0) { s = 0.0; q = f; }
+            else if (-d >= a) { s = 1.0; q = a + 2.0 * d + f; }
+            else { s = -d / a; q = d * s + f; }
+        } else {
+            s = s / det;
+            t = t / det;
+            q = s * (a * s + b * t + 2.0 * d) + t * (b * s + c * t + 2.0 * e) + f;
+        }
+    } else if (s < 0.0) {
+        const double t0 = b + d, t1 = c + e;
+        if (t1 > t0) {
+            const double num = t1 - t0, den = a - 2.0 * b + c;
+            if (num >= den) { s = 1.0; t = 0.0; q = a + 2.0 * d + f; }
+            else {
+                s = num / den;
+                t = 1.0 - s;
+                q = s * (a * s + b * t + 2.0 * d) + t * (b * s + c * t + 2.0 * e) + f;
+            }
+        } else {
+            s = 0.0;
+            if (t1 <= 0.0) { t = 1.0; q = c + 2.0 * e + f; }
+            else if (e >= 0.0) { t = 0.0; q = f; }
+            else { t = -e / c; q = e * t + f; }
+        }
+    } else if (t < 0.0) {
+        const double t0 = b + e, t1 = a + d;
+        if (t1 > t0) {
+            const double num = t1 - t0, den = a - 2.0 * b + c;
+            if (num >= den) { t = 1.0; s = 0.0; q = c + 2.0 * e + f; }
+            else {
+                t = num / den;
+                s = 1.0 - t;
+                q = s * (a * s + b * t + 2.0 * d) + t * (b * s + c * t + 2.0 * e) + f;
+            }
+        } else {
+            t = 0.0;
+            if (t1 <= 0.0) { s = 1.0; q = a + 2.0 * d + f; }
+            else if (d >= 0.0) { s = 0.0; q = f; }
+            else { s = -d / a; q = d * s + f; }
+        }
+    } else {
+        const double num = c + e - b - d;
+        if (num <= 0.0) { s = 0.0; t = 1.0; q = c + 2.0 * e + f; }
+        else {
+            const double den = a - 2.0 * b + c;
+            if (num >= den) { s = 1.0; t = 0.0; q = a + 2.0 * d + f; }
+            else {
+                s = num / den;
+                t = 1.0 - s;
+                q = s * (a * s + b * t + 2.0 * d) + t * (b * s + c * t + 2.0 * e) + f;
+            }
+        }
+    }
+    para[0] = 1.0 - s - t;
+    para[1] = s;
+    para[2] = t;
+    return (0.0 > q) ? 0.0 : q;
+}
+
+__device__ int find_edge(const DevBody &B, int v0, int v1)
+{
+    const int hi = (v0 > v1) ? v0 : v1, lo = (v0 > v1) ? v1 : v0;
+    int a = 0, b = B.edgeN - 1;
+    while (a <= b) {
+        const int m = (a + b) / 2;
+        const int *e = B.e + 4 * m;
+        if (hi == e[0] && lo == e[1]) {
+            return m;
+        }
+        if ((hi > e[0]) || ((hi == e[0]) && (lo > e[1]))) {
+            a = m + 1;
+        } else {
+            b = m - 1;
+        }
+    }
+    return -1;
+}
+
+// closest point on facet fid and its pseudo-normal (computational_geometry.c:689-761)
+__device__ bool closest_on_facet(const double p[3], int fid, const DevBody &B, double pi[3], double N[3])
+{
+    const double *T = B.tri + 9 * (long long)fid;
+    const double v0[3] = {T[0], T[1], T[2]};
+    const double e01[3] = {T[3], T[4], T[5]};
+    const double e02[3] = {T[6], T[7], T[8]};
+    const int *fv = B.f + 3 * (long long)fid;
+    double para[3];
+    point_triangle(p, v0, e01, e02, para);
+    const double *nrm = nullptr;
+    if (0.0 == para[1]) {
+        if (0.0 == para[2]) {
+            nrm = B.Nv + 3 * fv[0];
+            for (int s = 0; s < 3; ++s) pi[s] = v0[s];
+        } else if (1.0 == para[2]) {
+            nrm = B.Nv + 3 * fv[2];
+            for (int s = 0; s < 3; ++s) pi[s] = B.v[3 * fv[2] + s];
+        } else {
+            const int e = find_edge(B, fv[0], fv[2]);
+            if (e < 0) return false;
+            nrm = B.Ne + 3 * e;
+            for (int s = 0; s < 3; ++s) pi[s] = v0[s] + para[2] * e02[s];
+        }
+    } else if (1.0 == para[1]) {
+        nrm = B.Nv + 3 * fv[1];
+        for (int s = 0; s < 3; ++s) pi[s] = B.v[3 * fv[1] + s];
+    } else if (0.0 == para[2]) {
+        const int e = find_edge(B, fv[0], fv[1]);
+        if (e < 0) return false;
+        nrm = B.Ne + 3 * e;
+        for (int s = 0; s < 3; ++s) pi[s] = v0[s] + para[1] * e01[s];
+    } else if (0.0 == para[0]) {
+        const int e = find_edge(B, fv[1], fv[2]);
+        if (e < 0) return false;
+        nrm = B.Ne + 3 * e;
+        for (int s = 0; s < 3; ++s) pi[s] = v0[s] + para[1] * e01[s] + para[2] * e02[s];
+    } else {
+        nrm = B.Nf + 3 * (long long)fid;
+        for (int s = 0; s < 3; ++s) pi[s] = v0[s] + para[1] * e01[s] + para[2] * e02[s];
+    }
+    for (int s = 0; s < 3; ++s) N[s] = nrm[s];
+    return true;
+}
+
+// boundary point pi, image point pm and normal N (computational_geometry.c:762-783)
+__device__ bool surface_data(const double p[3], int fid, const DevBody &B, double pi[3], double pm[3], double N[3])
+{
+    if (0 >= B.faceN) {
+        N[0] = p[0] - B.O[0];
+        N[1] = p[1] - B.O[1];
+        N[2] = p[2] - B.O[2];
+        double dist = sqrt(dot3(N, N));
+        for (int s = 0; s < 3; ++s) N[s] = N[s] / dist;
+        dist = B.r - dist;
+        for (int s = 0; s < 3; ++s) pi[s] = p[s] + dist * N[s];
+    } else if (!closest_on_facet(p, fid, B, pi, N)) {
+        return false;
+    }
+    for (int s = 0; s < 3; ++s) pm[s] = pi[s] + pi[s] - p[s];
+    return true;
+}
+
+__device__ __forceinline__ void add_weighted(const double Uoh[6], double tiny, double w, double &wsum, double Uo[6])
+{
+    if (tiny > w) w = tiny;
+    w = 1.0 / w;
+    for (int n = 0; n < 6; ++n) Uo[n] = Uo[n] + Uoh[n] * w;
+    wsum = wsum + w;
+}
+
+// inverse distance weighting (immersed_boundary.c:413-473); type TYPED: fluid
+// nodes, TYPEF: fluid nodes that were fluid before this mapping (not joined),
+// r >= 1: nodes of body did in ghost layer r
+__device__ double idw(const IbGrid &G, const ModelParams &mp, const double *U, const int *flags,
+                      const unsigned char *joined, const int c[3], const double p[3], int h, int type, int did,
+                      double Uo[6], int *status)
+{
+    const Grid &g = G.g;
+    const long long nn = g.nn;
+    const int *fdid = flags;
+    const int *fgst = flags + 3 * nn;
+    double wsum = 0.0;
+    for (int n = 0; n < 6; ++n) Uo[n] = 0.0;
+    const int rmax = g.n[0] + g.n[1] + g.n[2];
+    for (int r = h, tally = 0; 0 == tally; ++r) {
+        if (r > rmax) {
+            atomicExch(status, 1);  // no qualifying node: the reference would not terminate
+            break;
+        }
+        for (int kh = -r; kh <= r; ++kh) {
+            for (int jh = -r; jh <= r; ++jh) {
+                for (int ih = -r; ih <= r; ++ih) {
+                    const int i = c[0] + ih, j = c[1] + jh, k = c[2] + kh;
+                    if (!in_pin(g, k, j, i)) continue;
+                    const long long id = node_of(g, i, j, k);
+                    if (did != fdid[id]) continue;
+                    if (type == kTypeF) {
+                        if (joined[id]) continue;
+                    } else if (type != kTypeD) {
+                        if (type != fgst[id]) continue;
+                    }
+                    ++tally;
+                    double ph[3], Uh[5], Uoh[6];
+                    node_point(G, k, j, i, ph);
+                    for (int v = 0; v < 5; ++v) Uh[v] = U[v * nn + id];
+                    to_primitive(mp.gamma, mp.gasR, Uh, Uoh);
+                    add_weighted(Uoh, G.tinyL, dist2(p, ph), wsum, Uo);
+                }
+            }
+        }
+    }
+    return wsum;
+}
+
+__device__ void orthogonal_space(const double N[3], double Ta[3], double Tb[3])
+{
+    int mark = 2;
+    if (fabs(N[mark]) > fabs(N[1])) mark = 1;
+    if (fabs(N[mark]) > fabs(N[0])) mark = 0;
+    if (0 == mark) {
+        Ta[0] = 0.0; Ta[1] = -N[2]; Ta[2] = N[1];
+    } else if (1 == mark) {
+        Ta[0] = N[2]; Ta[1] = 0.0; Ta[2] = -N[0];
+    } else {
+        Ta[0] = -N[1]; Ta[1] = N[0]; Ta[2] = 0.0;
+    }
+    const double nrm = sqrt(dot3(Ta, Ta));
+    for (int s = 0; s < 3; ++s) Ta[s] = Ta[s] / nrm;
+    Tb[0] = Ta[1] * N[2] - Ta[2] * N[1];
+    Tb[1] = Ta[2] * N[0] - Ta[0] * N[2];
+    Tb[2] = Ta[0] * N[1] - Ta[1] * N[0];
+}
+
+// ---------------------------------------------------------------------------
+// ghost layer r of every body (immersed_boundary.c:294-338)
+// ---------------------------------------------------------------------------
+struct BoxList {
+    int lo[8][3];
+    int ext[8][3];
+    long long start[9];
+    int body0;
+    int nb;
+};
+
+__global__ void ib_layer(IbGrid G, ModelParams mp, const DevBody *bodies, BoxList bl, double *U, int *flags,
+                         int tn, int r, int *status)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= bl.start[bl.nb]) return;
+    int q = 0;
+    while (t >= bl.start[q + 1]) ++q;
+    t -= bl.start[q];
+    const int n = bl.body0 + q;
+    const int i = bl.lo[q][0] + (int)(t % bl.ext[q][0]);
+    const long long rest = t / bl.ext[q][0];
+    const int j = bl.lo[q][1] + (int)(rest % bl.ext[q][1]);
+    const int k = bl.lo[q][2] + (int)(rest / bl.ext[q][1]);
+    const Grid &g = G.g;
+    const long long nn = g.nn;
+    const long long id = node_of(g, i, j, k);
+    if ((r != flags[3 * nn + id]) || (n + 1 != flags[id])) return;
+    const DevBody &B = bodies[n];
+    double *Ut = U + (long long)tn * 5 * nn;
+    double pG[3], UoG[6];
+    node_point(G, k, j, i, pG);
+    if (G.ibmLayer >= r) {
+        double pO[3], pI[3], N[3], UoO[6], UoI[6];
+        if (!surface_data(pG, flags[nn + id], B, pO, pI, N)) {
+            atomicExch(status, 2);
+            return;
+        }
+        const int cI[3] = {map_node(pI[0], G.dmin[0], g.dd[0], G.ng[0]), map_node(pI[1], G.dmin[1], g.dd[1], G.ng[1]),
+                           map_node(pI[2], G.dmin[2], g.dd[2], G.ng[2])};
+        // ReconstructFlow (immersed_boundary.c:357-412)
+        double wsum = idw(G, mp, Ut, flags, nullptr, cI, pI, kIbR, kTypeD, 0, UoI, status);
+        const double w = 1.0 / wsum;
+        const double rr[3] = {pO[0] - B.O[0], pO[1] - B.O[1], pO[2] - B.O[2]};
+        double Vs[3];
+        Vs[0] = B.W[1] * rr[2] - B.W[2] * rr[1];
+        Vs[1] = B.W[2] * rr[0] - B.W[0] * rr[2];
+        Vs[2] = B.W[0] * rr[1] - B.W[1] * rr[0];
+        Vs[0] = B.V[0] + Vs[0];
+        Vs[1] = B.V[1] + Vs[1];
+        Vs[2] = B.V[2] + Vs[2];
+        if (0.0 < B.cf) {
+            UoO[1] = Vs[0];
+            UoO[2] = Vs[1];
+            UoO[3] = Vs[2];
+        } else {
+            const double V[3] = {UoI[1] * w, UoI[2] * w, UoI[3] * w};
+            double Ta[3], Tb[3], rhs[3];
+            orthogonal_space(N, Ta, Tb);
+            rhs[0] = dot3(Vs, N);
+            rhs[1] = dot3(V, Ta);
+            rhs[2] = dot3(V, Tb);
+            for (int s = 0; s < 3; ++s) UoO[s + 1] = N[s] * rhs[0] + Ta[s] * rhs[1] + Tb[s] * rhs[2];
+        }
+        UoO[4] = UoI[4] * w;
+        UoO[5] = (0.0 > B.T) ? UoI[5] * w : B.T;
+        add_weighted(UoO, G.tinyL, dist2(pI, pO), wsum, UoI);
+        for (int v = 0; v < 6; ++v) UoI[v] = UoI[v] / wsum;
+        // method of images
+        UoG[1] = UoO[1] + UoO[1] - UoI[1];
+        UoG[2] = UoO[2] + UoO[2] - UoI[2];
+        UoG[3] = UoO[3] + UoO[3] - UoI[3];
+        UoG[4] = UoI[4];
+        UoG[5] = UoI[5];
+    } else {
+        const int cG[3] = {i, j, k};
+        const double ws = idw(G, mp, Ut, flags, nullptr, cG, pG, 1, r - 1, n + 1, UoG, status);
+        for (int v = 0; v < 6; ++v) UoG[v] = UoG[v] / ws;
+    }
+    UoG[0] = UoG[4] / (UoG[5] * mp.gasR);
+    double Uc[5];
+    to_conservative(mp.gamma, UoG, Uc);
+    for (int v = 0; v < 5; ++v) Ut[v * nn + id] = Uc[v];
+}
+
+// ---------------------------------------------------------------------------
+// node mapping
+// ---------------------------------------------------------------------------
+__global__ void map_init(Grid g, const DevBody *bodies, int *flags)
+{
+    const int Lx = g.hi[0] - g.lo[0], Ly = g.hi[1] - g.lo[1], Lz = g.hi[2] - g.lo[2];
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)Lx * Ly * Lz) return;
+    const int i = g.lo[0] + (int)(t % Lx);
+    const long long rest = t / Lx;
+    const int j = g.lo[1] + (int)(rest % Ly);
+    const int k = g.lo[2] + (int)(rest / Ly);
+    const long long nn = g.nn;
+    const long long id = node_of(g, i, j, k);
+    const int did = flags[id];
+    flags[3 * nn + id] = did;  // keep the old domain field in gst
+    if (did == 0) {
+        flags[nn + id] = 0;
+        return;
+    }
+    if (bodies[did - 1].state == 1) return;
+    if (flags[2 * nn + id] > 0) flags[id] = 0;
+}
+
+constexpr int kMapThreads = 128;
+constexpr int kMaxSmemFacets = 2048;  // 9 doubles each: 144 KB
+
+__global__ void __launch_bounds__(kMapThreads) map_body(IbGrid G, const DevBody *bodies, int n, BoxList bl,
+                                                        int *flags, int *status)
+{
+    extern __shared__ double stri[];
+    const DevBody &B = bodies[n];
+    const bool staged = (B.faceN > 0) && (B.faceN <= kMaxSmemFacets);
+    if (staged) {
+        for (int q = threadIdx.x; q < 9 * B.faceN; q += blockDim.x) stri[q] = B.tri[q];
+        __syncthreads();
+    }
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= bl.start[1]) return;
+    const int i = bl.lo[0][0] + (int)(t % bl.ext[0][0]);
+    const long long rest = t / bl.ext[0][0];
+    const int j = bl.lo[0][1] + (int)(rest % bl.ext[0][1]);
+    const int k = bl.lo[0][2] + (int)(rest / bl.ext[0][1]);
+    const Grid &g = G.g;
+    const long long nn = g.nn;
+    const long long id = node_of(g, i, j, k);
+    if (0 != flags[id]) return;
+    double p[3];
+    node_point(G, k, j, i, p);
+    if (0 >= B.faceN) {
+        if (B.r * B.r >= dist2(B.O, p)) {
+            flags[id] = n + 1;
+            flags[nn + id] = 0;
+        }
+        return;
+    }
+    // nearest facet, first minimum wins (computational_geometry.c:463-494)
+    const double *tri = staged ? stri : B.tri;
+    double best = FLT_MAX;
+    int cid = 0;
+    for (int f = 0; f < B.faceN; ++f) {
+        const double *T = tri + 9 * f;
+        const double v0[3] = {T[0], T[1], T[2]};
+        const double e01[3] = {T[3], T[4], T[5]};
+        const double e02[3] = {T[6], T[7], T[8]};
+        double para[3];
+        const double q = point_triangle(p, v0, e01, e02, para);
+        if (best > q) {
+            best = q;
+            cid = f;
+        }
+    }
+    double pi[3], N[3];
+    if (!closest_on_facet(p, cid, B, pi, N)) {
+        atomicExch(status, 2);
+        return;
+    }
+    pi[0] = p[0] - pi[0];
+    pi[1] = p[1] - pi[1];
+    pi[2] = p[2] - pi[2];
+    if (!(0.0 < dot3(pi, N))) {
+        flags[id] = n + 1;
+        flags[nn + id] = cid;
+    }
+}
+
+__device__ __forceinline__ int layer_of(const IbGrid &G, int q)
+{
+    for (int r = 1; r <= G.gl; ++r) {
+        if (G.pathSep[r] > q) return r;
+    }
+    return 0;
+}
+
+// interfacial layer, ghost layer and the joined mark (SetInterfacialField)
+__global__ void map_interface(IbGrid G, int *flags, unsigned char *joined)
+{
+    const Grid &g = G.g;
+    const int Lx = g.hi[0] - g.lo[0], Ly = g.hi[1] - g.lo[1], Lz = g.hi[2] - g.lo[2];
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)Lx * Ly * Lz) return;
+    const int i = g.lo[0] + (int)(t % Lx);
+    const long long rest = t / Lx;
+    const int j = g.lo[1] + (int)(rest % Ly);
+    const int k = g.lo[2] + (int)(rest / Ly);
+    const long long nn = g.nn;
+    const long long id = node_of(g, i, j, k);
+    const int did = flags[id];
+    joined[id] = (flags[3 * nn + id] != did && did == 0) ? 1 : 0;
+    int lid = 0, gst = 0;
+    if (did != 0) {
+        for (int q = 0; q < G.pathSep[0]; ++q) {
+            const int kh = k + G.path[q][2], jh = j + G.path[q][1], ih = i + G.path[q][0];
+            if (!in_pin(g, kh, jh, ih)) continue;
+            if (did != flags[node_of(g, ih, jh, kh)]) {
+                lid = layer_of(G, q);
+                break;
+            }
+        }
+        if (lid > 0) {
+            for (int q = 0; q < G.pathSep[0]; ++q) {
+                const int kh = k + G.path[q][2], jh = j + G.path[q][1], ih = i + G.path[q][0];
+                if (!in_pin(g, kh, jh, ih)) continue;
+                if (0 == flags[node_of(g, ih, jh, kh)]) {
+                    gst = layer_of(G, q);
+                    break;
+                }
+            }
+        }
+    }
+    flags[2 * nn + id] = lid;
+    flags[3 * nn + id] = gst;
+}
+
+// refill newly uncovered fluid nodes from fluid nodes that stayed fluid
+__global__ void map_refill(IbGrid G, ModelParams mp, double *U, int *flags, const unsigned char *joined, int *status)
+{
+    const Grid &g = G.g;
+    const int Lx = g.hi[0] - g.lo[0], Ly = g.hi[1] - g.lo[1], Lz = g.hi[2] - g.lo[2];
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)Lx * Ly * Lz) return;
+    const int i = g.lo[0] + (int)(t % Lx);
+    const long long rest = t / Lx;
+    const int j = g.lo[1] + (int)(rest % Ly);
+    const int k = g.lo[2] + (int)(rest / Ly);
+    const long long nn = g.nn;
+    const long long id = node_of(g, i, j, k);
+    if (!joined[id]) return;
+    const int c[3] = {i, j, k};
+    double p[3], Uo[6];
+    node_point(G, k, j, i, p);
+    const double ws = idw(G, mp, U, flags, joined, c, p, kIbR, kTypeF, 0, Uo, status);
+    for (int v = 0; v < 6; ++v) Uo[v] = Uo[v] / ws;
+    Uo[0] = Uo[4] / (Uo[5] * mp.gasR);
+    double Uc[5];
+    to_conservative(mp.gamma, Uo, Uc);
+    for (int v = 0; v < 5; ++v) U[v * nn + id] = Uc[v];
+    flags[nn + id] = -1;
+}
+
+// facet table v0, e01, e02 (BuildTriangle, computational_geometry.c:449-462)
+__global__ void build_tri(const int *f, const double *v, double *tri, int faceN)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= faceN) return;
+    for (int s = 0; s < 3; ++s) {
+        const double v0 = v[3 * f[3 * q + 0] + s];
+        const double v1 = v[3 * f[3 * q + 1] + s];
+        const double v2 = v[3 * f[3 * q + 2] + s];
+        tri[9 * q + s] = v0;
+        tri[9 * q + 3 + s] = v1 - v0;
+        tri[9 * q + 6 + s] = v2 - v0;
+    }
+}
+
+IbGrid make_ibgrid(const Grid &g, const acfd_partition_t &part, int ibmLayer)
+{
+    IbGrid G;
+    G.g = g;
+    for (int s = 0; s < 3; ++s) {
+        G.ng[s] = part.ng[s];
+        G.dmin[s] = part.domain[s][0];
+        G.d[s] = part.d[s];
+    }
+    G.tinyL = part.tinyL;
+    G.gl = part.gl;
+    G.ibmLayer = ibmLayer;
+    for (int q = 0; q < 4; ++q) G.pathSep[q] = part.pathSep[q];
+    for (int q = 0; q < 30; ++q)
+        for (int s = 0; s < 3; ++s) G.path[q][s] = part.path[q][s];
+    return G;
+}
+
+// node box of a body confined to PIN (immersed_boundary.c:151-154)
+void body_box(const acfd_partition_t &part, const DevBody &B, int lo[3], int ext[3])
+{
+    for (int s = 0; s < 3; ++s) {
+        const int nlo = part.ns[0][s][0], nhi = part.ns[0][s][1];
+        const int a = confine((int)((B.box[s][0] - part.domain[s][0]) * part.dd[s] + 0.5) + part.ng[s], nlo, nhi);
+        const int b = confine((int)((B.box[s][1] - part.domain[s][0]) * part.dd[s] + 0.5) + part.ng[s], nlo, nhi) + 1;
+        lo[s] = a;
+        ext[s] = std::max(0, b - a);
+    }
+}
+
+int read_status(IbState *ib, cudaStream_t st)
+{
+    int h = 0;
+    ACFD_CUDA(cudaMemcpyAsync(&h, ib->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ACFD_CUDA(cudaStreamSynchronize(st));
+    if (h == 1) {
+        set_error("immersed boundary: no qualifying node for inverse distance weighting");
+        return ACFD_ERR_DEVICE;
+    }
+    if (h == 2) {
+        set_error("immersed boundary: edge of the closest facet not found in the edge list");
+        return ACFD_ERR_NOT_FOUND;
+    }
+    return ACFD_OK;
+}
+
+unsigned blocks_for(long long n, int bs)
+{
+    return (unsigned)((n + bs - 1) / bs);
+}
+
+}  // namespace
+
+int ib_create(IbState **out)
+{
+    IbState *ib = new IbState();
+    cudaError_t e = cudaMalloc(&ib->status, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(ib->status, 0, sizeof(int));
+    if (e != cudaSuccess) {
+        delete ib;
+        return cuda_status(e, "ib_create");
+    }
+    *out = ib;
+    return ACFD_OK;
+}
+
+static void ib_release_geometry(IbState *ib)
+{
+    for (void *p : ib->buffers) cudaFree(p);
+    ib->buffers.clear();
+    cudaFree(ib->dev);
+    ib->dev = nullptr;
+    ib->host.clear();
+    ib->count = 0;
+}
+
+void ib_destroy(IbState *ib)
+{
+    if (!ib) return;
+    ib_release_geometry(ib);
+    cudaFree(ib->joined);
+    cudaFree(ib->status);
+    delete ib;
+}
+
+int ib_count(const IbState *ib)
+{
+    return ib ? ib->count : 0;
+}
+
+int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, cudaStream_t st)
+{
+    ACFD_CUDA(cudaStreamSynchronize(st));
+    ib_release_geometry(ib);
+    if (totN == 0) return ACFD_OK;
+    ib->host.resize(totN);
+    auto dcopy = [&](const void *src, size_t bytes, void **dst) -> int {
+        *dst = nullptr;
+        if (bytes == 0) return ACFD_OK;
+        if (!src) {
+            set_error("acfd_geo_upload: missing geometry array");
+            return ACFD_ERR_ARG;
+        }
+        ACFD_CUDA(cudaMalloc(dst, bytes));
+        ib->buffers.push_back(*dst);
+        ACFD_CUDA(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+        return ACFD_OK;
+    };
+    for (int n = 0; n < totN; ++n) {
+        const acfd_polyhedron_t &P = poly[n];
+        DevBody &B = ib->host[n];
+        B.faceN = P.faceN;
+        B.edgeN = P.edgeN;
+        B.vertN = P.vertN;
+        B.state = P.state;
+        B.r = P.r;
+        B.T = P.T;
+        B.cf = P.cf;
+        for (int s = 0; s < 3; ++s) {
+            B.O[s] = P.O[s];
+            B.V[s] = P.V[s];
+            B.W[s] = P.W[s];
+            B.box[s][0] = P.box[s][0];
+            B.box[s][1] = P.box[s][1];
+        }
+        B.f = nullptr; B.Nf = nullptr; B.e = nullptr; B.Ne = nullptr; B.v = nullptr; B.Nv = nullptr; B.tri = nullptr;
+        if (P.faceN > 0) {
+            void *f, *Nf, *e, *Ne, *v, *Nv, *tri;
+            int st2;
+            if ((st2 = dcopy(P.f, sizeof(int) * 3 * P.faceN, &f)) != ACFD_OK) return st2;
+            if ((st2 = dcopy(P.Nf, sizeof(double) * 3 * P.faceN, &Nf)) != ACFD_OK) return st2;
+            if ((st2 = dcopy(P.e, sizeof(int) * 4 * P.edgeN, &e)) != ACFD_OK) return st2;
+            if ((st2 = dcopy(P.Ne, sizeof(double) * 3 * P.edgeN, &Ne)) != ACFD_OK) return st2;
+            if ((st2 = dcopy(P.v, sizeof(double) * 3 * P.vertN, &v)) != ACFD_OK) return st2;
+            if ((st2 = dcopy(P.Nv, sizeof(double) * 3 * P.vertN, &Nv)) != ACFD_OK) return st2;
+            ACFD_CUDA(cudaMalloc(&tri, sizeof(double) * 9 * P.faceN));
+            ib->buffers.push_back(tri);
+            build_tri<<<blocks_for(P.faceN, 128), 128>>>((const int *)f, (const double *)v, (double *)tri, P.faceN);
+            ACFD_CUDA(cudaGetLastError());
+            B.f = (const int *)f;
+            B.Nf = (const double *)Nf;
+            B.e = (const int *)e;
+            B.Ne = (const double *)Ne;
+            B.v = (const double *)v;
+            B.Nv = (const double *)Nv;
+            B.tri = (const double *)tri;
+        }
+    }
+    ACFD_CUDA(cudaMalloc(&ib->dev, sizeof(DevBody) * totN));
+    ACFD_CUDA(cudaMemcpy(ib->dev, ib->host.data(), sizeof(DevBody) * totN, cudaMemcpyHostToDevice));
+    ACFD_CUDA(cudaDeviceSynchronize());
+    ib->count = totN;
+    return ACFD_OK;
+}
+
+static int boxes_of(IbState *ib, const acfd_partition_t &part, int n0, BoxList &bl)
+{
+    bl.body0 = n0;
+    bl.nb = std::min(8, ib->count - n0);
+    bl.start[0] = 0;
+    for (int q = 0; q < bl.nb; ++q) {
+        body_box(part, ib->host[n0 + q], bl.lo[q], bl.ext[q]);
+        bl.start[q + 1] = bl.start[q] + (long long)bl.ext[q][0] * bl.ext[q][1] * bl.ext[q][2];
+    }
+    return ACFD_OK;
+}
+
+int ib_treat(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partition_t &part, double *U, int *flags,
+             int tn, cudaStream_t st)
+{
+    if (!ib || ib->count == 0) return ACFD_OK;
+    const IbGrid G = make_ibgrid(g, part, m.ibmLayer);
+    for (int r = 1; r <= part.gl; ++r) {
+        for (int n0 = 0; n0 < ib->count; n0 += 8) {
+            BoxList bl;
+            boxes_of(ib, part, n0, bl);
+            const long long total = bl.start[bl.nb];
+            if (total == 0) continue;
+            ib_layer<<<blocks_for(total, 128), 128, 0, st>>>(G, m, ib->dev, bl, U, flags, tn, r, ib->status);
+            ACFD_CUDA(cudaGetLastError());
+        }
+    }
+    return ACFD_OK;
+}
+
+int ib_check(IbState *ib, cudaStream_t st)
+{
+    if (!ib || ib->count == 0) return ACFD_OK;
+    return read_status(ib, st);
+}
+
+int ib_compute_geometric_field(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partition_t &part,
+                               double *U, int *flags, cudaStream_t st)
+{
+    if (!ib || ib->count == 0) return ACFD_OK;
+    const IbGrid G = make_ibgrid(g, part, m.ibmLayer);
+    if (ib->joined_n < g.nn) {
+        cudaFree(ib->joined);
+        ib->joined = nullptr;
+        ACFD_CUDA(cudaMalloc(&ib->joined, (size_t)g.nn));
+        ib->joined_n = g.nn;
+    }
+    const long long pin = (long long)(g.hi[0] - g.lo[0]) * (g.hi[1] - g.lo[1]) * (g.hi[2] - g.lo[2]);
+    map_init<<<blocks_for(pin, 256), 256, 0, st>>>(g, ib->dev, flags);
+    ACFD_CUDA(cudaGetLastError());
+    static bool attr_set = false;
+    if (!attr_set) {
+        ACFD_CUDA(cudaFuncSetAttribute(map_body, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(sizeof(double) * 9 * kMaxSmemFacets)));
+        attr_set = true;
+    }
+    for (int n = 0; n < ib->count; ++n) {
+        const DevBody &B = ib->host[n];
+        if (B.state == 1) continue;
+        BoxList bl;
+        bl.body0 = n;
+        bl.nb = 1;
+        body_box(part, B, bl.lo[0], bl.ext[0]);
+        bl.start[0] = 0;
+        bl.start[1] = (long long)bl.ext[0][0] * bl.ext[0][1] * bl.ext[0][2];
+        if (bl.start[1] == 0) continue;
+        const size_t smem = (B.faceN > 0 && B.faceN <= kMaxSmemFacets) ? sizeof(double) * 9 * B.faceN : 0;
+        map_body<<<blocks_for(bl.start[1], kMapThreads), kMapThreads, smem, st>>>(G, ib->dev, n, bl, flags,
+                                                                                  ib->status);
+        ACFD_CUDA(cudaGetLastError());
+    }
+    map_interface<<<blocks_for(pin, 256), 256, 0, st>>>(G, flags, ib->joined);
+    ACFD_CUDA(cudaGetLastError());
+    map_refill<<<blocks_for(pin, 128), 128, 0, st>>>(G, m, U, flags, ib->joined, ib->status);
+    ACFD_CUDA(cudaGetLastError());
+    return read_status(ib, st);
+}
+
+}  // namespace acfd

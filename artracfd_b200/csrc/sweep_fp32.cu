@@ -1,0 +1,25 @@
+// Stage kernels, FP32 stencil form with FP64 accumulation.
+#define ACFD_FORM 2
+#define ACFD_NS form_fp32
+#include "sweep_impl.cuh"
+
+namespace acfd {
+
+int launch_stage_fp32(const Grid &g, const ModelParams &m, const StageArgs &a, int s, bool viscous,
+                       cudaStream_t st)
+{
+    return form_fp32::launch_stage_impl(g, m, a, s, viscous, st);
+}
+
+int launch_weno_batch_fp32(int scheme, const double *F, double *out, int count, cudaStream_t st)
+{
+    return form_fp32::launch_weno_batch_impl(scheme, F, out, count, st);
+}
+
+int launch_fhat_batch_fp32(const ModelParams &m, int s, const double *U, double *out, int count,
+                            cudaStream_t st)
+{
+    return form_fp32::launch_fhat_batch_impl(m, s, U, out, count, st);
+}
+
+}  // namespace acfd

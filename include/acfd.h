@@ -1,0 +1,223 @@
+/*
+ * acfd.h -- C ABI of libacfd_gpu, the sm_100a implementation of the
+ * ArtraCFD fluid time step (WENO3/WENO5 characteristic flux-split
+ * convection, central viscous flux, RK2/RK3 stage updates inside Strang
+ * operator splitting, CFL wave-speed reduction, domain and immersed-boundary
+ * ghost-node fill).
+ *
+ * Every entry point is plain C: integers, doubles, plain structs and raw
+ * pointers.  Each returns an int status (ACFD_OK == 0); on failure the message
+ * is available from acfd_last_error().  Nothing here calls exit().
+ *
+ * Conventions shared with the reference code (ArtraCFD, C99):
+ *   - node index (k * n[Y] + j) * n[X] + i            cfd_commons.c:323-326
+ *   - time levels TO=0, TN=1, TM=2                     commons.h:45-48
+ *   - conservative vector rho, rho*u, rho*v, rho*w, rho*eT   commons.h:50
+ *   - boundary slots 0 interior, 1..6 west, east, south, north, front, back
+ *     (commons.h:61-88), boundary kinds INFLOW=0 .. PERIODIC=4
+ *   - partition ranges ns[15][3][2], np[3][3][2]       domain_partition.c:64-128
+ */
+#ifndef ACFD_H_
+#define ACFD_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ACFD_ABI_VERSION 1
+
+/* status codes */
+#define ACFD_OK 0
+#define ACFD_ERR_ARG 1        /* invalid argument or size */
+#define ACFD_ERR_CUDA 2       /* a CUDA runtime call failed */
+#define ACFD_ERR_STATE 3      /* call out of order (e.g. no geometry uploaded) */
+#define ACFD_ERR_DEVICE 4     /* a kernel reported an error through the device status word */
+#define ACFD_ERR_NOMEM 5      /* device allocation failed */
+#define ACFD_ERR_NOT_FOUND 6  /* e.g. edge search failed (computational_geometry.c:158-160) */
+
+/* time levels and operators (commons.h:27-48) */
+#define ACFD_TO 0
+#define ACFD_TN 1
+#define ACFD_TM 2
+#define ACFD_X 0
+#define ACFD_Y 1
+#define ACFD_Z 2
+#define ACFD_DIMS 3
+#define ACFD_PHI 4
+
+/* arithmetic forms selectable with acfd_set_precision() */
+#define ACFD_FP64_EXACT 0   /* reference operation order, no FMA contraction */
+#define ACFD_FP64 1         /* FP64, reassociated and FMA-contracted (the plain GPU path) */
+#define ACFD_FP32_BULK 2    /* stencil/flux/WENO in FP32, RK accumulation and reductions in FP64 */
+#define ACFD_FP32_HYBRID 3  /* FP32 bulk + learned smoothness sensor selecting linear upwind-5 */
+
+/* masks for host <-> device node transfers */
+#define ACFD_SYNC_TO 0x1u     /* U[TO] */
+#define ACFD_SYNC_TN 0x2u     /* U[TN] */
+#define ACFD_SYNC_TM 0x4u     /* U[TM] */
+#define ACFD_SYNC_U 0x7u      /* all three levels */
+#define ACFD_SYNC_FLAGS 0x8u  /* did, fid, lid, gst */
+#define ACFD_SYNC_ALL 0xFu
+
+/*
+ * Node record.  Same member order, types and size (136 bytes) as the
+ * reference's Node (commons.h:128-134) so that a host Node array can be passed
+ * as it is.
+ */
+typedef struct acfd_node {
+    int did;          /* domain identifier: 0 fluid, n+1 inside body n, -1 outside PIN */
+    int fid;          /* closest facet identifier */
+    int lid;          /* interfacial layer identifier */
+    int gst;          /* ghost layer identifier */
+    double U[3][5];   /* conservative vector at time levels TO, TN, TM */
+} acfd_node_t;
+
+/*
+ * Domain discretisation: the members of the reference Partition
+ * (commons.h:136-159) that the fluid step reads, as plain arrays.
+ */
+typedef struct acfd_partition {
+    int m[3];               /* mesh cells per dimension */
+    int n[3];               /* nodes per dimension including ghosts */
+    int ng[3];              /* ghost layers per dimension */
+    int gl;                 /* ghost layers required by the scheme */
+    int collapse;           /* collapse tag (commons.h:36-43) */
+    double d[3];            /* mesh size */
+    double dd[3];           /* reciprocal mesh size */
+    double tinyL;           /* squared smallest length scale */
+    int ns[15][3][2];       /* node range of each partition region */
+    int np[3][3][2];        /* computational node range with dimension priority */
+    int path[30][3];        /* interfacial neighbour search path */
+    int pathSep[4];         /* separators in the search path */
+    int typeBC[7];          /* boundary kind of each slot */
+    int N[7][3];            /* outward normal of each slot */
+    double varBC[7][6];     /* given primitive rho,u,v,w,p,T of each slot */
+    double domain[3][2];    /* physical extent */
+} acfd_partition_t;
+
+/* Numerical and physical model: the reference Model (commons.h:244-268). */
+typedef struct acfd_model {
+    int tScheme;      /* 0 RK2, 1 RK3 */
+    int sScheme;      /* 0 WENO3, 1 WENO5 */
+    int sL, sR;       /* stencil offsets */
+    int multidim;     /* 0 operator splitting, 1 operator-by-operator */
+    int jacobMean;    /* 0 arithmetic, 1 Roe */
+    int fluxSplit;    /* 0 local Lax-Friedrichs, 1 Steger-Warming */
+    int psi;          /* phase interaction type */
+    int ibmLayer;     /* interfacial layers using flow reconstruction */
+    int gState;       /* gravity on/off */
+    int sState;       /* source term on/off */
+    double refMa, refMu, gamma, gasR, cv;
+    double refL, refRho, refV, refT;
+    double g[3];      /* normalised gravity */
+} acfd_model_t;
+
+/*
+ * One immersed body: the members of the reference Polyhedron
+ * (commons.h:173-204) read by the ghost-node fill and node mapping.
+ * faceN <= 0 marks an analytical sphere (centre O, radius r).
+ * Arrays are host pointers; acfd_geo_upload copies them.
+ */
+typedef struct acfd_polyhedron {
+    int faceN, edgeN, vertN;
+    int state;              /* 1 stationary, 2 no force, otherwise moving */
+    double r;               /* radius (sphere) or bounding radius */
+    double O[3];            /* centroid */
+    double V[3];            /* translational velocity at TO */
+    double W[3];            /* rotational velocity at TO */
+    double T;               /* wall temperature, < 0 adiabatic */
+    double cf;              /* roughness, > 0 no-slip */
+    double box[3][2];       /* bounding box */
+    const int *f;           /* faceN x 3 face-vertex list */
+    const double *Nf;       /* faceN x 3 face normals */
+    const int *e;           /* edgeN x 4 edge-vertex-face list, sorted */
+    const double *Ne;       /* edgeN x 3 edge normals */
+    const double *v;        /* vertN x 3 vertices */
+    const double *Nv;       /* vertN x 3 vertex normals */
+} acfd_polyhedron_t;
+
+typedef struct acfd_case acfd_case_t;
+
+/* ---- life cycle -------------------------------------------------------- */
+
+/* Allocate device state for one case on the current CUDA device.
+ * Replaces the device side of AllocateProgramMemory (preprocess.c:47-59). */
+int acfd_init(const acfd_partition_t *part, const acfd_model_t *model, acfd_case_t **out);
+/* Release all device memory of the case (postprocess.c:25-33 counterpart). */
+int acfd_finalize(acfd_case_t *cs);
+/* Copy the last error message of the calling thread into buf. */
+int acfd_last_error(char *buf, size_t len);
+/* Library ABI version (ACFD_ABI_VERSION). */
+int acfd_abi_version(void);
+/* Bind the case to a CUDA stream (cudaStream_t passed as void*; NULL = the
+ * library's own stream). */
+int acfd_set_stream(acfd_case_t *cs, void *stream);
+/* Select the arithmetic form (ACFD_FP64_EXACT, ACFD_FP64, ACFD_FP32_BULK,
+ * ACFD_FP32_HYBRID). */
+int acfd_set_precision(acfd_case_t *cs, int mode);
+
+/* ---- host <-> device coherence ----------------------------------------- */
+
+/* Upload a host Node array (n[X]*n[Y]*n[Z] records, reference layout).
+ * mask selects U levels and/or flags. */
+int acfd_sync_to_device(acfd_case_t *cs, const acfd_node_t *node, unsigned mask);
+/* Download device state into a host Node array.  Host pages that are not
+ * selected by mask are left untouched. */
+int acfd_sync_to_host(acfd_case_t *cs, acfd_node_t *node, unsigned mask);
+/* Device pointers of the structure-of-arrays state for callers that keep data
+ * on the GPU: U[level][var][node] with node = (k*n[Y]+j)*pitch+i, and the four
+ * int32 flag planes did, fid, lid, gst.  pitch >= n[X]. */
+int acfd_device_state(acfd_case_t *cs, double **U, int **flags, int *pitch, size_t *plane);
+
+/* ---- the fluid time step ----------------------------------------------- */
+
+/* Fluid part of ComputeTimeStep (solve.c:132-151): per-direction maximum of
+ * |u_s| + c over PIN nodes with did == 0 of U[TO].  The body-speed part and
+ * dt = CFL * min(d/Vmax) stay with the caller. */
+int acfd_cfl(acfd_case_t *cs, double vmax[3]);
+/* EvolveFluidDynamics (fluid_dynamics.c:55-116): one time step of size dt on
+ * U[TO], including every TreatBoundary of the stages. */
+int acfd_evolve_fluid(acfd_case_t *cs, double dt);
+/* One directional solve DiscretizeTime(dt, s) (fluid_dynamics.c:121-148):
+ * all RK stages of one sweep s in {X,Y,Z,ACFD_DIMS(=unsplit),ACFD_PHI}. */
+int acfd_discretize_time(acfd_case_t *cs, double dt, int s);
+/* One stage LLLU (fluid_dynamics.c:157-242):
+ * U[tm] = coeA*U[to] + coeB*(U[tn] + dt/ds * L_s U[tn]) on fluid PIN nodes.
+ * No boundary treatment. */
+int acfd_lllu(acfd_case_t *cs, double dt, double coeA, double coeB,
+        int to, int tn, int tm, int s);
+/* TreatBoundary (boundary_treatment.c:28-65): immersed ghost nodes first,
+ * then the domain ghost shells layer by layer, faces W,E,S,N,F,B. */
+int acfd_treat_boundary(acfd_case_t *cs, int tn);
+/* Capture one EvolveFluidDynamics into a CUDA graph keyed by dt and replay it
+ * (same result as acfd_evolve_fluid). */
+int acfd_evolve_fluid_graph(acfd_case_t *cs, double dt);
+
+/* ---- immersed boundaries ---------------------------------------------- */
+
+/* Upload (or replace after host-side motion) the body list. */
+int acfd_geo_upload(acfd_case_t *cs, const acfd_polyhedron_t *poly, int totN);
+/* ComputeGeometricField (immersed_boundary.c:65-264): did, fid, lid, gst and
+ * the reconstruction of newly uncovered fluid nodes on U[TO]. */
+int acfd_compute_geometric_field(acfd_case_t *cs);
+/* TreatImmersedBoundary (immersed_boundary.c:270-340) on level tn. */
+int acfd_treat_ib(acfd_case_t *cs, int tn);
+
+/* ---- per-point device twins (batched; host arrays in and out) --------- */
+
+/* WENO3 (weno3.c:35-55) / WENO5 (weno5.c:35-62) on count stencils:
+ * F is count x 5 x 5 (stencil point, component), Fhat count x 5. */
+int acfd_weno_batch(int scheme, int mode, const double *F, double *Fhat, int count);
+/* ComputeFhat (convective_flux.c:48-84) on count interfaces:
+ * Ust is count x 6 x 5 (stencil points sL..sR of U along s; WENO3 uses the
+ * first 4), Fhat count x 5. */
+int acfd_fhat_batch(const acfd_model_t *model, int s, int mode, const double *Ust,
+        double *Fhat, int count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ACFD_H_ */
