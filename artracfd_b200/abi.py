@@ -17,6 +17,12 @@ LIB_PATH = os.path.join(HERE, "lib", "libacfd_gpu.so")
 
 # status codes
 ACFD_OK = 0
+ACFD_ERR_ARG = 1
+ACFD_ERR_CUDA = 2
+ACFD_ERR_STATE = 3
+ACFD_ERR_DEVICE = 4
+ACFD_ERR_NOMEM = 5
+ACFD_ERR_NOT_FOUND = 6
 # levels / operators
 TO, TN, TM = 0, 1, 2
 X, Y, Z, DIMS, PHI = 0, 1, 2, 3, 4
@@ -153,6 +159,7 @@ def load_library(path: str | None = None):
         "acfd_abi_version": [],
         "acfd_set_stream": [vp, vp],
         "acfd_set_precision": [vp, i],
+        "acfd_stats": [vp, ctypes.POINTER(ctypes.c_longlong)],
         "acfd_sync_to_device": [vp, vp, u],
         "acfd_sync_to_host": [vp, vp, u],
         "acfd_device_state": [vp, ctypes.POINTER(dp), ctypes.POINTER(ctypes.POINTER(ctypes.c_int)),

@@ -79,6 +79,8 @@ struct acfd_case {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     int graph_mode = -1;
+    long long launches = 0;        // kernels launched by this case (graph replays included)
+    long long graph_kernels = 0;   // kernels in the captured step graph
 };
 
 namespace {
@@ -139,12 +141,16 @@ int treat_boundary(acfd_case *cs, int tn)
             return st;
         }
     }
+    if (cs->ib && ib_count(cs->ib) > 0) {
+        cs->launches += (long long)cs->part.gl * ((ib_count(cs->ib) + 7) / 8);
+    }
     double *U = level(cs, tn);
     for (const auto &grp : cs->bc_groups) {
         int st = launch_domain_boundary(cs->grid, cs->mp, cs->part, grp.data(), (int)grp.size(), U, cs->stream);
         if (st != ACFD_OK) {
             return st;
         }
+        ++cs->launches;
     }
     return ACFD_OK;
 }
@@ -162,6 +168,7 @@ int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int 
     a.coeB = coeB;
     a.accumulate = 0;
     if (p == ACFD_PHI) {
+        ++cs->launches;
         return launch_stage_phi(cs->grid, cs->mp, a, cs->stream);
     }
     int s0 = p, s1 = p + 1;
@@ -170,6 +177,25 @@ int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int 
         s1 = 3;
     }
     const bool visc = viscous(cs);
+    // the stencil of the first and last interface of a line must stay inside
+    // the node array (a sweep along a collapsed axis has no ghost layers)
+    const int half = (cs->model.sScheme == 1) ? 3 : 2;
+    for (int s = s0; s < s1; ++s) {
+        const Grid &g = cs->grid;
+        if (g.lo[s] - half < 0 || g.hi[s] - 1 + half > g.n[s] - 1) {
+            set_error("sweep along axis %d needs %d ghost layers (nodes %d, PIN [%d,%d))", s, half, g.n[s],
+                      g.lo[s], g.hi[s]);
+            return ACFD_ERR_ARG;
+        }
+        if (visc) {
+            for (int t = 0; t < 3; ++t) {
+                if (t != s && (g.lo[t] < 1 || g.hi[t] > g.n[t] - 1)) {
+                    set_error("viscous sweep needs one node beyond PIN on axis %d", t);
+                    return ACFD_ERR_ARG;
+                }
+            }
+        }
+    }
     for (int s = s0; s < s1; ++s) {
         a.accumulate = (cs->model.multidim == 1 && s != 0) ? 1 : 0;
         int st;
@@ -181,6 +207,7 @@ int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int 
         if (st != ACFD_OK) {
             return st;
         }
+        ++cs->launches;
     }
     return ACFD_OK;
 }
@@ -240,6 +267,7 @@ int evolve(acfd_case *cs)
 int set_dt(acfd_case *cs, double dt)
 {
     set_scalar<<<1, 1, 0, cs->stream>>>(cs->d_dt, dt);
+    ++cs->launches;
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "set_scalar launch");
 }
@@ -489,6 +517,7 @@ int acfd_cfl(acfd_case_t *cs, double vmax[3])
         return ACFD_ERR_ARG;
     }
     TRY(launch_cfl(cs->grid, cs->mp, cs->U, cs->flags, cs->cfl_part, cs->cfl_out, cs->stream));
+    cs->launches += 2;
     ACFD_CUDA(cudaMemcpyAsync(cs->h_cfl, cs->cfl_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, cs->stream));
     ACFD_CUDA(cudaStreamSynchronize(cs->stream));
     for (int s = 0; s < 3; ++s) {
@@ -512,7 +541,10 @@ int acfd_evolve_fluid_graph(acfd_case_t *cs, double dt)
     if (!cs->graph_exec || cs->graph_mode != cs->mode) {
         release_graph(cs);
         ACFD_CUDA(cudaStreamBeginCapture(cs->stream, cudaStreamCaptureModeThreadLocal));
+        const long long before = cs->launches;
         int st = evolve(cs);
+        cs->graph_kernels = cs->launches - before;
+        cs->launches = before;
         cudaGraph_t graph = nullptr;
         cudaError_t e = cudaStreamEndCapture(cs->stream, &graph);
         if (st != ACFD_OK) {
@@ -527,6 +559,14 @@ int acfd_evolve_fluid_graph(acfd_case_t *cs, double dt)
         cs->graph_mode = cs->mode;
     }
     ACFD_CUDA(cudaGraphLaunch(cs->graph_exec, cs->stream));
+    cs->launches += cs->graph_kernels;
+    return ACFD_OK;
+}
+
+int acfd_stats(acfd_case_t *cs, long long *launches)
+{
+    TRY(check_case(cs));
+    if (launches) *launches = cs->launches;
     return ACFD_OK;
 }
 

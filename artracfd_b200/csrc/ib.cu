@@ -406,7 +406,12 @@ __global__ void ib_layer(IbGrid G, ModelParams mp, const DevBody *bodies, BoxLis
     node_point(G, k, j, i, pG);
     if (G.ibmLayer >= r) {
         double pO[3], pI[3], N[3], UoO[6], UoI[6];
-        if (!surface_data(pG, flags[nn + id], B, pO, pI, N)) {
+        const int fid = flags[nn + id];
+        if (B.faceN > 0 && (fid < 0 || fid >= B.faceN)) {
+            atomicExch(status, 3);  // ghost node without a valid closest facet
+            return;
+        }
+        if (!surface_data(pG, fid, B, pO, pI, N)) {
             atomicExch(status, 2);
             return;
         }
@@ -674,6 +679,10 @@ int read_status(IbState *ib, cudaStream_t st)
     if (h == 2) {
         set_error("immersed boundary: edge of the closest facet not found in the edge list");
         return ACFD_ERR_NOT_FOUND;
+    }
+    if (h == 3) {
+        set_error("immersed boundary: ghost node with a closest-facet id outside the body's facets");
+        return ACFD_ERR_DEVICE;
     }
     return ACFD_OK;
 }

@@ -54,6 +54,12 @@ class Solver:
     def set_stream(self, stream_ptr: int | None):
         check(self.lib.acfd_set_stream(self.h, ctypes.c_void_p(stream_ptr) if stream_ptr else None), self.lib)
 
+    def launches(self) -> int:
+        """Kernels launched by this case so far (graph replays included)."""
+        n = ctypes.c_longlong()
+        check(self.lib.acfd_stats(self.h, ctypes.byref(n)), self.lib)
+        return n.value
+
     @property
     def node_count(self) -> int:
         n = self.part.n

@@ -1,0 +1,372 @@
+"""Benchmark of the fluid time step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--mode fp64|fp64_exact|fp32] [--n 128]
+
+Workload: the viscous Taylor-Green vortex at 128^3 cells (129^3 = 2,146,689
+computed nodes), WENO5 + central viscous flux, Roe average, LLF splitting,
+RK3, CFL 0.5 -- synthetic initial data of the named shape (no data set).
+A step is one full time step: the CFL reduction (read back to the host),
+the host dt, and EvolveFluidDynamics (6 directional half-step sweeps x 3 RK
+stages, each followed by the ghost fill), replayed as one CUDA graph.
+
+Metric: Mcell-steps/s = computed nodes x completed steps / seconds, device
+timed with CUDA events on the solver's stream, max over ranks.  The state
+(3 levels x 5 variables x 2.5 M nodes, 295 MB of FP64) is larger than L2, so
+no flush is needed between steps.  With --gpus N each rank advances its own
+replica (the path has no exchange step), so value = N x per-rank rate.
+
+One JSON line is printed by rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s: learned-sensor FP32 vs plain FP64 WENO5 on B200 at L1 err<=1e-3"
+UNIT = "Mcell-steps/s"
+WORKLOAD = "viscous Taylor-Green vortex 128^3 cells (129^3 nodes), WENO5/LLF/Roe, RK3, CFL 0.5, Re 1600, Ma 0.1"
+
+# algorithmic figures per computed node (3D split WENO5/RK3: 6 sweeps x 3 stages)
+BYTES_PER_NODE_STEP = 1920.0          # FP64 state: stage 1 reads 40 B writes 40 B; stages 2,3 read 80 B write 40 B
+FLOP_PER_NODE_STAGE_VISCOUS = 1535.0  # ComputeFhat 1380 + ComputeFvhat 115 + LU/SolveOperator 40 (reference C source)
+STAGE_BYTES = (80.0, 120.0, 120.0)
+
+
+def profiled_traffic(mode: str):
+    """DRAM bytes per stage launch from the committed ncu summary of the
+    stage kernels (mean over the captured X and Y/Z launches), or None."""
+    name = {"fp64": "stage_sweep_fp64_tgv128.md", "fp32": "stage_sweep_fp32_tgv128.md"}.get(mode)
+    if not name:
+        return None
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("| DRAM traffic per launch (MB)"):
+            vals = [float(c.strip().strip("*")) for c in line.split("|")[2:] if c.strip()]
+            return sum(vals) / len(vals) * 1e6 if vals else None
+    return None
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fp64_peak_tflops(torch):
+    """Measured FP64 reference: cuBLAS DGEMM 8192^3, best of 5."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    return 2.0 * 8192 ** 3 / best / 1e12
+
+
+def cpu_baseline_reference(n: int, steps: int = 1, procs: int = 1):
+    """The unmodified reference (oracle/_ref, compiled from its own sources)
+    on the host cores: ``procs`` independent processes, each one TGV case of
+    the bench's shape timed for ``steps`` time steps (ComputeTimeStep +
+    EvolveFluidDynamics).  Returns (Mcell-steps/s aggregate, details)."""
+    from artracfd_b200 import configs
+    spec = configs.tgv(n=n)
+    work = tempfile.mkdtemp(prefix="acfd_cpu_")
+    case = os.path.join(work, "tgv")
+    spec.write(case)
+    code = (
+        "import sys,time,os; sys.path.insert(0,%r)\n"
+        "from oracle.oracle import Reference\n"
+        "import contextlib, io\n"
+        "r=Reference(); d=sys.argv[1]\n"
+        "devnull=os.open(os.devnull, os.O_WRONLY); os.dup2(devnull,1)\n"
+        "r.load(d)\n"
+        "t=[]\n"
+        "for k in range(%d):\n"
+        "    t0=time.perf_counter(); dt=r.time_step(); r.evolve_fluid(dt); t.append(time.perf_counter()-t0)\n"
+        "sys.stderr.write('STEPTIMES '+' '.join('%%.6f'%%x for x in t)+'\\n')\n" % (ROOT, steps))
+    ps = []
+    for q in range(procs):
+        d = os.path.join(work, f"p{q}")
+        subprocess.run(["cp", "-r", case, d], check=True)
+        ps.append(subprocess.Popen([sys.executable, "-c", code, d], stderr=subprocess.PIPE, stdout=subprocess.DEVNULL,
+                                   text=True))
+    times = []
+    for p in ps:
+        _, err = p.communicate()
+        for line in err.splitlines():
+            if line.startswith("STEPTIMES"):
+                times.append([float(x) for x in line.split()[1:]])
+    if not times:
+        return None, {}
+    nodes = (n + 1) ** 3
+    per_step = max(sum(t) / len(t) for t in times)
+    rate = len(times) * nodes / per_step / 1e6
+    subprocess.run(["rm", "-rf", work])
+    return rate, {"seconds_per_step": per_step, "procs": len(times), "steps": steps}
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    from artracfd_b200 import abi, configs
+    from artracfd_b200.solver import Solver
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    spec = configs.tgv(n=args.n)
+    part, model = spec.descriptors()
+    nodes_pin = (args.n + 1) ** 3
+    node = spec.initial_nodes(part, model)
+    mode = {"fp64": abi.FP64, "fp64_exact": abi.FP64_EXACT, "fp32": abi.FP32_BULK}[args.mode]
+    stream = torch.cuda.Stream()
+    s = Solver(part, model, mode)
+    s.set_stream(stream.cuda_stream)
+    s.upload(node)
+    s.treat_boundary(abi.TO)
+
+    def step():
+        dt = s.time_step(spec.cfl)
+        s.evolve(dt, graph=True)
+        return dt
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    launches0 = s.launches()
+    with ClockSampler(local_rank) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    gpu_launches = s.launches() - launches0
+    sec = e0.elapsed_time(e1) / 1e3
+    if dist:
+        t = torch.tensor([sec], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sec = float(t.item())
+        dist.barrier()
+    value = world * nodes_pin * args.steps / sec / 1e6
+    # per-stage launch timing of the dominant kernel (the stage sweep) on the
+    # solver's stream: one eager step, events around each LLLU stage
+    stage_ms = []
+    bc_ms = []
+    dt = s.time_step(spec.cfl)
+    order = [2, 1, 0, 0, 1, 2]
+    coefs = [(0.0, 1.0, abi.TO, abi.TO, abi.TN), (0.75, 0.25, abi.TO, abi.TN, abi.TM),
+             (1.0 / 3.0, 2.0 / 3.0, abi.TO, abi.TM, abi.TO)]
+    stage_bytes = 0.0
+    with torch.cuda.stream(stream):
+        for sd in order:
+            for q, (a, b, to, tn, tm) in enumerate(coefs):
+                ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+                ev[0].record(stream)
+                s.lllu(0.5 * dt, a, b, to, tn, tm, sd)
+                ev[1].record(stream)
+                s.treat_boundary(tm)
+                ev[2].record(stream)
+                ev[2].synchronize()
+                stage_ms.append(ev[0].elapsed_time(ev[1]))
+                bc_ms.append(ev[1].elapsed_time(ev[2]))
+                stage_bytes += STAGE_BYTES[q] * nodes_pin
+    hbm_peak, peak_kind = load_peaks()
+    mean_stage = sum(stage_ms) / len(stage_ms) / 1e3
+    achieved = stage_bytes / len(stage_ms) / mean_stage / 1e9
+    flop_rate = FLOP_PER_NODE_STAGE_VISCOUS * nodes_pin / mean_stage / 1e12
+    fp64_peak = fp64_peak_tflops(torch) if rank == 0 else None
+    # e2e through the C ABI with host buffers: upload of the host node array,
+    # K steps (CFL read back each step), download of the result
+    host = node.copy()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.upload(host)
+    s.treat_boundary(abi.TO)
+    for _ in range(args.steps):
+        step()
+    s.download(host)
+    e2e_sec = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_sec], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_sec = float(t.item())
+    node_bytes = host.nbytes
+    s.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    cpu = None
+    if not args.no_cpu_baseline:
+        rate, det = cpu_baseline_reference(args.n, steps=1, procs=1)
+        if rate is not None:
+            cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"1 time step of the same TGV {args.n}^3 case by the unmodified reference "
+                             f"(oracle/_ref, gcc -O2 -std=c99), 1 process on 1 core: "
+                             f"{det['seconds_per_step']:.2f} s/step"}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": {"fp64": "f64", "fp64_exact": "f64", "fp32": "f32/f64"}[args.mode],
+        "data": "synthetic (analytic TGV initial field)",
+        "config": {"workload": WORKLOAD, "form": args.mode, "nodes_per_gpu": nodes_pin,
+                   "l2": "state 295 MB > 126 MB L2, no flush", "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "traffic": profiled_traffic(args.mode),
+                     "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum per stage launch "
+                                     "(profiles/), algorithmic bytes per launch = "
+                                     f"{stage_bytes / len(stage_ms):.4g}",
+                     "kernel": "stage sweep (LLLU), mean over the 18 stages of one step",
+                     "peak_kind": peak_kind,
+                     "fp64": {"achieved_tflops": flop_rate, "peak_tflops": fp64_peak,
+                              "frac": (flop_rate / fp64_peak) if fp64_peak else None,
+                              "peak_kind": "measured cuBLAS DGEMM 8192^3 in this run",
+                              "flop_per_node_stage": FLOP_PER_NODE_STAGE_VISCOUS}},
+        "stage_ms": {"sweep_mean": sum(stage_ms) / len(stage_ms), "ghost_fill_mean": sum(bc_ms) / len(bc_ms)},
+        "clocks": clk.summary(),
+        "e2e": {"value": world * nodes_pin * args.steps / e2e_sec / 1e6, "unit": UNIT,
+                "h2d_bytes_per_step": (node_bytes + 8 * args.steps) / args.steps,
+                "d2h_bytes_per_step": (node_bytes + 24 * args.steps) / args.steps,
+                "what": "C-ABI loop with host node arrays: acfd_sync_to_device, K x (acfd_cfl + host dt + "
+                        "acfd_evolve_fluid_graph), acfd_sync_to_host; wall clock"},
+        "gpu_launches": gpu_launches,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    procs = os.cpu_count() or 1
+    procs = max(1, min(procs, args.ref_procs))
+    t0 = time.perf_counter()
+    rates = []
+    rate, det = cpu_baseline_reference(args.n, steps=max(1, args.steps), procs=procs)
+    if rate is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference harness oracle/_ref not built"}))
+        return
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": 0, "ms_per_step": det["seconds_per_step"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (analytic TGV initial field)",
+        "config": {"workload": WORKLOAD, "form": "reference CPU (serial C99)", "procs": det["procs"]},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": det["procs"], "kind": "reference",
+                         "sample": f"{det['procs']} independent processes of the unmodified reference, "
+                                   f"{det['steps']} time step(s) each of TGV {args.n}^3"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": time.perf_counter() - t0,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="fp64", choices=["fp64", "fp64_exact", "fp32"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-procs", type=int, default=16)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

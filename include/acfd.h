@@ -157,6 +157,10 @@ int acfd_set_stream(acfd_case_t *cs, void *stream);
 /* Select the arithmetic form (ACFD_FP64_EXACT, ACFD_FP64, ACFD_FP32_BULK,
  * ACFD_FP32_HYBRID). */
 int acfd_set_precision(acfd_case_t *cs, int mode);
+/* Number of kernels this case has launched so far (graph replays count their
+ * kernel nodes).  No reference counterpart: instrumentation (the reference
+ * only times whole steps, timer.c:22-35). */
+int acfd_stats(acfd_case_t *cs, long long *launches);
 
 /* ---- host <-> device coherence ----------------------------------------- */
 

@@ -1,0 +1,101 @@
+"""The oracle (CPU restatement) pinned against the reference: committed golden
+fixtures made by the reference itself, the reference's own per-point
+functions (when oracle/_ref is built), and analytic known answers."""
+import numpy as np
+import pytest
+
+from artracfd_b200 import abi
+from oracle.oracle import Oracle, Reference, reference_available
+
+import golden_io
+
+CASES = golden_io.names()
+
+
+@pytest.fixture(scope="module")
+def orc():
+    return Oracle()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_steps_match_reference_bitwise(orc, name):
+    b = golden_io.Bundle(name)
+    node = b.initial_nodes()
+    for k in range(len(b.dt)):
+        dt = orc.time_step(node, b.part, b.model, b.cfl, b.geo)
+        assert dt == b.dt[k], f"step {k + 1}: dt {dt!r} != reference {b.dt[k]!r}"
+        orc.evolve_fluid(node, b.part, b.model, dt, b.geo)
+        got = node["U"][:, 0, :]
+        ref = b.U_after(k + 1)
+        assert np.array_equal(got, ref), f"step {k + 1}: max |diff| {np.nanmax(np.abs(got - ref))}"
+
+
+@pytest.mark.parametrize("name", [n for n in CASES if golden_io.Bundle(n).has_motion])
+def test_oracle_geometric_field_matches_reference(orc, name):
+    """ComputeGeometricField + TreatImmersedBoundary after a body motion:
+    flags bit-exact, reconstructed values bitwise."""
+    b = golden_io.Bundle(name)
+    node = b.initial_nodes()
+    orc.compute_geometric_field(node, b.part, b.model, b.geo_moved)
+    orc.treat_ib(node, b.part, b.model, abi.TO, b.geo_moved)
+    flags = np.stack([node[f] for f in ("did", "fid", "lid", "gst")], 1)
+    assert np.array_equal(flags, b.z["flagss"])
+    assert np.array_equal(node["U"][:, 0, :], b.z["Us"])
+
+
+def test_weno5_reduces_to_linear_scheme_on_smooth_data(orc):
+    """Known answer: for smooth data the WENO5 weights tend to (0.1, 0.6, 0.3),
+    so the reconstruction tends to the linear fifth-order upwind value."""
+    x = np.arange(5) * 1e-3
+    F = np.stack([np.sin(1.0 + x + 0.1 * r) for r in range(5)], axis=1)
+    lin = (2 * F[0] - 13 * F[1] + 47 * F[2] + 27 * F[3] - 3 * F[4]) / 60.0
+    got = orc.weno5(F)
+    assert np.allclose(got, lin, rtol=0, atol=1e-9)
+
+
+def test_weno5_is_non_oscillatory_at_a_jump(orc):
+    F = np.zeros((5, 5))
+    F[3:, :] = 1.0
+    got = orc.weno5(F)
+    assert np.all(got < 1e-5)  # the stencil across the jump gets ~zero weight
+
+
+@pytest.mark.skipif(not reference_available(), reason="oracle/_ref not built")
+def test_per_point_functions_match_reference():
+    orc = Oracle()
+    ref = Reference()
+    rng = np.random.default_rng(7)
+    for _ in range(200):
+        F = rng.normal(size=(5, 5)) * 10.0 ** rng.integers(-3, 3)
+        assert np.array_equal(orc.weno5(F), ref.weno5(F))
+        assert np.array_equal(orc.weno3(F[:3]), ref.weno3(F[:3]))
+
+
+def _sod_exact_plateaus():
+    # exact Riemann solution of the Sod problem (gamma = 1.4)
+    return 0.42632, 0.26557
+
+
+@pytest.mark.slow
+def test_sod_density_plateaus_known_answer(orc):
+    """Known answer: the oracle run of the Sod case (128x8x8, t = 0.2) has the
+    exact Riemann density plateaus behind the rarefaction and the shock."""
+    from artracfd_b200 import configs
+    spec = configs.sod()
+    part, model = spec.descriptors()
+    node = spec.initial_nodes(part, model)
+    orc.treat_boundary(node, part, model, abi.TO)
+    now, end = 0.0, spec.end_time
+    while now < end:
+        dt = orc.time_step(node, part, model, spec.cfl)
+        now += dt
+        if now > end:
+            dt = end - (now - dt)
+            now = end
+        orc.evolve_fluid(node, part, model, dt)
+    n = list(part.n)
+    rho = node["U"][:, 0, 0].reshape(n[2], n[1], n[0])[n[2] // 2, n[1] // 2]
+    x = part.domain[0][0] + (np.arange(n[0]) - part.ng[0]) * part.d[0]
+    p3, p4 = _sod_exact_plateaus()
+    assert abs(rho[(x > 0.52) & (x < 0.62)].mean() - p3) < 2e-3
+    assert abs(rho[(x > 0.72) & (x < 0.82)].mean() - p4) < 2e-3
