@@ -165,6 +165,7 @@ def load_library(path: str | None = None):
         "acfd_device_state": [vp, ctypes.POINTER(dp), ctypes.POINTER(ctypes.POINTER(ctypes.c_int)),
                               ctypes.POINTER(i), ctypes.POINTER(sz)],
         "acfd_cfl": [vp, dp],
+        "acfd_cfl_noalloc": [ctypes.POINTER(Partition), ctypes.POINTER(Model), vp, vp, i, vp, vp],
         "acfd_evolve_fluid": [vp, d],
         "acfd_evolve_fluid_graph": [vp, d],
         "acfd_discretize_time": [vp, d, i],

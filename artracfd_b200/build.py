@@ -28,6 +28,7 @@ COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcom
 UNITS = {
     "acfd_api.cu": [],
     "boundary.cu": ["--fmad=false"],
+    "cfl_noalloc.cu": ["--fmad=false"],
     "ib.cu": ["--fmad=false"],
     "sweep_exact.cu": ["--fmad=false"],
     "sweep_fast.cu": [],

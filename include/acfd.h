@@ -181,6 +181,20 @@ int acfd_device_state(acfd_case_t *cs, double **U, int **flags, int *pitch, size
  * |u_s| + c over PIN nodes with did == 0 of U[TO].  The body-speed part and
  * dt = CFL * min(d/Vmax) stay with the caller. */
 int acfd_cfl(acfd_case_t *cs, double vmax[3]);
+/* The same maximum for callers that must not allocate device memory (hosts
+ * whose device memory belongs to a pool allocator, or whose memory budget is
+ * fixed at start-up so that cudaMalloc/cudaFree may fail or synchronize the
+ * device in the time loop).  No counterpart in the reference.
+ * U_to: device pointer to the five U[TO] planes (plane stride pitch*n[Y]*n[Z]),
+ * did: device pointer to the did plane, vmax_dev: device pointer to 3 doubles
+ * (written), stream: cudaStream_t or NULL.  Allocates nothing: its scratch is
+ * a fixed 96 KiB device array in the library (4096 partial maxima), held on
+ * every GPU that loads the library until exit, which limits a case to
+ * 33,554,432 computed nodes (larger cases: ACFD_ERR_ARG).  The first call on a
+ * device looks up that array's address, so make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race. */
+int acfd_cfl_noalloc(const acfd_partition_t *part, const acfd_model_t *model, const double *U_to,
+        const int *did, int pitch, double *vmax_dev, void *stream);
 /* EvolveFluidDynamics (fluid_dynamics.c:55-116): one time step of size dt on
  * U[TO], including every TreatBoundary of the stages. */
 int acfd_evolve_fluid(acfd_case_t *cs, double dt);
