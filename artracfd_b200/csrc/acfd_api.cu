@@ -4,10 +4,14 @@
 // TreatBoundary, fluid_dynamics.c:55-148, boundary_treatment.c:28-65).
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "acfd_internal.cuh"
+#include "brick_geometry.cuh"
 
 namespace acfd {
 
@@ -30,6 +34,8 @@ int cuda_status(cudaError_t e, const char *what)
 int launch_stage_exact(const Grid &, const ModelParams &, const StageArgs &, int, bool, cudaStream_t);
 int launch_stage_fast(const Grid &, const ModelParams &, const StageArgs &, int, bool, cudaStream_t);
 int launch_stage_fp32(const Grid &, const ModelParams &, const StageArgs &, int, bool, cudaStream_t);
+int launch_stage_brick_fast(const Grid &, const ModelParams &, const StageArgs &, int, bool, cudaStream_t);
+int launch_stage_brick_fp32(const Grid &, const ModelParams &, const StageArgs &, int, bool, cudaStream_t);
 int launch_weno_batch_exact(int, const double *, double *, int, cudaStream_t);
 int launch_weno_batch_fast(int, const double *, double *, int, cudaStream_t);
 int launch_weno_batch_fp32(int, const double *, double *, int, cudaStream_t);
@@ -81,6 +87,10 @@ struct acfd_case {
     int graph_mode = -1;
     long long launches = 0;        // kernels launched by this case (graph replays included)
     long long graph_kernels = 0;   // kernels in the captured step graph
+    int *dstatus = nullptr;        // device error word (TMA wait time-outs)
+    CUtensorMap maps[3];           // state tensor maps of the brick kernels, one per sweep axis
+    bool maps_ok = false;
+    bool plain_kernels = false;    // use the global-memory stage kernels instead of the bricks
 };
 
 namespace {
@@ -88,6 +98,57 @@ namespace {
 bool viscous(const acfd_case *cs)
 {
     return cs->model.refMu > 0.0;
+}
+
+// 5-D tensor map of the whole state U[level][var][z][y][x] with the brick of
+// sweep axis s as its box (cuTensorMapEncodeTiled through the runtime's driver
+// entry point, so the library needs no -lcuda)
+int encode_state_maps(acfd_case *cs)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) {
+            set_error("cuTensorMapEncodeTiled not available from the driver");
+            return ACFD_ERR_CUDA;
+        }
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const Grid &g = cs->grid;
+    const cuuint64_t dims[5] = {(cuuint64_t)g.pitch, (cuuint64_t)g.n[1], (cuuint64_t)g.n[2], 5, 3};
+    const cuuint64_t strides[4] = {(cuuint64_t)g.pitch * 8, (cuuint64_t)g.pitch * g.n[1] * 8,
+                                   (cuuint64_t)g.nn * 8, (cuuint64_t)g.nn * 5 * 8};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    for (int s = 0; s < 3; ++s) {
+        int b[3];
+        brick_box(s, viscous(cs), b);
+        const cuuint32_t box[5] = {(cuuint32_t)b[0], (cuuint32_t)b[1], (cuuint32_t)b[2], 5, 1};
+        CUresult r = encode(&cs->maps[s], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, cs->U, dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) {
+            set_error("cuTensorMapEncodeTiled failed (%d) for sweep axis %d", (int)r, s);
+            return ACFD_ERR_CUDA;
+        }
+    }
+    cs->maps_ok = true;
+    return ACFD_OK;
+}
+
+// read and clear the device error word
+int check_device_status(acfd_case *cs)
+{
+    int h = 0;
+    ACFD_CUDA(cudaMemcpyAsync(&h, cs->dstatus, sizeof(int), cudaMemcpyDeviceToHost, cs->stream));
+    ACFD_CUDA(cudaStreamSynchronize(cs->stream));
+    if (h != 0) {
+        cudaMemsetAsync(cs->dstatus, 0, sizeof(int), cs->stream);
+        set_error("stage kernel reported device error %d (TMA load not completed within its wait limit)", h);
+        return ACFD_ERR_DEVICE;
+    }
+    return ACFD_OK;
 }
 
 double *level(acfd_case *cs, int l)
@@ -167,6 +228,10 @@ int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int 
     a.coeA = coeA;
     a.coeB = coeB;
     a.accumulate = 0;
+    a.to = to;
+    a.tn = tn;
+    a.maps = cs->maps;
+    a.status = cs->dstatus;
     if (p == ACFD_PHI) {
         ++cs->launches;
         return launch_stage_phi(cs->grid, cs->mp, a, cs->stream);
@@ -199,10 +264,17 @@ int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int 
     for (int s = s0; s < s1; ++s) {
         a.accumulate = (cs->model.multidim == 1 && s != 0) ? 1 : 0;
         int st;
+        const bool brick = cs->maps_ok && !cs->plain_kernels;
         switch (cs->mode) {
             case ACFD_FP64_EXACT: st = launch_stage_exact(cs->grid, cs->mp, a, s, visc, cs->stream); break;
-            case ACFD_FP64: st = launch_stage_fast(cs->grid, cs->mp, a, s, visc, cs->stream); break;
-            default: st = launch_stage_fp32(cs->grid, cs->mp, a, s, visc, cs->stream); break;
+            case ACFD_FP64:
+                st = brick ? launch_stage_brick_fast(cs->grid, cs->mp, a, s, visc, cs->stream)
+                           : launch_stage_fast(cs->grid, cs->mp, a, s, visc, cs->stream);
+                break;
+            default:
+                st = brick ? launch_stage_brick_fp32(cs->grid, cs->mp, a, s, visc, cs->stream)
+                           : launch_stage_fp32(cs->grid, cs->mp, a, s, visc, cs->stream);
+                break;
         }
         if (st != ACFD_OK) {
             return st;
@@ -384,7 +456,8 @@ int acfd_init(const acfd_partition_t *part, const acfd_model_t *model, acfd_case
         (e = cudaMalloc(&cs->d_dt, sizeof(double))) != cudaSuccess ||
         (e = cudaMalloc(&cs->cfl_part, sizeof(double) * 3 * kCflBlocks)) != cudaSuccess ||
         (e = cudaMalloc(&cs->cfl_out, sizeof(double) * 3)) != cudaSuccess ||
-        (e = cudaMallocHost(&cs->h_cfl, sizeof(double) * 3)) != cudaSuccess) {
+        (e = cudaMallocHost(&cs->h_cfl, sizeof(double) * 3)) != cudaSuccess ||
+        (e = cudaMalloc(&cs->dstatus, sizeof(int))) != cudaSuccess) {
         st = cuda_status(e, "acfd_init allocation");
         acfd_finalize(cs);
         return st;
@@ -392,6 +465,14 @@ int acfd_init(const acfd_partition_t *part, const acfd_model_t *model, acfd_case
     // padding and never-written nodes: flags -1 (outside PIN), U zero
     cudaMemsetAsync(cs->U, 0, ubytes, cs->stream);
     cudaMemsetAsync(cs->flags, 0xff, fbytes, cs->stream);
+    cudaMemsetAsync(cs->dstatus, 0, sizeof(int), cs->stream);
+    if ((st = encode_state_maps(cs)) != ACFD_OK) {
+        acfd_finalize(cs);
+        return st;
+    }
+    if (getenv("ACFD_PLAIN_KERNELS")) {
+        cs->plain_kernels = true;
+    }
     if ((st = ib_create(&cs->ib)) != ACFD_OK) {
         acfd_finalize(cs);
         return st;
@@ -421,6 +502,7 @@ int acfd_finalize(acfd_case_t *cs)
     cudaFree(cs->d_dt);
     cudaFree(cs->cfl_part);
     cudaFree(cs->cfl_out);
+    cudaFree(cs->dstatus);
     cudaFree(cs->staging);
     if (cs->h_cfl) cudaFreeHost(cs->h_cfl);
     if (cs->own_stream && cs->stream) cudaStreamDestroy(cs->stream);
@@ -496,6 +578,7 @@ int acfd_sync_to_host(acfd_case_t *cs, acfd_node_t *node, unsigned mask)
     TRY(launch_gather_nodes(cs->grid, cs->U, cs->flags, cs->staging, mask, cs->stream));
     ACFD_CUDA(cudaMemcpyAsync(node, cs->staging, total * sizeof(acfd_node_t), cudaMemcpyDeviceToHost, cs->stream));
     ACFD_CUDA(cudaStreamSynchronize(cs->stream));
+    TRY(check_device_status(cs));
     return ib_check(cs->ib, cs->stream);
 }
 
@@ -523,6 +606,7 @@ int acfd_cfl(acfd_case_t *cs, double vmax[3])
     for (int s = 0; s < 3; ++s) {
         vmax[s] = cs->h_cfl[s];
     }
+    TRY(check_device_status(cs));
     return ib_check(cs->ib, cs->stream);
 }
 

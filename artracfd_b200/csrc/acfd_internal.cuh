@@ -8,6 +8,7 @@
 // 64-byte boundary and whose accesses along x are fully coalesced.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -44,6 +45,9 @@ struct StageArgs {
     double dt_scale;      // this sweep uses dt_scale * (*dt) (0.5 for Strang halves)
     double coeA, coeB;
     int accumulate;       // operator-by-operator Y/Z: Um += coeB*r*Phi
+    int to, tn;           // level indices (the brick kernels address U through a tensor map)
+    const CUtensorMap *maps;  // host array: TMA map of the whole state for each sweep axis
+    int *status;          // device error word of the case
 };
 
 // ---------------------------------------------------------------------------

@@ -23,3 +23,15 @@ int launch_fhat_batch_fast(const ModelParams &m, int s, const double *U, double 
 }
 
 }  // namespace acfd
+
+#include "sweep_brick.cuh"
+
+namespace acfd {
+
+int launch_stage_brick_fast(const Grid &g, const ModelParams &m, const StageArgs &a, int s, bool viscous,
+                            cudaStream_t st)
+{
+    return form_fast::launch_brick_impl(g, m, a, s, viscous, st);
+}
+
+}  // namespace acfd
