@@ -160,6 +160,7 @@ def load_library(path: str | None = None):
         "acfd_set_stream": [vp, vp],
         "acfd_set_precision": [vp, i],
         "acfd_stats": [vp, ctypes.POINTER(ctypes.c_longlong)],
+        "acfd_synchronize": [vp],
         "acfd_sync_to_device": [vp, vp, u],
         "acfd_sync_to_host": [vp, vp, u],
         "acfd_device_state": [vp, ctypes.POINTER(dp), ctypes.POINTER(ctypes.POINTER(ctypes.c_int)),

@@ -91,6 +91,11 @@ struct FaceBox {
 };
 int launch_domain_boundary(const Grid &g, const ModelParams &m, const acfd_partition_t &part,
                            const FaceBox *boxes, int nbox, double *U, cudaStream_t st);
+// all groups of one TreatBoundary in one cooperative launch with grid barriers;
+// bar: two device words (arrival count, generation), zero at first use
+int launch_domain_boundary_fused(const Grid &g, const ModelParams &m, const acfd_partition_t &part,
+                                 const FaceBox *const *groups, const int *sizes, int ngroups, double *U,
+                                 unsigned *bar, int *status, cudaStream_t st);
 
 // CFL wave-speed maximum: partials (>= kCflBlocks*3 doubles) then out[3]
 constexpr int kCflBlocks = 296;

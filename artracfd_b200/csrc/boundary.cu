@@ -5,7 +5,9 @@
 // Compiled with --fmad=false: the primitive/conservative maps and the
 // method-of-images arithmetic are evaluated in the reference's order, so the
 // filled ghost values are bitwise those of the reference.
+#include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 
 #include "acfd_internal.cuh"
 
@@ -18,11 +20,13 @@ __device__ __forceinline__ long long node_of(const Grid &g, int i, int j, int k)
     return ((long long)k * g.n[1] + j) * g.pitch + i;
 }
 
+// loads bypass L1: in the fused ghost fill a value may have been written by
+// another SM in the previous phase of the same launch
 __device__ __forceinline__ void load5(const double *U, long long nn, long long id, double u[5])
 {
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-        u[v] = U[v * nn + id];
+        u[v] = __ldcg(U + v * nn + id);
     }
 }
 
@@ -70,6 +74,8 @@ struct FaceJobs {
     int njob;
 };
 
+__device__ void fill_node(const Grid &g, const ModelParams &mp, const FaceJob &J, long long t, double *U);
+
 __global__ void domain_fill(Grid g, ModelParams mp, FaceJobs jobs, double *U)
 {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -81,7 +87,77 @@ __global__ void domain_fill(Grid g, ModelParams mp, FaceJobs jobs, double *U)
             return;
         }
     }
-    const FaceJob &J = jobs.job[q];
+    fill_node(g, mp, jobs.job[q], t, U);
+}
+
+// All phases of one TreatBoundary in one cooperative launch: the blocks sweep
+// the boxes of a phase, then meet at a grid barrier before the next phase.
+constexpr int kMaxPhases = 16;
+struct PhasePlan {
+    FaceJobs phase[kMaxPhases];
+    int nphase;
+};
+
+constexpr long long kBarrierSpinLimit = 1LL << 22;
+
+// Grid barrier for co-resident blocks (cooperative launch).  bar[0] counts
+// arrivals, bar[1] is the generation.  A block that waits longer than the
+// spin limit records error 5 and returns false.
+__device__ bool grid_barrier(unsigned *bar, unsigned nblocks, int *status)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        volatile unsigned *gen = bar + 1;
+        const unsigned g0 = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == nblocks - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            long long it = 0;
+            while (*gen == g0) {
+                if (++it > kBarrierSpinLimit) {
+                    atomicExch(status, 5);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(20);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+__global__ void __launch_bounds__(1024) domain_fill_fused(Grid g, ModelParams mp, PhasePlan plan, double *U,
+                                                          unsigned *bar, int *status)
+{
+    const long long nthreads = (long long)gridDim.x * blockDim.x;
+    for (int ph = 0; ph < plan.nphase; ++ph) {
+        const FaceJobs &jobs = plan.phase[ph];
+        const long long total = jobs.job[0].count + (jobs.njob > 1 ? jobs.job[1].count : 0);
+        for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += nthreads) {
+            if (t < jobs.job[0].count) {
+                fill_node(g, mp, jobs.job[0], t, U);
+            } else {
+                fill_node(g, mp, jobs.job[1], t - jobs.job[0].count, U);
+            }
+        }
+        if (ph + 1 < plan.nphase) {
+            __threadfence();
+            if (!grid_barrier(bar, gridDim.x, status)) {
+                return;
+            }
+        }
+    }
+}
+
+__device__ void fill_node(const Grid &g, const ModelParams &mp, const FaceJob &J, long long t, double *U)
+{
     const int i = J.lo[0] + (int)(t % J.ext[0]);
     const long long rest = t / J.ext[0];
     const int j = J.lo[1] + (int)(rest % J.ext[1]);
@@ -354,6 +430,92 @@ int launch_domain_boundary(const Grid &g, const ModelParams &m, const acfd_parti
     domain_fill<<<blocks_for(total, 256), 256, 0, st>>>(g, m, jobs, U);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "domain_fill launch");
+}
+
+static int fill_jobs(const acfd_partition_t &part, const FaceBox *boxes, int nbox, FaceJobs &jobs)
+{
+    jobs.njob = nbox;
+    for (int q = 0; q < nbox; ++q) {
+        FaceJob &J = jobs.job[q];
+        const FaceBox &b = boxes[q];
+        const int p = b.face;
+        for (int s = 0; s < 3; ++s) {
+            J.lo[s] = b.box[s][0];
+            J.ext[s] = b.box[s][1] - b.box[s][0];
+            J.N[s] = part.N[p][s];
+            J.LN[s] = part.m[s] * part.N[p][s];
+        }
+        J.type = part.typeBC[p];
+        J.r = b.r;
+        J.count = (long long)J.ext[0] * J.ext[1] * J.ext[2];
+        for (int v = 0; v < 6; ++v) {
+            J.given[v] = part.varBC[p][v];
+        }
+    }
+    if (nbox == 1) {
+        jobs.job[1] = jobs.job[0];
+        jobs.job[1].count = 0;
+    }
+    return ACFD_OK;
+}
+
+int launch_domain_boundary_fused(const Grid &g, const ModelParams &m, const acfd_partition_t &part,
+                                 const FaceBox *const *groups, const int *sizes, int ngroups, double *U,
+                                 unsigned *bar, int *status, cudaStream_t st)
+{
+    if (ngroups <= 0) {
+        return ACFD_OK;
+    }
+    if (ngroups > kMaxPhases) {
+        set_error("fused ghost fill: %d phases (at most %d)", ngroups, kMaxPhases);
+        return ACFD_ERR_ARG;
+    }
+    PhasePlan plan;
+    plan.nphase = ngroups;
+    for (int q = 0; q < ngroups; ++q) {
+        if (sizes[q] < 1 || sizes[q] > 2) {
+            set_error("fused ghost fill: phase of %d faces", sizes[q]);
+            return ACFD_ERR_ARG;
+        }
+        fill_jobs(part, groups[q], sizes[q], plan.phase[q]);
+    }
+    // every block must be resident at once for the grid barrier
+    static int blocks_per_sm[64] = {0};
+    static int sms[64] = {0};
+    int dev = 0;
+    ACFD_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) {
+        set_error("device ordinal %d", dev);
+        return ACFD_ERR_ARG;
+    }
+    // few large blocks: the barrier cost grows with the number of arriving
+    // blocks (ACFD_BC_BLOCKS overrides the default of 64 x 1024 threads)
+    static int nb_env = -1;
+    if (nb_env < 0) {
+        const char *e = getenv("ACFD_BC_BLOCKS");
+        nb_env = e ? atoi(e) : 64;
+    }
+    if (!blocks_per_sm[dev]) {
+        ACFD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm[dev], domain_fill_fused, 1024, 0));
+        ACFD_CUDA(cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev));
+        if (blocks_per_sm[dev] < 1) {
+            set_error("fused ghost fill cannot be resident");
+            return ACFD_ERR_CUDA;
+        }
+    }
+    const unsigned nblocks = (unsigned)std::max(1, std::min(nb_env, sms[dev] * blocks_per_sm[dev]));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nblocks);
+    cfg.blockDim = dim3(1024);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    ACFD_CUDA(cudaLaunchKernelEx(&cfg, domain_fill_fused, g, m, plan, U, bar, status));
+    return ACFD_OK;
 }
 
 int launch_cfl(const Grid &g, const ModelParams &m, const double *U, const int *did, double *partials,

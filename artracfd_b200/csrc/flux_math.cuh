@@ -280,8 +280,32 @@ __device__ __forceinline__ double sutherland(double T)
 // ===========================================================================
 namespace fast {
 
+// Reciprocal for the fast forms.  FP64: the hardware approximation
+// (rcp.approx.ftz.f64) refined by two Newton-Raphson steps
+// y <- y + y*(1 - x*y), each of which doubles the number of correct bits, so
+// the result is within about one ulp of 1/x (not always correctly rounded).
+// FP32: the fast approximate reciprocal.  Inputs here are positive normal
+// numbers (densities, sound speeds, WENO denominators >= 1e-12).
 template <typename T>
-__device__ __forceinline__ T rcp(T x) { return T(1) / x; }
+__device__ __forceinline__ T rcp(T x);
+
+template <>
+__device__ __forceinline__ double rcp<double>(double x)
+{
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    return y;
+}
+
+template <>
+__device__ __forceinline__ float rcp<float>(float x)
+{
+    return __fdividef(1.0f, x);
+}
 
 // Roe/arithmetic interface state: Uo[1..3] velocity, Uo[4] total enthalpy,
 // Uo[5] sound speed.
@@ -333,7 +357,7 @@ __device__ __forceinline__ T weno5(T f0, T f1, T f2, T f3, T f4)
     const T q0 = T(2) * f0 - T(7) * f1 + T(11) * f2;
     const T q1 = -f1 + T(5) * f2 + T(2) * f3;
     const T q2 = T(2) * f2 + T(5) * f3 - f4;
-    return (a0 * q0 + a1 * q1 + a2 * q2) / (T(6) * (a0 + a1 + a2));
+    return (a0 * q0 + a1 * q1 + a2 * q2) * rcp<T>(T(6) * (a0 + a1 + a2));
 }
 
 template <typename T>
@@ -348,7 +372,7 @@ __device__ __forceinline__ T weno3(T f0, T f1, T f2)
     const T a1 = T(2) * d0;     // (2/3)/d1 scaled by 3*d0*d1
     const T q0 = -f0 + T(3) * f1;
     const T q1 = f1 + f2;
-    return (a0 * q0 + a1 * q1) / (T(2) * (a0 + a1));
+    return (a0 * q0 + a1 * q1) * rcp<T>(T(2) * (a0 + a1));
 }
 
 // linear fifth-order upwind reconstruction (the WENO5 limit omega = C)

@@ -104,7 +104,7 @@ stage_brick(Grid g, ModelParams mp, StageArgs a, const __grid_constant__ CUtenso
         const Real cvinv = Real(1.0 / mp.cv);
         for (int n = tid; n < LY::nodes; n += kBrickThreads) {
             const Real r = Real(sU[n]);
-            const Real ir = Real(1) / r;
+            const Real ir = fast::rcp<Real>(r);
             const Real u = Real(sU[LY::nodes + n]) * ir;
             const Real v = Real(sU[2 * LY::nodes + n]) * ir;
             const Real w = Real(sU[3 * LY::nodes + n]) * ir;
@@ -137,7 +137,7 @@ stage_brick(Grid g, ModelParams mp, StageArgs a, const __grid_constant__ CUtenso
         const Real hT = Uo[4];
         const Real cs = Uo[5];
         const Real qk = Real(0.5) * (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
-        const Real d = Real(1) / (Real(2) * cs);
+        const Real d = fast::rcp<Real>(Real(2) * cs);
         const Real b = (gamma - Real(1)) * (Real(2) * d * d);
         const Real b2 = Real(2) * b;
         Real lp[5], ln[5];
@@ -237,7 +237,7 @@ stage_brick(Grid g, ModelParams mp, StageArgs a, const __grid_constant__ CUtenso
             const Real Tc = sP[3 * NN + c], Tp = sP[3 * NN + pn];
             const Real Th = Real(0.5) * (Tc + Tp);
             const Real Ts = Th * Real(mp.refT);
-            const Real mu = Real(mp.refMu) * (Real(1.458e-6) * Ts * sqrt(Ts) / (Ts + Real(110.4)));
+            const Real mu = Real(mp.refMu) * (Real(1.458e-6) * Ts * sqrt(Ts) * fast::rcp<Real>(Ts + Real(110.4)));
             const Real heatK = Real(mp.gamma * mp.cv / 0.71) * mu;
             const Real divV = grad[0][0] + grad[1][1] + grad[2][2];
             Real tau[3];

@@ -1,0 +1,20 @@
+/*
+ * acfd_shim.h -- declarations of the reference-side drop-in (see acfd_shim.c).
+ */
+#ifndef ACFD_SHIM_H_
+#define ACFD_SHIM_H_
+
+#include "commons.h"
+
+/* 1 when the program was started with -m gpu */
+extern int g_acfd_gpu_mode;
+
+/* the reference's own functions, renamed at compile time by the Makefile */
+int RefSolve(Time *, Space *, const Model *);
+void RefEvolveFluidDynamics(const Real, Space *, const Model *);
+void RefTreatBoundary(const int, Space *, const Model *);
+
+/* release the device case (called by main before Postprocess) */
+void AcfdShimFinalize(void);
+
+#endif

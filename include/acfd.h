@@ -157,6 +157,9 @@ int acfd_set_stream(acfd_case_t *cs, void *stream);
 /* Select the arithmetic form (ACFD_FP64_EXACT, ACFD_FP64, ACFD_FP32_BULK,
  * ACFD_FP32_HYBRID). */
 int acfd_set_precision(acfd_case_t *cs, int mode);
+/* Wait for all work queued on the case and report device-side errors (the
+ * per-step wall clock of solve.c:81,89 needs a finished step). */
+int acfd_synchronize(acfd_case_t *cs);
 /* Number of kernels this case has launched so far (graph replays count their
  * kernel nodes).  No reference counterpart: instrumentation (the reference
  * only times whole steps, timer.c:22-35). */

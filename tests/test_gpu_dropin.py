@@ -1,0 +1,96 @@
+"""The drop-in program: the reference program linked with libacfd_gpu
+(artracfd_b200/shim), run with `-m gpu`, against the unmodified reference
+program (oracle/_ref/artracfd) on the same case directory.  Both write their
+fields as EnSight float32 files, which are compared."""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from artracfd_b200 import configs
+
+import cases
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DROPIN = os.path.join(ROOT, "artracfd_b200", "shim", "_build", "artracfd_gpu")
+REFBIN = os.path.join(ROOT, "oracle", "_ref", "artracfd")
+FIELDS = ("rho", "u", "v", "w", "p", "T", "did")
+
+
+def _run(binary, mode, case_dir, env_extra=None):
+    env = dict(os.environ)
+    env.update(env_extra or {})
+    r = subprocess.run([binary, "-m", mode], cwd=case_dir, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, (binary, r.stdout[-2000:], r.stderr[-2000:])
+    return r
+
+
+def _field(path):
+    # EnSight Gold binary variable file: 3 x 80-byte strings, part id, 80-byte
+    # "block" line, then float32 values
+    raw = open(path, "rb").read()
+    return np.frombuffer(raw[80 + 80 + 4 + 80:], dtype=np.float32)
+
+
+def _last_fields(case_dir):
+    names = sorted(f for f in os.listdir(case_dir) if f.startswith("field0") and f.endswith(".rho"))
+    stem = names[-1][:-4]
+    return stem, {f: _field(os.path.join(case_dir, f"{stem}.{f}")) for f in FIELDS}
+
+
+def _pair(tmp_path, spec):
+    a = tmp_path / "ref"
+    b = tmp_path / "gpu"
+    spec.write(str(a))
+    shutil.copytree(a, b)
+    return str(a), str(b)
+
+
+needs = pytest.mark.skipif(not (os.path.exists(DROPIN) and os.path.exists(REFBIN)),
+                           reason="drop-in or reference program not built")
+
+
+@needs
+def test_dropin_exact_mode_reproduces_reference_files(tmp_path):
+    spec = configs.sod(m=(32, 4, 4), stepN=6)
+    a, b = _pair(tmp_path, spec)
+    _run(REFBIN, "serial", a)
+    _run(DROPIN, "gpu", b, {"ACFD_MODE": "exact"})
+    sa, fa = _last_fields(a)
+    sb, fb = _last_fields(b)
+    assert sa == sb
+    for f in FIELDS:
+        assert np.array_equal(fa[f], fb[f]), f
+
+
+@needs
+@pytest.mark.parametrize("name", ["tgv", "channel", "spheres"])
+def test_dropin_fast_mode_close_to_reference(tmp_path, name):
+    spec = cases.SMALL[name]()
+    spec.stepN = 4
+    a, b = _pair(tmp_path, spec)
+    _run(REFBIN, "serial", a)
+    _run(DROPIN, "gpu", b, {"ACFD_MODE": "fp64"})
+    sa, fa = _last_fields(a)
+    sb, fb = _last_fields(b)
+    assert sa == sb
+    assert np.array_equal(fa["did"], fb["did"])
+    for f in FIELDS[:-1]:
+        scale = max(np.abs(fa[f]).max(), np.abs(fa["rho"]).max() * 1e-3)
+        assert np.abs(fa[f] - fb[f]).max() <= 1e-5 * scale, f
+
+
+@needs
+def test_dropin_serial_mode_is_the_reference(tmp_path):
+    spec = configs.sod(m=(32, 4, 4), stepN=3)
+    a, b = _pair(tmp_path, spec)
+    _run(REFBIN, "serial", a)
+    _run(DROPIN, "serial", b)
+    sa, fa = _last_fields(a)
+    sb, fb = _last_fields(b)
+    for f in FIELDS:
+        assert np.array_equal(fa[f], fb[f])

@@ -128,6 +128,23 @@ def test_treat_boundary_and_cfl_bitwise(name, orc):
     assert np.array_equal(got["U"], node["U"])
 
 
+@pytest.mark.parametrize("name", ["channel", "gravity_box", "tgv", "spheres"])
+def test_fused_ghost_fill_equals_phase_launches(name, monkeypatch):
+    """The single cooperative ghost-fill launch (grid barriers between the
+    ordered phases) gives the same bits as one launch per phase."""
+    b = golden_io.Bundle(name)
+    outs = []
+    for fused in (False, True):
+        if fused:
+            monkeypatch.setenv("ACFD_BC_FUSED", "1")
+        else:
+            monkeypatch.delenv("ACFD_BC_FUSED", raising=False)
+        o, _ = gpu_run(b, abi.FP64, 2, dts=list(b.dt))
+        outs.append(o)
+    for a, c in zip(*outs):
+        assert np.array_equal(a, c)
+
+
 @pytest.mark.parametrize("s_dir", [0, 1, 2])
 def test_single_stage_lllu(s_dir, orc):
     b = golden_io.Bundle("channel")
