@@ -161,6 +161,15 @@ def load_library(path: str | None = None):
         "acfd_set_precision": [vp, i],
         "acfd_stats": [vp, ctypes.POINTER(ctypes.c_longlong)],
         "acfd_synchronize": [vp],
+        "acfd_autotune": [vp, ctypes.POINTER(ctypes.c_int)],
+        "acfd_mlp_param_count": [],
+        "acfd_sensor_load": [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_float],
+        "acfd_sensor_update": [vp, ctypes.POINTER(ctypes.c_ulonglong)],
+        "acfd_sensor_flags": [vp, ctypes.POINTER(vp)],
+        "acfd_sensor_features": [vp, i, vp, vp],
+        "acfd_mlp_forward": [vp, vp, i, vp, vp],
+        "acfd_mlp_grad": [vp, vp, vp, i, ctypes.c_float, vp, vp, vp],
+        "acfd_mlp_adam": [vp, vp, vp, vp, i, ctypes.c_float, ctypes.c_float, vp],
         "acfd_sync_to_device": [vp, vp, u],
         "acfd_sync_to_host": [vp, vp, u],
         "acfd_device_state": [vp, ctypes.POINTER(dp), ctypes.POINTER(ctypes.POINTER(ctypes.c_int)),

@@ -33,6 +33,7 @@ UNITS = {
     "sweep_exact.cu": ["--fmad=false"],
     "sweep_fast.cu": [],
     "sweep_fp32.cu": [],
+    "sensor.cu": [],
 }
 
 

@@ -2,6 +2,7 @@
 // coherence, and the schedule of one fluid time step
 // (EvolveFluidDynamics -> DiscretizeTime -> RungeKutta2/3 -> LLLU +
 // TreatBoundary, fluid_dynamics.c:55-148, boundary_treatment.c:28-65).
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -36,6 +37,7 @@ int launch_stage_fast(const Grid &, const ModelParams &, const StageArgs &, int,
 int launch_stage_fp32(const Grid &, const ModelParams &, const StageArgs &, int, bool, cudaStream_t);
 int launch_stage_brick_fast(const Grid &, const ModelParams &, const StageArgs &, int, bool, cudaStream_t);
 int launch_stage_brick_fp32(const Grid &, const ModelParams &, const StageArgs &, int, bool, cudaStream_t);
+int launch_stage_brick_hybrid(const Grid &, const ModelParams &, const StageArgs &, int, bool, cudaStream_t);
 int launch_weno_batch_exact(int, const double *, double *, int, cudaStream_t);
 int launch_weno_batch_fast(int, const double *, double *, int, cudaStream_t);
 int launch_weno_batch_fp32(int, const double *, double *, int, cudaStream_t);
@@ -88,13 +90,21 @@ struct acfd_case {
     long long launches = 0;        // kernels launched by this case (graph replays included)
     long long graph_kernels = 0;   // kernels in the captured step graph
     int *dstatus = nullptr;        // device error word (TMA wait time-outs)
-    CUtensorMap maps[3];           // state tensor maps of the brick kernels, one per sweep axis
+    CUtensorMap maps[3 * kTileVariants];  // state tensor maps of the brick kernels per (axis, tile variant)
     bool maps_ok = false;
+    int tile_var[3] = {0, 0, 0};   // tile variant of each sweep axis (acfd_autotune)
     bool plain_kernels = false;    // use the global-memory stage kernels instead of the bricks
     bool bc_multi = false;         // one launch per ghost-fill phase instead of the fused launch
     unsigned *bcbar = nullptr;     // grid-barrier words of the fused ghost fill
     std::vector<const FaceBox *> bc_ptrs;
     std::vector<int> bc_sizes;
+    // learned sensor of the hybrid form
+    float *sensor_params = nullptr;          // device, acfd_mlp_param_count() floats
+    uint8_t *sensor_flags = nullptr;         // device, [3][nn]
+    float2 *sensor_rp = nullptr;             // device, [nn] (rho, p) scratch of the flag pass
+    unsigned long long *sensor_count = nullptr;
+    float sensor_logit = 0.0f;               // flag where the logit exceeds this
+    bool sensor_ok = false;
 };
 
 namespace {
@@ -126,15 +136,17 @@ int encode_state_maps(acfd_case *cs)
                                    (cuuint64_t)g.nn * 8, (cuuint64_t)g.nn * 5 * 8};
     const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
     for (int s = 0; s < 3; ++s) {
-        int b[3];
-        brick_box(s, viscous(cs), b);
-        const cuuint32_t box[5] = {(cuuint32_t)b[0], (cuuint32_t)b[1], (cuuint32_t)b[2], 5, 1};
-        CUresult r = encode(&cs->maps[s], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, cs->U, dims, strides, box, estr,
-                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (r != CUDA_SUCCESS) {
-            set_error("cuTensorMapEncodeTiled failed (%d) for sweep axis %d", (int)r, s);
-            return ACFD_ERR_CUDA;
+        for (int var = 0; var < kTileVariants; ++var) {
+            int b[3];
+            brick_box(s, viscous(cs), var, b);
+            const cuuint32_t box[5] = {(cuuint32_t)b[0], (cuuint32_t)b[1], (cuuint32_t)b[2], 5, 1};
+            CUresult r = encode(&cs->maps[s * kTileVariants + var], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, cs->U, dims,
+                                strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) {
+                set_error("cuTensorMapEncodeTiled failed (%d) for sweep axis %d, tile variant %d", (int)r, s, var);
+                return ACFD_ERR_CUDA;
+            }
         }
     }
     cs->maps_ok = true;
@@ -250,6 +262,10 @@ int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int 
     a.tn = tn;
     a.maps = cs->maps;
     a.status = cs->dstatus;
+    a.flags = cs->sensor_flags;
+    for (int s = 0; s < 3; ++s) {
+        a.var[s] = cs->tile_var[s];
+    }
     if (p == ACFD_PHI) {
         ++cs->launches;
         return launch_stage_phi(cs->grid, cs->mp, a, cs->stream);
@@ -288,6 +304,10 @@ int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int 
             case ACFD_FP64:
                 st = brick ? launch_stage_brick_fast(cs->grid, cs->mp, a, s, visc, cs->stream)
                            : launch_stage_fast(cs->grid, cs->mp, a, s, visc, cs->stream);
+                break;
+            case ACFD_FP32_HYBRID:
+                st = brick ? launch_stage_brick_hybrid(cs->grid, cs->mp, a, s, visc, cs->stream)
+                           : launch_stage_fp32(cs->grid, cs->mp, a, s, visc, cs->stream);
                 break;
             default:
                 st = brick ? launch_stage_brick_fp32(cs->grid, cs->mp, a, s, visc, cs->stream)
@@ -334,6 +354,14 @@ int evolve(acfd_case *cs)
         {2, 1, 0, 0, 1, 2}, {2, 1, 1, 2, -1, -1}, {2, 0, 0, 2, -1, -1}, {1, 0, 0, 1, -1, -1},
         {-1, -1, -1, -1, -1, -1}, {2, 2, -1, -1, -1, -1}, {-1, -1, -1, -1, -1, -1},
         {1, 1, -1, -1, -1, -1}, {0, 0, -1, -1, -1, -1}};
+    if (cs->mode == ACFD_FP32_HYBRID) {
+        // sensor flags from U[TO], fixed for the whole step: the flags are
+        // dilated by one node in the sweep, which covers the motion of a
+        // feature during a step at CFL < 1
+        TRY(launch_sensor_flags(cs->grid, cs->mp, cs->U, cs->flags, cs->sensor_params, cs->sensor_logit,
+                                cs->sensor_rp, cs->sensor_flags, nullptr, cs->stream));
+        cs->launches += 2;
+    }
     if (cs->model.sState != 0) {
         TRY(discretize(cs, 0.5, ACFD_PHI));
     }
@@ -527,6 +555,10 @@ int acfd_finalize(acfd_case_t *cs)
     cudaFree(cs->cfl_out);
     cudaFree(cs->dstatus);
     cudaFree(cs->bcbar);
+    cudaFree(cs->sensor_params);
+    cudaFree(cs->sensor_flags);
+    cudaFree(cs->sensor_rp);
+    cudaFree(cs->sensor_count);
     cudaFree(cs->staging);
     if (cs->h_cfl) cudaFreeHost(cs->h_cfl);
     if (cs->own_stream && cs->stream) cudaStreamDestroy(cs->stream);
@@ -559,8 +591,8 @@ int acfd_set_precision(acfd_case_t *cs, int mode)
         set_error("acfd_set_precision: unknown mode %d", mode);
         return ACFD_ERR_ARG;
     }
-    if (mode == ACFD_FP32_HYBRID) {
-        set_error("acfd_set_precision: the hybrid form needs a loaded sensor");
+    if (mode == ACFD_FP32_HYBRID && !cs->sensor_ok) {
+        set_error("acfd_set_precision: the hybrid form needs a loaded sensor (acfd_sensor_load)");
         return ACFD_ERR_STATE;
     }
     if (mode != cs->mode) {
@@ -668,6 +700,135 @@ int acfd_evolve_fluid_graph(acfd_case_t *cs, double dt)
     }
     ACFD_CUDA(cudaGraphLaunch(cs->graph_exec, cs->stream));
     cs->launches += cs->graph_kernels;
+    return ACFD_OK;
+}
+
+int acfd_autotune(acfd_case_t *cs, int tiles[3])
+{
+    TRY(check_case(cs));
+    if (cs->mode == ACFD_FP64_EXACT || !cs->maps_ok || cs->plain_kernels) {
+        for (int s = 0; s < 3; ++s) {
+            if (tiles) tiles[s] = cs->tile_var[s];
+        }
+        return ACFD_OK;  // the exact form has no tile choice
+    }
+    cudaEvent_t e0, e1;
+    ACFD_CUDA(cudaEventCreate(&e0));
+    ACFD_CUDA(cudaEventCreate(&e1));
+    int st = set_dt(cs, 0.0);
+    const int half = (cs->model.sScheme == 1) ? 3 : 2;
+    for (int s = 0; s < 3 && st == ACFD_OK; ++s) {
+        const Grid &g = cs->grid;
+        if (g.lo[s] - half < 0 || g.hi[s] - 1 + half > g.n[s] - 1) {
+            continue;  // no sweep along a collapsed axis
+        }
+        float best = 1e30f;
+        int best_var = cs->tile_var[s];
+        for (int var = 0; var < kTileVariants && st == ACFD_OK; ++var) {
+            cs->tile_var[s] = var;
+            // stage 1 writes U[TN] only, which every step overwrites first
+            st = stage(cs, 1.0, 0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN, s);  // warm-up
+            float total = 0.0f;
+            for (int rep = 0; rep < 3 && st == ACFD_OK; ++rep) {
+                cudaEventRecord(e0, cs->stream);
+                st = stage(cs, 1.0, 0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN, s);
+                cudaEventRecord(e1, cs->stream);
+                cudaEventSynchronize(e1);
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                total += ms;
+            }
+            if (st == ACFD_OK && total < best) {
+                best = total;
+                best_var = var;
+            }
+        }
+        cs->tile_var[s] = best_var;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != ACFD_OK) {
+        return st;
+    }
+    release_graph(cs);
+    TRY(check_device_status(cs));
+    for (int s = 0; s < 3; ++s) {
+        if (tiles) tiles[s] = cs->tile_var[s];
+    }
+    return ACFD_OK;
+}
+
+int acfd_sensor_load(acfd_case_t *cs, const float *params, float threshold)
+{
+    TRY(check_case(cs));
+    if (!params || !(threshold > 0.0f) || !(threshold < 1.0f)) {
+        set_error("acfd_sensor_load: parameters and a threshold in (0,1) are required");
+        return ACFD_ERR_ARG;
+    }
+    const int np = sensor_param_count();
+    if (!cs->sensor_params) {
+        ACFD_CUDA(cudaMalloc(&cs->sensor_params, sizeof(float) * np));
+        ACFD_CUDA(cudaMalloc(&cs->sensor_flags, (size_t)3 * cs->grid.nn));
+        ACFD_CUDA(cudaMalloc(&cs->sensor_rp, sizeof(float2) * cs->grid.nn));
+        ACFD_CUDA(cudaMalloc(&cs->sensor_count, sizeof(unsigned long long)));
+    }
+    ACFD_CUDA(cudaMemcpyAsync(cs->sensor_params, params, sizeof(float) * np, cudaMemcpyHostToDevice, cs->stream));
+    ACFD_CUDA(cudaMemsetAsync(cs->sensor_flags, 1, (size_t)3 * cs->grid.nn, cs->stream));
+    ACFD_CUDA(cudaStreamSynchronize(cs->stream));
+    cs->sensor_logit = logf(threshold / (1.0f - threshold));
+    cs->sensor_ok = true;
+    release_graph(cs);
+    return ACFD_OK;
+}
+
+int acfd_sensor_update(acfd_case_t *cs, unsigned long long *flagged)
+{
+    TRY(check_case(cs));
+    if (!cs->sensor_ok) {
+        set_error("acfd_sensor_update: no sensor loaded");
+        return ACFD_ERR_STATE;
+    }
+    ACFD_CUDA(cudaMemsetAsync(cs->sensor_count, 0, sizeof(unsigned long long), cs->stream));
+    TRY(launch_sensor_flags(cs->grid, cs->mp, cs->U, cs->flags, cs->sensor_params, cs->sensor_logit,
+                            cs->sensor_rp, cs->sensor_flags, cs->sensor_count, cs->stream));
+    cs->launches += 2;
+    if (flagged) {
+        ACFD_CUDA(cudaMemcpyAsync(flagged, cs->sensor_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                  cs->stream));
+        ACFD_CUDA(cudaStreamSynchronize(cs->stream));
+    }
+    return ACFD_OK;
+}
+
+int acfd_sensor_flags(acfd_case_t *cs, const unsigned char **flags)
+{
+    TRY(check_case(cs));
+    if (!flags) {
+        set_error("acfd_sensor_flags: null output");
+        return ACFD_ERR_ARG;
+    }
+    if (!cs->sensor_ok) {
+        set_error("acfd_sensor_flags: no sensor loaded");
+        return ACFD_ERR_STATE;
+    }
+    *flags = cs->sensor_flags;
+    return ACFD_OK;
+}
+
+int acfd_sensor_features(acfd_case_t *cs, int s, float *features, float *departure)
+{
+    TRY(check_case(cs));
+    if (s < 0 || s > 2 || !features || !departure) {
+        set_error("acfd_sensor_features: bad arguments");
+        return ACFD_ERR_ARG;
+    }
+    if (cs->model.sScheme != 1) {
+        set_error("acfd_sensor_features: the sensor is defined for WENO5");
+        return ACFD_ERR_ARG;
+    }
+    TRY(launch_sensor_features(cs->grid, cs->mp, cs->U, cs->flags, s, features, departure, cs->stream));
+    ++cs->launches;
+    ACFD_CUDA(cudaStreamSynchronize(cs->stream));
     return ACFD_OK;
 }
 

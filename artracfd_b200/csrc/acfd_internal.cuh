@@ -46,9 +46,40 @@ struct StageArgs {
     double coeA, coeB;
     int accumulate;       // operator-by-operator Y/Z: Um += coeB*r*Phi
     int to, tn;           // level indices (the brick kernels address U through a tensor map)
-    const CUtensorMap *maps;  // host array: TMA map of the whole state for each sweep axis
+    const CUtensorMap *maps;  // host array: TMA map of the whole state per (sweep axis, tile variant)
+    int var[3];               // tile variant of each sweep axis (brick_geometry.cuh)
     int *status;          // device error word of the case
+    const uint8_t *flags; // hybrid form: sensor flags [3][node] (1 = full WENO5)
 };
+
+// one case of a batch (batch.cu), as the batched kernels see it
+struct BatchCase {
+    Grid g;
+    ModelParams mp;
+    double *U;              // the case's state (3 levels x 5 variables)
+    const int *did;
+    const uint8_t *flags;   // sensor flags [3][nn] or null
+    int tiles[3][3];        // tile counts (x, y, z) of the stage kernel of each sweep axis
+};
+
+// RK coefficients and levels of one stage, common to all cases of a batch
+struct StageCoefs {
+    double coeA, coeB, dt_scale;
+    int to, tn, tm;
+};
+
+int launch_stage_batch(const BatchCase *cases, const CUtensorMap *maps, const long long *prefix, int ncase,
+                       const StageCoefs &sc, const double *dts, unsigned long long *counter, int *status, int blocks,
+                       int s, bool hybrid, cudaStream_t st);
+
+// learned sensor (sensor.cu)
+// rho_p: scratch of nn float2 (density and pressure of every node)
+int launch_sensor_flags(const Grid &g, const ModelParams &m, const double *U, const int *did, const float *params,
+                        float logit_threshold, float2 *rho_p, uint8_t *flags, unsigned long long *count,
+                        cudaStream_t st);
+int launch_sensor_features(const Grid &g, const ModelParams &m, const double *U, const int *did, int s, float *feat,
+                           float *dep, cudaStream_t st);
+int sensor_param_count();
 
 // ---------------------------------------------------------------------------
 // error state (per host thread)

@@ -1,6 +1,6 @@
-// Geometry of the shared-memory bricks of the stage kernels (fast FP64 and
-// FP32 forms), shared by the kernels and by the host code that encodes the
-// TMA tensor maps.
+// Geometry of the shared-memory bricks of the stage kernels (fast FP64, FP32
+// and hybrid forms), shared by the kernels and by the host code that encodes
+// the TMA tensor maps.
 //
 // A block owns a tile of interfaces: T[s] interfaces along the sweep axis s
 // (the first one is the left interface of the tile's first node, so the block
@@ -10,54 +10,62 @@
 // five conservative variables of one time level, loaded by one 5-D TMA copy.
 // The x origin of a brick is rounded down to an even node so that the copy
 // starts on a 16-byte boundary; the x extent is padded accordingly.
+//
+// Each axis has kTileVariants tile shapes (VAR); acfd_autotune times them on
+// the case and keeps the fastest.
 #pragma once
 
 namespace acfd {
 
-template <int S, bool VISC>
+constexpr int kTileVariants = 2;
+
+template <int S, bool VISC, int VAR = 0>
 struct Brick;
 
-// X sweep: 32 interfaces along x, 4 lines in y, 2 in z (256 threads)
-template <bool V>
-struct Brick<0, V> {
-    static constexpr int TX = 32, TY = 4, TZ = 2;
-    static constexpr int BX = 38, BY = V ? 6 : 4, BZ = V ? 4 : 2;
+// X sweep: VAR 0: 32 interfaces along x x 4 (y) x 2 (z); VAR 1: 64 x 2 x 2
+template <bool V, int VAR>
+struct Brick<0, V, VAR> {
+    static constexpr int TX = VAR ? 64 : 32, TY = VAR ? 2 : 4, TZ = 2;
+    static constexpr int BX = TX + 6, BY = TY + (V ? 2 : 0), BZ = TZ + (V ? 2 : 0);
     static constexpr int HX = 3, HY = V ? 1 : 0, HZ = V ? 1 : 0;  // halo before the tile origin
     static constexpr int SX = TX - 1, SY = TY, SZ = TZ;            // tile step in nodes
 };
 
-// Y sweep: 16 x-lines, 16 interfaces along y
-template <bool V>
-struct Brick<1, V> {
-    static constexpr int TX = 16, TY = 16, TZ = 1;
-    static constexpr int BX = V ? 20 : 18, BY = 21, BZ = V ? 3 : 1;
+// Y sweep: VAR 0: 16 x-lines x 16 interfaces along y; VAR 1: 32 x 8
+template <bool V, int VAR>
+struct Brick<1, V, VAR> {
+    static constexpr int TX = VAR ? 32 : 16, TY = VAR ? 8 : 16, TZ = 1;
+    static constexpr int BX = TX + (V ? 4 : 2), BY = TY + 5, BZ = V ? 3 : 1;
     static constexpr int HX = V ? 1 : 0, HY = 3, HZ = V ? 1 : 0;
     static constexpr int SX = TX, SY = TY - 1, SZ = TZ;
 };
 
-// Z sweep: 16 x-lines, 16 interfaces along z
-template <bool V>
-struct Brick<2, V> {
-    static constexpr int TX = 16, TY = 1, TZ = 16;
-    static constexpr int BX = V ? 20 : 18, BY = V ? 3 : 1, BZ = 21;
+// Z sweep: VAR 0: 16 x-lines x 16 interfaces along z; VAR 1: 32 x 8
+template <bool V, int VAR>
+struct Brick<2, V, VAR> {
+    static constexpr int TX = VAR ? 32 : 16, TY = 1, TZ = VAR ? 8 : 16;
+    static constexpr int BX = TX + (V ? 4 : 2), BY = V ? 3 : 1, BZ = TZ + 5;
     static constexpr int HX = V ? 1 : 0, HY = V ? 1 : 0, HZ = 3;
     static constexpr int SX = TX, SY = TY, SZ = TZ - 1;
 };
 
-// box extents (x, y, z) of the tensor map of sweep s
-inline void brick_box(int s, bool visc, int box[3])
+// box extents (x, y, z) of the tensor map of sweep s, tile variant var
+inline void brick_box(int s, bool visc, int var, int box[3])
 {
-#define ACFD_BOX(S_, V_)        \
-    box[0] = Brick<S_, V_>::BX; \
-    box[1] = Brick<S_, V_>::BY; \
-    box[2] = Brick<S_, V_>::BZ;
+#define ACFD_BOX(S_, V_, R_)            \
+    box[0] = Brick<S_, V_, R_>::BX;     \
+    box[1] = Brick<S_, V_, R_>::BY;     \
+    box[2] = Brick<S_, V_, R_>::BZ;
+#define ACFD_BOX_V(S_, R_)                                   \
+    if (visc) { ACFD_BOX(S_, true, R_) } else { ACFD_BOX(S_, false, R_) }
     if (s == 0) {
-        if (visc) { ACFD_BOX(0, true) } else { ACFD_BOX(0, false) }
+        if (var) { ACFD_BOX_V(0, 1) } else { ACFD_BOX_V(0, 0) }
     } else if (s == 1) {
-        if (visc) { ACFD_BOX(1, true) } else { ACFD_BOX(1, false) }
+        if (var) { ACFD_BOX_V(1, 1) } else { ACFD_BOX_V(1, 0) }
     } else {
-        if (visc) { ACFD_BOX(2, true) } else { ACFD_BOX(2, false) }
+        if (var) { ACFD_BOX_V(2, 1) } else { ACFD_BOX_V(2, 0) }
     }
+#undef ACFD_BOX_V
 #undef ACFD_BOX
 }
 

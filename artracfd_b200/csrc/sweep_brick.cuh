@@ -22,47 +22,60 @@ namespace ACFD_NS {
 constexpr long long kTmaWaitLimit = 1LL << 22;
 constexpr int kBrickThreads = 256;
 
-template <int S, bool VISC>
+template <int S, bool VISC, int VAR>
 struct BrickLayout {
-    typedef Brick<S, VISC> B;
+    typedef Brick<S, VISC, VAR> B;
     static constexpr int nodes = B::BX * B::BY * B::BZ;
     static constexpr int u_bytes = 5 * nodes * 8;
     static constexpr int p_bytes = VISC ? 4 * nodes * (int)sizeof(Real) : 0;
+    // FP32 form: a copy of the brick converted once, read by the interfaces
+    static constexpr bool conv = sizeof(Real) != sizeof(double);
+    static constexpr int r_bytes = conv ? 5 * nodes * (int)sizeof(Real) : 0;
     static constexpr int f_bytes = 5 * kBrickThreads * (int)sizeof(Real);
     static constexpr int p_off = (u_bytes + 127) / 128 * 128;
-    static constexpr int f_off = (p_off + p_bytes + 127) / 128 * 128;
-    static constexpr int bar_off = (f_off + f_bytes + 15) / 16 * 16;
+    static constexpr int r_off = (p_off + p_bytes + 127) / 128 * 128;
+    static constexpr int f_off = (r_off + r_bytes + 127) / 128 * 128;
+    // U[to] (or U[tm] when accumulating) of the nodes the block updates
+    static constexpr int o_bytes = 5 * kBrickThreads * 8;
+    static constexpr int o_off = (f_off + f_bytes + 127) / 128 * 128;
+    static constexpr int bar_off = (o_off + o_bytes + 15) / 16 * 16;
     static constexpr int total = bar_off + 16;
 };
 
-template <int S, int NP, bool VISC>
-__global__ void __launch_bounds__(kBrickThreads, 2)
-stage_brick(Grid g, ModelParams mp, StageArgs a, const __grid_constant__ CUtensorMap map)
+// One tile of interfaces (tile indices tbx, tby, tbz of the case's tiling):
+// the body shared by the per-case kernel and the persistent batched kernel.
+// The caller has initialised the block's mbarrier; `parity` is the phase this
+// tile's load completes.  Returns false when the load did not complete within
+// the wait limit (the block must then stop).
+template <int S, int NP, bool VISC, bool HYB, int VAR>
+__device__ __forceinline__ bool brick_tile(const Grid &g, const ModelParams &mp, const StageArgs &a,
+                                           const CUtensorMap *map, int tbx, int tby, int tbz, unsigned char *smem,
+                                           uint32_t parity)
 {
-    typedef Brick<S, VISC> B;
-    typedef BrickLayout<S, VISC> LY;
-    extern __shared__ __align__(128) unsigned char smem[];
+    typedef Brick<S, VISC, VAR> B;
+    typedef BrickLayout<S, VISC, VAR> LY;
     double *sU = reinterpret_cast<double *>(smem);
     Real *sP = reinterpret_cast<Real *>(smem + LY::p_off);
+    // the brick in the arithmetic type: the FP64 brick itself, or its FP32 copy
+    Real *sR = LY::conv ? reinterpret_cast<Real *>(smem + LY::r_off) : reinterpret_cast<Real *>(sU);
     Real *sF = reinterpret_cast<Real *>(smem + LY::f_off);
+    double *sO = reinterpret_cast<double *>(smem + LY::o_off);
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + LY::bar_off);
+    const bool visc_on = VISC && (mp.refMu > 0.0);
 
     const int tid = threadIdx.x + B::TX * (threadIdx.y + B::TY * threadIdx.z);
     // tile origin (first updated node) and brick origin
-    const int i0 = g.lo[0] + blockIdx.x * B::SX;
-    const int j0 = g.lo[1] + blockIdx.y * B::SY;
-    const int k0 = g.lo[2] + blockIdx.z * B::SZ;
+    const int i0 = g.lo[0] + tbx * B::SX;
+    const int j0 = g.lo[1] + tby * B::SY;
+    const int k0 = g.lo[2] + tbz * B::SZ;
     const int xs = (i0 - B::HX) & ~1;
     const int ys = j0 - B::HY;
     const int zs = k0 - B::HZ;
 
-    if (tid == 0) {
-        tma::mbar_init(bar, 1);
-    }
-    __syncthreads();
+    __syncthreads();  // every thread is done with the previous tile's shared data
     if (tid == 0) {
         tma::mbar_expect_tx(bar, LY::u_bytes);
-        tma::load_5d(sU, &map, xs, ys, zs, 0, a.tn, bar);
+        tma::load_5d(sU, map, xs, ys, zs, 0, a.tn, bar);
     }
 
     // this thread's interface: between node (i,j,k) and (i,j,k) + e_S
@@ -84,31 +97,57 @@ stage_brick(Grid g, ModelParams mp, StageArgs a, const __grid_constant__ CUtenso
         fl_left = (q >= 0) && (a.did[node] == 0);
         fl_right = (q + 1 < Ls) && (a.did[node + st] == 0);
     }
+    // everything else from global memory is read while the brick is in
+    // flight: the sensor flags of the interface's stencil (hybrid form), the
+    // step and the node-update operand U[to] (U[tm] when accumulating)
+    bool full_own = true;
+    if (HYB && NP == 6 && (fl_left || fl_right)) {
+        const uint8_t *fl = a.flags + (long long)S * g.nn;
+        full_own = (fl[node - st] | fl[node] | fl[node + st] | fl[node + 2 * st]) != 0;
+    }
+    const bool upd = fl_left && sl >= 1;  // the first interface of each line only feeds its right neighbour
+    const bool need_o = a.accumulate || (a.to != a.tn);
+    if (upd && need_o) {
+        const double *src = a.accumulate ? a.Um : a.Uo;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            sO[v * kBrickThreads + tid] = __ldcs(src + v * g.nn + node);
+        }
+    }
+    const double rdt = (a.dt_scale * a.dt[0]) * g.dd[S];
 
-    const bool ok = tma::mbar_wait_bounded(bar, 0, a.status, 4, kTmaWaitLimit);
+    const bool ok = tma::mbar_wait_bounded(bar, parity, a.status, 4, kTmaWaitLimit);
     if (!__syncthreads_and(ok)) {
         // time-out: give the copy a second bounded chance to land, then leave
         if (tid == 0) {
-            for (long long it = 0; it < kTmaWaitLimit && !tma::mbar_try_wait(bar, 0); ++it) {
+            for (long long it = 0; it < kTmaWaitLimit && !tma::mbar_try_wait(bar, parity); ++it) {
             }
         }
         __syncthreads();
-        return;
+        return false;
     }
 
     // brick index of node (x, y, z), variable v
     auto bidx = [&](int x, int y, int z) { return ((z - zs) * B::BY + (y - ys)) * B::BX + (x - xs); };
 
-    // A. primitives of every brick node (viscous cases)
-    if (VISC) {
+    // A. per brick node: the FP32 copy (FP32 form) and the primitives u, v, w,
+    // T (viscous cases)
+    if (LY::conv || visc_on) {
         const Real cvinv = Real(1.0 / mp.cv);
         for (int n = tid; n < LY::nodes; n += kBrickThreads) {
-            const Real r = Real(sU[n]);
+            Real uc[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                uc[v] = Real(sU[v * LY::nodes + n]);
+                if (LY::conv) sR[v * LY::nodes + n] = uc[v];
+            }
+            if (!visc_on) continue;
+            const Real r = uc[0];
             const Real ir = fast::rcp<Real>(r);
-            const Real u = Real(sU[LY::nodes + n]) * ir;
-            const Real v = Real(sU[2 * LY::nodes + n]) * ir;
-            const Real w = Real(sU[3 * LY::nodes + n]) * ir;
-            const Real e = Real(sU[4 * LY::nodes + n]) * ir;
+            const Real u = uc[1] * ir;
+            const Real v = uc[2] * ir;
+            const Real w = uc[3] * ir;
+            const Real e = uc[4] * ir;
             sP[n] = u;
             sP[LY::nodes + n] = v;
             sP[2 * LY::nodes + n] = w;
@@ -129,8 +168,8 @@ stage_brick(Grid g, ModelParams mp, StageArgs a, const __grid_constant__ CUtenso
         Real UL[5], UR[5], Uo[6];
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-            UL[v] = Real(sU[v * NN + c]);
-            UR[v] = Real(sU[v * NN + c + bs]);
+            UL[v] = sR[v * NN + c];
+            UR[v] = sR[v * NN + c + bs];
         }
         fast::interface_state<Real>(mp.jacobMean, gamma, UL, UR, Uo);
         const Real V[3] = {Uo[1], Uo[2], Uo[3]};
@@ -162,19 +201,55 @@ stage_brick(Grid g, ModelParams mp, StageArgs a, const __grid_constant__ CUtenso
                 }
             }
         }
+        // smooth interface (hybrid form): WENO5 with the linear weights.  The
+        // linear reconstruction commutes with the frozen projection, so the
+        // split fluxes need the projection of two reconstructed vectors only.
+        bool full = true;
+        if (HYB && NP == 6) {
+            // one path per warp: a warp with any flagged interface takes the
+            // full reconstruction for all its lanes instead of both paths
+            full = __any_sync(__activemask(), full_own);
+        }
+        Real G[5];
+        if (!full) {
+            Real up[5], um[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                const Real *P = sR + v * NN + c;
+                up[v] = fast::upwind5<Real>(P[-2 * bs], P[-bs], P[0], P[bs], P[2 * bs]);
+                um[v] = fast::upwind5<Real>(P[3 * bs], P[2 * bs], P[bs], P[0], P[-bs]);
+            }
+            Real wp[5], wm[5];
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                const Real *u = side ? um : up;
+                Real *w = side ? wm : wp;
+                const Real A = qk * u[0] - V[0] * u[1] - V[1] * u[2] - V[2] * u[3] + u[4];
+                const Real Bs = V[S] * u[0] - u[S + 1];
+                w[0] = b * A + d * Bs;
+                w[4] = b * A - d * Bs;
+#pragma unroll
+                for (int t = 0; t < 3; ++t) {
+                    w[t + 1] = (t == S) ? u[0] - b2 * A : u[t + 1] - b2 * V[t] * A;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < 5; ++r) {
+                G[r] = lp[r] * wp[r] + ln[r] * wm[r];
+            }
+        } else {
         // the two scalars of every stencil point
         Real A[NP], Bv[NP];
 #pragma unroll
         for (int m = 0; m < NP; ++m) {
             const int p = c + (first + m) * bs;
-            const Real u0 = Real(sU[p]), u1 = Real(sU[NN + p]), u2 = Real(sU[2 * NN + p]);
-            const Real u3 = Real(sU[3 * NN + p]), u4 = Real(sU[4 * NN + p]);
+            const Real u0 = sR[p], u1 = sR[NN + p], u2 = sR[2 * NN + p];
+            const Real u3 = sR[3 * NN + p], u4 = sR[4 * NN + p];
             A[m] = qk * u0 - V[0] * u1 - V[1] * u2 - V[2] * u3 + u4;
             const Real us = (S == 0) ? u1 : (S == 1 ? u2 : u3);
             Bv[m] = V[S] * u0 - us;
         }
         // field by field: W, WENO on both split fluxes
-        Real G[5];
 #pragma unroll
         for (int r = 0; r < 5; ++r) {
             Real W[NP];
@@ -186,9 +261,9 @@ stage_brick(Grid g, ModelParams mp, StageArgs a, const __grid_constant__ CUtenso
                 } else if (r == 4) {
                     W[m] = b * A[m] - d * Bv[m];
                 } else if (r == S + 1) {
-                    W[m] = Real(sU[p]) - b2 * A[m];
+                    W[m] = sR[p] - b2 * A[m];
                 } else {
-                    W[m] = Real(sU[r * NN + p]) - b2 * V[r - 1] * A[m];
+                    W[m] = sR[r * NN + p] - b2 * V[r - 1] * A[m];
                 }
             }
             Real hp, hn;
@@ -201,6 +276,7 @@ stage_brick(Grid g, ModelParams mp, StageArgs a, const __grid_constant__ CUtenso
             }
             G[r] = hp + hn;
         }
+        }  // full interface
         Real F[5];
         F[0] = G[0] + G[S + 1] + G[4];
         Real e4 = hT * (G[0] + G[4]) + V[S] * cs * (G[4] - G[0]) + (V[S] * V[S] - qk) * G[S + 1];
@@ -214,7 +290,7 @@ stage_brick(Grid g, ModelParams mp, StageArgs a, const __grid_constant__ CUtenso
             }
         }
         F[4] = e4;
-        if (VISC) {
+        if (visc_on) {
             // central viscous flux from the brick primitives
             const int pn = c + bs;
             Real grad[3][3];
@@ -262,54 +338,76 @@ stage_brick(Grid g, ModelParams mp, StageArgs a, const __grid_constant__ CUtenso
     }
     __syncthreads();
 
-    // C. node update (the first interface of each line only feeds its right neighbour)
-    if (fl_left && sl >= 1) {
+    // C. node update
+    if (upd) {
         const int lt = tid - ((S == 0) ? 1 : (S == 1 ? B::TX : B::TX * B::TY));
         const int c = bidx(i, j, k);
-        const double r = (a.dt_scale * a.dt[0]) * g.dd[S];
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
             const double phi = double(sF[v * kBrickThreads + lt]) - double(sF[v * kBrickThreads + tid]);
             const long long qv = v * g.nn + node;
             const double un = sU[v * LY::nodes + c];
             if (a.accumulate) {
-                a.Um[qv] = a.Um[qv] + a.coeB * r * phi;
+                a.Um[qv] = sO[v * kBrickThreads + tid] + a.coeB * rdt * phi;
             } else {
-                const double uo = (a.to == a.tn) ? un : a.Uo[qv];
-                a.Um[qv] = a.coeA * uo + a.coeB * (un + r * phi);
+                const double uo = need_o ? sO[v * kBrickThreads + tid] : un;
+                a.Um[qv] = a.coeA * uo + a.coeB * (un + rdt * phi);
             }
         }
     }
+    return true;
 }
 
-template <int S, int NP, bool VISC>
+// one tile per block
+template <int S, int NP, bool VISC, bool HYB, int VAR>
+__global__ void __launch_bounds__(kBrickThreads, 2)
+stage_brick(Grid g, ModelParams mp, StageArgs a, const __grid_constant__ CUtensorMap map)
+{
+    typedef BrickLayout<S, VISC, VAR> LY;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + LY::bar_off);
+    if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+        tma::mbar_init(bar, 1);
+    }
+    __syncthreads();
+    brick_tile<S, NP, VISC, HYB, VAR>(g, mp, a, &map, blockIdx.x, blockIdx.y, blockIdx.z, smem, 0);
+}
+
+template <int S, int NP, bool VISC, bool HYB, int VAR>
 static int launch_brick_one(const Grid &g, const ModelParams &m, const StageArgs &a, cudaStream_t st)
 {
-    typedef Brick<S, VISC> B;
-    typedef BrickLayout<S, VISC> LY;
+    typedef Brick<S, VISC, VAR> B;
+    typedef BrickLayout<S, VISC, VAR> LY;
     static bool configured[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !configured[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(stage_brick<S, NP, VISC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             LY::total);
+        cudaError_t e = cudaFuncSetAttribute(stage_brick<S, NP, VISC, HYB, VAR>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, LY::total);
         if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(stage_brick)");
         configured[dev] = true;
     }
     const int L0 = g.hi[0] - g.lo[0], L1 = g.hi[1] - g.lo[1], L2 = g.hi[2] - g.lo[2];
     dim3 grid((L0 + B::SX - 1) / B::SX, (L1 + B::SY - 1) / B::SY, (L2 + B::SZ - 1) / B::SZ);
     dim3 block(B::TX, B::TY, B::TZ);
-    stage_brick<S, NP, VISC><<<grid, block, LY::total, st>>>(g, m, a, a.maps[S]);
+    stage_brick<S, NP, VISC, HYB, VAR><<<grid, block, LY::total, st>>>(g, m, a, a.maps[S * kTileVariants + VAR]);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "stage_brick launch");
 }
 
-template <int NP, bool VISC>
+template <int S, int NP, bool VISC, bool HYB>
+static int launch_brick_var(const Grid &g, const ModelParams &m, const StageArgs &a, cudaStream_t st)
+{
+    if (a.var[S] == 1) return launch_brick_one<S, NP, VISC, HYB, 1>(g, m, a, st);
+    return launch_brick_one<S, NP, VISC, HYB, 0>(g, m, a, st);
+}
+
+template <int NP, bool VISC, bool HYB>
 static int launch_brick_np(const Grid &g, const ModelParams &m, const StageArgs &a, int s, cudaStream_t st)
 {
-    if (s == 0) return launch_brick_one<0, NP, VISC>(g, m, a, st);
-    if (s == 1) return launch_brick_one<1, NP, VISC>(g, m, a, st);
-    return launch_brick_one<2, NP, VISC>(g, m, a, st);
+    if (s == 0) return launch_brick_var<0, NP, VISC, HYB>(g, m, a, st);
+    if (s == 1) return launch_brick_var<1, NP, VISC, HYB>(g, m, a, st);
+    return launch_brick_var<2, NP, VISC, HYB>(g, m, a, st);
 }
 
 static int launch_brick_impl(const Grid &g, const ModelParams &m, const StageArgs &a, int s, bool viscous,
@@ -319,10 +417,130 @@ static int launch_brick_impl(const Grid &g, const ModelParams &m, const StageArg
         return ACFD_OK;
     }
     if (m.sScheme == 1) {
-        return viscous ? launch_brick_np<6, true>(g, m, a, s, st) : launch_brick_np<6, false>(g, m, a, s, st);
+        return viscous ? launch_brick_np<6, true, false>(g, m, a, s, st)
+                       : launch_brick_np<6, false, false>(g, m, a, s, st);
     }
-    return viscous ? launch_brick_np<4, true>(g, m, a, s, st) : launch_brick_np<4, false>(g, m, a, s, st);
+    return viscous ? launch_brick_np<4, true, false>(g, m, a, s, st) : launch_brick_np<4, false, false>(g, m, a, s, st);
 }
+
+#if ACFD_FORM == 2
+// ---------------------------------------------------------------------------
+// persistent stage kernel of a batch of independent cases: resident blocks
+// pull (case, tile) work items from a counter until every tile of every case
+// is done.  Viscous brick geometry for all cases (inviscid ones skip the
+// viscous part at run time).
+// ---------------------------------------------------------------------------
+template <int S, bool HYB>
+__global__ void __launch_bounds__(kBrickThreads, 2)
+stage_batch(const BatchCase *cases, const CUtensorMap *maps, const long long *prefix, int ncase, StageCoefs sc,
+            const double *dts, unsigned long long *counter, int *status)
+{
+    typedef BrickLayout<S, true, 0> LY;
+    typedef Brick<S, true, 0> B;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + LY::bar_off);
+    __shared__ long long item_s;
+    const int tid = threadIdx.x + B::TX * (threadIdx.y + B::TY * threadIdx.z);
+    if (tid == 0) {
+        tma::mbar_init(bar, 1);
+    }
+    __syncthreads();
+    const long long total = prefix[ncase];
+    uint32_t parity = 0;
+    for (;;) {
+        if (tid == 0) {
+            item_s = (long long)atomicAdd(counter, 1ULL);
+        }
+        __syncthreads();
+        const long long item = item_s;
+        if (item >= total) {
+            break;
+        }
+        int lo = 0, hi = ncase - 1;  // the case whose tiles contain item
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (prefix[mid] <= item) lo = mid; else hi = mid - 1;
+        }
+        const BatchCase &C = cases[lo];
+        const long long t = item - prefix[lo];
+        const int nx = C.tiles[S][0], ny = C.tiles[S][1];
+        const int tx = (int)(t % nx);
+        const int ty = (int)((t / nx) % ny);
+        const int tz = (int)(t / ((long long)nx * ny));
+        StageArgs a;
+        const long long lv = 5LL * C.g.nn;
+        a.Uo = C.U + sc.to * lv;
+        a.Un = C.U + sc.tn * lv;
+        a.Um = C.U + sc.tm * lv;
+        a.did = C.did;
+        a.dt = dts + lo;
+        a.dt_scale = sc.dt_scale;
+        a.coeA = sc.coeA;
+        a.coeB = sc.coeB;
+        a.accumulate = 0;
+        a.to = sc.to;
+        a.tn = sc.tn;
+        a.maps = nullptr;
+        a.var[0] = a.var[1] = a.var[2] = 0;
+        a.status = status;
+        a.flags = C.flags;
+        if (!brick_tile<S, 6, true, HYB, 0>(C.g, C.mp, a, maps + 3 * lo + S, tx, ty, tz, smem, parity)) {
+            break;
+        }
+        parity ^= 1u;
+    }
+}
+
+template <int S, bool HYB>
+static int launch_batch_one(const BatchCase *cases, const CUtensorMap *maps, const long long *prefix, int ncase,
+                            const StageCoefs &sc, const double *dts, unsigned long long *counter, int *status,
+                            int blocks, cudaStream_t st)
+{
+    typedef Brick<S, true, 0> B;
+    typedef BrickLayout<S, true, 0> LY;
+    static bool configured[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(stage_batch<S, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             LY::total);
+        if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(stage_batch)");
+        configured[dev] = true;
+    }
+    stage_batch<S, HYB><<<blocks, dim3(B::TX, B::TY, B::TZ), LY::total, st>>>(cases, maps, prefix, ncase, sc, dts,
+                                                                            counter, status);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "stage_batch launch");
+}
+
+static int launch_batch_impl(const BatchCase *cases, const CUtensorMap *maps, const long long *prefix, int ncase,
+                             const StageCoefs &sc, const double *dts, unsigned long long *counter, int *status,
+                             int blocks, int s, bool hybrid, cudaStream_t st)
+{
+    if (hybrid) {
+        if (s == 0) return launch_batch_one<0, true>(cases, maps, prefix, ncase, sc, dts, counter, status, blocks, st);
+        if (s == 1) return launch_batch_one<1, true>(cases, maps, prefix, ncase, sc, dts, counter, status, blocks, st);
+        return launch_batch_one<2, true>(cases, maps, prefix, ncase, sc, dts, counter, status, blocks, st);
+    }
+    if (s == 0) return launch_batch_one<0, false>(cases, maps, prefix, ncase, sc, dts, counter, status, blocks, st);
+    if (s == 1) return launch_batch_one<1, false>(cases, maps, prefix, ncase, sc, dts, counter, status, blocks, st);
+    return launch_batch_one<2, false>(cases, maps, prefix, ncase, sc, dts, counter, status, blocks, st);
+}
+
+// hybrid form (WENO5 only): interfaces the sensor did not flag use the
+// linear-weight limit
+static int launch_brick_hybrid_impl(const Grid &g, const ModelParams &m, const StageArgs &a, int s, bool viscous,
+                                    cudaStream_t st)
+{
+    if (g.hi[0] <= g.lo[0] || g.hi[1] <= g.lo[1] || g.hi[2] <= g.lo[2]) {
+        return ACFD_OK;
+    }
+    if (m.sScheme != 1 || !a.flags) {
+        return launch_brick_impl(g, m, a, s, viscous, st);
+    }
+    return viscous ? launch_brick_np<6, true, true>(g, m, a, s, st) : launch_brick_np<6, false, true>(g, m, a, s, st);
+}
+#endif
 
 }  // namespace ACFD_NS
 }  // namespace acfd

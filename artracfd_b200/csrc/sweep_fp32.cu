@@ -35,3 +35,24 @@ int launch_stage_brick_fp32(const Grid &g, const ModelParams &m, const StageArgs
 }
 
 }  // namespace acfd
+
+namespace acfd {
+
+int launch_stage_brick_hybrid(const Grid &g, const ModelParams &m, const StageArgs &a, int s, bool viscous,
+                              cudaStream_t st)
+{
+    return form_fp32::launch_brick_hybrid_impl(g, m, a, s, viscous, st);
+}
+
+}  // namespace acfd
+
+namespace acfd {
+
+int launch_stage_batch(const BatchCase *cases, const CUtensorMap *maps, const long long *prefix, int ncase,
+                       const StageCoefs &sc, const double *dts, unsigned long long *counter, int *status, int blocks,
+                       int s, bool hybrid, cudaStream_t st)
+{
+    return form_fp32::launch_batch_impl(cases, maps, prefix, ncase, sc, dts, counter, status, blocks, s, hybrid, st);
+}
+
+}  // namespace acfd

@@ -54,6 +54,27 @@ class Solver:
     def set_stream(self, stream_ptr: int | None):
         check(self.lib.acfd_set_stream(self.h, ctypes.c_void_p(stream_ptr) if stream_ptr else None), self.lib)
 
+    def autotune(self):
+        """Pick the fastest compiled tile shape per sweep axis on this case
+        (acfd_autotune); returns the chosen variant per axis."""
+        t = (ctypes.c_int * 3)()
+        check(self.lib.acfd_autotune(self.h, t), self.lib)
+        return list(t)
+
+    # learned sensor -------------------------------------------------------
+    def sensor_load(self, params: np.ndarray, threshold: float):
+        """Trained sensor parameters and the probability threshold above which
+        a node keeps the full WENO5 reconstruction (acfd_sensor_load)."""
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        check(self.lib.acfd_sensor_load(self.h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(threshold)),
+              self.lib)
+
+    def sensor_update(self) -> int:
+        """Evaluate the sensor on U[TO]; returns the number of flags set."""
+        n = ctypes.c_ulonglong()
+        check(self.lib.acfd_sensor_update(self.h, ctypes.byref(n)), self.lib)
+        return n.value
+
     def launches(self) -> int:
         """Kernels launched by this case so far (graph replays included)."""
         n = ctypes.c_longlong()

@@ -182,35 +182,29 @@ def cpu_baseline_reference(n: int, steps: int = 1, procs: int = 1):
     return rate, {"seconds_per_step": per_step, "procs": len(times), "steps": steps}
 
 
-def run_ours(args, rank, world, local_rank):
-    import numpy as np
-    import torch
+FORMS = {"fp64": "FP64", "fp64_exact": "FP64_EXACT", "fp32": "FP32_BULK", "hybrid": "FP64"}
+DTYPES = {"fp64": "f64", "fp64_exact": "f64", "fp32": "f32/f64", "hybrid": "f32/f64"}
 
-    from artracfd_b200 import abi, configs
+
+def _solver(part, model, form, stream):
+    from artracfd_b200 import abi
     from artracfd_b200.solver import Solver
-
-    torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist  # noqa: F811
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    spec = configs.tgv(n=args.n)
-    part, model = spec.descriptors()
-    nodes_pin = (args.n + 1) ** 3
-    node = spec.initial_nodes(part, model)
-    mode = {"fp64": abi.FP64, "fp64_exact": abi.FP64_EXACT, "fp32": abi.FP32_BULK}[args.mode]
-    stream = torch.cuda.Stream()
-    s = Solver(part, model, mode)
+    s = Solver(part, model, getattr(abi, FORMS[form]))
     s.set_stream(stream.cuda_stream)
-    s.upload(node)
-    s.treat_boundary(abi.TO)
+    if form == "hybrid":
+        from artracfd_b200 import sensor as sensor_mod
+        sensor_mod.attach(s)
+    return s
 
+
+def _timed_steps(torch, s, spec, steps, warmup, dist, stream, clock_index):
+    """W untimed steps, then K steps between CUDA events on the solver's
+    stream (barrier + synchronize on both sides); seconds (max over ranks),
+    kernel launches and the clocks sampled meanwhile."""
     def step():
-        dt = s.time_step(spec.cfl)
-        s.evolve(dt, graph=True)
-        return dt
+        s.evolve(s.time_step(spec.cfl), graph=True)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
     if dist:
@@ -219,30 +213,35 @@ def run_ours(args, rank, world, local_rank):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     launches0 = s.launches()
-    with ClockSampler(local_rank) as clk:
+    with ClockSampler(clock_index) as clk:
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             step()
         e1.record(stream)
         e1.synchronize()
     torch.cuda.synchronize()
-    gpu_launches = s.launches() - launches0
     sec = e0.elapsed_time(e1) / 1e3
     if dist:
         t = torch.tensor([sec], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         sec = float(t.item())
         dist.barrier()
-    value = world * nodes_pin * args.steps / sec / 1e6
-    # per-stage launch timing of the dominant kernel (the stage sweep) on the
-    # solver's stream: one eager step, events around each LLLU stage
-    stage_ms = []
-    bc_ms = []
+    return sec, s.launches() - launches0, clk.summary()
+
+
+def _stage_profile(torch, s, spec, nodes_pin, stream):
+    """One eager step with events around each LLLU stage and each ghost fill
+    on the solver's stream: mean stage and fill times (ms), and the
+    algorithmic bytes per stage launch."""
+    from artracfd_b200 import abi
+    stage_ms, bc_ms = [], []
     dt = s.time_step(spec.cfl)
     order = [2, 1, 0, 0, 1, 2]
     coefs = [(0.0, 1.0, abi.TO, abi.TO, abi.TN), (0.75, 0.25, abi.TO, abi.TN, abi.TM),
              (1.0 / 3.0, 2.0 / 3.0, abi.TO, abi.TM, abi.TO)]
     stage_bytes = 0.0
+    if s.mode == abi.FP32_HYBRID:
+        s.sensor_update()
     with torch.cuda.stream(stream):
         for sd in order:
             for q, (a, b, to, tn, tm) in enumerate(coefs):
@@ -256,10 +255,103 @@ def run_ours(args, rank, world, local_rank):
                 stage_ms.append(ev[0].elapsed_time(ev[1]))
                 bc_ms.append(ev[1].elapsed_time(ev[2]))
                 stage_bytes += STAGE_BYTES[q] * nodes_pin
+    return sum(stage_ms) / len(stage_ms), sum(bc_ms) / len(bc_ms), stage_bytes / len(stage_ms)
+
+
+def _pin_mask(part):
+    import numpy as np
+    n = [int(x) for x in part.n]
+    ns = np.array(part.ns)[0]
+    m = np.zeros((n[2], n[1], n[0]), dtype=bool)
+    m[ns[2, 0]:ns[2, 1], ns[1, 0]:ns[1, 1], ns[0, 0]:ns[0, 1]] = True
+    return m.ravel()
+
+
+def _accuracy(part, model, node, spec, form, steps, stream):
+    """The form against the plain FP64 path on the same initial state and
+    the same dt sequence: relative L1 and Linf errors of density, pressure
+    and momentum over the computed nodes after `steps` steps."""
+    import numpy as np
+    from artracfd_b200 import abi
+    ref = _solver(part, model, "fp64", stream)
+    ref.upload(node)
+    ref.treat_boundary(abi.TO)
+    dts = []
+    for _ in range(steps):
+        dt = ref.time_step(spec.cfl)
+        ref.evolve(dt, graph=True)
+        dts.append(dt)
+    a = ref.download()["U"][:, 0, :].copy()
+    ref.close()
+    s = _solver(part, model, form, stream)
+    s.upload(node)
+    s.treat_boundary(abi.TO)
+    for dt in dts:
+        s.evolve(dt, graph=True)
+    b = s.download()["U"][:, 0, :].copy()
+    s.close()
+    pin = _pin_mask(part)
+    a, b = a[pin], b[pin]
+    gm1 = model.gamma - 1.0
+
+    def pres(u):
+        return gm1 * (u[:, 4] - 0.5 * (u[:, 1] ** 2 + u[:, 2] ** 2 + u[:, 3] ** 2) / u[:, 0])
+
+    out = {"steps": steps, "against": "plain FP64 path (fast form), same initial state and dt sequence"}
+    for name, fa, fb in (("rho", a[:, 0], b[:, 0]), ("p", pres(a), pres(b)), ("mom", a[:, 1:4], b[:, 1:4])):
+        d = np.abs(fb - fa)
+        out["l1_" + name] = float(d.sum() / np.abs(fa).sum()) if np.isfinite(d).all() else float("inf")
+        out["linf_" + name] = float(d.max() / np.abs(fa).max()) if np.isfinite(d).all() else float("inf")
+    return out
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from artracfd_b200 import abi, configs
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    spec = configs.tgv(n=args.n)
+    part, model = spec.descriptors()
+    nodes_pin = (args.n + 1) ** 3
+    node = spec.initial_nodes(part, model)
+    stream = torch.cuda.Stream()
     hbm_peak, peak_kind = load_peaks()
-    mean_stage = sum(stage_ms) / len(stage_ms) / 1e3
-    achieved = stage_bytes / len(stage_ms) / mean_stage / 1e9
-    flop_rate = FLOP_PER_NODE_STAGE_VISCOUS * nodes_pin / mean_stage / 1e12
+
+    # the plain FP64 path, timed first (the comparison of the headline)
+    plain = None
+    if args.mode != "fp64":
+        s = _solver(part, model, "fp64", stream)
+        s.upload(node)
+        s.treat_boundary(abi.TO)
+        tiles64 = s.autotune()
+        sec64, _, clk64 = _timed_steps(torch, s, spec, args.steps, args.warmup, dist, stream, local_rank)
+        st64, bc64, by64 = _stage_profile(torch, s, spec, nodes_pin, stream)
+        s.close()
+        plain = {"value": world * nodes_pin * args.steps / sec64 / 1e6, "ms_per_step": sec64 / args.steps * 1e3,
+                 "stage_ms": {"sweep_mean": st64, "ghost_fill_mean": bc64},
+                 "hbm_frac": by64 / (st64 / 1e3) / 1e9 / hbm_peak, "tiles": tiles64, "clocks": clk64}
+
+    # the form named by --mode (default: the learned-sensor hybrid)
+    s = _solver(part, model, args.mode, stream)
+    s.upload(node)
+    s.treat_boundary(abi.TO)
+    tiles = s.autotune()
+    sensor_info = None
+    if args.mode == "hybrid":
+        flagged = s.sensor_update()
+        sensor_info = {"flagged_fraction_at_start": flagged / (3.0 * nodes_pin)}
+    sec, gpu_launches, clocks = _timed_steps(torch, s, spec, args.steps, args.warmup, dist, stream, local_rank)
+    value = world * nodes_pin * args.steps / sec / 1e6
+    if args.mode == "hybrid":
+        sensor_info["flagged_fraction_after_timed_steps"] = s.sensor_update() / (3.0 * nodes_pin)
+    stage_mean, bc_mean, bytes_per_stage = _stage_profile(torch, s, spec, nodes_pin, stream)
+    achieved = bytes_per_stage / (stage_mean / 1e3) / 1e9
+    flop_rate = FLOP_PER_NODE_STAGE_VISCOUS * nodes_pin / (stage_mean / 1e3) / 1e12
     fp64_peak = fp64_peak_tflops(torch) if rank == 0 else None
     # e2e through the C ABI with host buffers: upload of the host node array,
     # K steps (CFL read back each step), download of the result
@@ -269,7 +361,7 @@ def run_ours(args, rank, world, local_rank):
     s.upload(host)
     s.treat_boundary(abi.TO)
     for _ in range(args.steps):
-        step()
+        s.evolve(s.time_step(spec.cfl), graph=True)
     s.download(host)
     e2e_sec = time.perf_counter() - t0
     if dist:
@@ -278,6 +370,9 @@ def run_ours(args, rank, world, local_rank):
         e2e_sec = float(t.item())
     node_bytes = host.nbytes
     s.close()
+    accuracy = None
+    if args.mode in ("fp32", "hybrid") and args.accuracy_steps > 0:
+        accuracy = _accuracy(part, model, node, spec, args.mode, args.accuracy_steps, stream)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -294,29 +389,35 @@ def run_ours(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": {"fp64": "f64", "fp64_exact": "f64", "fp32": "f32/f64"}[args.mode],
+        "scaling": "weak", "vs_baseline": None, "dtype": DTYPES[args.mode],
         "data": "synthetic (analytic TGV initial field)",
         "config": {"workload": WORKLOAD, "form": args.mode, "nodes_per_gpu": nodes_pin,
                    "l2": "state 295 MB > 126 MB L2, no flush", "parallelism": f"replicas x{world}"},
+        "plain_fp64": plain,
+        "speedup_vs_plain_fp64": (value / plain["value"]) if plain else None,
+        "accuracy": accuracy,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": profiled_traffic(args.mode),
                      "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum per stage launch "
                                      "(profiles/), algorithmic bytes per launch = "
-                                     f"{stage_bytes / len(stage_ms):.4g}",
+                                     f"{bytes_per_stage:.4g}",
                      "kernel": "stage sweep (LLLU), mean over the 18 stages of one step",
                      "peak_kind": peak_kind,
                      "fp64": {"achieved_tflops": flop_rate, "peak_tflops": fp64_peak,
                               "frac": (flop_rate / fp64_peak) if fp64_peak else None,
                               "peak_kind": "measured cuBLAS DGEMM 8192^3 in this run",
-                              "flop_per_node_stage": FLOP_PER_NODE_STAGE_VISCOUS}},
-        "stage_ms": {"sweep_mean": sum(stage_ms) / len(stage_ms), "ghost_fill_mean": sum(bc_ms) / len(bc_ms)},
-        "clocks": clk.summary(),
+                              "flop_per_node_stage": FLOP_PER_NODE_STAGE_VISCOUS,
+                              "note": "reference FP64 flop count; meaningful as a fraction for the FP64 forms"}},
+        "stage_ms": {"sweep_mean": stage_mean, "ghost_fill_mean": bc_mean},
+        "clocks": clocks,
         "e2e": {"value": world * nodes_pin * args.steps / e2e_sec / 1e6, "unit": UNIT,
                 "h2d_bytes_per_step": (node_bytes + 8 * args.steps) / args.steps,
                 "d2h_bytes_per_step": (node_bytes + 24 * args.steps) / args.steps,
                 "what": "C-ABI loop with host node arrays: acfd_sync_to_device, K x (acfd_cfl + host dt + "
                         "acfd_evolve_fluid_graph), acfd_sync_to_host; wall clock"},
         "gpu_launches": gpu_launches,
+        "tiles": tiles,
+        "sensor": sensor_info,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
@@ -354,7 +455,8 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--mode", default="fp64", choices=["fp64", "fp64_exact", "fp32"])
+    ap.add_argument("--mode", default="hybrid", choices=["fp64", "fp64_exact", "fp32", "hybrid"])
+    ap.add_argument("--accuracy-steps", type=int, default=200)
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-procs", type=int, default=16)

@@ -160,6 +160,11 @@ int acfd_set_precision(acfd_case_t *cs, int mode);
 /* Wait for all work queued on the case and report device-side errors (the
  * per-step wall clock of solve.c:81,89 needs a finished step). */
 int acfd_synchronize(acfd_case_t *cs);
+/* Tile autotuner (no reference counterpart): times the compiled tile shapes
+ * of the stage kernel of each sweep axis on this case's current state (RK
+ * stage 1, which writes only U[TN]) and keeps the fastest; tiles[3]
+ * (optional) receives the chosen variant per axis. */
+int acfd_autotune(acfd_case_t *cs, int tiles[3]);
 /* Number of kernels this case has launched so far (graph replays count their
  * kernel nodes).  No reference counterpart: instrumentation (the reference
  * only times whole steps, timer.c:22-35). */
@@ -225,6 +230,36 @@ int acfd_geo_upload(acfd_case_t *cs, const acfd_polyhedron_t *poly, int totN);
 int acfd_compute_geometric_field(acfd_case_t *cs);
 /* TreatImmersedBoundary (immersed_boundary.c:270-340) on level tn. */
 int acfd_treat_ib(acfd_case_t *cs, int tn);
+
+/* ---- learned smoothness sensor (no counterpart in the reference) ------- */
+
+/* Number of float parameters of the sensor MLP (10 -> 32 -> 32 -> 1):
+ * W1[32][10], b1[32], W2[32][32], b2[32], w3[32], b3. */
+int acfd_mlp_param_count(void);
+/* Load trained parameters (host array) into the case and set the probability
+ * threshold above which a node keeps the full WENO5 reconstruction; enables
+ * acfd_set_precision(ACFD_FP32_HYBRID). */
+int acfd_sensor_load(acfd_case_t *cs, const float *params, float threshold);
+/* Evaluate the sensor on U[TO] for the three sweep axes (the hybrid step does
+ * this itself at its start); *flagged (optional) = number of flags set. */
+int acfd_sensor_update(acfd_case_t *cs, unsigned long long *flagged);
+/* Device pointer to the flags of the last evaluation: 3 planes (sweep axis
+ * x, y, z) of uint8 in the node layout of acfd_device_state; 1 = full WENO5. */
+int acfd_sensor_flags(acfd_case_t *cs, const unsigned char **flags);
+/* Training data along axis s for every PIN node, in PIN order (x fastest):
+ * features (device, count x 10) and the WENO5 weight departure of the
+ * node's two interfaces (device, count; -1 for non-fluid nodes). */
+int acfd_sensor_features(acfd_case_t *cs, int s, float *features, float *departure);
+/* MLP on device arrays: probabilities of n samples. */
+int acfd_mlp_forward(const float *params, const float *X, int n, float *prob, void *stream);
+/* Sum over n samples of the weighted binary cross-entropy (weight pos_weight
+ * for label 1) and of its gradient; *grad (param_count) and *loss are
+ * accumulated, the caller zeroes them. */
+int acfd_mlp_grad(const float *params, const float *X, const float *Y, int n, float pos_weight, float *grad,
+        float *loss, void *stream);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on grad * scale. */
+int acfd_mlp_adam(float *params, const float *grad, float *m, float *v, int step, float lr, float scale,
+        void *stream);
 
 /* ---- per-point device twins (batched; host arrays in and out) --------- */
 
