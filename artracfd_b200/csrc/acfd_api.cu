@@ -57,8 +57,18 @@ int ib_treat(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partit
              int *flags, int tn, cudaStream_t st);
 int ib_check(IbState *ib, cudaStream_t st);
 
+bool pdl_enabled()
+{
+    static const bool on = [] {
+        const char *e = getenv("ACFD_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 __global__ void set_scalar(double *p, double v)
 {
+    pdl_wait();
     *p = v;
 }
 
@@ -260,7 +270,9 @@ int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int 
     a.accumulate = 0;
     a.to = to;
     a.tn = tn;
+    a.tm = tm;
     a.maps = cs->maps;
+    a.omaps = nullptr;
     a.status = cs->dstatus;
     a.flags = cs->sensor_flags;
     for (int s = 0; s < 3; ++s) {
@@ -384,9 +396,8 @@ int evolve(acfd_case *cs)
 
 int set_dt(acfd_case *cs, double dt)
 {
-    set_scalar<<<1, 1, 0, cs->stream>>>(cs->d_dt, dt);
+    cudaError_t e = launch_k(set_scalar, dim3(1), dim3(1), 0, cs->stream, cs->d_dt, dt);
     ++cs->launches;
-    cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "set_scalar launch");
 }
 

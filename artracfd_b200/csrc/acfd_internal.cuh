@@ -13,6 +13,7 @@
 #include <stdint.h>
 
 #include "acfd.h"
+#include "launch.cuh"
 
 namespace acfd {
 
@@ -45,8 +46,9 @@ struct StageArgs {
     double dt_scale;      // this sweep uses dt_scale * (*dt) (0.5 for Strang halves)
     double coeA, coeB;
     int accumulate;       // operator-by-operator Y/Z: Um += coeB*r*Phi
-    int to, tn;           // level indices (the brick kernels address U through a tensor map)
+    int to, tn, tm;       // level indices (the brick kernels address U through a tensor map)
     const CUtensorMap *maps;  // host array: TMA map of the whole state per (sweep axis, tile variant)
+    const CUtensorMap *omaps; // host array: node-update box maps of the persistent FP32 kernel (or null)
     int var[3];               // tile variant of each sweep axis (brick_geometry.cuh)
     int *status;          // device error word of the case
     const uint8_t *flags; // hybrid form: sensor flags [3][node] (1 = full WENO5)
@@ -73,7 +75,8 @@ int launch_stage_batch(const BatchCase *cases, const CUtensorMap *maps, const lo
                        int s, bool hybrid, cudaStream_t st);
 
 // learned sensor (sensor.cu)
-// rho_p: scratch of nn float2 (density and pressure of every node)
+// Flags of the PIN nodes (the caller sets the others to 1 once); rho_p:
+// scratch of nn float2 (density and pressure of every node)
 int launch_sensor_flags(const Grid &g, const ModelParams &m, const double *U, const int *did, const float *params,
                         float logit_threshold, float2 *rho_p, uint8_t *flags, unsigned long long *count,
                         cudaStream_t st);

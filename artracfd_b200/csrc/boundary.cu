@@ -78,6 +78,7 @@ __device__ void fill_node(const Grid &g, const ModelParams &mp, const FaceJob &J
 
 __global__ void domain_fill(Grid g, ModelParams mp, FaceJobs jobs, double *U)
 {
+    pdl_wait();
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     int q = 0;
     if (t >= jobs.job[0].count) {
@@ -234,6 +235,7 @@ __device__ __forceinline__ double vmax_of(double a, double b)
 
 __global__ void cfl_partial(Grid g, ModelParams mp, const double *U, const int *did, double *part)
 {
+    pdl_wait();
     const int Lx = g.hi[0] - g.lo[0], Ly = g.hi[1] - g.lo[1], Lz = g.hi[2] - g.lo[2];
     const long long total = (long long)Lx * Ly * Lz;
     double m0 = 0.0, m1 = 0.0, m2 = 0.0;
@@ -280,6 +282,7 @@ __global__ void cfl_partial(Grid g, ModelParams mp, const double *U, const int *
 
 __global__ void cfl_final(const double *part, int nblocks, double *out)
 {
+    pdl_wait();
     const int s = threadIdx.x;
     if (s < 3) {
         double m = 0.0;
@@ -293,6 +296,7 @@ __global__ void cfl_final(const double *part, int nblocks, double *out)
 // gravity source stage: LLLU with p = PHI (fluid_dynamics.c:177-214)
 __global__ void stage_phi(Grid g, ModelParams mp, StageArgs a)
 {
+    pdl_wait();
     const int Lx = g.hi[0] - g.lo[0], Ly = g.hi[1] - g.lo[1], Lz = g.hi[2] - g.lo[2];
     const long long total = (long long)Lx * Ly * Lz;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -427,8 +431,7 @@ int launch_domain_boundary(const Grid &g, const ModelParams &m, const acfd_parti
     if (total == 0) {
         return ACFD_OK;
     }
-    domain_fill<<<blocks_for(total, 256), 256, 0, st>>>(g, m, jobs, U);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_k(domain_fill, dim3(blocks_for(total, 256)), dim3(256), 0, st, g, m, jobs, U);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "domain_fill launch");
 }
 
@@ -521,9 +524,8 @@ int launch_domain_boundary_fused(const Grid &g, const ModelParams &m, const acfd
 int launch_cfl(const Grid &g, const ModelParams &m, const double *U, const int *did, double *partials,
                double *out, cudaStream_t st)
 {
-    cfl_partial<<<kCflBlocks, 256, 0, st>>>(g, m, U, did, partials);
-    cfl_final<<<1, 32, 0, st>>>(partials, kCflBlocks, out);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_k(cfl_partial, dim3(kCflBlocks), dim3(256), 0, st, g, m, U, did, partials);
+    if (e == cudaSuccess) e = launch_k(cfl_final, dim3(1), dim3(32), 0, st, (const double *)partials, (int)kCflBlocks, out);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "cfl launch");
 }
 
@@ -533,8 +535,7 @@ int launch_stage_phi(const Grid &g, const ModelParams &m, const StageArgs &a, cu
     if (total <= 0) {
         return ACFD_OK;
     }
-    stage_phi<<<blocks_for(total, 256), 256, 0, st>>>(g, m, a);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_k(stage_phi, dim3(blocks_for(total, 256)), dim3(256), 0, st, g, m, a);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "stage_phi launch");
 }
 

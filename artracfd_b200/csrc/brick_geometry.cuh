@@ -49,6 +49,42 @@ struct Brick<2, V, VAR> {
     static constexpr int SX = TX, SY = TY, SZ = TZ - 1;
 };
 
+// Node-update box of a tile (persistent FP32 stage kernel): the nodes the
+// tile updates, with x from the even node at or below the first one, read by
+// one TMA copy of U[to] (or U[tm]); the x extent is even (16-byte rule).
+template <int S, int VAR>
+struct OBox;
+template <int VAR>
+struct OBox<0, VAR> {
+    static constexpr int OX = Brick<0, false, VAR>::TX, OY = Brick<0, false, VAR>::TY, OZ = Brick<0, false, VAR>::TZ;
+};
+template <int VAR>
+struct OBox<1, VAR> {
+    static constexpr int OX = Brick<1, false, VAR>::TX + 2, OY = Brick<1, false, VAR>::TY - 1,
+                         OZ = Brick<1, false, VAR>::TZ;
+};
+template <int VAR>
+struct OBox<2, VAR> {
+    static constexpr int OX = Brick<2, false, VAR>::TX + 2, OY = Brick<2, false, VAR>::TY,
+                         OZ = Brick<2, false, VAR>::TZ - 1;
+};
+
+inline void update_box(int s, int var, int box[3])
+{
+#define ACFD_OBOX(S_, R_)           \
+    box[0] = OBox<S_, R_>::OX;      \
+    box[1] = OBox<S_, R_>::OY;      \
+    box[2] = OBox<S_, R_>::OZ;
+    if (s == 0) {
+        if (var) { ACFD_OBOX(0, 1) } else { ACFD_OBOX(0, 0) }
+    } else if (s == 1) {
+        if (var) { ACFD_OBOX(1, 1) } else { ACFD_OBOX(1, 0) }
+    } else {
+        if (var) { ACFD_OBOX(2, 1) } else { ACFD_OBOX(2, 0) }
+    }
+#undef ACFD_OBOX
+}
+
 // box extents (x, y, z) of the tensor map of sweep s, tile variant var
 inline void brick_box(int s, bool visc, int var, int box[3])
 {

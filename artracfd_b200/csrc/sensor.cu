@@ -302,6 +302,7 @@ __global__ void mlp_adam_kernel(float *params, const float *grad, float *m, floa
 // pass 1: density and pressure of every node, as float2
 __global__ void rho_p_kernel(long long nn, double gm1, const double *U, float2 *rp)
 {
+    pdl_wait();
     const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= nn) return;
     const double r = U[id];
@@ -336,11 +337,12 @@ constexpr int kFlagWarps = 8;
 // quad shuffles.  Layer-1 accumulators are reused as layer-2 A fragments.
 // Flags: flags[s][node] = 1 where the network's logit exceeds the threshold
 // or the node is not a fluid node, 0 elsewhere; nodes outside PIN keep the 1
-// written by the caller's fill.  count (optional) accumulates the flags set.
+// written when the sensor was loaded.  count (optional) accumulates the flags set.
 __global__ void __launch_bounds__(kFlagWarps * 32) flags_mma_kernel(Grid g, const float2 *rp, const int *did,
                                                                     const float *params, float logit_threshold,
                                                                     uint8_t *flags, unsigned long long *count)
 {
+    pdl_wait();
     // one 32 x 16 f16 feature tile per warp, rows padded to 12 words so that
     // the fragment loads (8 rows x 4 words) hit 32 distinct banks
     constexpr int kRow = 12;
@@ -483,15 +485,13 @@ int launch_sensor_flags(const Grid &g, const ModelParams &m, const double *U, co
                         cudaStream_t st)
 {
     const long long pin = (long long)(g.hi[0] - g.lo[0]) * (g.hi[1] - g.lo[1]) * (g.hi[2] - g.lo[2]);
-    ACFD_CUDA(cudaMemsetAsync(flags, 1, (size_t)3 * g.nn, st));
     if (pin <= 0) return ACFD_OK;
-    sensor::rho_p_kernel<<<(unsigned)((g.nn + 255) / 256), 256, 0, st>>>(g.nn, m.gamma - 1.0, U, rho_p);
-    ACFD_CUDA(cudaGetLastError());
+    ACFD_CUDA(launch_k(sensor::rho_p_kernel, dim3((unsigned)((g.nn + 255) / 256)), dim3(256), 0, st, g.nn,
+                       m.gamma - 1.0, U, rho_p));
     const long long groups = ((pin + 31) / 32) * 3;
     const long long blocks = std::min<long long>((groups + sensor::kFlagWarps - 1) / sensor::kFlagWarps, 148LL * 8);
-    sensor::flags_mma_kernel<<<(unsigned)blocks, sensor::kFlagWarps * 32, 0, st>>>(g, rho_p, did, params,
-                                                                                    logit_threshold, flags, count);
-    ACFD_CUDA(cudaGetLastError());
+    ACFD_CUDA(launch_k(sensor::flags_mma_kernel, dim3((unsigned)blocks), dim3(sensor::kFlagWarps * 32), 0, st, g,
+                       (const float2 *)rho_p, did, params, logit_threshold, flags, count));
     return ACFD_OK;
 }
 

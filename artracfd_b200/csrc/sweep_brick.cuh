@@ -38,9 +38,207 @@ struct BrickLayout {
     // U[to] (or U[tm] when accumulating) of the nodes the block updates
     static constexpr int o_bytes = 5 * kBrickThreads * 8;
     static constexpr int o_off = (f_off + f_bytes + 127) / 128 * 128;
-    static constexpr int bar_off = (o_off + o_bytes + 15) / 16 * 16;
+    // hybrid form: queue of the interfaces reconstructed with full WENO5
+    static constexpr int q_off = o_off + o_bytes;
+    static constexpr int q_bytes = (kBrickThreads + 4) * 4;
+    static constexpr int bar_off = (q_off + q_bytes + 15) / 16 * 16;
     static constexpr int total = bar_off + 16;
 };
+
+// Roe (or arithmetic) state of an interface and the factors of its
+// characteristic projection and flux splitting.
+template <typename Real>
+struct IfaceState {
+    Real V[3], hT, cs, qk, d, b, b2;
+    Real lp[5], ln[5];  // split eigenvalues
+};
+
+// interface between brick nodes c and c + bs (sR: the brick, NN nodes per variable)
+template <int S, int NN>
+__device__ __forceinline__ IfaceState<Real> iface_state(const ModelParams &mp, const Real *sR, int c, int bs)
+{
+    IfaceState<Real> is;
+    const Real gamma = Real(mp.gamma);
+    Real UL[5], UR[5], Uo[6];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        UL[v] = sR[v * NN + c];
+        UR[v] = sR[v * NN + c + bs];
+    }
+    fast::interface_state<Real>(mp.jacobMean, gamma, UL, UR, Uo);
+    is.V[0] = Uo[1];
+    is.V[1] = Uo[2];
+    is.V[2] = Uo[3];
+    is.hT = Uo[4];
+    is.cs = Uo[5];
+    is.qk = Real(0.5) * (is.V[0] * is.V[0] + is.V[1] * is.V[1] + is.V[2] * is.V[2]);
+    is.d = fast::rcp<Real>(Real(2) * is.cs);
+    is.b = (gamma - Real(1)) * (Real(2) * is.d * is.d);
+    is.b2 = Real(2) * is.b;
+    Real lam[5];
+    lam[0] = is.V[S] - is.cs;
+    lam[1] = lam[2] = lam[3] = is.V[S];
+    lam[4] = is.V[S] + is.cs;
+    if (mp.fluxSplit == 0) {
+        const Real ls = fabs(is.V[S]) + is.cs;
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+            is.lp[r] = Real(0.5) * (lam[r] + ls);
+            is.ln[r] = Real(0.5) * (lam[r] - ls);
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+            const Real sr = sqrt(lam[r] * lam[r] + Real(1.0e-6));
+            is.lp[r] = Real(0.5) * (lam[r] + sr);
+            is.ln[r] = Real(0.5) * (lam[r] - sr);
+        }
+    }
+    return is;
+}
+
+// Characteristic split fluxes G of the interface with WENO5 (NP = 6) or WENO3
+// (NP = 4) on every field, the projection W = L*U taken field by field
+// through the two scalars A = q*U0 - V.U[1..3] + U4 and B = V_s*U0 - U_{s+1}.
+template <int S, int NP, int NN>
+__device__ __forceinline__ void conv_weno(const IfaceState<Real> &is, const Real *sR, int c, int bs, Real G[5])
+{
+    constexpr int first = -(NP / 2 - 1);
+    Real A[NP], Bv[NP];
+#pragma unroll
+    for (int m = 0; m < NP; ++m) {
+        const int p = c + (first + m) * bs;
+        const Real u0 = sR[p], u1 = sR[NN + p], u2 = sR[2 * NN + p];
+        const Real u3 = sR[3 * NN + p], u4 = sR[4 * NN + p];
+        A[m] = is.qk * u0 - is.V[0] * u1 - is.V[1] * u2 - is.V[2] * u3 + u4;
+        const Real us = (S == 0) ? u1 : (S == 1 ? u2 : u3);
+        Bv[m] = is.V[S] * u0 - us;
+    }
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        Real W[NP];
+#pragma unroll
+        for (int m = 0; m < NP; ++m) {
+            const int p = c + (first + m) * bs;
+            if (r == 0) {
+                W[m] = is.b * A[m] + is.d * Bv[m];
+            } else if (r == 4) {
+                W[m] = is.b * A[m] - is.d * Bv[m];
+            } else if (r == S + 1) {
+                W[m] = sR[p] - is.b2 * A[m];
+            } else {
+                W[m] = sR[r * NN + p] - is.b2 * is.V[r - 1] * A[m];
+            }
+        }
+        const Real lp = is.lp[r], ln = is.ln[r];
+        Real hp, hn;
+        if (NP == 6) {
+            hp = fast::weno5<Real>(lp * W[0], lp * W[1], lp * W[2], lp * W[3], lp * W[4]);
+            hn = fast::weno5<Real>(ln * W[5], ln * W[4], ln * W[3], ln * W[2], ln * W[1]);
+        } else {
+            hp = fast::weno3<Real>(lp * W[0], lp * W[1], lp * W[2]);
+            hn = fast::weno3<Real>(ln * W[3], ln * W[2], ln * W[1]);
+        }
+        G[r] = hp + hn;
+    }
+}
+
+// Smooth interface (hybrid form): WENO5 with the linear weights.  The linear
+// reconstruction commutes with the frozen projection, so the split fluxes
+// need the projection of two reconstructed vectors only.
+template <int S, int NN>
+__device__ __forceinline__ void conv_linear(const IfaceState<Real> &is, const Real *sR, int c, int bs, Real G[5])
+{
+    Real up[5], um[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        const Real *P = sR + v * NN + c;
+        up[v] = fast::upwind5<Real>(P[-2 * bs], P[-bs], P[0], P[bs], P[2 * bs]);
+        um[v] = fast::upwind5<Real>(P[3 * bs], P[2 * bs], P[bs], P[0], P[-bs]);
+    }
+    Real wp[5], wm[5];
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+        const Real *u = side ? um : up;
+        Real *w = side ? wm : wp;
+        const Real A = is.qk * u[0] - is.V[0] * u[1] - is.V[1] * u[2] - is.V[2] * u[3] + u[4];
+        const Real Bs = is.V[S] * u[0] - u[S + 1];
+        w[0] = is.b * A + is.d * Bs;
+        w[4] = is.b * A - is.d * Bs;
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            w[t + 1] = (t == S) ? u[0] - is.b2 * A : u[t + 1] - is.b2 * is.V[t] * A;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        G[r] = is.lp[r] * wp[r] + is.ln[r] * wm[r];
+    }
+}
+
+// back projection F = R*G of the split characteristic fluxes
+template <int S>
+__device__ __forceinline__ void back_project(const IfaceState<Real> &is, const Real G[5], Real F[5])
+{
+    const Real *V = is.V;
+    F[0] = G[0] + G[S + 1] + G[4];
+    Real e4 = is.hT * (G[0] + G[4]) + V[S] * is.cs * (G[4] - G[0]) + (V[S] * V[S] - is.qk) * G[S + 1];
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        if (t == S) {
+            F[t + 1] = V[S] * (G[0] + G[S + 1] + G[4]) + is.cs * (G[4] - G[0]);
+        } else {
+            F[t + 1] = V[t] * (G[0] + G[4]) + G[t + 1];
+            e4 += V[t] * G[t + 1];
+        }
+    }
+    F[4] = e4;
+}
+
+// central viscous flux of the interface from the brick primitives u, v, w, T
+// (sP), subtracted from F
+template <int S, typename B, int NN>
+__device__ __forceinline__ void visc_flux(const Grid &g, const ModelParams &mp, const Real *sP, int c, int bs,
+                                          Real F[5])
+{
+    const int pn = c + bs;
+    Real grad[3][3];
+    const Real ddS = Real(g.dd[S]);
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        grad[v][S] = (sP[v * NN + pn] - sP[v * NN + c]) * ddS;
+    }
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        if (t == S) continue;
+        const int bt = (t == 0) ? 1 : (t == 1 ? B::BX : B::BX * B::BY);
+        const Real ddt = Real(0.25) * Real(g.dd[t]);
+#pragma unroll
+        for (int v = 0; v < 3; ++v) {
+            const Real *P = sP + v * NN;
+            grad[v][t] = (P[c + bt] + P[pn + bt] - P[c - bt] - P[pn - bt]) * ddt;
+        }
+    }
+    const Real Tc = sP[3 * NN + c], Tp = sP[3 * NN + pn];
+    const Real Th = Real(0.5) * (Tc + Tp);
+    const Real Ts = Th * Real(mp.refT);
+    const Real mu = Real(mp.refMu) * (Real(1.458e-6) * Ts * sqrt(Ts) * fast::rcp<Real>(Ts + Real(110.4)));
+    const Real heatK = Real(mp.gamma * mp.cv / 0.71) * mu;
+    const Real divV = grad[0][0] + grad[1][1] + grad[2][2];
+    Real tau[3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        tau[v] = (v == S) ? mu * (Real(2) * grad[S][S] - Real(2.0 / 3.0) * divV) : mu * (grad[S][v] + grad[v][S]);
+    }
+    Real e5 = heatK * (Tp - Tc) * ddS;
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        const Real vh = Real(0.5) * (sP[v * NN + c] + sP[v * NN + pn]);
+        F[v + 1] -= tau[v];
+        e5 += tau[v] * vh;
+    }
+    F[4] -= e5;
+}
 
 // One tile of interfaces (tile indices tbx, tby, tbz of the case's tiling):
 // the body shared by the per-case kernel and the persistent batched kernel.
@@ -60,6 +258,8 @@ __device__ __forceinline__ bool brick_tile(const Grid &g, const ModelParams &mp,
     Real *sR = LY::conv ? reinterpret_cast<Real *>(smem + LY::r_off) : reinterpret_cast<Real *>(sU);
     Real *sF = reinterpret_cast<Real *>(smem + LY::f_off);
     double *sO = reinterpret_cast<double *>(smem + LY::o_off);
+    int *sQ = reinterpret_cast<int *>(smem + LY::q_off);
+    int *sQn = sQ + kBrickThreads;
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + LY::bar_off);
     const bool visc_on = VISC && (mp.refMu > 0.0);
 
@@ -74,6 +274,7 @@ __device__ __forceinline__ bool brick_tile(const Grid &g, const ModelParams &mp,
 
     __syncthreads();  // every thread is done with the previous tile's shared data
     if (tid == 0) {
+        *sQn = 0;
         tma::mbar_expect_tx(bar, LY::u_bytes);
         tma::load_5d(sU, map, xs, ys, zs, 0, a.tn, bar);
     }
@@ -156,184 +357,53 @@ __device__ __forceinline__ bool brick_tile(const Grid &g, const ModelParams &mp,
         __syncthreads();
     }
 
-    // B. interface flux
+    // B. interface flux.  Hybrid form: an interface whose stencil carries a
+    // sensor flag is queued; after the others, the block's first threads
+    // reconstruct the queued interfaces with full WENO5, so that a few flags
+    // cost a few lanes instead of whole warps.
+    const int bs = (S == 0) ? 1 : (S == 1 ? B::BX : B::BX * B::BY);  // brick stride along s
     if (fl_left || fl_right) {
-        const int c = bidx(i, j, k);                       // node i of the interface
-        const int bs = (S == 0) ? 1 : (S == 1 ? B::BX : B::BX * B::BY);  // brick stride along s
-        constexpr int NN = LY::nodes;
-        constexpr int ctr = NP / 2 - 1;
-        constexpr int first = -ctr;
-        const Real gamma = Real(mp.gamma);
-        // Roe / arithmetic state of the interface
-        Real UL[5], UR[5], Uo[6];
-#pragma unroll
-        for (int v = 0; v < 5; ++v) {
-            UL[v] = sR[v * NN + c];
-            UR[v] = sR[v * NN + c + bs];
-        }
-        fast::interface_state<Real>(mp.jacobMean, gamma, UL, UR, Uo);
-        const Real V[3] = {Uo[1], Uo[2], Uo[3]};
-        const Real hT = Uo[4];
-        const Real cs = Uo[5];
-        const Real qk = Real(0.5) * (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
-        const Real d = fast::rcp<Real>(Real(2) * cs);
-        const Real b = (gamma - Real(1)) * (Real(2) * d * d);
-        const Real b2 = Real(2) * b;
-        Real lp[5], ln[5];
-        {
-            Real lam[5];
-            lam[0] = V[S] - cs;
-            lam[1] = lam[2] = lam[3] = V[S];
-            lam[4] = V[S] + cs;
-            if (mp.fluxSplit == 0) {
-                const Real ls = fabs(V[S]) + cs;
-#pragma unroll
-                for (int r = 0; r < 5; ++r) {
-                    lp[r] = Real(0.5) * (lam[r] + ls);
-                    ln[r] = Real(0.5) * (lam[r] - ls);
-                }
-            } else {
-#pragma unroll
-                for (int r = 0; r < 5; ++r) {
-                    const Real sr = sqrt(lam[r] * lam[r] + Real(1.0e-6));
-                    lp[r] = Real(0.5) * (lam[r] + sr);
-                    ln[r] = Real(0.5) * (lam[r] - sr);
-                }
-            }
-        }
-        // smooth interface (hybrid form): WENO5 with the linear weights.  The
-        // linear reconstruction commutes with the frozen projection, so the
-        // split fluxes need the projection of two reconstructed vectors only.
-        bool full = true;
-        if (HYB && NP == 6) {
-            // one path per warp: a warp with any flagged interface takes the
-            // full reconstruction for all its lanes instead of both paths
-            full = __any_sync(__activemask(), full_own);
-        }
-        Real G[5];
-        if (!full) {
-            Real up[5], um[5];
-#pragma unroll
-            for (int v = 0; v < 5; ++v) {
-                const Real *P = sR + v * NN + c;
-                up[v] = fast::upwind5<Real>(P[-2 * bs], P[-bs], P[0], P[bs], P[2 * bs]);
-                um[v] = fast::upwind5<Real>(P[3 * bs], P[2 * bs], P[bs], P[0], P[-bs]);
-            }
-            Real wp[5], wm[5];
-#pragma unroll
-            for (int side = 0; side < 2; ++side) {
-                const Real *u = side ? um : up;
-                Real *w = side ? wm : wp;
-                const Real A = qk * u[0] - V[0] * u[1] - V[1] * u[2] - V[2] * u[3] + u[4];
-                const Real Bs = V[S] * u[0] - u[S + 1];
-                w[0] = b * A + d * Bs;
-                w[4] = b * A - d * Bs;
-#pragma unroll
-                for (int t = 0; t < 3; ++t) {
-                    w[t + 1] = (t == S) ? u[0] - b2 * A : u[t + 1] - b2 * V[t] * A;
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < 5; ++r) {
-                G[r] = lp[r] * wp[r] + ln[r] * wm[r];
-            }
-        } else {
-        // the two scalars of every stencil point
-        Real A[NP], Bv[NP];
-#pragma unroll
-        for (int m = 0; m < NP; ++m) {
-            const int p = c + (first + m) * bs;
-            const Real u0 = sR[p], u1 = sR[NN + p], u2 = sR[2 * NN + p];
-            const Real u3 = sR[3 * NN + p], u4 = sR[4 * NN + p];
-            A[m] = qk * u0 - V[0] * u1 - V[1] * u2 - V[2] * u3 + u4;
-            const Real us = (S == 0) ? u1 : (S == 1 ? u2 : u3);
-            Bv[m] = V[S] * u0 - us;
-        }
-        // field by field: W, WENO on both split fluxes
-#pragma unroll
-        for (int r = 0; r < 5; ++r) {
-            Real W[NP];
-#pragma unroll
-            for (int m = 0; m < NP; ++m) {
-                const int p = c + (first + m) * bs;
-                if (r == 0) {
-                    W[m] = b * A[m] + d * Bv[m];
-                } else if (r == 4) {
-                    W[m] = b * A[m] - d * Bv[m];
-                } else if (r == S + 1) {
-                    W[m] = sR[p] - b2 * A[m];
-                } else {
-                    W[m] = sR[r * NN + p] - b2 * V[r - 1] * A[m];
-                }
-            }
-            Real hp, hn;
-            if (NP == 6) {
-                hp = fast::weno5<Real>(lp[r] * W[0], lp[r] * W[1], lp[r] * W[2], lp[r] * W[3], lp[r] * W[4]);
-                hn = fast::weno5<Real>(ln[r] * W[5], ln[r] * W[4], ln[r] * W[3], ln[r] * W[2], ln[r] * W[1]);
-            } else {
-                hp = fast::weno3<Real>(lp[r] * W[0], lp[r] * W[1], lp[r] * W[2]);
-                hn = fast::weno3<Real>(ln[r] * W[3], ln[r] * W[2], ln[r] * W[1]);
-            }
-            G[r] = hp + hn;
-        }
-        }  // full interface
+        const int c = bidx(i, j, k);  // node i of the interface
+        const IfaceState<Real> is = iface_state<S, LY::nodes>(mp, sR, c, bs);
         Real F[5];
-        F[0] = G[0] + G[S + 1] + G[4];
-        Real e4 = hT * (G[0] + G[4]) + V[S] * cs * (G[4] - G[0]) + (V[S] * V[S] - qk) * G[S + 1];
+        const bool defer = HYB && NP == 6 && full_own;
+        if (defer) {
 #pragma unroll
-        for (int t = 0; t < 3; ++t) {
-            if (t == S) {
-                F[t + 1] = V[S] * (G[0] + G[S + 1] + G[4]) + cs * (G[4] - G[0]);
+            for (int v = 0; v < 5; ++v) F[v] = Real(0);
+            const int slot = atomicAdd(sQn, 1);
+            sQ[slot] = tid;
+        } else {
+            Real G[5];
+            if (HYB && NP == 6) {
+                conv_linear<S, LY::nodes>(is, sR, c, bs, G);
             } else {
-                F[t + 1] = V[t] * (G[0] + G[4]) + G[t + 1];
-                e4 += V[t] * G[t + 1];
+                conv_weno<S, NP, LY::nodes>(is, sR, c, bs, G);
             }
+            back_project<S>(is, G, F);
         }
-        F[4] = e4;
         if (visc_on) {
-            // central viscous flux from the brick primitives
-            const int pn = c + bs;
-            Real grad[3][3];
-            const Real ddS = Real(g.dd[S]);
-#pragma unroll
-            for (int v = 0; v < 3; ++v) {
-                grad[v][S] = (sP[v * NN + pn] - sP[v * NN + c]) * ddS;
-            }
-#pragma unroll
-            for (int t = 0; t < 3; ++t) {
-                if (t == S) continue;
-                const int bt = (t == 0) ? 1 : (t == 1 ? B::BX : B::BX * B::BY);
-                const Real ddt = Real(0.25) * Real(g.dd[t]);
-#pragma unroll
-                for (int v = 0; v < 3; ++v) {
-                    const Real *P = sP + v * NN;
-                    grad[v][t] = (P[c + bt] + P[pn + bt] - P[c - bt] - P[pn - bt]) * ddt;
-                }
-            }
-            const Real Tc = sP[3 * NN + c], Tp = sP[3 * NN + pn];
-            const Real Th = Real(0.5) * (Tc + Tp);
-            const Real Ts = Th * Real(mp.refT);
-            const Real mu = Real(mp.refMu) * (Real(1.458e-6) * Ts * sqrt(Ts) * fast::rcp<Real>(Ts + Real(110.4)));
-            const Real heatK = Real(mp.gamma * mp.cv / 0.71) * mu;
-            const Real divV = grad[0][0] + grad[1][1] + grad[2][2];
-            Real tau[3];
-#pragma unroll
-            for (int v = 0; v < 3; ++v) {
-                tau[v] = (v == S) ? mu * (Real(2) * grad[S][S] - Real(2.0 / 3.0) * divV)
-                                  : mu * (grad[S][v] + grad[v][S]);
-            }
-            Real e5 = heatK * (Tp - Tc) * ddS;
-#pragma unroll
-            for (int v = 0; v < 3; ++v) {
-                const Real vh = Real(0.5) * (sP[v * NN + c] + sP[v * NN + pn]);
-                F[v + 1] -= tau[v];
-                e5 += tau[v] * vh;
-            }
-            F[4] -= e5;
+            visc_flux<S, B, LY::nodes>(g, mp, sP, c, bs, F);
         }
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
             sF[v * kBrickThreads + tid] = F[v];
+        }
+    }
+    if (HYB && NP == 6) {
+        __syncthreads();
+        const int nq = *sQn;
+        if (tid < nq) {
+            const int lt = sQ[tid];
+            const int tx = lt % B::TX, ty = (lt / B::TX) % B::TY, tz = lt / (B::TX * B::TY);
+            const int c = bidx(i0 + tx - (S == 0), j0 + ty - (S == 1), k0 + tz - (S == 2));
+            const IfaceState<Real> is = iface_state<S, LY::nodes>(mp, sR, c, bs);
+            Real G[5], F[5];
+            conv_weno<S, NP, LY::nodes>(is, sR, c, bs, G);
+            back_project<S>(is, G, F);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                sF[v * kBrickThreads + lt] += F[v];
+            }
         }
     }
     __syncthreads();
@@ -370,6 +440,7 @@ stage_brick(Grid g, ModelParams mp, StageArgs a, const __grid_constant__ CUtenso
         tma::mbar_init(bar, 1);
     }
     __syncthreads();
+    pdl_wait();
     brick_tile<S, NP, VISC, HYB, VAR>(g, mp, a, &map, blockIdx.x, blockIdx.y, blockIdx.z, smem, 0);
 }
 
@@ -390,8 +461,8 @@ static int launch_brick_one(const Grid &g, const ModelParams &m, const StageArgs
     const int L0 = g.hi[0] - g.lo[0], L1 = g.hi[1] - g.lo[1], L2 = g.hi[2] - g.lo[2];
     dim3 grid((L0 + B::SX - 1) / B::SX, (L1 + B::SY - 1) / B::SY, (L2 + B::SZ - 1) / B::SZ);
     dim3 block(B::TX, B::TY, B::TZ);
-    stage_brick<S, NP, VISC, HYB, VAR><<<grid, block, LY::total, st>>>(g, m, a, a.maps[S * kTileVariants + VAR]);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_k(stage_brick<S, NP, VISC, HYB, VAR>, grid, block, LY::total, st, g, m, a,
+                             a.maps[S * kTileVariants + VAR]);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "stage_brick launch");
 }
 
@@ -445,6 +516,7 @@ stage_batch(const BatchCase *cases, const CUtensorMap *maps, const long long *pr
         tma::mbar_init(bar, 1);
     }
     __syncthreads();
+    pdl_wait();
     const long long total = prefix[ncase];
     uint32_t parity = 0;
     for (;;) {
@@ -480,7 +552,9 @@ stage_batch(const BatchCase *cases, const CUtensorMap *maps, const long long *pr
         a.accumulate = 0;
         a.to = sc.to;
         a.tn = sc.tn;
+        a.tm = sc.tm;
         a.maps = nullptr;
+        a.omaps = nullptr;
         a.var[0] = a.var[1] = a.var[2] = 0;
         a.status = status;
         a.flags = C.flags;
@@ -507,9 +581,8 @@ static int launch_batch_one(const BatchCase *cases, const CUtensorMap *maps, con
         if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(stage_batch)");
         configured[dev] = true;
     }
-    stage_batch<S, HYB><<<blocks, dim3(B::TX, B::TY, B::TZ), LY::total, st>>>(cases, maps, prefix, ncase, sc, dts,
-                                                                            counter, status);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_k(stage_batch<S, HYB>, dim3(blocks), dim3(B::TX, B::TY, B::TZ), LY::total, st, cases,
+                             maps, prefix, ncase, sc, dts, counter, status);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "stage_batch launch");
 }
 

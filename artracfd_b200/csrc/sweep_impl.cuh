@@ -260,6 +260,7 @@ __device__ __forceinline__ void update_node(const StageArgs &a, long long nn, lo
 template <int NP, bool VISC>
 __global__ void __launch_bounds__(kTileX) stage_x(Grid g, ModelParams mp, StageArgs a)
 {
+    pdl_wait();
     __shared__ Real sF[kKeep][kTileX];
     const int L = g.hi[0] - g.lo[0];
     const int IF = L + 1;
@@ -307,6 +308,7 @@ __global__ void __launch_bounds__(kTileX) stage_x(Grid g, ModelParams mp, StageA
 template <int S, int NP, bool VISC>
 __global__ void __launch_bounds__(kColX *kTileS) stage_yz(Grid g, ModelParams mp, StageArgs a, int seg)
 {
+    pdl_wait();
     __shared__ Real sF[kTileS + 1][kKeep][kColX];
     constexpr int T2 = (S == 1) ? 2 : 1;  // the other transverse direction
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -382,7 +384,7 @@ static int launch_np(const Grid &g, const ModelParams &m, const StageArgs &a, in
             set_error("X sweep grid too large");
             return ACFD_ERR_ARG;
         }
-        stage_x<NP, VISC><<<(unsigned)blocks, kTileX, 0, st>>>(g, m, a);
+        ACFD_CUDA(launch_k(stage_x<NP, VISC>, dim3((unsigned)blocks), dim3(kTileX), 0, st, g, m, a));
     } else {
         const long long Lx = L0;
         const long long Lt = (s == 1) ? L2 : L1;
@@ -399,9 +401,9 @@ static int launch_np(const Grid &g, const ModelParams &m, const StageArgs &a, in
         dim3 grid((unsigned)cols, (unsigned)nseg);
         dim3 block(kColX, kTileS);
         if (s == 1) {
-            stage_yz<1, NP, VISC><<<grid, block, 0, st>>>(g, m, a, (int)seg);
+            ACFD_CUDA(launch_k(stage_yz<1, NP, VISC>, grid, block, 0, st, g, m, a, (int)seg));
         } else {
-            stage_yz<2, NP, VISC><<<grid, block, 0, st>>>(g, m, a, (int)seg);
+            ACFD_CUDA(launch_k(stage_yz<2, NP, VISC>, grid, block, 0, st, g, m, a, (int)seg));
         }
     }
     cudaError_t e = cudaGetLastError();
