@@ -28,6 +28,10 @@ TO, TN, TM = 0, 1, 2
 X, Y, Z, DIMS, PHI = 0, 1, 2, 3, 4
 # arithmetic forms
 FP64_EXACT, FP64, FP32_BULK, FP32_HYBRID = 0, 1, 2, 3
+# stage-kernel variants (acfd_set_tiles): bricks below BRICK_VARIANTS, then
+# the line-march kernels with 1, 2, 4 waves, then from PLANE_VARIANT the
+# plane-march kernels (Y/Z sweeps) with 1, 2, 4 waves
+BRICK_VARIANTS, PLANE_VARIANT, STAGE_VARIANTS = 2, 5, 8
 # sync masks
 SYNC_TO, SYNC_TN, SYNC_TM, SYNC_U, SYNC_FLAGS, SYNC_ALL = 0x1, 0x2, 0x4, 0x7, 0x8, 0xF
 # boundary kinds (commons.h:83-87)
@@ -162,6 +166,7 @@ def load_library(path: str | None = None):
         "acfd_stats": [vp, ctypes.POINTER(ctypes.c_longlong)],
         "acfd_synchronize": [vp],
         "acfd_autotune": [vp, ctypes.POINTER(ctypes.c_int)],
+        "acfd_set_tiles": [vp, ctypes.POINTER(ctypes.c_int)],
         "acfd_mlp_param_count": [],
         "acfd_sensor_load": [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_float],
         "acfd_sensor_update": [vp, ctypes.POINTER(ctypes.c_ulonglong)],

@@ -38,6 +38,13 @@ int launch_stage_fp32(const Grid &, const ModelParams &, const StageArgs &, int,
 int launch_stage_brick_fast(const Grid &, const ModelParams &, const StageArgs &, int, bool, cudaStream_t);
 int launch_stage_brick_fp32(const Grid &, const ModelParams &, const StageArgs &, int, bool, cudaStream_t);
 int launch_stage_brick_hybrid(const Grid &, const ModelParams &, const StageArgs &, int, bool, cudaStream_t);
+int launch_stage_march_fast(const Grid &, const ModelParams &, const StageArgs &, int, bool, int, cudaStream_t);
+int launch_stage_march_fp32(const Grid &, const ModelParams &, const StageArgs &, int, bool, bool, int,
+                            cudaStream_t);
+int launch_stage_plane_fast(const Grid &, const ModelParams &, const StageArgs &, int, bool, const PlaneTile &,
+                            const CUtensorMap &, cudaStream_t);
+int launch_stage_plane_fp32(const Grid &, const ModelParams &, const StageArgs &, int, bool, bool,
+                            const PlaneTile &, const CUtensorMap &, cudaStream_t);
 int launch_weno_batch_exact(int, const double *, double *, int, cudaStream_t);
 int launch_weno_batch_fast(int, const double *, double *, int, cudaStream_t);
 int launch_weno_batch_fp32(int, const double *, double *, int, cudaStream_t);
@@ -65,6 +72,19 @@ bool pdl_enabled()
     }();
     return on;
 }
+
+// Stage-kernel variants: the brick tile shapes (0 .. kTileVariants-1), the
+// line-march kernels and the plane-march kernels (Y/Z sweeps; X sweeps of a
+// plane variant use the line march), each launched with 1, 2 or 4 waves
+constexpr int kMarchVariants = 3;
+constexpr int kMarchWaves[kMarchVariants] = {1, 2, 4};
+constexpr int kPlaneVariants = 3;
+constexpr int kPlaneWaves[kPlaneVariants] = {1, 2, 4};
+constexpr int kPlaneFirst = kTileVariants + kMarchVariants;
+constexpr int kStageVariants = kPlaneFirst + kPlaneVariants;
+static_assert(ACFD_BRICK_VARIANTS == kTileVariants && ACFD_STAGE_VARIANTS == kStageVariants &&
+                  ACFD_PLANE_VARIANT == kPlaneFirst,
+              "stage-variant numbering of the C ABI");
 
 __global__ void set_scalar(double *p, double v)
 {
@@ -102,10 +122,21 @@ struct acfd_case {
     int *dstatus = nullptr;        // device error word (TMA wait time-outs)
     CUtensorMap maps[3 * kTileVariants];  // state tensor maps of the brick kernels per (axis, tile variant)
     bool maps_ok = false;
-    int tile_var[3] = {0, 0, 0};   // tile variant of each sweep axis (acfd_autotune)
+    // stage-kernel variant of each sweep axis per arithmetic form (acfd_autotune,
+    // acfd_set_tiles): brick tile shapes, then line-march launch sizes
+    int tile_var[4][3] = {{0, 0, 0},
+                          {0, 0, 0},
+                          {0, kPlaneFirst, kPlaneFirst},
+                          {0, kPlaneFirst, kPlaneFirst}};
+    int sms = 148;                 // SM count of the case's device
+    CUtensorMap pmaps[3];          // plane-march state maps (Y and Z sweeps)
+    bool pmaps_ok = false;
     bool plain_kernels = false;    // use the global-memory stage kernels instead of the bricks
     bool bc_multi = false;         // one launch per ghost-fill phase instead of the fused launch
     unsigned *bcbar = nullptr;     // grid-barrier words of the fused ghost fill
+    int2 *bc_pairs = nullptr;      // ghost fill as one gather (all faces copies)
+    int bc_npairs = 0;
+    bool bc_gather = false;
     std::vector<const FaceBox *> bc_ptrs;
     std::vector<int> bc_sizes;
     // learned sensor of the hybrid form
@@ -160,6 +191,23 @@ int encode_state_maps(acfd_case *cs)
         }
     }
     cs->maps_ok = true;
+    // plane-march maps: one plane of the tile with its halo, five variables
+    for (int s = 1; s < 3; ++s) {
+        const PlaneTile pt = plane_tile(g, s, viscous(cs), 1, cs->sms);
+        const cuuint32_t box[5] = {(cuuint32_t)pt.BXp, (cuuint32_t)(s == 1 ? 1 : pt.BC),
+                                   (cuuint32_t)(s == 2 ? 1 : pt.BC), 5, 1};
+        if (pt.BXp > 256 || pt.BC > 256) {
+            return ACFD_OK;  // no plane maps for this grid
+        }
+        CUresult r = encode(&cs->pmaps[s], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, cs->U, dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) {
+            set_error("cuTensorMapEncodeTiled failed (%d) for the plane map of axis %d", (int)r, s);
+            return ACFD_ERR_CUDA;
+        }
+    }
+    cs->pmaps_ok = true;
     return ACFD_OK;
 }
 
@@ -226,6 +274,83 @@ void build_bc_plan(acfd_case *cs)
     }
 }
 
+// Ghost fill of copy-only cases as one gather.  The reference fills the faces
+// in order (boundary_treatment.c:51-63); when every face is periodic or
+// outflow, every write copies one node into another, so replaying the
+// ordered fill on node indices instead of values gives, for each node the
+// fill changes, the node whose value (from before the fill) it ends with.
+// When no such source node is itself changed, one gather reproduces the
+// ordered fill bit for bit.  Returns false (keep the ordered launches) for any
+// other boundary kind or overlap.
+bool build_bc_gather(acfd_case *cs)
+{
+    const acfd_partition_t &p = cs->part;
+    const Grid &g = cs->grid;
+    for (int face = 1; face <= 6; ++face) {
+        if (p.typeBC[face] != 1 && p.typeBC[face] != 4) {
+            return false;
+        }
+    }
+    if (g.nn * 5 > (long long)INT32_MAX) {
+        return false;
+    }
+    std::vector<int> sym((size_t)g.nn);
+    for (long long q = 0; q < g.nn; ++q) {
+        sym[(size_t)q] = (int)q;
+    }
+    auto idx = [&](int i, int j, int k) { return ((long long)k * g.n[1] + j) * g.pitch + i; };
+    for (const auto &grp : cs->bc_groups) {
+        for (const FaceBox &b : grp) {
+            const int *N = p.N[b.face];
+            const int periodic = (p.typeBC[b.face] == 4);
+            int off[3];
+            for (int s = 0; s < 3; ++s) {
+                off[s] = (b.r != 0 && periodic) ? p.m[s] * N[s] : N[s];
+            }
+            for (int k = b.box[2][0]; k < b.box[2][1]; ++k) {
+                for (int j = b.box[1][0]; j < b.box[1][1]; ++j) {
+                    for (int i = b.box[0][0]; i < b.box[0][1]; ++i) {
+                        const int si = i - off[0], sj = j - off[1], sk = k - off[2];
+                        if (si < 0 || sj < 0 || sk < 0 || si >= g.n[0] || sj >= g.n[1] || sk >= g.n[2]) {
+                            return false;
+                        }
+                        sym[(size_t)idx(i, j, k)] = sym[(size_t)idx(si, sj, sk)];
+                    }
+                }
+            }
+        }
+    }
+    std::vector<int2> pairs;
+    std::vector<char> changed((size_t)g.nn, 0);
+    for (long long q = 0; q < g.nn; ++q) {
+        if (sym[(size_t)q] != (int)q) {
+            pairs.push_back(make_int2((int)q, sym[(size_t)q]));
+            changed[(size_t)q] = 1;
+        }
+    }
+    for (const int2 &pr : pairs) {
+        if (changed[(size_t)pr.y]) {
+            return false;  // a source is itself rewritten: order matters
+        }
+    }
+    if (pairs.empty()) {
+        return false;
+    }
+    if (cudaMalloc(&cs->bc_pairs, pairs.size() * sizeof(int2)) != cudaSuccess) {
+        cudaGetLastError();
+        cs->bc_pairs = nullptr;
+        return false;
+    }
+    if (cudaMemcpy(cs->bc_pairs, pairs.data(), pairs.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(cs->bc_pairs);
+        cs->bc_pairs = nullptr;
+        return false;
+    }
+    cs->bc_npairs = (int)pairs.size();
+    return true;
+}
+
 int treat_boundary(acfd_case *cs, int tn)
 {
     if (cs->ib && ib_count(cs->ib) > 0) {
@@ -238,6 +363,10 @@ int treat_boundary(acfd_case *cs, int tn)
         cs->launches += (long long)cs->part.gl * ((ib_count(cs->ib) + 7) / 8);
     }
     double *U = level(cs, tn);
+    if (cs->bc_gather) {
+        ++cs->launches;
+        return launch_ghost_gather(cs->grid, cs->bc_pairs, cs->bc_npairs, U, cs->stream);
+    }
     if (!cs->bc_multi) {
         if (cs->bc_groups.empty()) {
             return ACFD_OK;
@@ -276,7 +405,8 @@ int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int 
     a.status = cs->dstatus;
     a.flags = cs->sensor_flags;
     for (int s = 0; s < 3; ++s) {
-        a.var[s] = cs->tile_var[s];
+        const int v = cs->tile_var[cs->mode][s];
+        a.var[s] = v < kTileVariants ? v : 0;
     }
     if (p == ACFD_PHI) {
         ++cs->launches;
@@ -310,20 +440,40 @@ int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int 
     for (int s = s0; s < s1; ++s) {
         a.accumulate = (cs->model.multidim == 1 && s != 0) ? 1 : 0;
         int st;
-        const bool brick = cs->maps_ok && !cs->plain_kernels;
+        const int var = cs->tile_var[cs->mode][s];
+        const bool plane_v = !cs->plain_kernels && var >= kPlaneFirst && var < kStageVariants;
+        const bool plane = plane_v && s != 0 && cs->pmaps_ok;
+        const bool march = !cs->plain_kernels && !plane && var >= kTileVariants && var < kStageVariants;
+        const bool brick = !march && !plane && cs->maps_ok && !cs->plain_kernels;
+        // march launch size: waves x SMs x resident warps per SM (two blocks of
+        // eight warps in the FP32 forms, one in FP64)
+        const int waves = plane_v ? kPlaneWaves[var - kPlaneFirst] : march ? kMarchWaves[var - kTileVariants] : 1;
+        const int target32 = waves * cs->sms * 16, target64 = waves * cs->sms * 8;
+        PlaneTile pt = {};
+        if (plane) {
+            pt = plane_tile(cs->grid, s, visc, waves, cs->sms);
+        }
         switch (cs->mode) {
             case ACFD_FP64_EXACT: st = launch_stage_exact(cs->grid, cs->mp, a, s, visc, cs->stream); break;
             case ACFD_FP64:
-                st = brick ? launch_stage_brick_fast(cs->grid, cs->mp, a, s, visc, cs->stream)
-                           : launch_stage_fast(cs->grid, cs->mp, a, s, visc, cs->stream);
+                st = plane   ? launch_stage_plane_fast(cs->grid, cs->mp, a, s, visc, pt, cs->pmaps[s], cs->stream)
+                     : march ? launch_stage_march_fast(cs->grid, cs->mp, a, s, visc, target64, cs->stream)
+                     : brick ? launch_stage_brick_fast(cs->grid, cs->mp, a, s, visc, cs->stream)
+                             : launch_stage_fast(cs->grid, cs->mp, a, s, visc, cs->stream);
                 break;
             case ACFD_FP32_HYBRID:
-                st = brick ? launch_stage_brick_hybrid(cs->grid, cs->mp, a, s, visc, cs->stream)
-                           : launch_stage_fp32(cs->grid, cs->mp, a, s, visc, cs->stream);
+                st = plane   ? launch_stage_plane_fp32(cs->grid, cs->mp, a, s, visc, true, pt, cs->pmaps[s],
+                                                       cs->stream)
+                     : march ? launch_stage_march_fp32(cs->grid, cs->mp, a, s, visc, true, target32, cs->stream)
+                     : brick ? launch_stage_brick_hybrid(cs->grid, cs->mp, a, s, visc, cs->stream)
+                             : launch_stage_fp32(cs->grid, cs->mp, a, s, visc, cs->stream);
                 break;
             default:
-                st = brick ? launch_stage_brick_fp32(cs->grid, cs->mp, a, s, visc, cs->stream)
-                           : launch_stage_fp32(cs->grid, cs->mp, a, s, visc, cs->stream);
+                st = plane   ? launch_stage_plane_fp32(cs->grid, cs->mp, a, s, visc, false, pt, cs->pmaps[s],
+                                                       cs->stream)
+                     : march ? launch_stage_march_fp32(cs->grid, cs->mp, a, s, visc, false, target32, cs->stream)
+                     : brick ? launch_stage_brick_fp32(cs->grid, cs->mp, a, s, visc, cs->stream)
+                             : launch_stage_fp32(cs->grid, cs->mp, a, s, visc, cs->stream);
                 break;
         }
         if (st != ACFD_OK) {
@@ -476,6 +626,7 @@ int acfd_init(const acfd_partition_t *part, const acfd_model_t *model, acfd_case
     cs->part = *part;
     cs->model = *model;
     ACFD_CUDA(cudaGetDevice(&cs->device));
+    ACFD_CUDA(cudaDeviceGetAttribute(&cs->sms, cudaDevAttrMultiProcessorCount, cs->device));
     Grid &g = cs->grid;
     for (int s = 0; s < 3; ++s) {
         g.n[s] = part->n[s];
@@ -540,6 +691,16 @@ int acfd_init(const acfd_partition_t *part, const acfd_model_t *model, acfd_case
         return st;
     }
     build_bc_plan(cs);
+    // the ordered per-phase launches stay available for comparison
+    // (ACFD_BC_PHASES=1 in the environment)
+    if (!getenv("ACFD_BC_PHASES") && !getenv("ACFD_BC_FUSED")) {
+        if ((e = cudaStreamSynchronize(cs->stream)) != cudaSuccess) {
+            st = cuda_status(e, "acfd_init");
+            acfd_finalize(cs);
+            return st;
+        }
+        cs->bc_gather = build_bc_gather(cs);
+    }
     if ((e = cudaStreamSynchronize(cs->stream)) != cudaSuccess) {
         st = cuda_status(e, "acfd_init");
         acfd_finalize(cs);
@@ -566,6 +727,7 @@ int acfd_finalize(acfd_case_t *cs)
     cudaFree(cs->cfl_out);
     cudaFree(cs->dstatus);
     cudaFree(cs->bcbar);
+    cudaFree(cs->bc_pairs);
     cudaFree(cs->sensor_params);
     cudaFree(cs->sensor_flags);
     cudaFree(cs->sensor_rp);
@@ -717,9 +879,10 @@ int acfd_evolve_fluid_graph(acfd_case_t *cs, double dt)
 int acfd_autotune(acfd_case_t *cs, int tiles[3])
 {
     TRY(check_case(cs));
-    if (cs->mode == ACFD_FP64_EXACT || !cs->maps_ok || cs->plain_kernels) {
+    int *var_of = cs->tile_var[cs->mode];
+    if (cs->mode == ACFD_FP64_EXACT || cs->plain_kernels) {
         for (int s = 0; s < 3; ++s) {
-            if (tiles) tiles[s] = cs->tile_var[s];
+            if (tiles) tiles[s] = var_of[s];
         }
         return ACFD_OK;  // the exact form has no tile choice
     }
@@ -727,6 +890,11 @@ int acfd_autotune(acfd_case_t *cs, int tiles[3])
     ACFD_CUDA(cudaEventCreate(&e0));
     ACFD_CUDA(cudaEventCreate(&e1));
     int st = set_dt(cs, 0.0);
+    if (st == ACFD_OK && cs->mode == ACFD_FP32_HYBRID) {
+        // the flags of the current state, as a step would use them
+        st = launch_sensor_flags(cs->grid, cs->mp, cs->U, cs->flags, cs->sensor_params, cs->sensor_logit,
+                                 cs->sensor_rp, cs->sensor_flags, nullptr, cs->stream);
+    }
     const int half = (cs->model.sScheme == 1) ? 3 : 2;
     for (int s = 0; s < 3 && st == ACFD_OK; ++s) {
         const Grid &g = cs->grid;
@@ -734,15 +902,18 @@ int acfd_autotune(acfd_case_t *cs, int tiles[3])
             continue;  // no sweep along a collapsed axis
         }
         float best = 1e30f;
-        int best_var = cs->tile_var[s];
-        for (int var = 0; var < kTileVariants && st == ACFD_OK; ++var) {
-            cs->tile_var[s] = var;
-            // stage 1 writes U[TN] only, which every step overwrites first
-            st = stage(cs, 1.0, 0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN, s);  // warm-up
+        int best_var = var_of[s];
+        for (int var = cs->maps_ok ? 0 : kTileVariants; var < kStageVariants && st == ACFD_OK; ++var) {
+            var_of[s] = var;
+            // RK stage 1 (U[TO] -> U[TN]) then the timed RK stage 2 (U[TO],
+            // U[TN] -> U[TM]), which reads two levels like stages 2 and 3 of
+            // every step; both levels written are overwritten by every step
+            st = stage(cs, 1.0, 0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN, s);
+            if (st == ACFD_OK) st = stage(cs, 1.0, 0.75, 0.25, ACFD_TO, ACFD_TN, ACFD_TM, s);  // warm-up
             float total = 0.0f;
             for (int rep = 0; rep < 3 && st == ACFD_OK; ++rep) {
                 cudaEventRecord(e0, cs->stream);
-                st = stage(cs, 1.0, 0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN, s);
+                st = stage(cs, 1.0, 0.75, 0.25, ACFD_TO, ACFD_TN, ACFD_TM, s);
                 cudaEventRecord(e1, cs->stream);
                 cudaEventSynchronize(e1);
                 float ms = 0.0f;
@@ -754,7 +925,7 @@ int acfd_autotune(acfd_case_t *cs, int tiles[3])
                 best_var = var;
             }
         }
-        cs->tile_var[s] = best_var;
+        var_of[s] = best_var;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -764,8 +935,28 @@ int acfd_autotune(acfd_case_t *cs, int tiles[3])
     release_graph(cs);
     TRY(check_device_status(cs));
     for (int s = 0; s < 3; ++s) {
-        if (tiles) tiles[s] = cs->tile_var[s];
+        if (tiles) tiles[s] = var_of[s];
     }
+    return ACFD_OK;
+}
+
+int acfd_set_tiles(acfd_case_t *cs, const int tiles[3])
+{
+    TRY(check_case(cs));
+    if (!tiles) {
+        set_error("acfd_set_tiles: null tiles");
+        return ACFD_ERR_ARG;
+    }
+    for (int s = 0; s < 3; ++s) {
+        if (tiles[s] < 0 || tiles[s] >= kStageVariants || (tiles[s] < kTileVariants && !cs->maps_ok)) {
+            set_error("acfd_set_tiles: variant %d of axis %d not available", tiles[s], s);
+            return ACFD_ERR_ARG;
+        }
+    }
+    for (int s = 0; s < 3; ++s) {
+        cs->tile_var[cs->mode][s] = tiles[s];
+    }
+    release_graph(cs);
     return ACFD_OK;
 }
 

@@ -74,6 +74,68 @@ int launch_stage_batch(const BatchCase *cases, const CUtensorMap *maps, const lo
                        const StageCoefs &sc, const double *dts, unsigned long long *counter, int *status, int blocks,
                        int s, bool hybrid, cudaStream_t st);
 
+// Plane-march stage kernels (Y/Z sweeps): geometry of one launch, computed on
+// the host and passed by value.  A block owns WX consecutive x by NR rows of
+// the other transverse axis over one segment of the sweep axis; a producer
+// warp streams halo'd planes of U[tn] into a ring of kPlaneSlots slots.
+constexpr int kPlaneSlots = 6;
+constexpr int kPlaneMaxThreads = 256;
+constexpr int kPlaneSmemMax = 110 * 1024;
+
+// bytes of one ring slot: a TMA destination in shared memory starts on a
+// 128-byte boundary, so the slot stride is rounded up to it
+__host__ __device__ inline int plane_slot_bytes(int BXp, int BC)
+{
+    return (BXp * BC * 5 * 8 + 127) & ~127;
+}
+
+struct PlaneTile {
+    int WX, NR;    // tile: x extent and rows of the other transverse axis
+    int ntx, ntc;  // tiles along x and along the rows
+    int nseg;      // segments along the sweep axis
+    int BXp, BC;   // plane box: x extent (even, covers the x halo) and rows with halo
+    int ncw;       // consumer warps (the producer is warp ncw)
+};
+
+// tile geometry of the plane march along s (1 or 2); `waves` scales the
+// number of blocks (segments along s, each at least 8 planes long)
+inline PlaneTile plane_tile(const Grid &g, int s, bool visc, int waves, int sms)
+{
+    PlaneTile pt;
+    const int T2 = (s == 1) ? 2 : 1;
+    const int Lx = g.hi[0] - g.lo[0], Lt = g.hi[T2] - g.lo[T2], Ls = g.hi[s] - g.lo[s];
+    const int hv = visc ? 1 : 0;
+    pt.ntx = (Lx + 63) / 64;
+    if (pt.ntx < 1) pt.ntx = 1;
+    pt.WX = (Lx + pt.ntx - 1) / pt.ntx;
+    if (pt.WX < 1) pt.WX = 1;
+    pt.NR = (kPlaneMaxThreads - 32) / pt.WX;
+    if (pt.NR > Lt) pt.NR = Lt;
+    if (pt.NR < 1) pt.NR = 1;
+    pt.ntc = (Lt + pt.NR - 1) / pt.NR;
+    pt.BXp = (pt.WX + 2 * hv + 2) & ~1;
+    // the ring of kPlaneSlots planes must fit the shared-memory budget
+    while (pt.NR > 1 && kPlaneSlots * plane_slot_bytes(pt.BXp, pt.NR + 2 * hv) + 2 * kPlaneSlots * 8 > kPlaneSmemMax) {
+        --pt.NR;
+    }
+    pt.ntc = (Lt + pt.NR - 1) / pt.NR;
+    pt.ncw = (pt.WX * pt.NR + 31) / 32;
+    pt.BC = pt.NR + 2 * hv;
+    const long long tiles = (long long)pt.ntx * pt.ntc;
+    const long long target = (long long)waves * 2 * sms;
+    long long nseg = (target + tiles - 1) / tiles;
+    const int cap = Ls / 8 > 1 ? Ls / 8 : 1;
+    if (nseg > cap) nseg = cap;
+    if (nseg < 1) nseg = 1;
+    pt.nseg = (int)nseg;
+    return pt;
+}
+
+inline int plane_smem_bytes(const PlaneTile &pt)
+{
+    return kPlaneSlots * plane_slot_bytes(pt.BXp, pt.BC) + 2 * kPlaneSlots * 8;
+}
+
 // learned sensor (sensor.cu)
 // Flags of the PIN nodes (the caller sets the others to 1 once); rho_p:
 // scratch of nn float2 (density and pressure of every node)
@@ -125,6 +187,9 @@ struct FaceBox {
 };
 int launch_domain_boundary(const Grid &g, const ModelParams &m, const acfd_partition_t &part,
                            const FaceBox *boxes, int nbox, double *U, cudaStream_t st);
+// ghost fill as one gather: U[dst] = U[src] for every (dst, src) pair, all
+// five variables of the level U
+int launch_ghost_gather(const Grid &g, const int2 *pairs, int count, double *U, cudaStream_t st);
 // all groups of one TreatBoundary in one cooperative launch with grid barriers;
 // bar: two device words (arrival count, generation), zero at first use
 int launch_domain_boundary_fused(const Grid &g, const ModelParams &m, const acfd_partition_t &part,

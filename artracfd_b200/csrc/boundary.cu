@@ -396,6 +396,31 @@ unsigned blocks_for(long long n, int bs)
 
 }  // namespace
 
+// Ghost fill of a case whose faces are all copies (periodic, outflow): every
+// changed node takes the value of one unchanged node, so the ordered faces
+// collapse into one gather (pairs: destination, source node index)
+__global__ void ghost_gather(long long nn, const int2 *__restrict__ pairs, int count, double *U)
+{
+    pdl_wait();
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+        const int2 q = pairs[t];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            U[v * nn + q.x] = U[v * nn + q.y];
+        }
+    }
+}
+
+int launch_ghost_gather(const Grid &g, const int2 *pairs, int count, double *U, cudaStream_t st)
+{
+    if (count <= 0) {
+        return ACFD_OK;
+    }
+    const int blocks = (int)blocks_for(count, 256);
+    cudaError_t e = launch_k(ghost_gather, dim3(blocks), dim3(256), 0, st, g.nn, pairs, count, U);
+    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "ghost_gather launch");
+}
+
 int launch_domain_boundary(const Grid &g, const ModelParams &m, const acfd_partition_t &part,
                            const FaceBox *boxes, int nbox, double *U, cudaStream_t st)
 {

@@ -35,3 +35,27 @@ int launch_stage_brick_fast(const Grid &g, const ModelParams &m, const StageArgs
 }
 
 }  // namespace acfd
+
+#include "sweep_march.cuh"
+
+namespace acfd {
+
+int launch_stage_march_fast(const Grid &g, const ModelParams &m, const StageArgs &a, int s, bool viscous,
+                            int target, cudaStream_t st)
+{
+    return form_fast::launch_march_impl(g, m, a, s, viscous, false, target, st);
+}
+
+}  // namespace acfd
+
+#include "sweep_plane.cuh"
+
+namespace acfd {
+
+int launch_stage_plane_fast(const Grid &g, const ModelParams &m, const StageArgs &a, int s, bool viscous,
+                            const PlaneTile &pt, const CUtensorMap &map, cudaStream_t st)
+{
+    return form_fast::launch_plane_impl(g, m, a, s, viscous, false, pt, map, st);
+}
+
+}  // namespace acfd

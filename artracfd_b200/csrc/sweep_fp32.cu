@@ -56,3 +56,27 @@ int launch_stage_batch(const BatchCase *cases, const CUtensorMap *maps, const lo
 }
 
 }  // namespace acfd
+
+#include "sweep_march.cuh"
+
+namespace acfd {
+
+int launch_stage_march_fp32(const Grid &g, const ModelParams &m, const StageArgs &a, int s, bool viscous,
+                            bool hybrid, int target, cudaStream_t st)
+{
+    return form_fp32::launch_march_impl(g, m, a, s, viscous, hybrid, target, st);
+}
+
+}  // namespace acfd
+
+#include "sweep_plane.cuh"
+
+namespace acfd {
+
+int launch_stage_plane_fp32(const Grid &g, const ModelParams &m, const StageArgs &a, int s, bool viscous,
+                            bool hybrid, const PlaneTile &pt, const CUtensorMap &map, cudaStream_t st)
+{
+    return form_fp32::launch_plane_impl(g, m, a, s, viscous, hybrid, pt, map, st);
+}
+
+}  // namespace acfd

@@ -1,0 +1,290 @@
+// Plane-march stage kernels (fast FP64, FP32 and hybrid forms), Y and Z
+// sweeps.
+//
+// A block owns a tile of grid lines along the sweep axis s: WX consecutive x
+// by NR consecutive rows of the other transverse axis, over one segment of
+// the line.  It walks the segment plane by plane:
+//  * a producer warp streams the planes of U[tn] (the tile plus a one-node
+//    halo in x and in the rows, all five variables) into a ring of
+//    kPlaneSlots shared-memory slots with TMA copies, two planes ahead of the
+//    consumers (full/empty mbarrier pair per slot);
+//  * every consumer thread walks one line: its stencil window (nodes p-2..p+3
+//    of interface p+1/2) lives in registers and gains one node per plane, the
+//    transverse differences of the viscous flux come from the halo'd plane
+//    in shared memory, and the node update reads U[tn] of its node from the
+//    ring.
+// Every plane of U[tn] crosses from L2 once per tile (halo included), and the
+// loads run ahead of the arithmetic without holding registers.
+//
+// Included after sweep_march.cuh by sweep_fast.cu and sweep_fp32.cu.
+#pragma once
+
+#include "sweep_march.cuh"
+
+namespace acfd {
+namespace ACFD_NS {
+
+constexpr long long kPlaneWaitLimit = 1LL << 22;
+
+template <int S, int NP, bool VISC, bool HYB>
+__global__ void __launch_bounds__(kPlaneMaxThreads, sizeof(Real) == sizeof(float) ? 2 : 1)
+stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_constant__ CUtensorMap map)
+{
+    static_assert(S == 1 || S == 2, "plane march along y or z");
+    constexpr int T2 = (S == 1) ? 2 : 1;
+    constexpr int H = NP / 2;
+    constexpr int hv = VISC ? 1 : 0;
+    constexpr int NS = kPlaneSlots;
+    constexpr unsigned kAll = 0xffffffffu;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int pe = pt.BXp * pt.BC;  // elements of one variable in a plane
+    const int plane_bytes = pe * 5 * 8;
+    const int slot_doubles = plane_slot_bytes(pt.BXp, pt.BC) / 8;  // 128-byte aligned slots
+    double *ring = reinterpret_cast<double *>(smem);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)NS * slot_doubles * 8);
+    uint64_t *empty = full + NS;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < NS; ++q) {
+            tma::mbar_init(full + q, 1);
+            tma::mbar_init(empty + q, pt.ncw);
+        }
+    }
+    __syncthreads();
+    pdl_wait();
+
+    int b = blockIdx.x;
+    const int tx = b % pt.ntx;
+    b /= pt.ntx;
+    const int tc = b % pt.ntc;
+    const int seg = b / pt.ntc;
+    const int Ls = g.hi[S] - g.lo[S];
+    const int x0 = g.lo[0] + tx * pt.WX;
+    const int c0 = g.lo[T2] + tc * pt.NR;
+    const int p0 = g.lo[S] + (int)((long long)seg * Ls / pt.nseg);
+    const int p1 = g.lo[S] + (int)((long long)(seg + 1) * Ls / pt.nseg);
+    const int xs = (x0 - hv) & ~1;
+    const int cs = c0 - hv;
+    const int NQ = p1 - p0 + 2 * H;  // planes p0-H .. p1+H-1
+
+    if (warp == pt.ncw) {
+        // producer: plane q (node p0-H+q along s) into slot q % NS
+        if (lane == 0) {
+            int issued = 0;
+            for (int q = 0; q < NQ; ++q) {
+                const int slot = q % NS;
+                if (q >= NS && !tma::mbar_wait_bounded(empty + slot, ((q / NS) - 1) & 1, a.status, 5,
+                                                       kPlaneWaitLimit)) {
+                    break;
+                }
+                tma::mbar_expect_tx(full + slot, plane_bytes);
+                const int pos = p0 - H + q;
+                double *dst = ring + (size_t)slot * slot_doubles;
+                if (S == 1) {
+                    tma::load_5d(dst, &map, xs, pos, cs, 0, a.tn, full + slot);
+                } else {
+                    tma::load_5d(dst, &map, xs, cs, pos, 0, a.tn, full + slot);
+                }
+                issued = q + 1;
+            }
+            // the block must not end with copies in flight
+            for (int q = issued - NS > 0 ? issued - NS : 0; q < issued; ++q) {
+                tma::mbar_wait_bounded(full + q % NS, (q / NS) & 1, a.status, 5, kPlaneWaitLimit);
+            }
+        }
+        return;
+    }
+
+    // consumer thread: line (i, c)
+    const int t = threadIdx.x;
+    const int xl = t % pt.WX, rl = t / pt.WX;
+    const int i = x0 + xl, c = c0 + rl;
+    const bool active = (rl < pt.NR) && (i < g.hi[0]) && (c < g.hi[T2]);
+    // element of (i, c) in a plane (inactive threads: the tile's first node,
+    // whose halo neighbours exist)
+    const int e0 = active ? (rl + hv) * pt.BXp + (i - xs) : hv * pt.BXp + (x0 - xs);
+    const long long nn = g.nn;
+    const long long sx = (long long)g.pitch, sz = (long long)g.pitch * g.n[1];
+    const long long st = (S == 1) ? sx : sz;
+    const long long base = (S == 1) ? (long long)c * sz + i : (long long)c * sx + i;
+    const Real cvinv = Real(1.0 / mp.cv);
+    const bool same_o = (a.Uo == a.Un);
+    const double rdt = (a.dt_scale * a.dt[0]) * g.dd[S];
+    auto plane = [&](int q) { return ring + (size_t)(q % NS) * slot_doubles; };
+    auto wait_plane = [&](int q) {
+        const bool ok = tma::mbar_wait_bounded(full + q % NS, (q / NS) & 1, a.status, 5, kPlaneWaitLimit);
+        return __all_sync(kAll, ok);
+    };
+    auto release = [&](int q) {
+        __syncwarp();
+        if (lane == 0) tma::mbar_arrive(empty + q % NS);
+    };
+    auto node_of_plane = [&](const double *P, Real w[5]) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) w[v] = Real(P[v * pe + e0]);
+    };
+    // transverse differences at the plane's node from its halo neighbours:
+    // axis 0 (x, element stride 1) and axis T2 (rows, element stride BXp)
+    auto tdiff = [&](const double *P, Real (&D)[2][2]) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int tax = q == 0 ? 0 : T2;
+            const int es = q == 0 ? 1 : pt.BXp;
+            const int ep = e0 + es, em = e0 - es;
+            const Real rp = fast::rcp<Real>(Real(P[ep])), rm = fast::rcp<Real>(Real(P[em]));
+            const Real tp = Real(P[(1 + tax) * pe + ep]), tm = Real(P[(1 + tax) * pe + em]);
+            const Real sp = Real(P[(1 + S) * pe + ep]), sm = Real(P[(1 + S) * pe + em]);
+            D[q][0] = tp * rp - tm * rm;
+            D[q][1] = sp * rp - sm * rm;
+        }
+    };
+
+    Real W[NP][5];
+#pragma unroll
+    for (int m = 0; m < NP - 1; ++m) {
+        if (!wait_plane(m)) return;
+        node_of_plane(plane(m), W[m]);
+    }
+    Real Pc[4] = {Real(0), Real(0), Real(0), Real(0)};
+    Real Dc[2][2] = {{Real(0), Real(0)}, {Real(0), Real(0)}};
+    if (VISC) {
+        march_prims(W[H - 1], cvinv, Pc);
+        tdiff(plane(H - 1), Dc);
+    }
+    for (int q = 0; q < H; ++q) {
+        release(q);  // nodes p0-H .. p0-1 have no update
+    }
+    const uint8_t *__restrict__ fl = HYB ? a.flags + (long long)S * nn : nullptr;
+    unsigned fw = 0;
+    if (HYB && active) {
+        fw = (unsigned)fl[base + (long long)(p0 - 2) * st] | ((unsigned)fl[base + (long long)(p0 - 1) * st] << 1) |
+             ((unsigned)fl[base + (long long)p0 * st] << 2);
+    }
+    Real Fl[5];
+    for (int p = p0 - 1; p < p1; ++p) {
+        const int qf = p - p0 + 2 * H;  // front node p+H
+        const int q0 = p - p0 + H;      // node p
+        const long long id = base + (long long)p * st;
+        int did = 1;
+        double uo[5];
+        if (active && p >= p0) {
+            did = a.did[id];
+            if (!same_o && !a.accumulate) {
+#pragma unroll
+                for (int v = 0; v < 5; ++v) uo[v] = a.Uo[v * nn + id];
+            }
+        }
+        bool full_w = true;
+        if (HYB) {
+            if (active) fw |= (unsigned)fl[id + 2 * st] << 3;
+            full_w = (fw != 0u);
+        }
+        if (!wait_plane(qf)) return;
+        node_of_plane(plane(qf), W[NP - 1]);
+        Real Pn[4], Dn[2][2];
+        if (VISC) {
+            march_prims(W[H], cvinv, Pn);
+            tdiff(plane(q0 + 1), Dn);
+        }
+        Real F[5];
+        march_flux<S, NP, HYB>(mp, W, full_w, F);
+        if (VISC) {
+            march_visc<S>(g, mp, Pc, Pn, Dc, Dn, F);
+        }
+        if (p >= p0) {
+            if (active && did == 0) {
+                const double *P = plane(q0);
+#pragma unroll
+                for (int v = 0; v < 5; ++v) {
+                    const double phi = double(Fl[v]) - double(F[v]);
+                    const long long qv = v * nn + id;
+                    const double un = P[v * pe + e0];
+                    if (a.accumulate) {
+                        a.Um[qv] = a.Um[qv] + a.coeB * rdt * phi;
+                    } else {
+                        a.Um[qv] = a.coeA * (same_o ? un : uo[v]) + a.coeB * (un + rdt * phi);
+                    }
+                }
+            }
+            release(q0);
+        }
+#pragma unroll
+        for (int v = 0; v < 5; ++v) Fl[v] = F[v];
+#pragma unroll
+        for (int m = 0; m < NP - 1; ++m) {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) W[m][v] = W[m + 1][v];
+        }
+        if (VISC) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) Pc[q] = Pn[q];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                Dc[q][0] = Dn[q][0];
+                Dc[q][1] = Dn[q][1];
+            }
+        }
+        fw >>= 1;
+    }
+}
+
+template <int S, int NP, bool VISC, bool HYB>
+static int launch_plane_one(const Grid &g, const ModelParams &m, const StageArgs &a, const PlaneTile &pt,
+                            const CUtensorMap &map, cudaStream_t st)
+{
+    static bool configured[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int smem = plane_smem_bytes(pt);
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(stage_plane_yz<S, NP, VISC, HYB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, kPlaneSmemMax);
+        if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(stage_plane_yz)");
+        configured[dev] = true;
+    }
+    if (smem > kPlaneSmemMax) {
+        set_error("plane tile needs %d bytes of shared memory", smem);
+        return ACFD_ERR_ARG;
+    }
+    const unsigned blocks = (unsigned)pt.ntx * pt.ntc * pt.nseg;
+    cudaError_t e = launch_k(stage_plane_yz<S, NP, VISC, HYB>, dim3(blocks), dim3((pt.ncw + 1) * 32), smem, st, g, m,
+                             a, pt, map);
+    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "stage_plane_yz launch");
+}
+
+template <int NP, bool VISC, bool HYB>
+static int launch_plane_s(const Grid &g, const ModelParams &m, const StageArgs &a, int s, const PlaneTile &pt,
+                          const CUtensorMap &map, cudaStream_t st)
+{
+    if (s == 1) return launch_plane_one<1, NP, VISC, HYB>(g, m, a, pt, map, st);
+    return launch_plane_one<2, NP, VISC, HYB>(g, m, a, pt, map, st);
+}
+
+// Y/Z sweeps only; `map` is the state map with box (BXp, 1, BC) (y sweep) or
+// (BXp, BC, 1) (z sweep), five variables, one level
+static int launch_plane_impl(const Grid &g, const ModelParams &m, const StageArgs &a, int s, bool viscous,
+                             bool hybrid, const PlaneTile &pt, const CUtensorMap &map, cudaStream_t st)
+{
+    if (g.hi[0] <= g.lo[0] || g.hi[1] <= g.lo[1] || g.hi[2] <= g.lo[2]) {
+        return ACFD_OK;
+    }
+    if (s != 1 && s != 2) {
+        set_error("plane march: sweep axis %d", s);
+        return ACFD_ERR_ARG;
+    }
+    if (m.sScheme == 1) {
+        if constexpr (sizeof(Real) == sizeof(float)) {
+            if (hybrid && a.flags) {
+                return viscous ? launch_plane_s<6, true, true>(g, m, a, s, pt, map, st)
+                               : launch_plane_s<6, false, true>(g, m, a, s, pt, map, st);
+            }
+        }
+        return viscous ? launch_plane_s<6, true, false>(g, m, a, s, pt, map, st)
+                       : launch_plane_s<6, false, false>(g, m, a, s, pt, map, st);
+    }
+    return viscous ? launch_plane_s<4, true, false>(g, m, a, s, pt, map, st)
+                   : launch_plane_s<4, false, false>(g, m, a, s, pt, map, st);
+}
+
+}  // namespace ACFD_NS
+}  // namespace acfd

@@ -55,11 +55,19 @@ class Solver:
         check(self.lib.acfd_set_stream(self.h, ctypes.c_void_p(stream_ptr) if stream_ptr else None), self.lib)
 
     def autotune(self):
-        """Pick the fastest compiled tile shape per sweep axis on this case
-        (acfd_autotune); returns the chosen variant per axis."""
+        """Pick the fastest stage-kernel variant per sweep axis on this case
+        for the current arithmetic form (acfd_autotune); returns the chosen
+        variant per axis."""
         t = (ctypes.c_int * 3)()
         check(self.lib.acfd_autotune(self.h, t), self.lib)
         return list(t)
+
+    def set_tiles(self, tiles):
+        """Select the stage-kernel variant per sweep axis for the current
+        arithmetic form (acfd_set_tiles): below BRICK_VARIANTS the brick
+        kernels, from there the line-march kernels."""
+        t = (ctypes.c_int * 3)(*[int(v) for v in tiles])
+        check(self.lib.acfd_set_tiles(self.h, t), self.lib)
 
     # learned sensor -------------------------------------------------------
     def sensor_load(self, params: np.ndarray, threshold: float):

@@ -160,11 +160,26 @@ int acfd_set_precision(acfd_case_t *cs, int mode);
 /* Wait for all work queued on the case and report device-side errors (the
  * per-step wall clock of solve.c:81,89 needs a finished step). */
 int acfd_synchronize(acfd_case_t *cs);
-/* Tile autotuner (no reference counterpart): times the compiled tile shapes
- * of the stage kernel of each sweep axis on this case's current state (RK
- * stage 1, which writes only U[TN]) and keeps the fastest; tiles[3]
- * (optional) receives the chosen variant per axis. */
+/* Stage-kernel variants of the fast forms (no reference counterpart):
+ * 0 .. ACFD_BRICK_VARIANTS-1 are the shared-memory brick kernels with their
+ * tile shapes; the next three the line-march kernels launched with 1, 2 or 4
+ * waves of resident warps; ACFD_PLANE_VARIANT .. ACFD_STAGE_VARIANTS-1 the
+ * plane-march kernels (Y and Z sweeps; an X sweep given one of these uses the
+ * line march) with 1, 2 or 4 waves of blocks.  The choice is kept per
+ * arithmetic form; the FP32 forms start on the brick for X and the first
+ * plane variant for Y and Z, the FP64 form on the first brick. */
+#define ACFD_BRICK_VARIANTS 2
+#define ACFD_PLANE_VARIANT 5
+#define ACFD_STAGE_VARIANTS 8
+/* Tile autotuner: times every stage-kernel variant of each sweep axis on this
+ * case's current state (RK stage 2, reading U[TO] and U[TN] and writing
+ * U[TM], after a stage 1 into U[TN]; both are overwritten by every step) for
+ * the current arithmetic form and keeps the fastest; tiles[3] (optional)
+ * receives the chosen variant per axis. */
 int acfd_autotune(acfd_case_t *cs, int tiles[3]);
+/* Select the stage-kernel variant of each sweep axis for the current
+ * arithmetic form (tests and experiments; acfd_autotune picks by timing). */
+int acfd_set_tiles(acfd_case_t *cs, const int tiles[3]);
 /* Number of kernels this case has launched so far (graph replays count their
  * kernel nodes).  No reference counterpart: instrumentation (the reference
  * only times whole steps, timer.c:22-35). */

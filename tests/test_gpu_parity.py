@@ -145,6 +145,29 @@ def test_fused_ghost_fill_equals_phase_launches(name, monkeypatch):
         assert np.array_equal(a, c)
 
 
+@pytest.mark.parametrize("name", ["tgv", "sod", "tgv_weno3_rk2"])
+def test_gather_ghost_fill_equals_phase_launches(name, monkeypatch):
+    """Copy-only cases (periodic and outflow faces) fill their ghosts with one
+    gather launch built from a replay of the ordered fill on node indices;
+    it gives the same bits as the ordered per-phase launches."""
+    b = golden_io.Bundle(name)
+    outs = []
+    for phases in (True, False):
+        if phases:
+            monkeypatch.setenv("ACFD_BC_PHASES", "1")
+        else:
+            monkeypatch.delenv("ACFD_BC_PHASES", raising=False)
+        o, _ = gpu_run(b, abi.FP64, 2, dts=list(b.dt))
+        outs.append(o)
+    for a, c in zip(*outs):
+        assert np.array_equal(a, c)
+    with Solver(b.part, b.model, abi.FP64) as s:
+        s.upload(b.initial_nodes())
+        n0 = s.launches()
+        s.treat_boundary(abi.TO)
+        assert s.launches() - n0 == 1
+
+
 @pytest.mark.parametrize("s_dir", [0, 1, 2])
 def test_single_stage_lllu(s_dir, orc):
     b = golden_io.Bundle("channel")
