@@ -74,8 +74,8 @@ bool pdl_enabled()
 }
 
 // Stage-kernel variants: the brick tile shapes (0 .. kTileVariants-1), the
-// line-march kernels and the plane-march kernels (Y/Z sweeps; X sweeps of a
-// plane variant use the line march), each launched with 1, 2 or 4 waves
+// line-march kernels and the plane-march kernels, each launched with 1, 2 or
+// 4 waves
 constexpr int kMarchVariants = 3;
 constexpr int kMarchWaves[kMarchVariants] = {1, 2, 4};
 constexpr int kPlaneVariants = 3;
@@ -126,10 +126,11 @@ struct acfd_case {
     // acfd_set_tiles): brick tile shapes, then line-march launch sizes
     int tile_var[4][3] = {{0, 0, 0},
                           {0, 0, 0},
-                          {0, kPlaneFirst, kPlaneFirst},
-                          {0, kPlaneFirst, kPlaneFirst}};
+                          {0, kPlaneFirst + 2, kPlaneFirst + 2},
+                          {0, kPlaneFirst + 2, kPlaneFirst + 2}};
     int sms = 148;                 // SM count of the case's device
-    CUtensorMap pmaps[3];          // plane-march state maps (Y and Z sweeps)
+    CUtensorMap pmaps[3];          // plane-march state maps per sweep axis
+    int pbox[3][2] = {{0, 0}, {0, 0}, {0, 0}};  // their box: x extent and rows
     bool pmaps_ok = false;
     bool plain_kernels = false;    // use the global-memory stage kernels instead of the bricks
     bool bc_multi = false;         // one launch per ghost-fill phase instead of the fused launch
@@ -192,10 +193,14 @@ int encode_state_maps(acfd_case *cs)
     }
     cs->maps_ok = true;
     // plane-march maps: one plane of the tile with its halo, five variables
-    for (int s = 1; s < 3; ++s) {
+    for (int s = 0; s < 3; ++s) {
         const PlaneTile pt = plane_tile(g, s, viscous(cs), 1, cs->sms);
-        const cuuint32_t box[5] = {(cuuint32_t)pt.BXp, (cuuint32_t)(s == 1 ? 1 : pt.BC),
+        // X and Y sweeps load a y-plane (rows along z), Z sweeps a z-plane
+        // (rows along y)
+        const cuuint32_t box[5] = {(cuuint32_t)pt.BXp, (cuuint32_t)(s == 2 ? pt.BC : 1),
                                    (cuuint32_t)(s == 2 ? 1 : pt.BC), 5, 1};
+        cs->pbox[s][0] = pt.BXp;
+        cs->pbox[s][1] = pt.BC;
         if (pt.BXp > 256 || pt.BC > 256) {
             return ACFD_OK;  // no plane maps for this grid
         }
@@ -442,7 +447,7 @@ int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int 
         int st;
         const int var = cs->tile_var[cs->mode][s];
         const bool plane_v = !cs->plain_kernels && var >= kPlaneFirst && var < kStageVariants;
-        const bool plane = plane_v && s != 0 && cs->pmaps_ok;
+        const bool plane = plane_v && cs->pmaps_ok;
         const bool march = !cs->plain_kernels && !plane && var >= kTileVariants && var < kStageVariants;
         const bool brick = !march && !plane && cs->maps_ok && !cs->plain_kernels;
         // march launch size: waves x SMs x resident warps per SM (two blocks of
@@ -452,6 +457,11 @@ int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int 
         PlaneTile pt = {};
         if (plane) {
             pt = plane_tile(cs->grid, s, visc, waves, cs->sms);
+            if (pt.BXp != cs->pbox[s][0] || pt.BC != cs->pbox[s][1]) {
+                set_error("plane tile (%d x %d) does not match the encoded box (%d x %d) of axis %d", pt.BXp, pt.BC,
+                          cs->pbox[s][0], cs->pbox[s][1], s);
+                return ACFD_ERR_STATE;
+            }
         }
         switch (cs->mode) {
             case ACFD_FP64_EXACT: st = launch_stage_exact(cs->grid, cs->mp, a, s, visc, cs->stream); break;

@@ -89,37 +89,52 @@ __host__ __device__ inline int plane_slot_bytes(int BXp, int BC)
     return (BXp * BC * 5 * 8 + 127) & ~127;
 }
 
+// shared memory of a plane-march block: the ring, the X sweep's double-
+// buffered interface fluxes (nflux interfaces, five values of at most 8
+// bytes) and the full/empty barriers
+__host__ __device__ inline int plane_smem_total(int BXp, int BC, int nflux)
+{
+    return kPlaneSlots * plane_slot_bytes(BXp, BC) + ((2 * nflux * 5 * 8 + 127) & ~127) + 2 * kPlaneSlots * 8;
+}
+
 struct PlaneTile {
-    int WX, NR;    // tile: x extent and rows of the other transverse axis
+    int WX, NR;    // tile: nodes updated along x and rows of the row axis
+    int TR;        // consumer threads per row (WX; WX + 1 interfaces on X sweeps)
     int ntx, ntc;  // tiles along x and along the rows
-    int nseg;      // segments along the sweep axis
+    int nseg;      // segments along the march axis
     int BXp, BC;   // plane box: x extent (even, covers the x halo) and rows with halo
     int ncw;       // consumer warps (the producer is warp ncw)
+    int swap;      // Y/Z kernel: 1 = a Z sweep run with axes 1 and 2 exchanged
+    long long st, rs;  // Y/Z kernel: node strides along the line and along the rows
 };
 
-// tile geometry of the plane march along s (1 or 2); `waves` scales the
-// number of blocks (segments along s, each at least 8 planes long)
+// Tile geometry of the plane march of sweep s.  Y and Z sweeps march along s
+// with rows along the other transverse axis; X sweeps march along y with rows
+// along z and an x halo of three nodes (the WENO5 stencil).  `waves` scales
+// the number of blocks (segments of the march axis, each at least 8 planes).
 inline PlaneTile plane_tile(const Grid &g, int s, bool visc, int waves, int sms)
 {
-    PlaneTile pt;
-    const int T2 = (s == 1) ? 2 : 1;
-    const int Lx = g.hi[0] - g.lo[0], Lt = g.hi[T2] - g.lo[T2], Ls = g.hi[s] - g.lo[s];
+    PlaneTile pt = {};
+    const int T2 = (s == 1) ? 2 : (s == 2 ? 1 : 2);  // row axis
+    const int M = (s == 0) ? 1 : s;                    // march axis
+    const int Lx = g.hi[0] - g.lo[0], Lt = g.hi[T2] - g.lo[T2], Ls = g.hi[M] - g.lo[M];
     const int hv = visc ? 1 : 0;
+    const int hx = (s == 0) ? 3 : hv;  // x halo
     pt.ntx = (Lx + 63) / 64;
     if (pt.ntx < 1) pt.ntx = 1;
     pt.WX = (Lx + pt.ntx - 1) / pt.ntx;
     if (pt.WX < 1) pt.WX = 1;
-    pt.NR = (kPlaneMaxThreads - 32) / pt.WX;
+    pt.TR = (s == 0) ? pt.WX + 1 : pt.WX;
+    pt.NR = (kPlaneMaxThreads - 32) / pt.TR;
     if (pt.NR > Lt) pt.NR = Lt;
     if (pt.NR < 1) pt.NR = 1;
-    pt.ntc = (Lt + pt.NR - 1) / pt.NR;
-    pt.BXp = (pt.WX + 2 * hv + 2) & ~1;
-    // the ring of kPlaneSlots planes must fit the shared-memory budget
-    while (pt.NR > 1 && kPlaneSlots * plane_slot_bytes(pt.BXp, pt.NR + 2 * hv) + 2 * kPlaneSlots * 8 > kPlaneSmemMax) {
+    pt.BXp = (pt.WX + 2 * hx + 2) & ~1;
+    // the ring of kPlaneSlots planes (and the X sweep's flux exchange) must fit
+    while (pt.NR > 1 && plane_smem_total(pt.BXp, pt.NR + 2 * hv, s == 0 ? pt.TR * pt.NR : 0) > kPlaneSmemMax) {
         --pt.NR;
     }
     pt.ntc = (Lt + pt.NR - 1) / pt.NR;
-    pt.ncw = (pt.WX * pt.NR + 31) / 32;
+    pt.ncw = (pt.TR * pt.NR + 31) / 32;
     pt.BC = pt.NR + 2 * hv;
     const long long tiles = (long long)pt.ntx * pt.ntc;
     const long long target = (long long)waves * 2 * sms;
@@ -131,9 +146,9 @@ inline PlaneTile plane_tile(const Grid &g, int s, bool visc, int waves, int sms)
     return pt;
 }
 
-inline int plane_smem_bytes(const PlaneTile &pt)
+inline int plane_smem_bytes(const PlaneTile &pt, int s)
 {
-    return kPlaneSlots * plane_slot_bytes(pt.BXp, pt.BC) + 2 * kPlaneSlots * 8;
+    return plane_smem_total(pt.BXp, pt.BC, s == 0 ? pt.TR * pt.NR : 0);
 }
 
 // learned sensor (sensor.cu)

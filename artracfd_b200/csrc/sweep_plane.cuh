@@ -1,6 +1,6 @@
-// Plane-march stage kernels (fast FP64, FP32 and hybrid forms), Y and Z
-// sweeps.
+// Plane-march stage kernels (fast FP64, FP32 and hybrid forms).
 //
+// Y and Z sweeps:
 // A block owns a tile of grid lines along the sweep axis s: WX consecutive x
 // by NR consecutive rows of the other transverse axis, over one segment of
 // the line.  It walks the segment plane by plane:
@@ -19,6 +19,8 @@
 // Included after sweep_march.cuh by sweep_fast.cu and sweep_fp32.cu.
 #pragma once
 
+#include <utility>
+
 #include "sweep_march.cuh"
 
 namespace acfd {
@@ -26,12 +28,18 @@ namespace ACFD_NS {
 
 constexpr long long kPlaneWaitLimit = 1LL << 22;
 
-template <int S, int NP, bool VISC, bool HYB>
+// One instantiation serves both axes: the kernel is written for the Y sweep
+// (S = 1, rows along z).  A Z sweep runs it on a grid descriptor with axes 1
+// and 2 exchanged (pt.swap = 1): the line and row strides come from pt, the
+// momentum components rho*v and rho*w trade places in every read of the
+// planes and of U[to] and in every write of U[tm], and the TMA coordinates of
+// a plane are (x, row, position) instead of (x, position, row).
+template <int NP, bool VISC, bool HYB>
 __global__ void __launch_bounds__(kPlaneMaxThreads, sizeof(Real) == sizeof(float) ? 2 : 1)
 stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_constant__ CUtensorMap map)
 {
-    static_assert(S == 1 || S == 2, "plane march along y or z");
-    constexpr int T2 = (S == 1) ? 2 : 1;
+    constexpr int S = 1;
+    constexpr int T2 = 2;
     constexpr int H = NP / 2;
     constexpr int hv = VISC ? 1 : 0;
     constexpr int NS = kPlaneSlots;
@@ -80,7 +88,7 @@ stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_c
                 tma::mbar_expect_tx(full + slot, plane_bytes);
                 const int pos = p0 - H + q;
                 double *dst = ring + (size_t)slot * slot_doubles;
-                if (S == 1) {
+                if (!pt.swap) {
                     tma::load_5d(dst, &map, xs, pos, cs, 0, a.tn, full + slot);
                 } else {
                     tma::load_5d(dst, &map, xs, cs, pos, 0, a.tn, full + slot);
@@ -104,9 +112,11 @@ stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_c
     // whose halo neighbours exist)
     const int e0 = active ? (rl + hv) * pt.BXp + (i - xs) : hv * pt.BXp + (x0 - xs);
     const long long nn = g.nn;
-    const long long sx = (long long)g.pitch, sz = (long long)g.pitch * g.n[1];
-    const long long st = (S == 1) ? sx : sz;
-    const long long base = (S == 1) ? (long long)c * sz + i : (long long)c * sx + i;
+    const long long st = pt.st;                      // node stride along the line
+    const long long base = (long long)c * pt.rs + i;  // node (i, c) at position 0
+    // variable v of the kernel's frame is variable vg(v) of the state
+    const int o2 = pt.swap ? 3 : 2, o3 = pt.swap ? 2 : 3;
+    auto vg = [&](int v) { return v == 2 ? o2 : (v == 3 ? o3 : v); };
     const Real cvinv = Real(1.0 / mp.cv);
     const bool same_o = (a.Uo == a.Un);
     const double rdt = (a.dt_scale * a.dt[0]) * g.dd[S];
@@ -121,7 +131,7 @@ stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_c
     };
     auto node_of_plane = [&](const double *P, Real w[5]) {
 #pragma unroll
-        for (int v = 0; v < 5; ++v) w[v] = Real(P[v * pe + e0]);
+        for (int v = 0; v < 5; ++v) w[v] = Real(P[vg(v) * pe + e0]);
     };
     // transverse differences at the plane's node from its halo neighbours:
     // axis 0 (x, element stride 1) and axis T2 (rows, element stride BXp)
@@ -132,8 +142,9 @@ stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_c
             const int es = q == 0 ? 1 : pt.BXp;
             const int ep = e0 + es, em = e0 - es;
             const Real rp = fast::rcp<Real>(Real(P[ep])), rm = fast::rcp<Real>(Real(P[em]));
-            const Real tp = Real(P[(1 + tax) * pe + ep]), tm = Real(P[(1 + tax) * pe + em]);
-            const Real sp = Real(P[(1 + S) * pe + ep]), sm = Real(P[(1 + S) * pe + em]);
+            const int ot = vg(1 + tax) * pe, os = vg(1 + S) * pe;
+            const Real tp = Real(P[ot + ep]), tm = Real(P[ot + em]);
+            const Real sp = Real(P[os + ep]), sm = Real(P[os + em]);
             D[q][0] = tp * rp - tm * rm;
             D[q][1] = sp * rp - sm * rm;
         }
@@ -154,7 +165,7 @@ stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_c
     for (int q = 0; q < H; ++q) {
         release(q);  // nodes p0-H .. p0-1 have no update
     }
-    const uint8_t *__restrict__ fl = HYB ? a.flags + (long long)S * nn : nullptr;
+    const uint8_t *__restrict__ fl = HYB ? a.flags + (long long)(pt.swap ? 2 : 1) * nn : nullptr;
     unsigned fw = 0;
     if (HYB && active) {
         fw = (unsigned)fl[base + (long long)(p0 - 2) * st] | ((unsigned)fl[base + (long long)(p0 - 1) * st] << 1) |
@@ -171,7 +182,7 @@ stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_c
             did = a.did[id];
             if (!same_o && !a.accumulate) {
 #pragma unroll
-                for (int v = 0; v < 5; ++v) uo[v] = a.Uo[v * nn + id];
+                for (int v = 0; v < 5; ++v) uo[v] = a.Uo[vg(v) * nn + id];
             }
         }
         bool full_w = true;
@@ -197,8 +208,8 @@ stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_c
 #pragma unroll
                 for (int v = 0; v < 5; ++v) {
                     const double phi = double(Fl[v]) - double(F[v]);
-                    const long long qv = v * nn + id;
-                    const double un = P[v * pe + e0];
+                    const long long qv = vg(v) * nn + id;
+                    const double un = P[vg(v) * pe + e0];
                     if (a.accumulate) {
                         a.Um[qv] = a.Um[qv] + a.coeB * rdt * phi;
                     } else {
@@ -228,16 +239,237 @@ stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_c
     }
 }
 
-template <int S, int NP, bool VISC, bool HYB>
-static int launch_plane_one(const Grid &g, const ModelParams &m, const StageArgs &a, const PlaneTile &pt,
-                            const CUtensorMap &map, cudaStream_t st)
+// ---------------------------------------------------------------------------
+// X sweep: the block marches along y over a tile of WX nodes along x by NR
+// z-rows.  Each consumer thread owns one interface of its row (WX + 1 per
+// row, the first one only feeds its right neighbour): the x stencil comes
+// from the plane in shared memory (x halo of three nodes), the viscous
+// y differences from the neighbouring planes of the ring and the z
+// differences from the neighbouring rows of the plane.  Interface fluxes go
+// to the node on their right through a double-buffered shared array, one
+// named barrier of the consumer warps per plane.
+// ---------------------------------------------------------------------------
+template <int NP, bool VISC, bool HYB>
+__global__ void __launch_bounds__(kPlaneMaxThreads, sizeof(Real) == sizeof(float) ? 2 : 1)
+stage_plane_x(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_constant__ CUtensorMap map)
+{
+    constexpr int H = NP / 2;
+    constexpr int hv = VISC ? 1 : 0;
+    constexpr int NS = kPlaneSlots;
+    constexpr unsigned kAll = 0xffffffffu;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int pe = pt.BXp * pt.BC;
+    const int plane_bytes = pe * 5 * 8;
+    const int slot_doubles = plane_slot_bytes(pt.BXp, pt.BC) / 8;
+    const int nflux = pt.TR * pt.NR;
+    double *ring = reinterpret_cast<double *>(smem);
+    Real *sF = reinterpret_cast<Real *>(smem + (size_t)NS * slot_doubles * 8);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)NS * slot_doubles * 8 +
+                                                  ((2 * nflux * 5 * 8 + 127) & ~127));
+    uint64_t *empty = full + NS;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < NS; ++q) {
+            tma::mbar_init(full + q, 1);
+            tma::mbar_init(empty + q, pt.ncw);
+        }
+    }
+    __syncthreads();
+    pdl_wait();
+
+    int b = blockIdx.x;
+    const int tx = b % pt.ntx;
+    b /= pt.ntx;
+    const int tc = b % pt.ntc;
+    const int seg = b / pt.ntc;
+    const int Ly = g.hi[1] - g.lo[1];
+    const int x0 = g.lo[0] + tx * pt.WX;
+    const int c0 = g.lo[2] + tc * pt.NR;
+    const int j0 = g.lo[1] + (int)((long long)seg * Ly / pt.nseg);
+    const int j1 = g.lo[1] + (int)((long long)(seg + 1) * Ly / pt.nseg);
+    const int xs = (x0 - H) & ~1;
+    const int cs = c0 - hv;
+    const int NQ = j1 - j0 + 2 * hv;  // rows j0-hv .. j1-1+hv
+
+    if (warp == pt.ncw) {
+        if (lane == 0) {
+            int issued = 0;
+            for (int q = 0; q < NQ; ++q) {
+                const int slot = q % NS;
+                if (q >= NS && !tma::mbar_wait_bounded(empty + slot, ((q / NS) - 1) & 1, a.status, 5,
+                                                       kPlaneWaitLimit)) {
+                    break;
+                }
+                tma::mbar_expect_tx(full + slot, plane_bytes);
+                tma::load_5d(ring + (size_t)slot * slot_doubles, &map, xs, j0 - hv + q, cs, 0, a.tn, full + slot);
+                issued = q + 1;
+            }
+            for (int q = issued - NS > 0 ? issued - NS : 0; q < issued; ++q) {
+                tma::mbar_wait_bounded(full + q % NS, (q / NS) & 1, a.status, 5, kPlaneWaitLimit);
+            }
+        }
+        return;
+    }
+
+    // consumer thread: interface xi+1/2 of z-row c
+    const int t = threadIdx.x;
+    const int xl = t % pt.TR, rl = t / pt.TR;
+    const int xi = x0 - 1 + xl;
+    const int c = c0 + rl;
+    const bool row_ok = (rl < pt.NR) && (c < g.hi[2]);
+    const bool active = row_ok && (xi < g.hi[0]);          // interface computed
+    const bool upd = active && xl >= 1;                      // node xi updated
+    // element of node xi in a plane (inactive threads: the tile's first node)
+    const int e0 = active ? (rl + hv) * pt.BXp + (xi - xs) : hv * pt.BXp + (x0 - xs);
+    const long long nn = g.nn;
+    const long long sy = (long long)g.pitch, sz = (long long)g.pitch * g.n[1];
+    const long long xz = (long long)c * sz + xi;
+    const Real cvinv = Real(1.0 / mp.cv);
+    const bool same_o = (a.Uo == a.Un);
+    const double rdt = (a.dt_scale * a.dt[0]) * g.dd[0];
+    const uint8_t *__restrict__ fl = a.flags;  // sweep 0 flags
+    auto plane = [&](int q) { return ring + (size_t)(q % NS) * slot_doubles; };
+    auto wait_plane = [&](int q) {
+        const bool ok = tma::mbar_wait_bounded(full + q % NS, (q / NS) & 1, a.status, 5, kPlaneWaitLimit);
+        return __all_sync(kAll, ok);
+    };
+    auto release = [&](int q) {
+        __syncwarp();
+        if (lane == 0) tma::mbar_arrive(empty + q % NS);
+    };
+    const unsigned nbar = (unsigned)pt.ncw * 32u;
+    // the consumer warps leave together: a wait that gave up is or-reduced
+    // over the named barrier of the flux exchange
+    auto exchange_barrier = [&](bool abort) {
+        unsigned any;
+        asm volatile(
+            "{\n\t.reg .pred p, q;\n\t"
+            "setp.ne.u32 q, %1, 0;\n\t"
+            "bar.red.or.pred p, 1, %2, q;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(any)
+            : "r"((unsigned)abort), "r"(nbar)
+            : "memory");
+        return any != 0u;
+    };
+
+    bool ok = true;
+    for (int q = 0; q < 2 * hv; ++q) {
+        ok = ok && wait_plane(q);  // rows j0-1 and j0 (viscous)
+    }
+    int buf = 0;
+    for (int j = j0; j < j1; ++j) {
+        const int q = j - j0 + hv;  // plane of row j
+        const long long id = xz + (long long)j * sy;
+        int did = 1;
+        double uo[5];
+        if (upd) {
+            did = a.did[id];
+            if (!same_o && !a.accumulate) {
+#pragma unroll
+                for (int v = 0; v < 5; ++v) uo[v] = a.Uo[v * nn + id];
+            }
+        }
+        bool full_w = true;
+        if (HYB && active) {
+            full_w = (fl[id - 1] | fl[id] | fl[id + 1] | fl[id + 2]) != 0;
+        }
+        ok = ok && wait_plane(q + hv);  // row j+1 (viscous) or j
+        const double *P = plane(ok ? q : 0);
+        Real W[NP][5];
+#pragma unroll
+        for (int m = 0; m < NP; ++m) {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) W[m][v] = Real(P[v * pe + e0 - (H - 1) + m]);
+        }
+        Real F[5];
+        march_flux<0, NP, HYB>(mp, W, full_w, F);
+        if (VISC) {
+            Real Pc[4], Pn[4], Dc[2][2], Dn[2][2];
+            march_prims(W[H - 1], cvinv, Pc);
+            march_prims(W[H], cvinv, Pn);
+            const double *Pm = plane(q - 1), *Pp = plane(q + 1);
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                const int e = e0 + side;
+                Real(&D)[2][2] = side ? Dn : Dc;
+                // y: planes j+1 and j-1 (v and u)
+                {
+                    const Real rp = fast::rcp<Real>(Real(Pp[e])), rm = fast::rcp<Real>(Real(Pm[e]));
+                    D[0][0] = Real(Pp[2 * pe + e]) * rp - Real(Pm[2 * pe + e]) * rm;
+                    D[0][1] = Real(Pp[pe + e]) * rp - Real(Pm[pe + e]) * rm;
+                }
+                // z: rows c+1 and c-1 of plane j (w and u)
+                {
+                    const int ep = e + pt.BXp, em = e - pt.BXp;
+                    const Real rp = fast::rcp<Real>(Real(P[ep])), rm = fast::rcp<Real>(Real(P[em]));
+                    D[1][0] = Real(P[3 * pe + ep]) * rp - Real(P[3 * pe + em]) * rm;
+                    D[1][1] = Real(P[pe + ep]) * rp - Real(P[pe + em]) * rm;
+                }
+            }
+            march_visc<0>(g, mp, Pc, Pn, Dc, Dn, F);
+        }
+        Real *sFb = sF + (size_t)buf * nflux * 5;
+        if (active) {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) sFb[v * nflux + t] = F[v];
+        }
+        if (exchange_barrier(!ok)) {
+            break;
+        }
+        if (upd && did == 0) {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                const double phi = double(sFb[v * nflux + t - 1]) - double(F[v]);
+                const long long qv = v * nn + id;
+                const double un = P[v * pe + e0];
+                if (a.accumulate) {
+                    a.Um[qv] = a.Um[qv] + a.coeB * rdt * phi;
+                } else {
+                    a.Um[qv] = a.coeA * (same_o ? un : uo[v]) + a.coeB * (un + rdt * phi);
+                }
+            }
+        }
+        // the plane of row j-1 (viscous) or j is read for the last time
+        release(q - hv);
+        buf ^= 1;
+    }
+}
+
+template <int NP, bool VISC, bool HYB>
+static int launch_plane_x(const Grid &g, const ModelParams &m, const StageArgs &a, const PlaneTile &pt,
+                          const CUtensorMap &map, cudaStream_t st)
 {
     static bool configured[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
-    const int smem = plane_smem_bytes(pt);
+    const int smem = plane_smem_bytes(pt, 0);
     if (dev >= 0 && dev < 64 && !configured[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(stage_plane_yz<S, NP, VISC, HYB>,
+        cudaError_t e = cudaFuncSetAttribute(stage_plane_x<NP, VISC, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             kPlaneSmemMax);
+        if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(stage_plane_x)");
+        configured[dev] = true;
+    }
+    if (smem > kPlaneSmemMax) {
+        set_error("plane tile needs %d bytes of shared memory", smem);
+        return ACFD_ERR_ARG;
+    }
+    const unsigned blocks = (unsigned)pt.ntx * pt.ntc * pt.nseg;
+    cudaError_t e = launch_k(stage_plane_x<NP, VISC, HYB>, dim3(blocks), dim3((pt.ncw + 1) * 32), smem, st, g, m, a,
+                             pt, map);
+    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "stage_plane_x launch");
+}
+
+template <int NP, bool VISC, bool HYB>
+static int launch_plane_yz(const Grid &g, const ModelParams &m, const StageArgs &a, int s, const PlaneTile &pt0,
+                           const CUtensorMap &map, cudaStream_t st)
+{
+    static bool configured[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int smem = plane_smem_bytes(pt0, s);
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(stage_plane_yz<NP, VISC, HYB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, kPlaneSmemMax);
         if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(stage_plane_yz)");
         configured[dev] = true;
@@ -246,9 +478,26 @@ static int launch_plane_one(const Grid &g, const ModelParams &m, const StageArgs
         set_error("plane tile needs %d bytes of shared memory", smem);
         return ACFD_ERR_ARG;
     }
+    PlaneTile pt = pt0;
+    Grid gk = g;
+    const long long sy = (long long)g.pitch, sz = (long long)g.pitch * g.n[1];
+    if (s == 1) {
+        pt.swap = 0;
+        pt.st = sy;
+        pt.rs = sz;
+    } else {
+        // the Z sweep as a Y sweep of the grid with axes 1 and 2 exchanged
+        pt.swap = 1;
+        pt.st = sz;
+        pt.rs = sy;
+        std::swap(gk.n[1], gk.n[2]);
+        std::swap(gk.lo[1], gk.lo[2]);
+        std::swap(gk.hi[1], gk.hi[2]);
+        std::swap(gk.dd[1], gk.dd[2]);
+    }
     const unsigned blocks = (unsigned)pt.ntx * pt.ntc * pt.nseg;
-    cudaError_t e = launch_k(stage_plane_yz<S, NP, VISC, HYB>, dim3(blocks), dim3((pt.ncw + 1) * 32), smem, st, g, m,
-                             a, pt, map);
+    cudaError_t e = launch_k(stage_plane_yz<NP, VISC, HYB>, dim3(blocks), dim3((pt.ncw + 1) * 32), smem, st, gk, m, a,
+                             pt, map);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "stage_plane_yz launch");
 }
 
@@ -256,21 +505,17 @@ template <int NP, bool VISC, bool HYB>
 static int launch_plane_s(const Grid &g, const ModelParams &m, const StageArgs &a, int s, const PlaneTile &pt,
                           const CUtensorMap &map, cudaStream_t st)
 {
-    if (s == 1) return launch_plane_one<1, NP, VISC, HYB>(g, m, a, pt, map, st);
-    return launch_plane_one<2, NP, VISC, HYB>(g, m, a, pt, map, st);
+    if (s == 0) return launch_plane_x<NP, VISC, HYB>(g, m, a, pt, map, st);
+    return launch_plane_yz<NP, VISC, HYB>(g, m, a, s, pt, map, st);
 }
 
-// Y/Z sweeps only; `map` is the state map with box (BXp, 1, BC) (y sweep) or
-// (BXp, BC, 1) (z sweep), five variables, one level
+// `map` is the state map with box (BXp, 1, BC) (X and Y sweeps) or
+// (BXp, BC, 1) (Z sweep), five variables, one level
 static int launch_plane_impl(const Grid &g, const ModelParams &m, const StageArgs &a, int s, bool viscous,
                              bool hybrid, const PlaneTile &pt, const CUtensorMap &map, cudaStream_t st)
 {
     if (g.hi[0] <= g.lo[0] || g.hi[1] <= g.lo[1] || g.hi[2] <= g.lo[2]) {
         return ACFD_OK;
-    }
-    if (s != 1 && s != 2) {
-        set_error("plane march: sweep axis %d", s);
-        return ACFD_ERR_ARG;
     }
     if (m.sScheme == 1) {
         if constexpr (sizeof(Real) == sizeof(float)) {

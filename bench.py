@@ -46,7 +46,8 @@ STAGE_BYTES = (80.0, 120.0, 120.0)
 def profiled_traffic(mode: str):
     """DRAM bytes per stage launch from the committed ncu summary of the
     stage kernels (mean over the captured X and Y/Z launches), or None."""
-    name = {"fp64": "stage_sweep_fp64_tgv128.md", "fp32": "stage_sweep_fp32_tgv128.md"}.get(mode)
+    name = {"fp64": "stage_sweep_fp64_tgv128.md", "fp32": "stage_sweep_fp32_tgv128.md",
+            "hybrid": "stage_sweep_hybrid_tgv128.md"}.get(mode)
     if not name:
         return None
     p = os.path.join(ROOT, "profiles", name)
@@ -183,6 +184,8 @@ def cpu_baseline_reference(n: int, steps: int = 1, procs: int = 1):
 
 
 FORMS = {"fp64": "FP64", "fp64_exact": "FP64_EXACT", "fp32": "FP32_BULK", "hybrid": "FP64"}
+# arithmetic-form codes of the C ABI (ACFD_FP64_EXACT .. ACFD_FP32_HYBRID) -> bench names
+FORM_NAMES = {0: "fp64_exact", 1: "fp64", 2: "fp32", 3: "hybrid"}
 DTYPES = {"fp64": "f64", "fp64_exact": "f64", "fp32": "f32/f64", "hybrid": "f32/f64"}
 
 
@@ -213,12 +216,16 @@ def _timed_steps(torch, s, spec, steps, warmup, dist, stream, clock_index):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     launches0 = s.launches()
+    # NVTX range of the timed steps (an ncu launch list can be limited to it
+    # with --nvtx --nvtx-include "timed_<form>/")
+    torch.cuda.nvtx.range_push("timed_" + FORM_NAMES.get(s.mode, "form"))
     with ClockSampler(clock_index) as clk:
         e0.record(stream)
         for _ in range(steps):
             step()
         e1.record(stream)
         e1.synchronize()
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     sec = e0.elapsed_time(e1) / 1e3
     if dist:

@@ -164,10 +164,10 @@ int acfd_synchronize(acfd_case_t *cs);
  * 0 .. ACFD_BRICK_VARIANTS-1 are the shared-memory brick kernels with their
  * tile shapes; the next three the line-march kernels launched with 1, 2 or 4
  * waves of resident warps; ACFD_PLANE_VARIANT .. ACFD_STAGE_VARIANTS-1 the
- * plane-march kernels (Y and Z sweeps; an X sweep given one of these uses the
- * line march) with 1, 2 or 4 waves of blocks.  The choice is kept per
- * arithmetic form; the FP32 forms start on the brick for X and the first
- * plane variant for Y and Z, the FP64 form on the first brick. */
+ * plane-march kernels (a TMA ring of halo'd planes) with 1, 2 or 4 waves of
+ * blocks.  The choice is kept per arithmetic form; the FP32 forms start on the
+ * brick for X and the 4-wave plane march for Y and Z, the FP64 form on the
+ * first brick; acfd_autotune replaces these with the measured fastest. */
 #define ACFD_BRICK_VARIANTS 2
 #define ACFD_PLANE_VARIANT 5
 #define ACFD_STAGE_VARIANTS 8
