@@ -191,6 +191,14 @@ def load_library(path: str | None = None):
         "acfd_treat_ib": [vp, i],
         "acfd_weno_batch": [i, i, vp, vp, i],
         "acfd_fhat_batch": [ctypes.POINTER(Model), i, i, vp, vp, i],
+        "acfd_batch_init": [i, ctypes.POINTER(Partition), ctypes.POINTER(Model), pp],
+        "acfd_batch_finalize": [vp],
+        "acfd_batch_case": [vp, i, pp],
+        "acfd_batch_set_precision": [vp, i],
+        "acfd_batch_sensor_load": [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_float],
+        "acfd_batch_advance": [vp, dp, i, dp],
+        "acfd_batch_stats": [vp, ctypes.POINTER(ctypes.c_longlong)],
+        "acfd_batch_set_stream": [vp, vp],
     }
     for name, args in sigs.items():
         fn = getattr(lib, name)

@@ -116,3 +116,57 @@ def shock_cylinder(m=(1024, 512, 4), stepN=100, segments=64) -> CaseSpec:
         regions=[Region("plane", p1=(2.0, 0.0, 0.0), p2=(-1.0, 0.0, 0.0),
                         exprs=tuple("%.17g" % v for v in POST_SHOCK))],
         bodies=[body])
+
+
+def riemann_viscous(n=64, Re=1600.0, Ma=0.3, rng=None, cfl=0.5) -> CaseSpec:
+    """Viscous 3D Riemann problem on the unit cube: eight seeded constant
+    states in the octants, outflow on all faces.  As for the TGV, rho0 = 1 and
+    T0 = 1 define the reference state (refT from Ma, refMu from Re with the
+    unit cube's edge as length scale).  The octant states are drawn in
+    rho in [0.5, 2], p in [0.5, 2] * p0 (p0 = 1/(gamma Ma^2)), each velocity
+    component in [-0.5, 0.5]: the reference's time step has no viscous limit,
+    and Sutherland's law at the temperatures of wider draws (rho in [0.1, 10],
+    p in [0.1, 100]) would make the explicit viscous update unstable."""
+    rng = rng if rng is not None else np.random.default_rng(0)
+    refT = 1.0 / (Ma * Ma * GAMMA * GAS_R)
+    refMu = (1.0 / Re) / sutherland(refT)
+    p0 = 1.0 / (GAMMA * Ma * Ma)
+    O = Boundary(abi.OUTFLOW)
+
+    def state():
+        rho = rng.uniform(0.5, 2.0)
+        u, v, w = rng.uniform(-0.5, 0.5, size=3)
+        p = p0 * rng.uniform(0.5, 2.0)
+        return tuple("%.17g" % x for x in (rho, u, v, w, p))
+
+    first = state()
+    regions = []
+    for a in range(2):
+        for b in range(2):
+            for c in range(2):
+                if a == 0 and b == 0 and c == 0:
+                    continue
+                regions.append(Region("box", p1=(0.5 * a, 0.5 * b, 0.5 * c),
+                                      p2=(0.5 * a + 0.5, 0.5 * b + 0.5, 0.5 * c + 0.5), exprs=state()))
+    return CaseSpec(domain_lo=(0.0, 0.0, 0.0), domain_hi=(1.0, 1.0, 1.0), m=(n, n, n), end=1.0e6, cfl=cfl,
+                    stepN=0, refMu=refMu, refT=refT, init=first, boundaries=[O] * 6, regions=regions)
+
+
+def batch_cases(count=48, seed=42, sizes=range(64, 161, 16)):
+    """The batched sweep: `count` independent cases, each a viscous TGV or a
+    viscous 3D Riemann problem (equal odds), grid n^3 with n drawn uniformly
+    from `sizes`, Ma uniform in [0.1, 0.5], Re uniform in [400, 3200], all
+    from one seeded generator.  Returns a list of CaseSpec; spec.kind, spec.n,
+    spec.Ma and spec.Re describe each case."""
+    rng = np.random.default_rng(seed)
+    sizes = list(sizes)
+    out = []
+    for _ in range(count):
+        n = int(sizes[rng.integers(len(sizes))])
+        kind = "tgv" if rng.random() < 0.5 else "riemann"
+        Ma = float(rng.uniform(0.1, 0.5))
+        Re = float(rng.uniform(400.0, 3200.0))
+        spec = tgv(n=n, Re=Re, Ma=Ma, stepN=0) if kind == "tgv" else riemann_viscous(n=n, Re=Re, Ma=Ma, rng=rng)
+        spec.kind, spec.n, spec.Ma, spec.Re = kind, n, Ma, Re
+        out.append(spec)
+    return out

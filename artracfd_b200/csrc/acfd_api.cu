@@ -159,7 +159,7 @@ bool viscous(const acfd_case *cs)
 // 5-D tensor map of the whole state U[level][var][z][y][x] with the brick of
 // sweep axis s as its box (cuTensorMapEncodeTiled through the runtime's driver
 // entry point, so the library needs no -lcuda)
-int encode_state_maps(acfd_case *cs)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
@@ -168,9 +168,41 @@ int encode_state_maps(acfd_case *cs)
         cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
         if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) {
             set_error("cuTensorMapEncodeTiled not available from the driver");
-            return ACFD_ERR_CUDA;
+            return nullptr;
         }
         encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    return encode;
+}
+
+// map of the whole state of a case with the given box (x, y, z), five
+// variables, one level
+int encode_box_map(const Grid &g, double *U, const int b[3], CUtensorMap *out)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (!encode) {
+        return ACFD_ERR_CUDA;
+    }
+    const cuuint64_t dims[5] = {(cuuint64_t)g.pitch, (cuuint64_t)g.n[1], (cuuint64_t)g.n[2], 5, 3};
+    const cuuint64_t strides[4] = {(cuuint64_t)g.pitch * 8, (cuuint64_t)g.pitch * g.n[1] * 8,
+                                   (cuuint64_t)g.nn * 8, (cuuint64_t)g.nn * 5 * 8};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    const cuuint32_t box[5] = {(cuuint32_t)b[0], (cuuint32_t)b[1], (cuuint32_t)b[2], 5, 1};
+    CUresult r = encode(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, U, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (%d) for box %d x %d x %d", (int)r, b[0], b[1], b[2]);
+        return ACFD_ERR_CUDA;
+    }
+    return ACFD_OK;
+}
+
+int encode_state_maps(acfd_case *cs)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (!encode) {
+        return ACFD_ERR_CUDA;
     }
     const Grid &g = cs->grid;
     const cuuint64_t dims[5] = {(cuuint64_t)g.pitch, (cuuint64_t)g.n[1], (cuuint64_t)g.n[2], 5, 3};
@@ -1195,6 +1227,401 @@ int acfd_fhat_batch(const acfd_model_t *model, int s, int mode, const double *Us
     cudaFree(dU);
     cudaFree(dO);
     return st;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Batch of independent cases: one persistent stage launch per RK stage for
+// all cases (ComputeTimeStep, EvolveFluidDynamics of every case, advanced
+// together; no reference counterpart for the batching itself)
+// ===========================================================================
+struct acfd_batch {
+    std::vector<acfd_case *> cases;
+    int mode = ACFD_FP32_BULK;
+    int tScheme = 1;
+    cudaStream_t stream = nullptr;
+    bool own_stream = true;
+    int sms = 148;
+    int blocks = 0;                        // persistent blocks of the stage launch
+    BatchCase *d_cases = nullptr;          // [ncase]
+    CUtensorMap *d_maps = nullptr;         // [ncase][3] brick maps (viscous geometry, variant 0)
+    long long *d_prefix = nullptr;         // [3][ncase + 1] prefix sums of the tiles per sweep axis
+    double *d_dts = nullptr;               // [ncase] step dt of each case
+    double *d_cfl = nullptr;               // [ncase] CFL number of each case
+    double *d_mesh = nullptr;              // [ncase][3] mesh sizes
+    const double **d_vmax = nullptr;       // [ncase] the cases' CFL maxima (device pointers)
+    unsigned long long *d_counter = nullptr;  // work counters, one per stage launch of a step
+    int *d_status = nullptr;
+    BatchLevel *d_levels = nullptr;        // [ncase]
+    int4 *d_pairs = nullptr;               // ghost gather of the copy-only cases
+    long long npairs = 0;
+    std::vector<int> ordered_fill;         // cases whose ghosts need the ordered fill
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int graph_mode = -1;
+    long long graph_kernels = 0;
+    long long launches = 0;
+};
+
+namespace {
+
+constexpr int kBatchStagesPerStep = 18;  // 6 directional half steps x 3 RK stages (3D, RK3)
+
+void batch_release_graph(acfd_batch *b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    b->graph_mode = -1;
+}
+
+// one time step of every case: CFL maxima, dt on the device, sensor flags
+// (hybrid), then the Strang schedule Z,Y,X,X,Y,Z of RK stages, each one
+// persistent launch over all cases followed by the ghost fill
+int batch_step(acfd_batch *b)
+{
+    const int ncase = (int)b->cases.size();
+    for (acfd_case *cs : b->cases) {
+        TRY(launch_cfl(cs->grid, cs->mp, cs->U, cs->flags, cs->cfl_part, cs->cfl_out, b->stream));
+        b->launches += 2;
+    }
+    TRY(launch_batch_dt(b->d_vmax, b->d_mesh, b->d_cfl, b->d_dts, ncase, b->stream));
+    ++b->launches;
+    const bool hybrid = (b->mode == ACFD_FP32_HYBRID);
+    if (hybrid) {
+        for (acfd_case *cs : b->cases) {
+            TRY(launch_sensor_flags(cs->grid, cs->mp, cs->U, cs->flags, cs->sensor_params, cs->sensor_logit,
+                                    cs->sensor_rp, cs->sensor_flags, nullptr, b->stream));
+            b->launches += 2;
+        }
+    }
+    ACFD_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long) * kBatchStagesPerStep, b->stream));
+    static const int order[6] = {2, 1, 0, 0, 1, 2};
+    struct Coef {
+        double a, c;
+        int to, tn, tm;
+    };
+    static const Coef rk3[3] = {{0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN},
+                                {3.0 / 4.0, 1.0 / 4.0, ACFD_TO, ACFD_TN, ACFD_TM},
+                                {1.0 / 3.0, 2.0 / 3.0, ACFD_TO, ACFD_TM, ACFD_TO}};
+    static const Coef rk2[2] = {{0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN}, {1.0 / 2.0, 1.0 / 2.0, ACFD_TO, ACFD_TN, ACFD_TO}};
+    const Coef *rk = b->tScheme == 1 ? rk3 : rk2;
+    const int nstage = b->tScheme == 1 ? 3 : 2;
+    int launch = 0;
+    for (int h = 0; h < 6; ++h) {
+        const int s = order[h];
+        for (int q = 0; q < nstage; ++q) {
+            StageCoefs sc;
+            sc.coeA = rk[q].a;
+            sc.coeB = rk[q].c;
+            sc.dt_scale = 0.5;
+            sc.to = rk[q].to;
+            sc.tn = rk[q].tn;
+            sc.tm = rk[q].tm;
+            TRY(launch_stage_batch(b->d_cases, b->d_maps, b->d_prefix + (long long)s * (ncase + 1), ncase, sc,
+                                   b->d_dts, b->d_counter + launch, b->d_status, b->blocks, s, hybrid, b->stream));
+            ++launch;
+            ++b->launches;
+            if (b->npairs > 0) {
+                TRY(launch_batch_gather(b->d_levels, b->d_pairs, b->npairs, sc.tm, b->stream));
+                ++b->launches;
+            }
+            for (int c : b->ordered_fill) {
+                acfd_case *cs = b->cases[c];
+                const cudaStream_t keep = cs->stream;
+                cs->stream = b->stream;
+                const long long l0 = cs->launches;
+                const int st = treat_boundary(cs, sc.tm);
+                b->launches += cs->launches - l0;
+                cs->stream = keep;
+                TRY(st);
+            }
+        }
+    }
+    return ACFD_OK;
+}
+
+int batch_check(const acfd_batch *b)
+{
+    if (!b) {
+        set_error("null batch handle");
+        return ACFD_ERR_ARG;
+    }
+    return ACFD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int acfd_batch_init(int ncase, const acfd_partition_t *parts, const acfd_model_t *models, acfd_batch_t **out)
+{
+    if (ncase < 1 || !parts || !models || !out) {
+        set_error("acfd_batch_init: bad arguments");
+        return ACFD_ERR_ARG;
+    }
+    *out = nullptr;
+    for (int c = 0; c < ncase; ++c) {
+        const acfd_model_t &m = models[c];
+        const acfd_partition_t &p = parts[c];
+        if (m.sScheme != 1 || m.multidim != 0 || m.sState != 0 || p.collapse != 0 || m.tScheme != models[0].tScheme) {
+            set_error("acfd_batch_init: case %d: the batch advances 3D cases with WENO5, the split scheme, no "
+                      "gravity and one common RK scheme", c);
+            return ACFD_ERR_ARG;
+        }
+    }
+    acfd_batch *b = new acfd_batch();
+    b->tScheme = models[0].tScheme;
+    int st = ACFD_OK;
+    cudaError_t e;
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess || (e = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        st = cuda_status(e, "acfd_batch_init");
+        delete b;
+        return st;
+    }
+    for (int c = 0; c < ncase && st == ACFD_OK; ++c) {
+        acfd_case *cs = nullptr;
+        st = acfd_init(&parts[c], &models[c], &cs);
+        if (st == ACFD_OK) {
+            b->cases.push_back(cs);
+        }
+    }
+    std::vector<BatchCase> hc(ncase);
+    std::vector<CUtensorMap> hm((size_t)ncase * 3);
+    std::vector<long long> prefix((size_t)3 * (ncase + 1), 0);
+    std::vector<double> mesh((size_t)ncase * 3);
+    std::vector<const double *> vmax(ncase);
+    std::vector<BatchLevel> lv(ncase);
+    std::vector<int4> pairs;
+    for (int c = 0; c < ncase && st == ACFD_OK; ++c) {
+        acfd_case *cs = b->cases[c];
+        BatchCase &C = hc[c];
+        C.g = cs->grid;
+        C.mp = cs->mp;
+        C.U = cs->U;
+        C.did = cs->flags;
+        C.flags = nullptr;
+        const int L[3] = {cs->grid.hi[0] - cs->grid.lo[0], cs->grid.hi[1] - cs->grid.lo[1],
+                          cs->grid.hi[2] - cs->grid.lo[2]};
+        for (int s = 0; s < 3 && st == ACFD_OK; ++s) {
+            int box[3], step[3];
+            brick_box(s, true, 0, box);
+            brick_step(s, true, 0, step);
+            for (int a = 0; a < 3; ++a) {
+                C.tiles[s][a] = (L[a] + step[a] - 1) / step[a];
+            }
+            st = encode_box_map(cs->grid, cs->U, box, &hm[(size_t)c * 3 + s]);
+            prefix[(size_t)s * (ncase + 1) + c + 1] =
+                prefix[(size_t)s * (ncase + 1) + c] + (long long)C.tiles[s][0] * C.tiles[s][1] * C.tiles[s][2];
+        }
+        for (int s = 0; s < 3; ++s) {
+            mesh[(size_t)c * 3 + s] = cs->part.d[s];
+        }
+        vmax[c] = cs->cfl_out;
+        lv[c].U = cs->U;
+        lv[c].nn = cs->grid.nn;
+        if (cs->bc_gather) {
+            std::vector<int2> hp(cs->bc_npairs);
+            if ((e = cudaMemcpy(hp.data(), cs->bc_pairs, sizeof(int2) * hp.size(), cudaMemcpyDeviceToHost)) !=
+                cudaSuccess) {
+                st = cuda_status(e, "acfd_batch_init");
+            }
+            for (const int2 &q : hp) {
+                pairs.push_back(make_int4(c, q.x, q.y, 0));
+            }
+        } else {
+            b->ordered_fill.push_back(c);
+        }
+    }
+    // persistent stage launch: two resident blocks of the viscous bricks per SM
+    b->blocks = 2 * b->sms;
+    const size_t nbytes[] = {sizeof(BatchCase) * ncase, sizeof(CUtensorMap) * 3 * ncase,
+                             sizeof(long long) * prefix.size(), sizeof(double) * ncase, sizeof(double) * ncase,
+                             sizeof(double) * mesh.size(), sizeof(double *) * ncase,
+                             sizeof(unsigned long long) * kBatchStagesPerStep, sizeof(int),
+                             sizeof(BatchLevel) * ncase, sizeof(int4) * (pairs.size() ? pairs.size() : 1)};
+    void **ptrs[] = {(void **)&b->d_cases, (void **)&b->d_maps, (void **)&b->d_prefix, (void **)&b->d_dts,
+                     (void **)&b->d_cfl, (void **)&b->d_mesh, (void **)&b->d_vmax, (void **)&b->d_counter,
+                     (void **)&b->d_status, (void **)&b->d_levels, (void **)&b->d_pairs};
+    for (int q = 0; q < 11 && st == ACFD_OK; ++q) {
+        if ((e = cudaMalloc(ptrs[q], nbytes[q])) != cudaSuccess) {
+            st = cuda_status(e, "acfd_batch_init allocation");
+        }
+    }
+    if (st == ACFD_OK) {
+        b->npairs = (long long)pairs.size();
+        const void *src[] = {hc.data(), hm.data(), prefix.data(), nullptr, nullptr, mesh.data(), vmax.data(),
+                             nullptr, nullptr, lv.data(), pairs.data()};
+        for (int q = 0; q < 11 && st == ACFD_OK; ++q) {
+            if (src[q] && nbytes[q] && (q != 10 || b->npairs > 0)) {
+                if ((e = cudaMemcpy(*ptrs[q], src[q], nbytes[q], cudaMemcpyHostToDevice)) != cudaSuccess) {
+                    st = cuda_status(e, "acfd_batch_init copy");
+                }
+            }
+        }
+        if (st == ACFD_OK && (e = cudaMemset(b->d_status, 0, sizeof(int))) != cudaSuccess) {
+            st = cuda_status(e, "acfd_batch_init");
+        }
+    }
+    if (st != ACFD_OK) {
+        acfd_batch_finalize(b);
+        return st;
+    }
+    for (acfd_case *cs : b->cases) {
+        cs->mode = ACFD_FP32_BULK;
+    }
+    *out = b;
+    return ACFD_OK;
+}
+
+int acfd_batch_finalize(acfd_batch_t *b)
+{
+    if (!b) {
+        return ACFD_OK;
+    }
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_release_graph(b);
+    for (acfd_case *cs : b->cases) {
+        acfd_finalize(cs);
+    }
+    cudaFree(b->d_cases);
+    cudaFree(b->d_maps);
+    cudaFree(b->d_prefix);
+    cudaFree(b->d_dts);
+    cudaFree(b->d_cfl);
+    cudaFree(b->d_mesh);
+    cudaFree(b->d_vmax);
+    cudaFree(b->d_counter);
+    cudaFree(b->d_status);
+    cudaFree(b->d_levels);
+    cudaFree(b->d_pairs);
+    if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return ACFD_OK;
+}
+
+int acfd_batch_case(acfd_batch_t *b, int c, acfd_case_t **cs)
+{
+    TRY(batch_check(b));
+    if (c < 0 || c >= (int)b->cases.size() || !cs) {
+        set_error("acfd_batch_case: case %d of %d", c, (int)b->cases.size());
+        return ACFD_ERR_ARG;
+    }
+    *cs = b->cases[c];
+    return ACFD_OK;
+}
+
+int acfd_batch_set_precision(acfd_batch_t *b, int mode)
+{
+    TRY(batch_check(b));
+    if (mode != ACFD_FP32_BULK && mode != ACFD_FP32_HYBRID) {
+        set_error("acfd_batch_set_precision: the batch runs ACFD_FP32_BULK or ACFD_FP32_HYBRID, not %d", mode);
+        return ACFD_ERR_ARG;
+    }
+    std::vector<BatchCase> hc(b->cases.size());
+    ACFD_CUDA(cudaMemcpy(hc.data(), b->d_cases, sizeof(BatchCase) * hc.size(), cudaMemcpyDeviceToHost));
+    for (size_t c = 0; c < b->cases.size(); ++c) {
+        acfd_case *cs = b->cases[c];
+        if (mode == ACFD_FP32_HYBRID && !cs->sensor_ok) {
+            set_error("acfd_batch_set_precision: case %d has no sensor (acfd_batch_sensor_load)", (int)c);
+            return ACFD_ERR_STATE;
+        }
+        cs->mode = mode;
+        hc[c].flags = (mode == ACFD_FP32_HYBRID) ? cs->sensor_flags : nullptr;
+    }
+    ACFD_CUDA(cudaMemcpy(b->d_cases, hc.data(), sizeof(BatchCase) * hc.size(), cudaMemcpyHostToDevice));
+    if (mode != b->mode) {
+        batch_release_graph(b);
+    }
+    b->mode = mode;
+    return ACFD_OK;
+}
+
+int acfd_batch_sensor_load(acfd_batch_t *b, const float *params, float threshold)
+{
+    TRY(batch_check(b));
+    for (acfd_case *cs : b->cases) {
+        TRY(acfd_sensor_load(cs, params, threshold));
+    }
+    batch_release_graph(b);
+    return ACFD_OK;
+}
+
+int acfd_batch_advance(acfd_batch_t *b, const double *cfl, int steps, double *dts)
+{
+    TRY(batch_check(b));
+    const int ncase = (int)b->cases.size();
+    if (!cfl || steps < 0) {
+        set_error("acfd_batch_advance: bad arguments");
+        return ACFD_ERR_ARG;
+    }
+    ACFD_CUDA(cudaMemcpyAsync(b->d_cfl, cfl, sizeof(double) * ncase, cudaMemcpyHostToDevice, b->stream));
+    if (!b->exec || b->graph_mode != b->mode) {
+        batch_release_graph(b);
+        ACFD_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        const long long before = b->launches;
+        int st = batch_step(b);
+        b->graph_kernels = b->launches - before;
+        b->launches = before;
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+        if (st != ACFD_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        if (e != cudaSuccess) {
+            return cuda_status(e, "cudaStreamEndCapture");
+        }
+        b->graph = graph;
+        ACFD_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+        b->graph_mode = b->mode;
+    }
+    for (int k = 0; k < steps; ++k) {
+        ACFD_CUDA(cudaGraphLaunch(b->exec, b->stream));
+        b->launches += b->graph_kernels;
+        if (dts) {
+            ACFD_CUDA(cudaMemcpyAsync(dts + (size_t)k * ncase, b->d_dts, sizeof(double) * ncase,
+                                      cudaMemcpyDeviceToHost, b->stream));
+        }
+    }
+    ACFD_CUDA(cudaStreamSynchronize(b->stream));
+    int status = 0;
+    ACFD_CUDA(cudaMemcpy(&status, b->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status != 0) {
+        cudaMemset(b->d_status, 0, sizeof(int));
+        set_error("batch stage: device wait gave up (code %d)", status);
+        return ACFD_ERR_DEVICE;
+    }
+    for (acfd_case *cs : b->cases) {
+        TRY(check_device_status(cs));
+    }
+    return ACFD_OK;
+}
+
+int acfd_batch_set_stream(acfd_batch_t *b, void *stream)
+{
+    TRY(batch_check(b));
+    if (!stream) {
+        set_error("acfd_batch_set_stream: null stream");
+        return ACFD_ERR_ARG;
+    }
+    ACFD_CUDA(cudaStreamSynchronize(b->stream));
+    ACFD_CUDA(cudaStreamDestroy(b->stream));
+    b->stream = static_cast<cudaStream_t>(stream);
+    b->own_stream = false;
+    batch_release_graph(b);
+    return ACFD_OK;
+}
+
+int acfd_batch_stats(acfd_batch_t *b, long long *launches)
+{
+    TRY(batch_check(b));
+    if (launches) *launches = b->launches;
+    return ACFD_OK;
 }
 
 }  // extern "C"

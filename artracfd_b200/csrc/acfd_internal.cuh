@@ -74,6 +74,19 @@ int launch_stage_batch(const BatchCase *cases, const CUtensorMap *maps, const lo
                        const StageCoefs &sc, const double *dts, unsigned long long *counter, int *status, int blocks,
                        int s, bool hybrid, cudaStream_t st);
 
+// state of one case of a batch, as the batched ghost fill and time step see it
+struct BatchLevel {
+    double *U;       // the case's state (3 levels x 5 variables x nn)
+    long long nn;    // nodes per variable plane
+};
+// ghost fill of every case of a batch at level tn: pairs (case, dst, src, 0)
+int launch_batch_gather(const BatchLevel *cases, const int4 *pairs, long long count, int tn, cudaStream_t st);
+// time step of every case from its CFL maximum (ComputeTimeStep, solve.c:152):
+// dt = cfl * min(d0/v0, min(d1/v1, d2/v2)) with vmax[c] the case's three maxima
+// and d the mesh sizes (3 per case)
+int launch_batch_dt(const double *const *vmax, const double *d, const double *cfl, double *dts, int ncase,
+                    cudaStream_t st);
+
 // Plane-march stage kernels (Y/Z sweeps): geometry of one launch, computed on
 // the host and passed by value.  A block owns WX consecutive x by NR rows of
 // the other transverse axis over one segment of the sweep axis; a producer

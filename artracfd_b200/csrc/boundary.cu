@@ -421,6 +421,58 @@ int launch_ghost_gather(const Grid &g, const int2 *pairs, int count, double *U, 
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "ghost_gather launch");
 }
 
+// ghost fill of all cases of a batch in one launch (copy-only cases, see
+// ghost_gather)
+__global__ void batch_ghost_gather(const BatchLevel *__restrict__ cases, const int4 *__restrict__ pairs,
+                                   long long count, int tn)
+{
+    pdl_wait();
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < count;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int4 q = pairs[t];
+        const BatchLevel c = cases[q.x];
+        double *U = c.U + (long long)tn * 5 * c.nn;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            U[v * c.nn + q.y] = U[v * c.nn + q.z];
+        }
+    }
+}
+
+int launch_batch_gather(const BatchLevel *cases, const int4 *pairs, long long count, int tn, cudaStream_t st)
+{
+    if (count <= 0) {
+        return ACFD_OK;
+    }
+    const long long want = (count + 255) / 256;
+    const unsigned blocks = (unsigned)(want < 148 * 64 ? want : 148 * 64);
+    cudaError_t e = launch_k(batch_ghost_gather, dim3(blocks), dim3(256), 0, st, cases, pairs, count, tn);
+    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "batch_ghost_gather launch");
+}
+
+// per-case dt of a batch, in the order of the reference's expression
+__global__ void batch_dt(const double *const *vmax, const double *d, const double *cfl, double *dts, int ncase)
+{
+    pdl_wait();
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncase) {
+        return;
+    }
+    const double *v = vmax[c];
+    const double a = d[3 * c + 1] / v[1];
+    const double b = d[3 * c + 2] / v[2];
+    const double inner = (a < b) ? a : b;
+    const double x = d[3 * c] / v[0];
+    dts[c] = cfl[c] * ((x < inner) ? x : inner);
+}
+
+int launch_batch_dt(const double *const *vmax, const double *d, const double *cfl, double *dts, int ncase,
+                    cudaStream_t st)
+{
+    cudaError_t e = launch_k(batch_dt, dim3((ncase + 127) / 128), dim3(128), 0, st, vmax, d, cfl, dts, ncase);
+    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "batch_dt launch");
+}
+
 int launch_domain_boundary(const Grid &g, const ModelParams &m, const acfd_partition_t &part,
                            const FaceBox *boxes, int nbox, double *U, cudaStream_t st)
 {

@@ -85,6 +85,26 @@ inline void update_box(int s, int var, int box[3])
 #undef ACFD_OBOX
 }
 
+// tile steps (nodes updated per tile along x, y, z) of sweep s, variant var
+inline void brick_step(int s, bool visc, int var, int st[3])
+{
+#define ACFD_STEP(S_, V_, R_)             \
+    st[0] = Brick<S_, V_, R_>::SX;        \
+    st[1] = Brick<S_, V_, R_>::SY;        \
+    st[2] = Brick<S_, V_, R_>::SZ;
+#define ACFD_STEP_V(S_, R_)                                   \
+    if (visc) { ACFD_STEP(S_, true, R_) } else { ACFD_STEP(S_, false, R_) }
+    if (s == 0) {
+        if (var) { ACFD_STEP_V(0, 1) } else { ACFD_STEP_V(0, 0) }
+    } else if (s == 1) {
+        if (var) { ACFD_STEP_V(1, 1) } else { ACFD_STEP_V(1, 0) }
+    } else {
+        if (var) { ACFD_STEP_V(2, 1) } else { ACFD_STEP_V(2, 0) }
+    }
+#undef ACFD_STEP_V
+#undef ACFD_STEP
+}
+
 // box extents (x, y, z) of the tensor map of sweep s, tile variant var
 inline void brick_box(int s, bool visc, int var, int box[3])
 {

@@ -43,9 +43,10 @@ FLOP_PER_NODE_STAGE_VISCOUS = 1535.0  # ComputeFhat 1380 + ComputeFvhat 115 + LU
 STAGE_BYTES = (80.0, 120.0, 120.0)
 
 
-def profiled_traffic(mode: str):
-    """DRAM bytes per stage launch from the committed ncu summary of the
-    stage kernels (mean over the captured X and Y/Z launches), or None."""
+def profiled_traffic(mode: str, axes=(0, 1, 2)):
+    """DRAM bytes per RK-stage-2 launch from the committed ncu summary of the
+    stage kernels (mean over the captured launches of the given sweep axes),
+    or None."""
     name = {"fp64": "stage_sweep_fp64_tgv128.md", "fp32": "stage_sweep_fp32_tgv128.md",
             "hybrid": "stage_sweep_hybrid_tgv128.md"}.get(mode)
     if not name:
@@ -56,6 +57,7 @@ def profiled_traffic(mode: str):
     for line in open(p):
         if line.startswith("| DRAM traffic per launch (MB)"):
             vals = [float(c.strip().strip("*")) for c in line.split("|")[2:] if c.strip()]
+            vals = [vals[a] for a in axes if a < len(vals)]
             return sum(vals) / len(vals) * 1e6 if vals else None
     return None
 
@@ -236,10 +238,11 @@ def _timed_steps(torch, s, spec, steps, warmup, dist, stream, clock_index):
     return sec, s.launches() - launches0, clk.summary()
 
 
-def _stage_profile(torch, s, spec, nodes_pin, stream):
+def _stage_profile(torch, s, spec, nodes_pin, stream, per_axis=None):
     """One eager step with events around each LLLU stage and each ghost fill
     on the solver's stream: mean stage and fill times (ms), and the
-    algorithmic bytes per stage launch."""
+    algorithmic bytes per stage launch.  per_axis (a dict, optional)
+    receives the stage times and algorithmic bytes of each sweep axis."""
     from artracfd_b200 import abi
     stage_ms, bc_ms = [], []
     dt = s.time_step(spec.cfl)
@@ -262,6 +265,10 @@ def _stage_profile(torch, s, spec, nodes_pin, stream):
                 stage_ms.append(ev[0].elapsed_time(ev[1]))
                 bc_ms.append(ev[1].elapsed_time(ev[2]))
                 stage_bytes += STAGE_BYTES[q] * nodes_pin
+                if per_axis is not None:
+                    ax = per_axis.setdefault(sd, {"ms": [], "bytes": []})
+                    ax["ms"].append(stage_ms[-1])
+                    ax["bytes"].append(STAGE_BYTES[q] * nodes_pin)
     return sum(stage_ms) / len(stage_ms), sum(bc_ms) / len(bc_ms), stage_bytes / len(stage_ms)
 
 
@@ -356,8 +363,27 @@ def run_ours(args, rank, world, local_rank):
     value = world * nodes_pin * args.steps / sec / 1e6
     if args.mode == "hybrid":
         sensor_info["flagged_fraction_after_timed_steps"] = s.sensor_update() / (3.0 * nodes_pin)
-    stage_mean, bc_mean, bytes_per_stage = _stage_profile(torch, s, spec, nodes_pin, stream)
-    achieved = bytes_per_stage / (stage_mean / 1e3) / 1e9
+    per_axis = {}
+    stage_mean, bc_mean, bytes_per_stage = _stage_profile(torch, s, spec, nodes_pin, stream, per_axis)
+    # the dominant kernel: the stage-kernel family (tile variant class) with
+    # the largest share of the stage time; its algorithmic bytes over its
+    # mean launch duration
+    fam_of = lambda v: "brick" if v < abi.BRICK_VARIANTS else ("plane" if v >= abi.PLANE_VARIANT else "line-march")
+    fams = {}
+    for ax, d in per_axis.items():
+        f = fams.setdefault(fam_of(tiles[ax]), {"ms": [], "bytes": [], "axes": []})
+        f["ms"] += d["ms"]
+        f["bytes"] += d["bytes"]
+        f["axes"].append(ax)
+    dom_name, dom = max(fams.items(), key=lambda kv: sum(kv[1]["ms"]))
+    dom_ms = sum(dom["ms"]) / len(dom["ms"])
+    dom_bytes = sum(dom["bytes"]) / len(dom["bytes"])
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    dom_share = sum(dom["ms"]) / sum(sum(d["ms"]) for d in fams.values())
+    # ncu traffic of RK stage 2 (120 B algorithmic per node), scaled to the
+    # mean RK-stage mix of one step (106.7 B per node)
+    tr2 = profiled_traffic(args.mode, tuple(sorted(dom["axes"])))
+    traffic = tr2 * (dom_bytes / (STAGE_BYTES[1] * nodes_pin)) if tr2 else None
     flop_rate = FLOP_PER_NODE_STAGE_VISCOUS * nodes_pin / (stage_mean / 1e3) / 1e12
     fp64_peak = fp64_peak_tflops(torch) if rank == 0 else None
     # e2e through the C ABI with host buffers: upload of the host node array,
@@ -404,11 +430,15 @@ def run_ours(args, rank, world, local_rank):
         "speedup_vs_plain_fp64": (value / plain["value"]) if plain else None,
         "accuracy": accuracy,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "traffic": profiled_traffic(args.mode),
-                     "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum per stage launch "
-                                     "(profiles/), algorithmic bytes per launch = "
-                                     f"{bytes_per_stage:.4g}",
-                     "kernel": "stage sweep (LLLU), mean over the 18 stages of one step",
+                     "frac": achieved / hbm_peak, "traffic": traffic,
+                     "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of an RK-stage-2 launch "
+                                     "of this kernel (profiles/stage_sweep_<form>_tgv128.md), scaled to the mean "
+                                     f"RK-stage mix; algorithmic bytes per launch = {dom_bytes:.4g}",
+                     "kernel": f"{dom_name} stage kernel of sweep axes {sorted(dom['axes'])} "
+                               f"({dom_share * 100:.0f}% of the stage time), mean over its launches in one step",
+                     "all_stage_kernels": {"achieved": bytes_per_stage / (stage_mean / 1e3) / 1e9,
+                                           "frac": bytes_per_stage / (stage_mean / 1e3) / 1e9 / hbm_peak},
+                     "per_axis_ms": {str(ax): sum(d["ms"]) / len(d["ms"]) for ax, d in sorted(per_axis.items())},
                      "peak_kind": peak_kind,
                      "fp64": {"achieved_tflops": flop_rate, "peak_tflops": fp64_peak,
                               "frac": (flop_rate / fp64_peak) if fp64_peak else None,
@@ -426,6 +456,105 @@ def run_ours(args, rank, world, local_rank):
         "tiles": tiles,
         "sensor": sensor_info,
         "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_batch(args, rank, world, local_rank):
+    """The batched sweep: 48 independent viscous TGV and 3D Riemann cases
+    (configs.batch_cases, seed 42) advanced together by the batch API in the
+    learned-sensor FP32 form, against the same cases run one at a time by the
+    single-case API on the plain FP64 path.  Both are device-timed with CUDA
+    events (the one-at-a-time runs include their per-step host dt, as a user
+    running cases one by one does); the batch's dt stays on the device."""
+    import numpy as np
+    import torch
+    from concurrent.futures import ThreadPoolExecutor
+
+    from artracfd_b200 import abi, configs, sensor
+    from artracfd_b200.batch import Batch
+    from artracfd_b200.solver import Solver
+
+    torch.cuda.set_device(local_rank)
+    specs = configs.batch_cases(count=args.batch_cases, seed=42)
+    descs = [s.descriptors() for s in specs]
+    pin = [int(np.prod(np.array(p.ns)[0, :, 1] - np.array(p.ns)[0, :, 0])) for p, _ in descs]
+    steps = args.steps
+    stream = torch.cuda.Stream()
+    b = Batch(descs)
+    b.set_stream(stream.cuda_stream)
+    rho64 = []
+    sec64 = 0.0
+    pool = ThreadPoolExecutor(1)
+    fut = pool.submit(specs[0].initial_nodes, *descs[0])
+    for c, spec in enumerate(specs):
+        node = fut.result()
+        if c + 1 < len(specs):
+            fut = pool.submit(specs[c + 1].initial_nodes, *descs[c + 1])
+        b.upload(c, node)
+        b.treat_boundary(c)
+        with Solver(*descs[c], abi.FP64) as s:
+            s.set_stream(stream.cuda_stream)
+            s.upload(node)
+            s.treat_boundary(abi.TO)
+            s.evolve(s.time_step(spec.cfl), graph=True)  # graph capture outside the timed steps
+            s.upload(node)
+            s.treat_boundary(abi.TO)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                s.evolve(s.time_step(spec.cfl), graph=True)
+            e1.record(stream)
+            e1.synchronize()
+            sec64 += e0.elapsed_time(e1) / 1e3
+            rho64.append(s.download()["U"][:, 0, 0].copy())
+        del node
+    pool.shutdown()
+    params, thr, _ = sensor.load(sensor.WEIGHTS)
+    b.sensor_load(params, thr)
+    b.set_precision(abi.FP32_HYBRID)
+    cfl = [s.cfl for s in specs]
+    # the first advance captures the step graph; time the remaining steps
+    b.advance(cfl, 1)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = b.launches()
+    e0.record(stream)
+    b.advance(cfl, steps - 1)
+    e1.record(stream)
+    e1.synchronize()
+    secb = e0.elapsed_time(e1) / 1e3
+    launches = b.launches() - l0
+    errs = []
+    for c in range(len(specs)):
+        r = b.download(c)["U"][:, 0, 0]
+        m = np.array(descs[c][0].ns)[0]
+        n = list(descs[c][0].n)
+        mask = np.zeros((n[2], n[1], n[0]), dtype=bool)
+        mask[m[2, 0]:m[2, 1], m[1, 0]:m[1, 1], m[0, 0]:m[0, 1]] = True
+        mask = mask.ravel()
+        errs.append(float(np.abs(r[mask] - rho64[c][mask]).sum() / np.abs(rho64[c][mask]).sum()))
+    b.close()
+    total = sum(pin)
+    line = {
+        "metric": METRIC, "workload": "batch", "value": total * (steps - 1) / secb / 1e6, "unit": UNIT,
+        "n_gpus": 1, "steps": steps - 1, "higher_is_better": True, "dtype": "f32/f64",
+        "data": "synthetic (seeded TGV and 3D Riemann initial fields)",
+        "config": {"workload": f"{len(specs)} independent viscous TGV / 3D Riemann cases, n^3 with n in "
+                               "{64..160 step 16}, Ma U[0.1,0.5], Re U[400,3200], seed 42; WENO5/RK3",
+                   "cases": len(specs), "pin_nodes": total,
+                   "kinds": {k: sum(1 for s in specs if s.kind == k) for k in ("tgv", "riemann")},
+                   "form": "hybrid (learned sensor, FP32 bulk)", "persistent_launches_per_step": 18},
+        "ms_per_step": secb / (steps - 1) * 1e3,
+        "one_at_a_time_fp64": {"value": total * steps / sec64 / 1e6, "ms_per_step_all_cases": sec64 / steps * 1e3,
+                               "what": "each case alone through the single-case API, plain FP64 path, host dt "
+                                       "per step, CUDA graph per step"},
+        "speedup_vs_one_at_a_time_fp64": (total * (steps - 1) / secb) / (total * steps / sec64),
+        "accuracy": {"l1_rho_max_over_cases": max(errs), "l1_rho_mean": sum(errs) / len(errs),
+                     "against": "the same case on the plain FP64 path after the same number of steps "
+                                "(each with its own dt sequence)"},
+        "gpu_launches": launches,
     }
     print(json.dumps(line), flush=True)
 
@@ -467,12 +596,17 @@ def main():
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-procs", type=int, default=16)
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch"],
+                    help="tgv: the headline line (TGV 128^3); batch: the 48-case batched sweep")
+    ap.add_argument("--batch-cases", type=int, default=48)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.workload == "batch":
+        run_batch(args, rank, world, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
 

@@ -276,6 +276,40 @@ int acfd_mlp_grad(const float *params, const float *X, const float *Y, int n, fl
 int acfd_mlp_adam(float *params, const float *grad, float *m, float *v, int step, float lr, float scale,
         void *stream);
 
+/* ---- batch of independent cases (no reference counterpart) ------------ */
+
+/* Many independent cases advanced together: each RK stage of every case is
+ * one persistent launch over the tiles of all cases (the brick stage kernel
+ * of the FP32 forms), each case keeps its own grid, model, boundary
+ * conditions and time step (computed on the device from its CFL maximum, as
+ * ComputeTimeStep does, solve.c:108-153), and one time step of the whole
+ * batch is captured and replayed as a CUDA graph.  Cases must be 3D, WENO5,
+ * dimension-split, without gravity, with one common RK scheme and no
+ * immersed bodies. */
+typedef struct acfd_batch acfd_batch_t;
+/* Create a batch of ncase cases (parts[c], models[c]); each case gets its own
+ * device state as acfd_init would allocate it. */
+int acfd_batch_init(int ncase, const acfd_partition_t *parts, const acfd_model_t *models, acfd_batch_t **out);
+int acfd_batch_finalize(acfd_batch_t *b);
+/* The case handle of case c, for acfd_sync_to_device / acfd_sync_to_host /
+ * acfd_treat_boundary / acfd_cfl on that case (not acfd_batch_finalize'd
+ * separately). */
+int acfd_batch_case(acfd_batch_t *b, int c, acfd_case_t **cs);
+/* ACFD_FP32_BULK (default) or ACFD_FP32_HYBRID (after acfd_batch_sensor_load). */
+int acfd_batch_set_precision(acfd_batch_t *b, int mode);
+/* Load the learned sensor into every case (see acfd_sensor_load). */
+int acfd_batch_sensor_load(acfd_batch_t *b, const float *params, float threshold);
+/* Advance every case by `steps` time steps; cfl[c] is the CFL number of case
+ * c; dts (optional, steps x ncase doubles) receives the dt of every case and
+ * step.  Returns after the work has finished. */
+int acfd_batch_advance(acfd_batch_t *b, const double *cfl, int steps, double *dts);
+/* Run the batch's work on the caller's CUDA stream (cudaStream_t as void*);
+ * the library's own stream is released. */
+int acfd_batch_set_stream(acfd_batch_t *b, void *stream);
+/* Kernels launched by the batch so far (graph replays count their kernel
+ * nodes). */
+int acfd_batch_stats(acfd_batch_t *b, long long *launches);
+
 /* ---- per-point device twins (batched; host arrays in and out) --------- */
 
 /* WENO3 (weno3.c:35-55) / WENO5 (weno5.c:35-62) on count stencils:

@@ -1,0 +1,93 @@
+"""The batch of independent cases (acfd_batch_*) against the same cases run one
+at a time through the single-case API.
+
+Each RK stage of the batch is one persistent launch over the tiles of all
+cases with the brick stage kernel; a case of the batch computes every
+interface exactly as the single-case brick kernel does, and its dt comes from
+its own CFL maximum in the reference's expression, so the batch reproduces
+the single-case runs bit for bit: states, and dt at every step.  The cases
+mix periodic (TGV), outflow (Riemann), outflow + periodic (Sod) and
+inflow/outflow/wall/periodic boundaries (channel, the ordered ghost fill).
+"""
+import numpy as np
+import pytest
+
+from artracfd_b200 import abi, configs, sensor
+from artracfd_b200.batch import Batch
+from artracfd_b200.solver import Solver
+
+import cases
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 3
+
+
+def _specs():
+    rng = np.random.default_rng(7)
+    return [configs.tgv(n=16, Re=800.0, Ma=0.2, stepN=0),
+            configs.riemann_viscous(n=16, Re=1000.0, Ma=0.3, rng=rng),
+            configs.tgv(n=24, Re=1200.0, Ma=0.4, stepN=0),
+            configs.sod(m=(32, 4, 4)),
+            cases.channel()]
+
+
+def _single(spec, part, model, mode, steps, params=None, thr=0.5):
+    node = spec.initial_nodes(part, model)
+    dts, out = [], None
+    with Solver(part, model, abi.FP64 if params is not None else mode) as s:
+        s.upload(node)
+        s.treat_boundary(abi.TO)
+        if params is not None:
+            s.sensor_load(params, thr)
+            s.set_precision(abi.FP32_HYBRID)
+        s.set_tiles([0, 0, 0])
+        for _ in range(steps):
+            dt = s.time_step(spec.cfl)
+            s.evolve(dt)
+            dts.append(dt)
+        out = s.download()["U"][:, 0, :].copy()
+    return np.array(dts), out
+
+
+def _batch(specs, descs, mode, steps, params=None, thr=0.5):
+    with Batch(descs) as b:
+        for c, spec in enumerate(specs):
+            b.upload(c, spec.initial_nodes(*descs[c]))
+            b.treat_boundary(c)
+        if params is not None:
+            b.sensor_load(params, thr)
+        b.set_precision(mode)
+        dts = b.advance([s.cfl for s in specs], steps)
+        outs = [b.download(c)["U"][:, 0, :].copy() for c in range(len(specs))]
+        launches = b.launches()
+    return dts, outs, launches
+
+
+def test_batch_equals_single_cases_fp32():
+    specs = _specs()
+    descs = [s.descriptors() for s in specs]
+    dts, outs, launches = _batch(specs, descs, abi.FP32_BULK, STEPS)
+    assert launches > 0
+    for c, spec in enumerate(specs):
+        sdt, sout = _single(spec, *descs[c], abi.FP32_BULK, STEPS)
+        assert np.array_equal(dts[:, c], sdt), (c, dts[:, c], sdt)
+        assert np.array_equal(outs[c], sout), (c, np.nanmax(np.abs(outs[c] - sout)))
+
+
+@pytest.mark.skipif(not __import__("os").path.exists(sensor.WEIGHTS), reason="no trained sensor weights")
+def test_batch_equals_single_cases_hybrid():
+    specs = _specs()
+    descs = [s.descriptors() for s in specs]
+    params, thr, _ = sensor.load(sensor.WEIGHTS)
+    dts, outs, _ = _batch(specs, descs, abi.FP32_HYBRID, STEPS, params, thr)
+    for c, spec in enumerate(specs):
+        sdt, sout = _single(spec, *descs[c], abi.FP32_HYBRID, STEPS, params, thr)
+        assert np.array_equal(dts[:, c], sdt), c
+        assert np.array_equal(outs[c], sout), (c, np.nanmax(np.abs(outs[c] - sout)))
+
+
+def test_batch_rejects_unsupported_cases():
+    spec = configs.tgv(n=10, sScheme=0, stepN=0)  # WENO3
+    with pytest.raises(abi.AcfdError):
+        Batch([spec.descriptors()])

@@ -7,7 +7,7 @@ import re
 import numpy as np
 import pytest
 
-from artracfd_b200 import abi
+from artracfd_b200 import abi, configs
 from artracfd_b200.abi import load_library
 
 import cases
@@ -64,3 +64,16 @@ def test_initial_field_matches_reference_on_pin_nodes():
     assert np.allclose(mine["U"][pin, 0, :], ref[pin], rtol=1e-13, atol=1e-13)
     for q, f in enumerate(("did", "fid", "lid", "gst")):
         assert np.array_equal(mine[f][pin], b.z["flags0"][pin, q])
+
+
+def test_batch_cases_are_seeded_and_cover_the_stated_ranges():
+    a = configs.batch_cases(count=48, seed=42)
+    b = configs.batch_cases(count=48, seed=42)
+    assert len(a) == 48
+    assert [(s.kind, s.n, s.Ma, s.Re) for s in a] == [(s.kind, s.n, s.Ma, s.Re) for s in b]
+    assert {s.kind for s in a} == {"tgv", "riemann"}
+    assert all(s.n in range(64, 161, 16) for s in a)
+    assert all(0.1 <= s.Ma <= 0.5 and 400.0 <= s.Re <= 3200.0 for s in a)
+    for s in a[:4]:
+        part, model = s.descriptors()
+        assert model.refMu > 0.0 and part.collapse == 0
