@@ -32,6 +32,8 @@ FP64_EXACT, FP64, FP32_BULK, FP32_HYBRID = 0, 1, 2, 3
 # the line-march kernels with 1, 2, 4 waves, then from PLANE_VARIANT the
 # plane-march kernels (Y/Z sweeps) with 1, 2, 4 waves
 BRICK_VARIANTS, PLANE_VARIANT, STAGE_VARIANTS = 2, 5, 8
+# stage kernel of a batch (acfd_batch_set_kernel)
+BATCH_BRICK, BATCH_PLANE = 0, 1
 # sync masks
 SYNC_TO, SYNC_TN, SYNC_TM, SYNC_U, SYNC_FLAGS, SYNC_ALL = 0x1, 0x2, 0x4, 0x7, 0x8, 0xF
 # boundary kinds (commons.h:83-87)
@@ -199,6 +201,7 @@ def load_library(path: str | None = None):
         "acfd_batch_advance": [vp, dp, i, dp],
         "acfd_batch_stats": [vp, ctypes.POINTER(ctypes.c_longlong)],
         "acfd_batch_set_stream": [vp, vp],
+        "acfd_batch_set_kernel": [vp, i],
     }
     for name, args in sigs.items():
         fn = getattr(lib, name)

@@ -1,9 +1,9 @@
 """A batch of independent cases advanced together (acfd_batch_*).
 
-Every RK stage of every case is one persistent launch over the tiles of all
-cases; each case keeps its own grid, model, boundary conditions and time step
-(dt from its own CFL maximum, on the device); one time step of the batch is a
-CUDA graph.
+Every RK stage of every case is one launch over the tiles of all cases (the
+plane-march kernel, or the persistent brick kernel); each case keeps its own
+grid, model, boundary conditions and time step (dt from its own CFL maximum,
+on the device); one time step of the batch is a CUDA graph.
 
     from artracfd_b200 import configs
     from artracfd_b200.batch import Batch
@@ -104,6 +104,11 @@ class Batch:
 
     def set_precision(self, mode: int):
         check(self.lib.acfd_batch_set_precision(self.h, mode), self.lib)
+
+    def set_kernel(self, kernel: int):
+        """abi.BATCH_PLANE (plane march, default when the cases allow it) or
+        abi.BATCH_BRICK (persistent brick kernel)."""
+        check(self.lib.acfd_batch_set_kernel(self.h, kernel), self.lib)
 
     def sensor_load(self, params: np.ndarray, threshold: float):
         p = np.ascontiguousarray(params, dtype=np.float32)

@@ -1257,6 +1257,13 @@ struct acfd_batch {
     int4 *d_pairs = nullptr;               // ghost gather of the copy-only cases
     long long npairs = 0;
     std::vector<int> ordered_fill;         // cases whose ghosts need the ordered fill
+    // plane-march stage kernels (all cases viscous or all inviscid, plane maps present)
+    bool plane_ok = false, plane = false, visc = false;
+    BatchPlane *d_planes = nullptr;        // [ncase][3]
+    CUtensorMap *d_pmaps = nullptr;        // [ncase][3]
+    long long *d_pprefix = nullptr;        // [3][ncase + 1] prefix sums of the plane blocks per sweep axis
+    long long pblocks[3] = {0, 0, 0};
+    int pthreads[3] = {0, 0, 0}, psmem[3] = {0, 0, 0};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int graph_mode = -1;
@@ -1320,8 +1327,15 @@ int batch_step(acfd_batch *b)
             sc.to = rk[q].to;
             sc.tn = rk[q].tn;
             sc.tm = rk[q].tm;
-            TRY(launch_stage_batch(b->d_cases, b->d_maps, b->d_prefix + (long long)s * (ncase + 1), ncase, sc,
-                                   b->d_dts, b->d_counter + launch, b->d_status, b->blocks, s, hybrid, b->stream));
+            if (b->plane) {
+                TRY(launch_stage_plane_batch(b->d_cases, b->d_planes, b->d_pmaps, b->d_pprefix + (long long)s * (ncase + 1),
+                                             b->pblocks[s], ncase, sc, b->d_dts, b->d_status, s, b->visc, hybrid,
+                                             b->pthreads[s], b->psmem[s], b->stream));
+            } else {
+                TRY(launch_stage_batch(b->d_cases, b->d_maps, b->d_prefix + (long long)s * (ncase + 1), ncase, sc,
+                                       b->d_dts, b->d_counter + launch, b->d_status, b->blocks, s, hybrid,
+                                       b->stream));
+            }
             ++launch;
             ++b->launches;
             if (b->npairs > 0) {
@@ -1439,6 +1453,66 @@ int acfd_batch_init(int ncase, const acfd_partition_t *parts, const acfd_model_t
     }
     // persistent stage launch: two resident blocks of the viscous bricks per SM
     b->blocks = 2 * b->sms;
+    // plane-march launches: one launch per stage over the plane blocks of all cases
+    std::vector<BatchPlane> hp((size_t)ncase * 3);
+    std::vector<CUtensorMap> hpm((size_t)ncase * 3);
+    std::vector<long long> pprefix((size_t)3 * (ncase + 1), 0);
+    if (st == ACFD_OK) {
+        b->visc = viscous(b->cases[0]);
+        b->plane_ok = true;
+        for (int c = 0; c < ncase && b->plane_ok; ++c) {
+            acfd_case *cs = b->cases[c];
+            if (!cs->pmaps_ok || viscous(cs) != b->visc) {
+                b->plane_ok = false;
+                break;
+            }
+            for (int s = 0; s < 3; ++s) {
+                BatchPlane &P = hp[(size_t)c * 3 + s];
+                P.pt = plane_tile(cs->grid, s, b->visc, 1, b->sms);
+                P.gk = cs->grid;
+                const long long sy = (long long)cs->grid.pitch, sz = (long long)cs->grid.pitch * cs->grid.n[1];
+                if (s == 1) {
+                    P.pt.swap = 0;
+                    P.pt.st = sy;
+                    P.pt.rs = sz;
+                } else if (s == 2) {
+                    // the Z sweep as a Y sweep of the grid with axes 1 and 2 exchanged
+                    P.pt.swap = 1;
+                    P.pt.st = sz;
+                    P.pt.rs = sy;
+                    std::swap(P.gk.n[1], P.gk.n[2]);
+                    std::swap(P.gk.lo[1], P.gk.lo[2]);
+                    std::swap(P.gk.hi[1], P.gk.hi[2]);
+                    std::swap(P.gk.dd[1], P.gk.dd[2]);
+                }
+                if (P.pt.BXp != cs->pbox[s][0] || P.pt.BC != cs->pbox[s][1]) {
+                    b->plane_ok = false;
+                }
+                hpm[(size_t)c * 3 + s] = cs->pmaps[s];
+                const long long nb = (long long)P.pt.ntx * P.pt.ntc * P.pt.nseg;
+                pprefix[(size_t)s * (ncase + 1) + c + 1] = pprefix[(size_t)s * (ncase + 1) + c] + nb;
+                b->pthreads[s] = std::max(b->pthreads[s], (P.pt.ncw + 1) * 32);
+                b->psmem[s] = std::max(b->psmem[s], plane_smem_bytes(P.pt, s));
+            }
+        }
+        for (int s = 0; s < 3; ++s) {
+            b->pblocks[s] = pprefix[(size_t)s * (ncase + 1) + ncase];
+        }
+        if (b->plane_ok) {
+            if ((e = cudaMalloc(&b->d_planes, sizeof(BatchPlane) * hp.size())) != cudaSuccess ||
+                (e = cudaMalloc(&b->d_pmaps, sizeof(CUtensorMap) * hpm.size())) != cudaSuccess ||
+                (e = cudaMalloc(&b->d_pprefix, sizeof(long long) * pprefix.size())) != cudaSuccess ||
+                (e = cudaMemcpy(b->d_planes, hp.data(), sizeof(BatchPlane) * hp.size(), cudaMemcpyHostToDevice)) !=
+                    cudaSuccess ||
+                (e = cudaMemcpy(b->d_pmaps, hpm.data(), sizeof(CUtensorMap) * hpm.size(), cudaMemcpyHostToDevice)) !=
+                    cudaSuccess ||
+                (e = cudaMemcpy(b->d_pprefix, pprefix.data(), sizeof(long long) * pprefix.size(),
+                                cudaMemcpyHostToDevice)) != cudaSuccess) {
+                st = cuda_status(e, "acfd_batch_init (plane maps)");
+            }
+        }
+        b->plane = b->plane_ok;
+    }
     const size_t nbytes[] = {sizeof(BatchCase) * ncase, sizeof(CUtensorMap) * 3 * ncase,
                              sizeof(long long) * prefix.size(), sizeof(double) * ncase, sizeof(double) * ncase,
                              sizeof(double) * mesh.size(), sizeof(double *) * ncase,
@@ -1499,6 +1573,9 @@ int acfd_batch_finalize(acfd_batch_t *b)
     cudaFree(b->d_status);
     cudaFree(b->d_levels);
     cudaFree(b->d_pairs);
+    cudaFree(b->d_planes);
+    cudaFree(b->d_pmaps);
+    cudaFree(b->d_pprefix);
     if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
     delete b;
     return ACFD_OK;
@@ -1599,6 +1676,22 @@ int acfd_batch_advance(acfd_batch_t *b, const double *cfl, int steps, double *dt
     for (acfd_case *cs : b->cases) {
         TRY(check_device_status(cs));
     }
+    return ACFD_OK;
+}
+
+int acfd_batch_set_kernel(acfd_batch_t *b, int kernel)
+{
+    TRY(batch_check(b));
+    if (kernel != ACFD_BATCH_BRICK && kernel != ACFD_BATCH_PLANE) {
+        set_error("acfd_batch_set_kernel: unknown kernel %d", kernel);
+        return ACFD_ERR_ARG;
+    }
+    if (kernel == ACFD_BATCH_PLANE && !b->plane_ok) {
+        set_error("acfd_batch_set_kernel: the plane-march batch needs all cases viscous or all inviscid");
+        return ACFD_ERR_STATE;
+    }
+    b->plane = (kernel == ACFD_BATCH_PLANE);
+    batch_release_graph(b);
     return ACFD_OK;
 }
 

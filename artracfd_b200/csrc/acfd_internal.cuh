@@ -164,6 +164,20 @@ inline int plane_smem_bytes(const PlaneTile &pt, int s)
     return plane_smem_total(pt.BXp, pt.BC, s == 0 ? pt.TR * pt.NR : 0);
 }
 
+// plane-march geometry of one case and sweep axis of a batch: the kernel's
+// grid descriptor (axes 1 and 2 exchanged for a Z sweep) and the plane tile
+struct BatchPlane {
+    Grid gk;
+    PlaneTile pt;
+};
+// plane-march stage of a batch: block b of the launch runs block
+// b - prefix[c] of case c (prefix[c] <= b < prefix[c+1]) with the case's plane
+// map pmaps[3c+s]; nthreads and smem are the largest over the cases
+int launch_stage_plane_batch(const BatchCase *cases, const BatchPlane *planes, const CUtensorMap *pmaps,
+                             const long long *prefix, long long blocks, int ncase, const StageCoefs &sc,
+                             const double *dts, int *status, int s, bool viscous, bool hybrid, int nthreads, int smem,
+                             cudaStream_t st);
+
 // learned sensor (sensor.cu)
 // Flags of the PIN nodes (the caller sets the others to 1 once); rho_p:
 // scratch of nn float2 (density and pressure of every node)

@@ -80,3 +80,16 @@ int launch_stage_plane_fp32(const Grid &g, const ModelParams &m, const StageArgs
 }
 
 }  // namespace acfd
+
+namespace acfd {
+
+int launch_stage_plane_batch(const BatchCase *cases, const BatchPlane *planes, const CUtensorMap *pmaps,
+                             const long long *prefix, long long blocks, int ncase, const StageCoefs &sc,
+                             const double *dts, int *status, int s, bool viscous, bool hybrid, int nthreads, int smem,
+                             cudaStream_t st)
+{
+    return form_fp32::launch_plane_batch_impl(cases, planes, pmaps, prefix, blocks, ncase, sc, dts, status, s, viscous,
+                                              hybrid, nthreads, smem, st);
+}
+
+}  // namespace acfd

@@ -34,9 +34,15 @@ constexpr long long kPlaneWaitLimit = 1LL << 22;
 // momentum components rho*v and rho*w trade places in every read of the
 // planes and of U[to] and in every write of U[tm], and the TMA coordinates of
 // a plane are (x, row, position) instead of (x, position, row).
+//
+// The block body is a device function of the block's index within the launch
+// (blk) so that the batched kernel runs the same code for a block of any case;
+// warps beyond the case's producer warp (a batch launch sized for its largest
+// tile) leave after the barrier set-up.
 template <int NP, bool VISC, bool HYB>
-__global__ void __launch_bounds__(kPlaneMaxThreads, sizeof(Real) == sizeof(float) ? 2 : 1)
-stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_constant__ CUtensorMap map)
+__device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams &mp, const StageArgs &a,
+                                               const PlaneTile &pt, const CUtensorMap *mapp, int blk,
+                                               unsigned char *smem)
 {
     constexpr int S = 1;
     constexpr int T2 = 2;
@@ -44,7 +50,6 @@ stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_c
     constexpr int hv = VISC ? 1 : 0;
     constexpr int NS = kPlaneSlots;
     constexpr unsigned kAll = 0xffffffffu;
-    extern __shared__ __align__(128) unsigned char smem[];
     const int pe = pt.BXp * pt.BC;  // elements of one variable in a plane
     const int plane_bytes = pe * 5 * 8;
     const int slot_doubles = plane_slot_bytes(pt.BXp, pt.BC) / 8;  // 128-byte aligned slots
@@ -60,8 +65,11 @@ stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_c
     }
     __syncthreads();
     pdl_wait();
+    if (warp > pt.ncw) {
+        return;
+    }
 
-    int b = blockIdx.x;
+    int b = blk;
     const int tx = b % pt.ntx;
     b /= pt.ntx;
     const int tc = b % pt.ntc;
@@ -89,9 +97,9 @@ stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_c
                 const int pos = p0 - H + q;
                 double *dst = ring + (size_t)slot * slot_doubles;
                 if (!pt.swap) {
-                    tma::load_5d(dst, &map, xs, pos, cs, 0, a.tn, full + slot);
+                    tma::load_5d(dst, mapp, xs, pos, cs, 0, a.tn, full + slot);
                 } else {
-                    tma::load_5d(dst, &map, xs, cs, pos, 0, a.tn, full + slot);
+                    tma::load_5d(dst, mapp, xs, cs, pos, 0, a.tn, full + slot);
                 }
                 issued = q + 1;
             }
@@ -239,6 +247,14 @@ stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_c
     }
 }
 
+template <int NP, bool VISC, bool HYB>
+__global__ void __launch_bounds__(kPlaneMaxThreads, sizeof(Real) == sizeof(float) ? 2 : 1)
+stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_constant__ CUtensorMap map)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    plane_yz_block<NP, VISC, HYB>(g, mp, a, pt, &map, (int)blockIdx.x, smem);
+}
+
 // ---------------------------------------------------------------------------
 // X sweep: the block marches along y over a tile of WX nodes along x by NR
 // z-rows.  Each consumer thread owns one interface of its row (WX + 1 per
@@ -250,14 +266,14 @@ stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_c
 // named barrier of the consumer warps per plane.
 // ---------------------------------------------------------------------------
 template <int NP, bool VISC, bool HYB>
-__global__ void __launch_bounds__(kPlaneMaxThreads, sizeof(Real) == sizeof(float) ? 2 : 1)
-stage_plane_x(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_constant__ CUtensorMap map)
+__device__ __forceinline__ void plane_x_block(const Grid &g, const ModelParams &mp, const StageArgs &a,
+                                              const PlaneTile &pt, const CUtensorMap *mapp, int blk,
+                                              unsigned char *smem)
 {
     constexpr int H = NP / 2;
     constexpr int hv = VISC ? 1 : 0;
     constexpr int NS = kPlaneSlots;
     constexpr unsigned kAll = 0xffffffffu;
-    extern __shared__ __align__(128) unsigned char smem[];
     const int pe = pt.BXp * pt.BC;
     const int plane_bytes = pe * 5 * 8;
     const int slot_doubles = plane_slot_bytes(pt.BXp, pt.BC) / 8;
@@ -276,8 +292,11 @@ stage_plane_x(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_co
     }
     __syncthreads();
     pdl_wait();
+    if (warp > pt.ncw) {
+        return;
+    }
 
-    int b = blockIdx.x;
+    int b = blk;
     const int tx = b % pt.ntx;
     b /= pt.ntx;
     const int tc = b % pt.ntc;
@@ -301,7 +320,7 @@ stage_plane_x(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_co
                     break;
                 }
                 tma::mbar_expect_tx(full + slot, plane_bytes);
-                tma::load_5d(ring + (size_t)slot * slot_doubles, &map, xs, j0 - hv + q, cs, 0, a.tn, full + slot);
+                tma::load_5d(ring + (size_t)slot * slot_doubles, mapp, xs, j0 - hv + q, cs, 0, a.tn, full + slot);
                 issued = q + 1;
             }
             for (int q = issued - NS > 0 ? issued - NS : 0; q < issued; ++q) {
@@ -437,6 +456,14 @@ stage_plane_x(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_co
 }
 
 template <int NP, bool VISC, bool HYB>
+__global__ void __launch_bounds__(kPlaneMaxThreads, sizeof(Real) == sizeof(float) ? 2 : 1)
+stage_plane_x(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_constant__ CUtensorMap map)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    plane_x_block<NP, VISC, HYB>(g, mp, a, pt, &map, (int)blockIdx.x, smem);
+}
+
+template <int NP, bool VISC, bool HYB>
 static int launch_plane_x(const Grid &g, const ModelParams &m, const StageArgs &a, const PlaneTile &pt,
                           const CUtensorMap &map, cudaStream_t st)
 {
@@ -530,6 +557,97 @@ static int launch_plane_impl(const Grid &g, const ModelParams &m, const StageArg
     return viscous ? launch_plane_s<4, true, false>(g, m, a, s, pt, map, st)
                    : launch_plane_s<4, false, false>(g, m, a, s, pt, map, st);
 }
+
+#if ACFD_FORM == 2
+// ---------------------------------------------------------------------------
+// batch: one launch covers the plane-march blocks of every case
+// ---------------------------------------------------------------------------
+template <int NP, bool VISC, bool HYB, bool XS>
+__global__ void __launch_bounds__(kPlaneMaxThreads, 2)
+stage_plane_batch(const BatchCase *__restrict__ cases, const BatchPlane *__restrict__ planes,
+                  const CUtensorMap *pmaps, const long long *__restrict__ prefix, int ncase, StageCoefs sc,
+                  const double *dts, int *status, int s)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    const long long item = blockIdx.x;
+    int lo = 0, hi = ncase - 1;  // the case whose blocks contain this one
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (prefix[mid] <= item) lo = mid; else hi = mid - 1;
+    }
+    const BatchCase &C = cases[lo];
+    const BatchPlane &P = planes[3 * lo + s];
+    StageArgs a;
+    const long long lv = 5LL * C.g.nn;
+    a.Uo = C.U + sc.to * lv;
+    a.Un = C.U + sc.tn * lv;
+    a.Um = C.U + sc.tm * lv;
+    a.did = C.did;
+    a.dt = dts + lo;
+    a.dt_scale = sc.dt_scale;
+    a.coeA = sc.coeA;
+    a.coeB = sc.coeB;
+    a.accumulate = 0;
+    a.to = sc.to;
+    a.tn = sc.tn;
+    a.tm = sc.tm;
+    a.maps = nullptr;
+    a.omaps = nullptr;
+    a.var[0] = a.var[1] = a.var[2] = 0;
+    a.status = status;
+    a.flags = C.flags;
+    const int blk = (int)(item - prefix[lo]);
+    if (XS) {
+        plane_x_block<NP, VISC, HYB>(P.gk, C.mp, a, P.pt, pmaps + 3 * lo + s, blk, smem);
+    } else {
+        plane_yz_block<NP, VISC, HYB>(P.gk, C.mp, a, P.pt, pmaps + 3 * lo + s, blk, smem);
+    }
+}
+
+template <bool VISC, bool HYB, bool XS>
+static int launch_plane_batch_one(const BatchCase *cases, const BatchPlane *planes, const CUtensorMap *pmaps,
+                                  const long long *prefix, long long blocks, int ncase, const StageCoefs &sc,
+                                  const double *dts, int *status, int s, int nthreads, int smem, cudaStream_t st)
+{
+    static bool configured[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(stage_plane_batch<6, VISC, HYB, XS>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, kPlaneSmemMax);
+        if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(stage_plane_batch)");
+        configured[dev] = true;
+    }
+    cudaError_t e = launch_k(stage_plane_batch<6, VISC, HYB, XS>, dim3((unsigned)blocks), dim3(nthreads), smem, st,
+                             cases, planes, pmaps, prefix, ncase, sc, dts, status, s);
+    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "stage_plane_batch launch");
+}
+
+static int launch_plane_batch_impl(const BatchCase *cases, const BatchPlane *planes, const CUtensorMap *pmaps,
+                                   const long long *prefix, long long blocks, int ncase, const StageCoefs &sc,
+                                   const double *dts, int *status, int s, bool viscous, bool hybrid, int nthreads,
+                                   int smem, cudaStream_t st)
+{
+    if (blocks <= 0) {
+        return ACFD_OK;
+    }
+    if (smem > kPlaneSmemMax || nthreads > kPlaneMaxThreads) {
+        set_error("batch plane launch: %d threads, %d bytes of shared memory", nthreads, smem);
+        return ACFD_ERR_ARG;
+    }
+#define ACFD_PB(V_, H_)                                                                                        \
+    return (s == 0) ? launch_plane_batch_one<V_, H_, true>(cases, planes, pmaps, prefix, blocks, ncase, sc, dts, \
+                                                           status, s, nthreads, smem, st)                       \
+                    : launch_plane_batch_one<V_, H_, false>(cases, planes, pmaps, prefix, blocks, ncase, sc, dts, \
+                                                            status, s, nthreads, smem, st);
+    if (viscous) {
+        if (hybrid) { ACFD_PB(true, true) } else { ACFD_PB(true, false) }
+    } else {
+        if (hybrid) { ACFD_PB(false, true) } else { ACFD_PB(false, false) }
+    }
+#undef ACFD_PB
+}
+#endif
 
 }  // namespace ACFD_NS
 }  // namespace acfd

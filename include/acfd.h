@@ -279,8 +279,8 @@ int acfd_mlp_adam(float *params, const float *grad, float *m, float *v, int step
 /* ---- batch of independent cases (no reference counterpart) ------------ */
 
 /* Many independent cases advanced together: each RK stage of every case is
- * one persistent launch over the tiles of all cases (the brick stage kernel
- * of the FP32 forms), each case keeps its own grid, model, boundary
+ * one launch over the tiles of all cases (the plane-march or the persistent
+ * brick stage kernel of the FP32 forms), each case keeps its own grid, model, boundary
  * conditions and time step (computed on the device from its CFL maximum, as
  * ComputeTimeStep does, solve.c:108-153), and one time step of the whole
  * batch is captured and replayed as a CUDA graph.  Cases must be 3D, WENO5,
@@ -303,6 +303,12 @@ int acfd_batch_sensor_load(acfd_batch_t *b, const float *params, float threshold
  * c; dts (optional, steps x ncase doubles) receives the dt of every case and
  * step.  Returns after the work has finished. */
 int acfd_batch_advance(acfd_batch_t *b, const double *cfl, int steps, double *dts);
+/* Stage kernel of the batch: ACFD_BATCH_PLANE (the plane march; the default
+ * when all cases are viscous or all inviscid) or ACFD_BATCH_BRICK (the
+ * persistent brick kernel that pulls (case, tile) items from a counter). */
+#define ACFD_BATCH_BRICK 0
+#define ACFD_BATCH_PLANE 1
+int acfd_batch_set_kernel(acfd_batch_t *b, int kernel);
 /* Run the batch's work on the caller's CUDA stream (cudaStream_t as void*);
  * the library's own stream is released. */
 int acfd_batch_set_stream(acfd_batch_t *b, void *stream);

@@ -1,9 +1,10 @@
 """The batch of independent cases (acfd_batch_*) against the same cases run one
 at a time through the single-case API.
 
-Each RK stage of the batch is one persistent launch over the tiles of all
-cases with the brick stage kernel; a case of the batch computes every
-interface exactly as the single-case brick kernel does, and its dt comes from
+Each RK stage of the batch is one launch over the tiles of all cases, with
+the plane-march kernel (the single-case plane variants) or the persistent
+brick kernel (the single-case brick variant 0); a case of the batch computes
+every interface exactly as the single-case kernel does, and its dt comes from
 its own CFL maximum in the reference's expression, so the batch reproduces
 the single-case runs bit for bit: states, and dt at every step.  The cases
 mix periodic (TGV), outflow (Riemann), outflow + periodic (Sod) and
@@ -23,16 +24,22 @@ pytestmark = pytest.mark.gpu
 STEPS = 3
 
 
-def _specs():
+def _specs(inviscid=True):
     rng = np.random.default_rng(7)
-    return [configs.tgv(n=16, Re=800.0, Ma=0.2, stepN=0),
-            configs.riemann_viscous(n=16, Re=1000.0, Ma=0.3, rng=rng),
-            configs.tgv(n=24, Re=1200.0, Ma=0.4, stepN=0),
-            configs.sod(m=(32, 4, 4)),
-            cases.channel()]
+    out = [configs.tgv(n=16, Re=800.0, Ma=0.2, stepN=0),
+           configs.riemann_viscous(n=16, Re=1000.0, Ma=0.3, rng=rng),
+           configs.tgv(n=24, Re=1200.0, Ma=0.4, stepN=0),
+           cases.channel()]
+    if inviscid:
+        out.insert(3, configs.sod(m=(32, 4, 4)))
+    return out
 
 
-def _single(spec, part, model, mode, steps, params=None, thr=0.5):
+BRICK = [0, 0, 0]
+PLANE = [abi.PLANE_VARIANT] * 3
+
+
+def _single(spec, part, model, mode, steps, params=None, thr=0.5, tiles=BRICK):
     node = spec.initial_nodes(part, model)
     dts, out = [], None
     with Solver(part, model, abi.FP64 if params is not None else mode) as s:
@@ -41,7 +48,7 @@ def _single(spec, part, model, mode, steps, params=None, thr=0.5):
         if params is not None:
             s.sensor_load(params, thr)
             s.set_precision(abi.FP32_HYBRID)
-        s.set_tiles([0, 0, 0])
+        s.set_tiles(tiles)
         for _ in range(steps):
             dt = s.time_step(spec.cfl)
             s.evolve(dt)
@@ -50,8 +57,10 @@ def _single(spec, part, model, mode, steps, params=None, thr=0.5):
     return np.array(dts), out
 
 
-def _batch(specs, descs, mode, steps, params=None, thr=0.5):
+def _batch(specs, descs, mode, steps, params=None, thr=0.5, kernel=None):
     with Batch(descs) as b:
+        if kernel is not None:
+            b.set_kernel(kernel)
         for c, spec in enumerate(specs):
             b.upload(c, spec.initial_nodes(*descs[c]))
             b.treat_boundary(c)
@@ -85,6 +94,39 @@ def test_batch_equals_single_cases_hybrid():
         sdt, sout = _single(spec, *descs[c], abi.FP32_HYBRID, STEPS, params, thr)
         assert np.array_equal(dts[:, c], sdt), c
         assert np.array_equal(outs[c], sout), (c, np.nanmax(np.abs(outs[c] - sout)))
+
+
+@pytest.mark.parametrize("kernel", ["plane", "brick"])
+def test_batch_viscous_cases_equal_single_cases(kernel):
+    """All cases viscous: the plane-march batch (the default) against the
+    single-case plane variants, and the brick batch against brick variant 0."""
+    specs = _specs(inviscid=False)
+    descs = [s.descriptors() for s in specs]
+    k, tiles = (abi.BATCH_PLANE, PLANE) if kernel == "plane" else (abi.BATCH_BRICK, BRICK)
+    dts, outs, _ = _batch(specs, descs, abi.FP32_BULK, STEPS, kernel=k)
+    for c, spec in enumerate(specs):
+        sdt, sout = _single(spec, *descs[c], abi.FP32_BULK, STEPS, tiles=tiles)
+        assert np.array_equal(dts[:, c], sdt), c
+        assert np.array_equal(outs[c], sout), (c, np.nanmax(np.abs(outs[c] - sout)))
+
+
+@pytest.mark.skipif(not __import__("os").path.exists(sensor.WEIGHTS), reason="no trained sensor weights")
+def test_batch_plane_hybrid_equals_single_cases():
+    specs = _specs(inviscid=False)
+    descs = [s.descriptors() for s in specs]
+    params, thr, _ = sensor.load(sensor.WEIGHTS)
+    dts, outs, _ = _batch(specs, descs, abi.FP32_HYBRID, STEPS, params, thr, kernel=abi.BATCH_PLANE)
+    for c, spec in enumerate(specs):
+        sdt, sout = _single(spec, *descs[c], abi.FP32_HYBRID, STEPS, params, thr, tiles=PLANE)
+        assert np.array_equal(dts[:, c], sdt), c
+        assert np.array_equal(outs[c], sout), (c, np.nanmax(np.abs(outs[c] - sout)))
+
+
+def test_batch_mixed_viscosity_has_no_plane_kernel():
+    specs = _specs(inviscid=True)
+    with Batch([s.descriptors() for s in specs]) as b:
+        with pytest.raises(abi.AcfdError):
+            b.set_kernel(abi.BATCH_PLANE)
 
 
 def test_batch_rejects_unsupported_cases():
