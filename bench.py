@@ -545,7 +545,9 @@ def run_batch(args, rank, world, local_rank):
                                "{64..160 step 16}, Ma U[0.1,0.5], Re U[400,3200], seed 42; WENO5/RK3",
                    "cases": len(specs), "pin_nodes": total,
                    "kinds": {k: sum(1 for s in specs if s.kind == k) for k in ("tgv", "riemann")},
-                   "form": "hybrid (learned sensor, FP32 bulk)", "persistent_launches_per_step": 18},
+                   "form": "hybrid (learned sensor, FP32 bulk)",
+                   "stage_kernel": "plane march: one launch per RK stage over the plane blocks of all cases",
+                   "stage_launches_per_step": 18},
         "ms_per_step": secb / (steps - 1) * 1e3,
         "one_at_a_time_fp64": {"value": total * steps / sec64 / 1e6, "ms_per_step_all_cases": sec64 / steps * 1e3,
                                "what": "each case alone through the single-case API, plain FP64 path, host dt "
