@@ -373,26 +373,31 @@ __global__ void __launch_bounds__(kFlagWarps * 32) flags_mma_kernel(Grid g, cons
         }
     }
     const float b3 = params[oB3];
+    // 32-bit work indices (the launcher checks that 3 * PIN and the node
+    // count fit): 64-bit divisions would cost more than the network
     const int Lx = g.hi[0] - g.lo[0], Ly = g.hi[1] - g.lo[1], Lz = g.hi[2] - g.lo[2];
-    const long long pin = (long long)Lx * Ly * Lz;
-    const long long ngroups = ((pin + 31) / 32) * 3;
-    const long long nwarps = (long long)gridDim.x * kFlagWarps;
+    const int pin = Lx * Ly * Lz;
+    const int ngroups = ((pin + 31) / 32) * 3;
+    const int nwarps = (int)gridDim.x * kFlagWarps;
+    const int sy = g.pitch, sz = g.pitch * g.n[1];
     unsigned nflag = 0;
-    for (long long grp = (long long)blockIdx.x * kFlagWarps + w; grp < ngroups; grp += nwarps) {
-        const int s = (int)(grp % 3);
-        const long long q = (grp / 3) * 32 + lane;
+    for (int grp = (int)blockIdx.x * kFlagWarps + w; grp < ngroups; grp += nwarps) {
+        const int gq3 = grp / 3;
+        const int s = grp - 3 * gq3;
+        const int q = gq3 * 32 + lane;
         const bool valid = q < pin;
         long long id = 0;
         float f[kIn];
 #pragma unroll
         for (int m = 0; m < kIn; ++m) f[m] = 0.0f;
         if (valid) {
-            const int i = g.lo[0] + (int)(q % Lx);
-            const long long rest = q / Lx;
-            const int j = g.lo[1] + (int)(rest % Ly);
-            const int k = g.lo[2] + (int)(rest / Ly);
-            id = node_of(g, i, j, k);
-            const long long st = stride(g, s);
+            const int rest = q / Lx;
+            const int i = g.lo[0] + (q - rest * Lx);
+            const int kk = rest / Ly;
+            const int j = g.lo[1] + (rest - kk * Ly);
+            const int k = g.lo[2] + kk;
+            id = (long long)(k * sz + j * sy + i);
+            const long long st = (s == 0) ? 1 : (s == 1 ? sy : sz);
             float2 v[5];
             float mr = 0.0f, mp = 0.0f;
 #pragma unroll
@@ -486,6 +491,10 @@ int launch_sensor_flags(const Grid &g, const ModelParams &m, const double *U, co
 {
     const long long pin = (long long)(g.hi[0] - g.lo[0]) * (g.hi[1] - g.lo[1]) * (g.hi[2] - g.lo[2]);
     if (pin <= 0) return ACFD_OK;
+    if (3 * pin + 96 > (long long)INT32_MAX || g.nn > (long long)INT32_MAX) {
+        set_error("sensor flags: case of %lld computed nodes exceeds the 32-bit work indices", pin);
+        return ACFD_ERR_ARG;
+    }
     ACFD_CUDA(launch_k(sensor::rho_p_kernel, dim3((unsigned)((g.nn + 255) / 256)), dim3(256), 0, st, g.nn,
                        m.gamma - 1.0, U, rho_p));
     const long long groups = ((pin + 31) / 32) * 3;
