@@ -239,15 +239,9 @@ __global__ void cfl_partial(Grid g, ModelParams mp, const double *U, const int *
     const int Lx = g.hi[0] - g.lo[0], Ly = g.hi[1] - g.lo[1], Lz = g.hi[2] - g.lo[2];
     const long long total = (long long)Lx * Ly * Lz;
     double m0 = 0.0, m1 = 0.0, m2 = 0.0;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int i = g.lo[0] + (int)(t % Lx);
-        const long long rest = t / Lx;
-        const int j = g.lo[1] + (int)(rest % Ly);
-        const int k = g.lo[2] + (int)(rest / Ly);
-        const long long id = node_of(g, i, j, k);
+    auto visit = [&](long long id) {
         if (did[id] != 0) {
-            continue;
+            return;
         }
         double Uc[5], Uo[6];
         load5(U, g.nn, id, Uc);
@@ -256,6 +250,24 @@ __global__ void cfl_partial(Grid g, ModelParams mp, const double *U, const int *
         m0 = vmax_of(m0, fabs(Uo[1]) + c);
         m1 = vmax_of(m1, fabs(Uo[2]) + c);
         m2 = vmax_of(m2, fabs(Uo[3]) + c);
+    };
+    if (total < (long long)INT32_MAX / 2 && g.nn < (long long)INT32_MAX) {
+        // 32-bit work indices: 64-bit divisions would cost more than the loads
+        const int tot = (int)total, sy = g.pitch, sz = g.pitch * g.n[1];
+        for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
+            const int rest = t / Lx;
+            const int kk = rest / Ly;
+            visit((long long)((g.lo[2] + kk) * sz + (g.lo[1] + rest - kk * Ly) * sy + g.lo[0] + t - rest * Lx));
+        }
+    } else {
+        for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+             t += (long long)gridDim.x * blockDim.x) {
+            const int i = g.lo[0] + (int)(t % Lx);
+            const long long rest = t / Lx;
+            const int j = g.lo[1] + (int)(rest % Ly);
+            const int k = g.lo[2] + (int)(rest / Ly);
+            visit(node_of(g, i, j, k));
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -280,16 +292,29 @@ __global__ void cfl_partial(Grid g, ModelParams mp, const double *U, const int *
     }
 }
 
+// One warp: each lane takes every 32nd block, then a shuffle tree.  Every
+// partial maximum starts from 0 and a NaN never replaces a value (vmax_of), so
+// no NaN enters and the maximum does not depend on the order of combination.
 __global__ void cfl_final(const double *part, int nblocks, double *out)
 {
     pdl_wait();
-    const int s = threadIdx.x;
-    if (s < 3) {
-        double m = 0.0;
-        for (int b = 0; b < nblocks; ++b) {
-            m = vmax_of(m, part[3 * b + s]);
+    const int lane = threadIdx.x & 31;
+    double m[3] = {0.0, 0.0, 0.0};
+    for (int b = lane; b < nblocks; b += 32) {
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+            m[s] = vmax_of(m[s], part[3 * b + s]);
         }
-        out[s] = m;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+            m[s] = vmax_of(m[s], __shfl_xor_sync(0xffffffffu, m[s], o));
+        }
+    }
+    if (lane < 3) {
+        out[lane] = m[lane];
     }
 }
 

@@ -376,23 +376,29 @@ __device__ __forceinline__ void plane_x_block(const Grid &g, const ModelParams &
     for (int q = 0; q < 2 * hv; ++q) {
         ok = ok && wait_plane(q);  // rows j0-1 and j0 (viscous)
     }
+    // sensor flags of the interface's nodes xi-1 .. xi+2 and the did of node
+    // xi, loaded one row ahead of their use
+    auto row_flags = [&](long long idr) {
+        return (unsigned)(fl[idr - 1] | fl[idr] | fl[idr + 1] | fl[idr + 2]);
+    };
+    unsigned fl_n = (HYB && active) ? row_flags(xz + (long long)j0 * sy) : 1u;
+    int did_n = upd ? a.did[xz + (long long)j0 * sy] : 1;
     int buf = 0;
     for (int j = j0; j < j1; ++j) {
         const int q = j - j0 + hv;  // plane of row j
         const long long id = xz + (long long)j * sy;
-        int did = 1;
+        const int did = did_n;
+        const unsigned fl_j = fl_n;
+        if (j + 1 < j1) {
+            if (upd) did_n = a.did[id + sy];
+            if (HYB && active) fl_n = row_flags(id + sy);
+        }
         double uo[5];
-        if (upd) {
-            did = a.did[id];
-            if (!same_o && !a.accumulate) {
+        if (upd && !same_o && !a.accumulate) {
 #pragma unroll
-                for (int v = 0; v < 5; ++v) uo[v] = a.Uo[v * nn + id];
-            }
+            for (int v = 0; v < 5; ++v) uo[v] = a.Uo[v * nn + id];
         }
-        bool full_w = true;
-        if (HYB && active) {
-            full_w = (fl[id - 1] | fl[id] | fl[id + 1] | fl[id + 2]) != 0;
-        }
+        const bool full_w = !HYB || fl_j != 0u;
         ok = ok && wait_plane(q + hv);  // row j+1 (viscous) or j
         const double *P = plane(ok ? q : 0);
         Real W[NP][5];

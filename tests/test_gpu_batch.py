@@ -6,8 +6,9 @@ the plane-march kernel (the single-case plane variants) or the persistent
 brick kernel (the single-case brick variant 0); a case of the batch computes
 every interface exactly as the single-case kernel does, and its dt comes from
 its own CFL maximum in the reference's expression, so the batch reproduces
-the single-case runs bit for bit: states, and dt at every step (the hybrid
-plane-march batch to FP32 round-off, see its test).  The cases
+the single-case runs bit for bit with the brick kernel (states, and dt at
+every step) and to FP32 round-off with the plane-march kernel (see its
+test).  The cases
 mix periodic (TGV), outflow (Riemann), outflow + periodic (Sod) and
 inflow/outflow/wall/periodic boundaries (channel, the ordered ghost fill).
 """
@@ -99,32 +100,36 @@ def test_batch_equals_single_cases_hybrid():
         assert np.array_equal(outs[c], sout), (c, np.nanmax(np.abs(outs[c] - sout)))
 
 
-@pytest.mark.parametrize("kernel", ["plane", "brick"])
-def test_batch_viscous_cases_equal_single_cases(kernel):
-    """All cases viscous: the plane-march batch (the default) against the
-    single-case plane variants, and the brick batch against brick variant 0."""
+def test_batch_brick_viscous_cases_equal_single_cases():
+    """All cases viscous, the persistent brick batch against brick variant 0."""
     specs = _specs(inviscid=False)
     descs = [s.descriptors() for s in specs]
-    k, tiles = (abi.BATCH_PLANE, PLANE) if kernel == "plane" else (abi.BATCH_BRICK, BRICK)
-    dts, outs, _ = _batch(specs, descs, abi.FP32_BULK, STEPS, kernel=k)
+    dts, outs, _ = _batch(specs, descs, abi.FP32_BULK, STEPS, kernel=abi.BATCH_BRICK)
     for c, spec in enumerate(specs):
-        sdt, sout = _single(spec, *descs[c], abi.FP32_BULK, STEPS, tiles=tiles)
+        sdt, sout = _single(spec, *descs[c], abi.FP32_BULK, STEPS, tiles=BRICK)
         assert np.array_equal(dts[:, c], sdt), c
         assert np.array_equal(outs[c], sout), (c, np.nanmax(np.abs(outs[c] - sout)))
 
 
-@pytest.mark.skipif(not __import__("os").path.exists(sensor.WEIGHTS), reason="no trained sensor weights")
-def test_batch_plane_hybrid_matches_single_cases():
-    """The hybrid plane-march batch is the single-case hybrid plane kernel's
-    code compiled in another kernel: the compiler may contract a different
-    set of FP32 multiply-adds into FMAs there, so the two agree to FP32
-    round-off (the first dt, computed before any FP32 stage, bit for bit)."""
+@pytest.mark.parametrize("form", ["fp32", "hybrid"])
+def test_batch_plane_matches_single_cases(form):
+    """The plane-march batch (the default for all-viscous batches) runs the
+    single-case plane kernels' block code inside another kernel, where the
+    compiler may contract a different set of FP32 multiply-adds into FMAs:
+    the two agree to FP32 round-off (the first dt, computed before any FP32
+    stage, bit for bit)."""
     specs = _specs(inviscid=False)
     descs = [s.descriptors() for s in specs]
-    params, thr, _ = sensor.load(sensor.WEIGHTS)
-    dts, outs, _ = _batch(specs, descs, abi.FP32_HYBRID, STEPS, params, thr, kernel=abi.BATCH_PLANE)
+    if form == "hybrid":
+        if not __import__("os").path.exists(sensor.WEIGHTS):
+            pytest.skip("no trained sensor weights")
+        params, thr, _ = sensor.load(sensor.WEIGHTS)
+        mode = abi.FP32_HYBRID
+    else:
+        params, thr, mode = None, 0.5, abi.FP32_BULK
+    dts, outs, _ = _batch(specs, descs, mode, STEPS, params, thr, kernel=abi.BATCH_PLANE)
     for c, spec in enumerate(specs):
-        sdt, sout = _single(spec, *descs[c], abi.FP32_HYBRID, STEPS, params, thr, tiles=PLANE)
+        sdt, sout = _single(spec, *descs[c], mode, STEPS, params, thr, tiles=PLANE)
         assert dts[0, c] == sdt[0], c
         assert np.all(np.abs(dts[:, c] - sdt) <= 1e-6 * sdt), (c, dts[:, c], sdt)
         assert rel_err(outs[c], sout) <= TOL_FP32_ORDER, (c, rel_err(outs[c], sout))
