@@ -56,7 +56,9 @@ int launch_fhat_batch_fp32(const ModelParams &, int, const double *, double *, i
 struct IbState;
 int ib_create(IbState **out);
 void ib_destroy(IbState *ib);
-int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, cudaStream_t st);
+int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, const acfd_partition_t &part,
+              cudaStream_t st);
+int ib_treat_launches(const IbState *ib, const acfd_partition_t &part);
 int ib_count(const IbState *ib);
 int ib_compute_geometric_field(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partition_t &part,
                                double *U, int *flags, cudaStream_t st);
@@ -397,7 +399,7 @@ int treat_boundary(acfd_case *cs, int tn)
         }
     }
     if (cs->ib && ib_count(cs->ib) > 0) {
-        cs->launches += (long long)cs->part.gl * ((ib_count(cs->ib) + 7) / 8);
+        cs->launches += ib_treat_launches(cs->ib, cs->part);
     }
     double *U = level(cs, tn);
     if (cs->bc_gather) {
@@ -1130,7 +1132,7 @@ int acfd_geo_upload(acfd_case_t *cs, const acfd_polyhedron_t *poly, int totN)
         set_error("acfd_geo_upload: bad body list");
         return ACFD_ERR_ARG;
     }
-    TRY(ib_upload(cs->ib, poly, totN, cs->stream));
+    TRY(ib_upload(cs->ib, poly, totN, cs->part, cs->stream));
     release_graph(cs);
     return ACFD_OK;
 }

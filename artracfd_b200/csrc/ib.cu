@@ -19,6 +19,7 @@
 //    fluid nodes or layer r-1 only; bodies do not read each other).
 #include <algorithm>
 #include <cfloat>
+#include <climits>
 #include <vector>
 
 #include "acfd_internal.cuh"
@@ -46,6 +47,9 @@ struct IbState {
     long long joined_n = 0;
     int *status = nullptr;  // device error word
     int count = 0;
+    int4 *ghosts = nullptr;  // ghost list of a boundary treatment
+    int *nghost = nullptr;
+    int ghost_cap = 0;
 };
 
 namespace {
@@ -383,8 +387,11 @@ struct BoxList {
     int nb;
 };
 
-__global__ void ib_layer(IbGrid G, ModelParams mp, const DevBody *bodies, BoxList bl, double *U, int *flags,
-                         int tn, int r, int *status)
+// Ghost list: every ghost node of layers 1..gl of every body, as
+// (i, j, k, body | layer << 24).  The flags do not change during a boundary
+// treatment and a node belongs to one body only, so a node is listed once;
+// the order of the list is free (nodes of one layer are independent).
+__global__ void ib_list(IbGrid G, BoxList bl, const int *flags, int4 *ghosts, int *nghost, int cap, int *status)
 {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= bl.start[bl.nb]) return;
@@ -397,69 +404,198 @@ __global__ void ib_layer(IbGrid G, ModelParams mp, const DevBody *bodies, BoxLis
     const int j = bl.lo[q][1] + (int)(rest % bl.ext[q][1]);
     const int k = bl.lo[q][2] + (int)(rest / bl.ext[q][1]);
     const Grid &g = G.g;
-    const long long nn = g.nn;
     const long long id = node_of(g, i, j, k);
-    if ((r != flags[3 * nn + id]) || (n + 1 != flags[id])) return;
-    const DevBody &B = bodies[n];
-    double *Ut = U + (long long)tn * 5 * nn;
-    double pG[3], UoG[6];
-    node_point(G, k, j, i, pG);
-    if (G.ibmLayer >= r) {
-        double pO[3], pI[3], N[3], UoO[6], UoI[6];
-        const int fid = flags[nn + id];
-        if (B.faceN > 0 && (fid < 0 || fid >= B.faceN)) {
-            atomicExch(status, 3);  // ghost node without a valid closest facet
-            return;
-        }
-        if (!surface_data(pG, fid, B, pO, pI, N)) {
-            atomicExch(status, 2);
-            return;
-        }
-        const int cI[3] = {map_node(pI[0], G.dmin[0], g.dd[0], G.ng[0]), map_node(pI[1], G.dmin[1], g.dd[1], G.ng[1]),
-                           map_node(pI[2], G.dmin[2], g.dd[2], G.ng[2])};
-        // ReconstructFlow (immersed_boundary.c:357-412)
-        double wsum = idw(G, mp, Ut, flags, nullptr, cI, pI, kIbR, kTypeD, 0, UoI, status);
-        const double w = 1.0 / wsum;
-        const double rr[3] = {pO[0] - B.O[0], pO[1] - B.O[1], pO[2] - B.O[2]};
-        double Vs[3];
-        Vs[0] = B.W[1] * rr[2] - B.W[2] * rr[1];
-        Vs[1] = B.W[2] * rr[0] - B.W[0] * rr[2];
-        Vs[2] = B.W[0] * rr[1] - B.W[1] * rr[0];
-        Vs[0] = B.V[0] + Vs[0];
-        Vs[1] = B.V[1] + Vs[1];
-        Vs[2] = B.V[2] + Vs[2];
-        if (0.0 < B.cf) {
-            UoO[1] = Vs[0];
-            UoO[2] = Vs[1];
-            UoO[3] = Vs[2];
-        } else {
-            const double V[3] = {UoI[1] * w, UoI[2] * w, UoI[3] * w};
-            double Ta[3], Tb[3], rhs[3];
-            orthogonal_space(N, Ta, Tb);
-            rhs[0] = dot3(Vs, N);
-            rhs[1] = dot3(V, Ta);
-            rhs[2] = dot3(V, Tb);
-            for (int s = 0; s < 3; ++s) UoO[s + 1] = N[s] * rhs[0] + Ta[s] * rhs[1] + Tb[s] * rhs[2];
-        }
-        UoO[4] = UoI[4] * w;
-        UoO[5] = (0.0 > B.T) ? UoI[5] * w : B.T;
-        add_weighted(UoO, G.tinyL, dist2(pI, pO), wsum, UoI);
-        for (int v = 0; v < 6; ++v) UoI[v] = UoI[v] / wsum;
-        // method of images
-        UoG[1] = UoO[1] + UoO[1] - UoI[1];
-        UoG[2] = UoO[2] + UoO[2] - UoI[2];
-        UoG[3] = UoO[3] + UoO[3] - UoI[3];
-        UoG[4] = UoI[4];
-        UoG[5] = UoI[5];
-    } else {
-        const int cG[3] = {i, j, k};
-        const double ws = idw(G, mp, Ut, flags, nullptr, cG, pG, 1, r - 1, n + 1, UoG, status);
-        for (int v = 0; v < 6; ++v) UoG[v] = UoG[v] / ws;
+    const int gst = flags[3 * g.nn + id];
+    if (gst < 1 || gst > G.gl || n + 1 != flags[id]) return;
+    const int slot = atomicAdd(nghost, 1);
+    if (slot >= cap) {
+        atomicExch(status, 4);
+        return;
     }
-    UoG[0] = UoG[4] / (UoG[5] * mp.gasR);
-    double Uc[5];
-    to_conservative(mp.gamma, UoG, Uc);
-    for (int v = 0; v < 5; ++v) Ut[v * nn + id] = Uc[v];
+    ghosts[slot] = make_int4(i, j, k, n | (gst << 24));
+}
+
+constexpr int kGhostWarps = 4;    // warps per block of ib_ghost
+constexpr int kIdwBatch = 4;      // candidates per lane evaluated before the ordered sum
+
+// Inverse distance weighting by one warp (the candidates of the serial
+// version's k, j, i loop order, 32 x kIdwBatch at a time).  Every lane
+// evaluates candidates and writes w and Uoh[n] * w to the warp's shared
+// scratch; lanes 0..6 then add them in candidate order, each lane one sum
+// (Uo[0..5], wsum), so every sum takes exactly the serial version's
+// additions in the same order.  All lanes return the same values.
+__device__ double idw_warp(const IbGrid &G, const ModelParams &mp, const double *U, const int *flags,
+                           const int c[3], const double p[3], int h, int type, int did, double Uo[6],
+                           double (*sp)[8], int *status)
+{
+    const Grid &g = G.g;
+    const long long nn = g.nn;
+    const int *fdid = flags;
+    const int *fgst = flags + 3 * nn;
+    const int lane = threadIdx.x & 31;
+    double acc = 0.0;
+    const int rmax = g.n[0] + g.n[1] + g.n[2];
+    bool failed = false;
+    for (int r = h, tally = 0; 0 == tally; ++r) {
+        if (r > rmax) {
+            failed = true;  // no qualifying node: the reference would not terminate
+            break;
+        }
+        const long long side = 2 * r + 1;
+        const long long total = side * side * side;
+        for (long long base = 0; base < total; base += 32 * kIdwBatch) {
+            bool qual[kIdwBatch];
+            long long ids[kIdwBatch];
+            int cc[kIdwBatch][3];
+#pragma unroll
+            for (int b = 0; b < kIdwBatch; ++b) {
+                const long long cand = base + 32 * b + lane;
+                qual[b] = false;
+                ids[b] = 0;
+                cc[b][0] = cc[b][1] = cc[b][2] = 0;
+                if (cand < total) {
+                    const int ih = (int)(cand % side) - r;
+                    const long long rest = cand / side;
+                    const int jh = (int)(rest % side) - r;
+                    const int kh = (int)(rest / side) - r;
+                    const int i = c[0] + ih, j = c[1] + jh, k = c[2] + kh;
+                    cc[b][0] = i;
+                    cc[b][1] = j;
+                    cc[b][2] = k;
+                    if (in_pin(g, k, j, i)) {
+                        ids[b] = node_of(g, i, j, k);
+                        qual[b] = true;
+                    }
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < kIdwBatch; ++b) {
+                if (qual[b]) {
+                    const long long id = ids[b];
+                    bool ok = (did == fdid[id]);
+                    if (ok && type != kTypeD) ok = (type == fgst[id]);
+                    qual[b] = ok;
+                }
+            }
+            unsigned mask[kIdwBatch];
+#pragma unroll
+            for (int b = 0; b < kIdwBatch; ++b) {
+                if (qual[b]) {
+                    const long long id = ids[b];
+                    double ph[3], Uh[5], Uoh[6];
+                    node_point(G, cc[b][2], cc[b][1], cc[b][0], ph);
+                    for (int v = 0; v < 5; ++v) Uh[v] = U[v * nn + id];
+                    to_primitive(mp.gamma, mp.gasR, Uh, Uoh);
+                    double w = dist2(p, ph);
+                    if (G.tinyL > w) w = G.tinyL;
+                    w = 1.0 / w;
+                    double *row = sp[32 * b + lane];
+                    for (int v = 0; v < 6; ++v) row[v] = Uoh[v] * w;
+                    row[6] = w;
+                }
+                mask[b] = __ballot_sync(0xffffffffu, qual[b]);
+                tally += __popc(mask[b]);
+            }
+            __syncwarp();
+            if (lane < 7) {
+#pragma unroll
+                for (int b = 0; b < kIdwBatch; ++b) {
+                    for (unsigned m = mask[b]; m; m &= m - 1) acc = acc + sp[32 * b + __ffs(m) - 1][lane];
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if (failed && lane == 0) atomicExch(status, 1);
+    for (int n = 0; n < 6; ++n) Uo[n] = __shfl_sync(0xffffffffu, acc, n);
+    return __shfl_sync(0xffffffffu, acc, 6);
+}
+
+// ghost layer r of every body (immersed_boundary.c:294-338), one warp per
+// listed ghost node; the scalar parts run redundantly in all lanes of the
+// warp, the searches of the reconstruction are shared out over the lanes
+__global__ void __launch_bounds__(kGhostWarps * 32) ib_ghost(IbGrid G, ModelParams mp, const DevBody *bodies,
+                                                             const int4 *ghosts, const int *nghost, int cap,
+                                                             double *U, const int *flags, int tn, int r,
+                                                             int *status)
+{
+    __shared__ double scratch[kGhostWarps][32 * kIdwBatch][8];
+    const int lane = threadIdx.x & 31;
+    double (*sp)[8] = scratch[threadIdx.x >> 5];
+    const int count = min(*nghost, cap);  // an overflowing list has set the status
+    const Grid &g = G.g;
+    const long long nn = g.nn;
+    double *Ut = U + (long long)tn * 5 * nn;
+    for (int e = blockIdx.x * kGhostWarps + (threadIdx.x >> 5); e < count; e += gridDim.x * kGhostWarps) {
+        const int4 q = ghosts[e];
+        if ((q.w >> 24) != r) continue;
+        const int n = q.w & 0xffffff;
+        const int i = q.x, j = q.y, k = q.z;
+        const long long id = node_of(g, i, j, k);
+        const DevBody &B = bodies[n];
+        double pG[3], UoG[6];
+        node_point(G, k, j, i, pG);
+        if (G.ibmLayer >= r) {
+            double pO[3], pI[3], N[3], UoO[6], UoI[6];
+            const int fid = flags[nn + id];
+            if (B.faceN > 0 && (fid < 0 || fid >= B.faceN)) {
+                if (lane == 0) atomicExch(status, 3);  // ghost node without a valid closest facet
+                continue;
+            }
+            if (!surface_data(pG, fid, B, pO, pI, N)) {
+                if (lane == 0) atomicExch(status, 2);
+                continue;
+            }
+            const int cI[3] = {map_node(pI[0], G.dmin[0], g.dd[0], G.ng[0]),
+                               map_node(pI[1], G.dmin[1], g.dd[1], G.ng[1]),
+                               map_node(pI[2], G.dmin[2], g.dd[2], G.ng[2])};
+            // ReconstructFlow (immersed_boundary.c:357-412)
+            double wsum = idw_warp(G, mp, Ut, flags, cI, pI, kIbR, kTypeD, 0, UoI, sp, status);
+            const double w = 1.0 / wsum;
+            const double rr[3] = {pO[0] - B.O[0], pO[1] - B.O[1], pO[2] - B.O[2]};
+            double Vs[3];
+            Vs[0] = B.W[1] * rr[2] - B.W[2] * rr[1];
+            Vs[1] = B.W[2] * rr[0] - B.W[0] * rr[2];
+            Vs[2] = B.W[0] * rr[1] - B.W[1] * rr[0];
+            Vs[0] = B.V[0] + Vs[0];
+            Vs[1] = B.V[1] + Vs[1];
+            Vs[2] = B.V[2] + Vs[2];
+            if (0.0 < B.cf) {
+                UoO[1] = Vs[0];
+                UoO[2] = Vs[1];
+                UoO[3] = Vs[2];
+            } else {
+                const double V[3] = {UoI[1] * w, UoI[2] * w, UoI[3] * w};
+                double Ta[3], Tb[3], rhs[3];
+                orthogonal_space(N, Ta, Tb);
+                rhs[0] = dot3(Vs, N);
+                rhs[1] = dot3(V, Ta);
+                rhs[2] = dot3(V, Tb);
+                for (int s = 0; s < 3; ++s) UoO[s + 1] = N[s] * rhs[0] + Ta[s] * rhs[1] + Tb[s] * rhs[2];
+            }
+            UoO[4] = UoI[4] * w;
+            UoO[5] = (0.0 > B.T) ? UoI[5] * w : B.T;
+            add_weighted(UoO, G.tinyL, dist2(pI, pO), wsum, UoI);
+            for (int v = 0; v < 6; ++v) UoI[v] = UoI[v] / wsum;
+            // method of images
+            UoG[1] = UoO[1] + UoO[1] - UoI[1];
+            UoG[2] = UoO[2] + UoO[2] - UoI[2];
+            UoG[3] = UoO[3] + UoO[3] - UoI[3];
+            UoG[4] = UoI[4];
+            UoG[5] = UoI[5];
+        } else {
+            const int cG[3] = {i, j, k};
+            const double ws = idw_warp(G, mp, Ut, flags, cG, pG, 1, r - 1, n + 1, UoG, sp, status);
+            for (int v = 0; v < 6; ++v) UoG[v] = UoG[v] / ws;
+        }
+        UoG[0] = UoG[4] / (UoG[5] * mp.gasR);
+        double Uc[5];
+        to_conservative(mp.gamma, UoG, Uc);
+        double mine = Uc[0];
+#pragma unroll
+        for (int v = 1; v < 5; ++v) mine = (lane == v) ? Uc[v] : mine;
+        if (lane < 5) Ut[lane * nn + id] = mine;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -684,6 +820,10 @@ int read_status(IbState *ib, cudaStream_t st)
         set_error("immersed boundary: ghost node with a closest-facet id outside the body's facets");
         return ACFD_ERR_DEVICE;
     }
+    if (h == 4) {
+        set_error("immersed boundary: ghost list overflow");
+        return ACFD_ERR_DEVICE;
+    }
     return ACFD_OK;
 }
 
@@ -715,6 +855,9 @@ static void ib_release_geometry(IbState *ib)
     ib->dev = nullptr;
     ib->host.clear();
     ib->count = 0;
+    ib->ghosts = nullptr;
+    ib->nghost = nullptr;
+    ib->ghost_cap = 0;
 }
 
 void ib_destroy(IbState *ib)
@@ -731,7 +874,7 @@ int ib_count(const IbState *ib)
     return ib ? ib->count : 0;
 }
 
-int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, cudaStream_t st)
+int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, const acfd_partition_t &part, cudaStream_t st)
 {
     ACFD_CUDA(cudaStreamSynchronize(st));
     ib_release_geometry(ib);
@@ -791,6 +934,33 @@ int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, cudaStream_t
     }
     ACFD_CUDA(cudaMalloc(&ib->dev, sizeof(DevBody) * totN));
     ACFD_CUDA(cudaMemcpy(ib->dev, ib->host.data(), sizeof(DevBody) * totN, cudaMemcpyHostToDevice));
+    // ghost list: a node is listed at most once, so the smaller of the
+    // bodies' node boxes and the computed nodes bounds it
+    if (totN >= (1 << 24) || part.gl >= 128) {
+        set_error("immersed boundary: %d bodies, %d ghost layers (at most %d, 127)", totN, part.gl, (1 << 24) - 1);
+        return ACFD_ERR_ARG;
+    }
+    long long cap = 0;
+    for (int n = 0; n < totN; ++n) {
+        int lo[3], ext[3];
+        body_box(part, ib->host[n], lo, ext);
+        cap += (long long)ext[0] * ext[1] * ext[2];
+    }
+    long long pin = 1;
+    for (int s = 0; s < 3; ++s) pin *= std::max(0, part.ns[0][s][1] - part.ns[0][s][0]);
+    cap = std::max(1LL, std::min(cap, pin));
+    if (cap > INT_MAX) {
+        set_error("immersed boundary: ghost list of %lld nodes", cap);
+        return ACFD_ERR_ARG;
+    }
+    void *gl_buf = nullptr, *cnt = nullptr;
+    ACFD_CUDA(cudaMalloc(&gl_buf, sizeof(int4) * (size_t)cap));
+    ib->buffers.push_back(gl_buf);
+    ACFD_CUDA(cudaMalloc(&cnt, sizeof(int)));
+    ib->buffers.push_back(cnt);
+    ib->ghosts = (int4 *)gl_buf;
+    ib->nghost = (int *)cnt;
+    ib->ghost_cap = (int)cap;
     ACFD_CUDA(cudaDeviceSynchronize());
     ib->count = totN;
     return ACFD_OK;
@@ -813,17 +983,30 @@ int ib_treat(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partit
 {
     if (!ib || ib->count == 0) return ACFD_OK;
     const IbGrid G = make_ibgrid(g, part, m.ibmLayer);
+    ACFD_CUDA(cudaMemsetAsync(ib->nghost, 0, sizeof(int), st));
+    for (int n0 = 0; n0 < ib->count; n0 += 8) {
+        BoxList bl;
+        boxes_of(ib, part, n0, bl);
+        const long long total = bl.start[bl.nb];
+        if (total == 0) continue;
+        ib_list<<<blocks_for(total, 256), 256, 0, st>>>(G, bl, flags, ib->ghosts, ib->nghost, ib->ghost_cap,
+                                                        ib->status);
+        ACFD_CUDA(cudaGetLastError());
+    }
+    // one warp per listed node, at most a few waves of resident warps
+    const unsigned blocks = (unsigned)std::min<long long>(blocks_for(ib->ghost_cap, kGhostWarps), 148LL * 12);
     for (int r = 1; r <= part.gl; ++r) {
-        for (int n0 = 0; n0 < ib->count; n0 += 8) {
-            BoxList bl;
-            boxes_of(ib, part, n0, bl);
-            const long long total = bl.start[bl.nb];
-            if (total == 0) continue;
-            ib_layer<<<blocks_for(total, 128), 128, 0, st>>>(G, m, ib->dev, bl, U, flags, tn, r, ib->status);
-            ACFD_CUDA(cudaGetLastError());
-        }
+        ib_ghost<<<blocks, kGhostWarps * 32, 0, st>>>(G, m, ib->dev, ib->ghosts, ib->nghost, ib->ghost_cap, U, flags,
+                                                      tn, r, ib->status);
+        ACFD_CUDA(cudaGetLastError());
     }
     return ACFD_OK;
+}
+
+int ib_treat_launches(const IbState *ib, const acfd_partition_t &part)
+{
+    if (!ib || ib->count == 0) return 0;
+    return (ib->count + 7) / 8 + part.gl;
 }
 
 int ib_check(IbState *ib, cudaStream_t st)
