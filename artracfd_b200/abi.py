@@ -125,6 +125,7 @@ class Polyhedron(ctypes.Structure):
         ("Ne", ctypes.POINTER(ctypes.c_double)),
         ("v", ctypes.POINTER(ctypes.c_double)),
         ("Nv", ctypes.POINTER(ctypes.c_double)),
+        ("area", ctypes.c_double),
     ]
 
 
@@ -191,6 +192,8 @@ def load_library(path: str | None = None):
         "acfd_geo_upload": [vp, ctypes.POINTER(Polyhedron), i],
         "acfd_compute_geometric_field": [vp],
         "acfd_treat_ib": [vp, i],
+        "acfd_integrate_surface_force": [vp, dp],
+        "acfd_collision_scan": [vp, vp, vp, vp],
         "acfd_weno_batch": [i, i, vp, vp, i],
         "acfd_fhat_batch": [ctypes.POINTER(Model), i, i, vp, vp, i],
         "acfd_batch_init": [i, ctypes.POINTER(Partition), ctypes.POINTER(Model), pp],

@@ -59,6 +59,10 @@ void ib_destroy(IbState *ib);
 int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, const acfd_partition_t &part,
               cudaStream_t st);
 int ib_treat_launches(const IbState *ib, const acfd_partition_t &part);
+int ib_surface_force(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partition_t &part,
+                     const double *U, const int *flags, double *force, cudaStream_t st);
+int ib_collision_scan(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partition_t &part,
+                      const int *flags, int *counts, int *gid, int *N, cudaStream_t st);
 int ib_count(const IbState *ib);
 int ib_compute_geometric_field(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partition_t &part,
                                double *U, int *flags, cudaStream_t st);
@@ -1151,6 +1155,26 @@ int acfd_treat_ib(acfd_case_t *cs, int tn)
         return ACFD_ERR_ARG;
     }
     return ib_treat(cs->ib, cs->grid, cs->mp, cs->part, cs->U, cs->flags, tn, cs->stream);
+}
+
+int acfd_integrate_surface_force(acfd_case_t *cs, double *force)
+{
+    TRY(check_case(cs));
+    if (!force) {
+        set_error("acfd_integrate_surface_force: null output");
+        return ACFD_ERR_ARG;
+    }
+    return ib_surface_force(cs->ib, cs->grid, cs->mp, cs->part, level(cs, ACFD_TO), cs->flags, force, cs->stream);
+}
+
+int acfd_collision_scan(acfd_case_t *cs, int *counts, int *gid, int *N)
+{
+    TRY(check_case(cs));
+    if (!counts || !gid || !N) {
+        set_error("acfd_collision_scan: null output");
+        return ACFD_ERR_ARG;
+    }
+    return ib_collision_scan(cs->ib, cs->grid, cs->mp, cs->part, cs->flags, counts, gid, N, cs->stream);
 }
 
 static ModelParams params_of(const acfd_model_t *model)

@@ -23,12 +23,13 @@
 #include <vector>
 
 #include "acfd_internal.cuh"
+#include "flux_math.cuh"
 
 namespace acfd {
 
 struct DevBody {
     int faceN, edgeN, vertN, state;
-    double r, O[3], V[3], W[3], T, cf;
+    double r, O[3], V[3], W[3], T, cf, area;
     double box[3][2];
     const int *f;
     const double *Nf;
@@ -50,6 +51,16 @@ struct IbState {
     int4 *ghosts = nullptr;  // ghost list of a boundary treatment
     int *nghost = nullptr;
     int ghost_cap = 0;
+    // surface-force integration and collision scan (allocated on first use)
+    double *sf_terms = nullptr;        // [box node][10]: Fp, Fv, Tt, p of ghost nodes of layer 2
+    unsigned char *sf_valid = nullptr; // [box node]: 1 = ghost node of layer 2 of the box's body
+    long long sf_cap = 0;
+    long long *sf_off = nullptr;       // [totN + 1] box offsets
+    int *sf_lid = nullptr;             // [totN] interfacial nodes of layer 2
+    double *sf_force = nullptr;        // [totN][9]
+    unsigned long long *col_key = nullptr;  // [totN][totN] first meeting (node order x path length + path index)
+    int *col_N = nullptr;              // [totN][totN][3] summed path offsets
+    int col_n = 0;
 };
 
 namespace {
@@ -599,6 +610,177 @@ __global__ void __launch_bounds__(kGhostWarps * 32) ib_ghost(IbGrid G, ModelPara
 }
 
 // ---------------------------------------------------------------------------
+// surface forces and contacts of the rigid-body step
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cross3(const double a[3], const double b[3], double c[3])
+{
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// Per-node terms of IntegrateSurfaceForce (solid_dynamics.c:86-146): a ghost
+// node of layer 2 of body n gets Fp = p N, the shear force Fv of no-slip
+// viscous bodies, the torque r x (Fp + Fv) and its pressure p, stored at its
+// position in the body's node box (the reference's k, j, i loop order) for
+// the ordered sums of sf_sum; interfacial nodes of layer 2 are counted.
+__global__ void sf_terms(IbGrid G, ModelParams mp, const DevBody *bodies, BoxList bl, long long off0,
+                         const double *U, const int *flags, double *terms, unsigned char *valid, int *lidN,
+                         int *status)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= bl.start[bl.nb]) return;
+    const long long slot = off0 + t;
+    int q = 0;
+    while (t >= bl.start[q + 1]) ++q;
+    t -= bl.start[q];
+    const int n = bl.body0 + q;
+    const int i = bl.lo[q][0] + (int)(t % bl.ext[q][0]);
+    const long long rest = t / bl.ext[q][0];
+    const int j = bl.lo[q][1] + (int)(rest % bl.ext[q][1]);
+    const int k = bl.lo[q][2] + (int)(rest / bl.ext[q][1]);
+    const Grid &g = G.g;
+    const long long nn = g.nn;
+    const long long id = node_of(g, i, j, k);
+    const DevBody &B = bodies[n];
+    valid[slot] = 0;
+    if (0 < B.state) return;
+    const int did = flags[id];
+    if (2 == flags[2 * nn + id] && n + 1 == did) atomicAdd(lidN + n, 1);
+    if (2 != flags[3 * nn + id] || n + 1 != did) return;
+    double pG[3], pO[3], pI[3], N[3];
+    node_point(G, k, j, i, pG);
+    const int fid = flags[nn + id];
+    if (B.faceN > 0 && (fid < 0 || fid >= B.faceN)) {
+        atomicExch(status, 3);
+        return;
+    }
+    if (!surface_data(pG, fid, B, pO, pI, N)) {
+        atomicExch(status, 2);
+        return;
+    }
+    const double r[3] = {pO[0] - B.O[0], pO[1] - B.O[1], pO[2] - B.O[2]};
+    double Uh[5], Uo[6];
+    for (int v = 0; v < 5; ++v) Uh[v] = U[v * nn + id];
+    to_primitive(mp.gamma, mp.gasR, Uh, Uo);
+    double Fp[3], Fv[3], Fs[3], Tt[3];
+    for (int s = 0; s < 3; ++s) Fp[s] = Uo[4] * N[s];
+    if (0.0 < mp.refMu && 0.0 < B.cf) {
+        const double mu = mp.refMu * exact::sutherland(Uo[5] * mp.refT);
+        double V[3];
+        cross3(B.W, r, V);
+        V[0] = Uo[1] - (B.V[0] + V[0]);
+        V[1] = Uo[2] - (B.V[1] + V[1]);
+        V[2] = Uo[3] - (B.V[2] + V[2]);
+        const double Vn = dot3(V, N);
+        for (int s = 0; s < 3; ++s) Fv[s] = mu * (V[s] - Vn * N[s]) / sqrt(dist2(pG, pO));
+    } else {
+        Fv[0] = Fv[1] = Fv[2] = 0.0;
+    }
+    for (int s = 0; s < 3; ++s) Fs[s] = Fp[s] + Fv[s];
+    cross3(r, Fs, Tt);
+    double *row = terms + 10 * slot;
+    for (int s = 0; s < 3; ++s) {
+        row[s] = Fp[s];
+        row[3 + s] = Fv[s];
+        row[6 + s] = Tt[s];
+    }
+    row[9] = Uo[4];
+    valid[slot] = 1;
+}
+
+// Ordered sums and calibration of IntegrateSurfaceForce (solid_dynamics.c:
+// 139-168), one warp per body: the warp walks the body's node box 32 nodes at
+// a time; lanes 0..8 add Fp, Fv, Tt and lanes 9, 10 the pressure offset sums
+// of the variance test, each over the ghost nodes in box order.
+__global__ void sf_sum(const DevBody *bodies, int totN, const long long *off, const double *terms,
+                       const unsigned char *valid, const int *lidN, double *force)
+{
+    const int lane = threadIdx.x & 31;
+    const int n = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (n >= totN) return;
+    const DevBody &B = bodies[n];
+    if (0 < B.state) return;
+    const long long a = off[n], b = off[n + 1];
+    double acc = 0.0, p0 = 0.0;
+    int gstN = 0;
+    for (long long base = a; base < b; base += 32) {
+        const long long t = base + lane;
+        const bool v = (t < b) && valid[t];
+        const unsigned mask = __ballot_sync(0xffffffffu, v);
+        if (!mask) continue;
+        if (0 == gstN) p0 = terms[10 * (base + __ffs(mask) - 1) + 9];
+        gstN += __popc(mask);
+        if (lane < 11) {
+            for (unsigned m = mask; m; m &= m - 1) {
+                const double *row = terms + 10 * (base + __ffs(m) - 1);
+                if (lane < 9) {
+                    acc = acc + row[lane];
+                } else if (lane == 9) {
+                    acc = acc + row[9] - p0;
+                } else {
+                    acc = acc + (row[9] - p0) * (row[9] - p0);
+                }
+            }
+        }
+    }
+    const double f1 = __shfl_sync(0xffffffffu, acc, 9);
+    const double f2 = __shfl_sync(0xffffffffu, acc, 10);
+    if (lane >= 9) return;
+    const int lid = lidN[n];
+    double out = 0.0;
+    if (0 != lid && 0 != gstN) {
+        const double percent = (double)FLT_EPSILON * (double)FLT_EPSILON;
+        double ds = B.area / lid;
+        const double var = (f2 - f1 * f1 / gstN) / gstN;
+        const double mean = f1 / gstN + p0;
+        if (percent * mean * mean > var) ds = 0.0;
+        out = -acc * ds;
+    }
+    force[9 * n + lane] = out;
+}
+
+// Contact scan of ApplyCollision (solid_dynamics.c:242-256, 327-357): every
+// interfacial node of layer 1 of a moving body p looks along the collision
+// search path; a node of another body q there makes q a contact of p, with
+// the path offset added to their line of impact.  The order of the
+// reference's contact list (first meeting in node order, then path order) is
+// kept as the smallest key node x path length + path index.
+__global__ void col_scan(IbGrid G, const DevBody *bodies, BoxList bl, const int *flags, int totN,
+                         unsigned long long *key, int *cN, int *status)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= bl.start[bl.nb]) return;
+    int q = 0;
+    while (t >= bl.start[q + 1]) ++q;
+    t -= bl.start[q];
+    const int p = bl.body0 + q;
+    if (1 == bodies[p].state) return;
+    const int i = bl.lo[q][0] + (int)(t % bl.ext[q][0]);
+    const long long rest = t / bl.ext[q][0];
+    const int j = bl.lo[q][1] + (int)(rest % bl.ext[q][1]);
+    const int k = bl.lo[q][2] + (int)(rest / bl.ext[q][1]);
+    const Grid &g = G.g;
+    const long long nn = g.nn;
+    const long long id = node_of(g, i, j, k);
+    if (1 != flags[2 * nn + id] || p + 1 != flags[id]) return;
+    const int end = G.pathSep[1];
+    for (int c = 0; c < end; ++c) {
+        const int kh = k + G.path[c][2], jh = j + G.path[c][1], ih = i + G.path[c][0];
+        if (!in_pin(g, kh, jh, ih)) continue;
+        const int d = flags[node_of(g, ih, jh, kh)];
+        if (0 == d || p + 1 == d) continue;
+        if (d < 0 || d > totN) {
+            atomicExch(status, 5);
+            continue;
+        }
+        const long long slot = (long long)p * totN + (d - 1);
+        atomicMin(key + slot, (unsigned long long)t * end + c);
+        for (int s = 0; s < 3; ++s) atomicAdd(cN + 3 * slot + s, G.path[c][s]);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // node mapping
 // ---------------------------------------------------------------------------
 __global__ void map_init(Grid g, const DevBody *bodies, int *flags)
@@ -824,6 +1006,10 @@ int read_status(IbState *ib, cudaStream_t st)
         set_error("immersed boundary: ghost list overflow");
         return ACFD_ERR_DEVICE;
     }
+    if (h == 5) {
+        set_error("collision scan: node with a body id outside the body list");
+        return ACFD_ERR_DEVICE;
+    }
     return ACFD_OK;
 }
 
@@ -860,10 +1046,31 @@ static void ib_release_geometry(IbState *ib)
     ib->ghost_cap = 0;
 }
 
+static void ib_release_solid(IbState *ib)
+{
+    cudaFree(ib->sf_terms);
+    cudaFree(ib->sf_valid);
+    cudaFree(ib->sf_off);
+    cudaFree(ib->sf_lid);
+    cudaFree(ib->sf_force);
+    cudaFree(ib->col_key);
+    cudaFree(ib->col_N);
+    ib->sf_terms = nullptr;
+    ib->sf_valid = nullptr;
+    ib->sf_off = nullptr;
+    ib->sf_lid = nullptr;
+    ib->sf_force = nullptr;
+    ib->col_key = nullptr;
+    ib->col_N = nullptr;
+    ib->sf_cap = 0;
+    ib->col_n = 0;
+}
+
 void ib_destroy(IbState *ib)
 {
     if (!ib) return;
     ib_release_geometry(ib);
+    ib_release_solid(ib);
     cudaFree(ib->joined);
     cudaFree(ib->status);
     delete ib;
@@ -902,6 +1109,7 @@ int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, const acfd_p
         B.r = P.r;
         B.T = P.T;
         B.cf = P.cf;
+        B.area = P.area;
         for (int s = 0; s < 3; ++s) {
             B.O[s] = P.O[s];
             B.V[s] = P.V[s];
@@ -1007,6 +1215,114 @@ int ib_treat_launches(const IbState *ib, const acfd_partition_t &part)
 {
     if (!ib || ib->count == 0) return 0;
     return (ib->count + 7) / 8 + part.gl;
+}
+
+// node boxes of all bodies, their offsets and the scratch of the surface
+// force and contact scans (allocated once per body list)
+static int solid_scratch(IbState *ib, const acfd_partition_t &part, std::vector<long long> &off)
+{
+    const int totN = ib->count;
+    off.assign(totN + 1, 0);
+    for (int n = 0; n < totN; ++n) {
+        int lo[3], ext[3];
+        body_box(part, ib->host[n], lo, ext);
+        off[n + 1] = off[n] + (long long)ext[0] * ext[1] * ext[2];
+    }
+    // kept across body uploads (moving bodies are uploaded every half step);
+    // grown with a margin when the boxes outgrow it
+    if (!ib->sf_off || ib->col_n != totN || off[totN] > ib->sf_cap) {
+        ib_release_solid(ib);
+        const long long cap = std::max(1LL, off[totN] + off[totN] / 4);
+        ACFD_CUDA(cudaMalloc(&ib->sf_terms, sizeof(double) * 10 * (size_t)cap));
+        ACFD_CUDA(cudaMalloc(&ib->sf_valid, (size_t)cap));
+        ACFD_CUDA(cudaMalloc(&ib->sf_off, sizeof(long long) * (totN + 1)));
+        ACFD_CUDA(cudaMalloc(&ib->sf_lid, sizeof(int) * totN));
+        ACFD_CUDA(cudaMalloc(&ib->sf_force, sizeof(double) * 9 * totN));
+        ACFD_CUDA(cudaMalloc(&ib->col_key, sizeof(unsigned long long) * totN * totN));
+        ACFD_CUDA(cudaMalloc(&ib->col_N, sizeof(int) * 3 * totN * totN));
+        ib->sf_cap = cap;
+        ib->col_n = totN;
+    }
+    return ACFD_OK;
+}
+
+int ib_surface_force(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partition_t &part,
+                     const double *U, const int *flags, double *force, cudaStream_t st)
+{
+    if (!ib || ib->count == 0) return ACFD_OK;
+    std::vector<long long> off;
+    int rc = solid_scratch(ib, part, off);
+    if (rc != ACFD_OK) return rc;
+    const int totN = ib->count;
+    const IbGrid G = make_ibgrid(g, part, m.ibmLayer);
+    ACFD_CUDA(cudaMemcpyAsync(ib->sf_off, off.data(), sizeof(long long) * (totN + 1), cudaMemcpyHostToDevice, st));
+    ACFD_CUDA(cudaMemsetAsync(ib->sf_lid, 0, sizeof(int) * totN, st));
+    for (int n0 = 0; n0 < totN; n0 += 8) {
+        BoxList bl;
+        boxes_of(ib, part, n0, bl);
+        const long long total = bl.start[bl.nb];
+        if (total == 0) continue;
+        sf_terms<<<blocks_for(total, 128), 128, 0, st>>>(G, m, ib->dev, bl, off[n0], U, flags, ib->sf_terms,
+                                                         ib->sf_valid, ib->sf_lid, ib->status);
+        ACFD_CUDA(cudaGetLastError());
+    }
+    sf_sum<<<blocks_for(32LL * totN, 128), 128, 0, st>>>(ib->dev, totN, ib->sf_off, ib->sf_terms, ib->sf_valid,
+                                                         ib->sf_lid, ib->sf_force);
+    ACFD_CUDA(cudaGetLastError());
+    std::vector<double> h((size_t)9 * totN);
+    ACFD_CUDA(cudaMemcpyAsync(h.data(), ib->sf_force, sizeof(double) * 9 * totN, cudaMemcpyDeviceToHost, st));
+    rc = read_status(ib, st);  // synchronizes the stream
+    if (rc != ACFD_OK) return rc;
+    for (int n = 0; n < totN; ++n) {
+        if (0 < ib->host[n].state) continue;  // rows of bodies without surface force stay as they are
+        for (int c = 0; c < 9; ++c) force[9 * n + c] = h[(size_t)9 * n + c];
+    }
+    return ACFD_OK;
+}
+
+int ib_collision_scan(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partition_t &part,
+                      const int *flags, int *counts, int *gid, int *N, cudaStream_t st)
+{
+    if (!ib || ib->count == 0) return ACFD_OK;
+    std::vector<long long> off;
+    int rc = solid_scratch(ib, part, off);
+    if (rc != ACFD_OK) return rc;
+    const int totN = ib->count;
+    const IbGrid G = make_ibgrid(g, part, m.ibmLayer);
+    const size_t pairs = (size_t)totN * totN;
+    ACFD_CUDA(cudaMemsetAsync(ib->col_key, 0xff, sizeof(unsigned long long) * pairs, st));
+    ACFD_CUDA(cudaMemsetAsync(ib->col_N, 0, sizeof(int) * 3 * pairs, st));
+    for (int n0 = 0; n0 < totN; n0 += 8) {
+        BoxList bl;
+        boxes_of(ib, part, n0, bl);
+        const long long total = bl.start[bl.nb];
+        if (total == 0) continue;
+        col_scan<<<blocks_for(total, 128), 128, 0, st>>>(G, ib->dev, bl, flags, totN, ib->col_key, ib->col_N,
+                                                         ib->status);
+        ACFD_CUDA(cudaGetLastError());
+    }
+    std::vector<unsigned long long> key(pairs);
+    std::vector<int> cn(3 * pairs);
+    ACFD_CUDA(cudaMemcpyAsync(key.data(), ib->col_key, sizeof(unsigned long long) * pairs, cudaMemcpyDeviceToHost,
+                              st));
+    ACFD_CUDA(cudaMemcpyAsync(cn.data(), ib->col_N, sizeof(int) * 3 * pairs, cudaMemcpyDeviceToHost, st));
+    rc = read_status(ib, st);
+    if (rc != ACFD_OK) return rc;
+    for (int p = 0; p < totN; ++p) {
+        std::vector<std::pair<unsigned long long, int>> met;
+        for (int q = 0; q < totN; ++q) {
+            const unsigned long long k = key[(size_t)p * totN + q];
+            if (k != ~0ULL) met.emplace_back(k, q);
+        }
+        std::sort(met.begin(), met.end());
+        counts[p] = (int)met.size();
+        for (size_t c = 0; c < met.size(); ++c) {
+            const size_t slot = (size_t)p * totN + met[c].second;
+            gid[(size_t)p * totN + c] = met[c].second + 1;
+            for (int s = 0; s < 3; ++s) N[3 * ((size_t)p * totN + c) + s] = cn[3 * slot + s];
+        }
+    }
+    return ACFD_OK;
 }
 
 int ib_check(IbState *ib, cudaStream_t st)

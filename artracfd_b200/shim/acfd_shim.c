@@ -11,11 +11,14 @@
  * other mode they call the reference functions unchanged.
  *
  * GPU mode keeps the node array coherent at exactly the places where host
- * code reads or writes it: before/after the host rigid-body step
- * (solid_dynamics.c:38-49) and before output (solve.c:91-104).
+ * code reads or writes it: before output (solve.c:91-104), and around the
+ * rigid-body step (solid_dynamics.c:38-49) only when that step runs on the
+ * host (ACFD_SOLID=host); by default its node scans run on the device
+ * (solid_gpu.c).
  *
  * Environment: ACFD_MODE = fp64 (default) | exact | fp32, ACFD_GRAPH = 1
- * (default, replay each step as a CUDA graph) | 0.
+ * (default, replay each step as a CUDA graph) | 0, ACFD_SOLID = device
+ * (default) | host.
  */
 #include "acfd_shim.h"
 
@@ -43,6 +46,7 @@ static acfd_case_t *g_case = NULL;
 static int g_host_current = 1;   /* host node array holds the latest state */
 static int g_dev_current = 0;    /* device holds the latest state */
 static int g_use_graph = 1;
+static int g_solid_host = 0;   /* ACFD_SOLID=host: rigid-body step on the host */
 
 static void Check(int status, const char *what)
 {
@@ -112,7 +116,7 @@ static void ToModel(const Model *m, acfd_model_t *o)
 }
 
 /* bodies as they are now on the host (after ApplyMotion) */
-static void UploadGeometry(const Space *space)
+void AcfdUploadGeometry(const Space *space)
 {
     const Geometry *geo = &(space->geo);
     if (0 >= geo->totN) {
@@ -142,6 +146,7 @@ static void UploadGeometry(const Space *space)
         o->Ne = (const double *)P->Ne;
         o->v = (const double *)P->v;
         o->Nv = (const double *)P->Nv;
+        o->area = P->area;
     }
     Check(acfd_geo_upload(g_case, list, geo->totN), "acfd_geo_upload");
     RetrieveStorage(list);
@@ -167,7 +172,9 @@ static void EnsureCase(Space *space, const Model *model)
     Check(acfd_set_precision(g_case, mode), "acfd_set_precision");
     env = getenv("ACFD_GRAPH");
     g_use_graph = !(env && 0 == strcmp(env, "0"));
-    UploadGeometry(space);
+    env = getenv("ACFD_SOLID");
+    g_solid_host = (env && 0 == strcmp(env, "host"));
+    AcfdUploadGeometry(space);
     g_dev_current = 0;
     g_host_current = 1;
 }
@@ -258,15 +265,23 @@ static Real GpuTimeStep(const Time *time, const Space *space)
     return time->numCFL * MinReal(part->d[X] / Vmax[X], MinReal(part->d[Y] / Vmax[Y], part->d[Z] / Vmax[Z]));
 }
 
-/* the host rigid-body half step, with the node array brought to the host
- * and the remapped nodes and moved bodies sent back */
+/* the rigid-body half step: by default with its node scans on the device
+ * (solid_gpu.c), the node array staying there; ACFD_SOLID=host runs the
+ * reference's EvolveSolidDynamics on the host instead, with the node array
+ * brought to the host and the remapped nodes and moved bodies sent back */
 static void GpuSolidStep(const Real now, const Real dt, Space *space, const Model *model)
 {
+    if (!g_solid_host) {
+        EnsureDevice(space);
+        AcfdDeviceSolidStep(g_case, now, dt, space, model);
+        g_host_current = 0;
+        return;
+    }
     EnsureHost(space);
     EvolveSolidDynamics(now, dt, space, model);
     g_dev_current = 0;
     EnsureDevice(space);
-    UploadGeometry(space);
+    AcfdUploadGeometry(space);
 }
 
 /* EvolveSolution (solve.c:48-107) with the fluid step on the device */

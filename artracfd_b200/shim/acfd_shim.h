@@ -5,6 +5,7 @@
 #define ACFD_SHIM_H_
 
 #include "commons.h"
+#include "acfd.h"
 
 /* 1 when the program was started with -m gpu */
 extern int g_acfd_gpu_mode;
@@ -16,5 +17,10 @@ void RefTreatBoundary(const int, Space *, const Model *);
 
 /* release the device case (called by main before Postprocess) */
 void AcfdShimFinalize(void);
+
+/* send the bodies as they are on the host to the device */
+void AcfdUploadGeometry(const Space *);
+/* the rigid-body half step with the node scans on the device (solid_gpu.c) */
+void AcfdDeviceSolidStep(acfd_case_t *, const Real now, const Real dt, Space *, const Model *);
 
 #endif

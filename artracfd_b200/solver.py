@@ -171,6 +171,30 @@ class Solver:
     def treat_ib(self, tn: int):
         check(self.lib.acfd_treat_ib(self.h, tn), self.lib)
 
+    def integrate_surface_force(self, force=None):
+        """IntegrateSurfaceForce (solid_dynamics.c:51-171) on the device:
+        (totN, 9) array of Fp, Fv, Tt per body; rows of bodies with state > 0
+        keep the values of ``force`` (zeros when not given)."""
+        n = len(self.geo)
+        out = np.zeros((n, 9)) if force is None else np.array(force, dtype=np.float64).reshape(n, 9)
+        if n:
+            check(self.lib.acfd_integrate_surface_force(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+                  self.lib)
+        return out
+
+    def collision_scan(self):
+        """Contact lists of ApplyCollision's node scan: for each body a list of
+        (body id, line of impact (3 ints)) in the reference's list order."""
+        n = len(self.geo)
+        if n == 0:
+            return []
+        counts = np.zeros(n, dtype=np.int32)
+        gid = np.zeros(n * n, dtype=np.int32)
+        N = np.zeros(n * n * 3, dtype=np.int32)
+        check(self.lib.acfd_collision_scan(self.h, counts.ctypes.data, gid.ctypes.data, N.ctypes.data), self.lib)
+        return [[(int(gid[p * n + c]), tuple(int(v) for v in N[3 * (p * n + c):3 * (p * n + c) + 3]))
+                 for c in range(counts[p])] for p in range(n)]
+
 
 def run(solver: Solver, numCFL: float, end: float, steps: int, now: float = 0.0):
     """The fluid part of EvolveSolution's loop (solve.c:65-89) without output

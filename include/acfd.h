@@ -136,6 +136,7 @@ typedef struct acfd_polyhedron {
     const double *Ne;       /* edgeN x 3 edge normals */
     const double *v;        /* vertN x 3 vertices */
     const double *Nv;       /* vertN x 3 vertex normals */
+    double area;            /* surface area (read by acfd_integrate_surface_force) */
 } acfd_polyhedron_t;
 
 typedef struct acfd_case acfd_case_t;
@@ -245,6 +246,26 @@ int acfd_geo_upload(acfd_case_t *cs, const acfd_polyhedron_t *poly, int totN);
 int acfd_compute_geometric_field(acfd_case_t *cs);
 /* TreatImmersedBoundary (immersed_boundary.c:270-340) on level tn. */
 int acfd_treat_ib(acfd_case_t *cs, int tn);
+/* IntegrateSurfaceForce (solid_dynamics.c:51-171) on the device, from U[TO]
+ * and the node flags: for every body with state <= 0 the pressure force Fp,
+ * the shear force Fv and the torque Tt, summed over the body's ghost nodes of
+ * layer 2 in the reference's node order and calibrated by its surface area
+ * over its interfacial nodes of layer 2 (bitwise equal to the reference
+ * except through pow() in the viscosity of no-slip viscous bodies).
+ * force: totN x 9 doubles (Fp[3], Fv[3], Tt[3] per body) in host memory;
+ * rows of bodies with state > 0 are left unchanged.  Uses the body list of
+ * the last acfd_geo_upload (centroid, velocities, roughness, area). */
+int acfd_integrate_surface_force(acfd_case_t *cs, double *force);
+/* The contact scan of ApplyCollision (solid_dynamics.c:242-256, the search of
+ * DetectColState and AddColObject :327-357) on the device: for every body p
+ * with state != 1, the bodies met by the collision search path
+ * (Partition.path[0 .. pathSep[1]-1]) from p's interfacial nodes of layer 1,
+ * in the order of the reference's contact list, each with its line of impact
+ * (the summed path offsets, before normalisation).  Host arrays, totN = the
+ * body count: counts[totN], gid[totN * totN] (body ids, did numbering: 1 =
+ * first body), N[totN * totN * 3]; contact c of body p is gid[p*totN + c],
+ * N[(p*totN + c)*3 + 0..2]. */
+int acfd_collision_scan(acfd_case_t *cs, int *counts, int *gid, int *N);
 
 /* ---- learned smoothness sensor (no counterpart in the reference) ------- */
 

@@ -166,6 +166,8 @@ class Reference:
             "ref_compute_geometric_field": (None, []),
             "ref_treat_ib": (None, [i]),
             "ref_evolve_solid": (None, [d, d]),
+            "ref_integrate_surface_force": (None, [_dp]),
+            "ref_collision_scan": (i, [i, _ip, _ip]),
             "ref_step": (d, []),
             "ref_weno5": (None, [_vp, _dp]),
             "ref_weno3": (None, [_vp, _dp]),
@@ -253,6 +255,21 @@ class Reference:
 
     def treat_boundary(self, tn: int) -> None:
         self.lib.ref_treat_boundary(tn)
+
+    def integrate_surface_force(self) -> np.ndarray:
+        out = np.zeros((self.lib.ref_geo_count(), 9))
+        self.lib.ref_integrate_surface_force(out.ctypes.data_as(_dp))
+        return out
+
+    def collision_scan(self):
+        n = self.lib.ref_geo_count()
+        res = []
+        for p in range(n):
+            gid = np.zeros(max(n, 1), dtype=np.int32)
+            N = np.zeros(3 * max(n, 1), dtype=np.int32)
+            c = self.lib.ref_collision_scan(p, gid.ctypes.data_as(_ip), N.ctypes.data_as(_ip))
+            res.append([(int(gid[q]), tuple(int(v) for v in N[3 * q:3 * q + 3])) for q in range(c)])
+        return res
 
     def compute_geometric_field(self) -> None:
         self.lib.ref_compute_geometric_field()

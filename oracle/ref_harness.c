@@ -4,7 +4,7 @@
  * Thin driver around the UNMODIFIED ArtraCFD sources, compiled from the
  * reference tree by oracle/Makefile into oracle/_ref/libacfd_ref.so.  It
  * exposes the reference's own functions (including the static ones of
- * solve.c, reached by including that file) with the plain types of
+ * solve.c and solid_dynamics.c, reached by including those files) with the plain types of
  * include/acfd.h so that tests can run the reference on exactly the inputs
  * given to the oracle restatement and to the GPU library.
  */
@@ -14,6 +14,7 @@
 #include <unistd.h>
 
 #include "solve.c" /* EvolveSolution / ComputeTimeStep are static there */
+#include "solid_dynamics.c" /* DetectColState (the contact search) is static there */
 
 #include "preprocess.h"
 #include "postprocess.h"
@@ -179,6 +180,7 @@ void ref_get_poly(int n, acfd_polyhedron_t *out)
     out->Ne = (const double *)P->Ne;
     out->v = (const double *)P->v;
     out->Nv = (const double *)P->Nv;
+    out->area = P->area;
 }
 
 double ref_compute_time_step(void)
@@ -209,6 +211,64 @@ void ref_treat_ib(int tn)
 void ref_evolve_solid(double now, double dt)
 {
     EvolveSolidDynamics(now, dt, &g_space, &g_model);
+}
+
+/* IntegrateSurfaceForce (solid_dynamics.c:51-171) on the loaded state;
+ * out: totN x 9 (Fp, Fv, Tt) as the bodies hold them afterwards. */
+void ref_integrate_surface_force(double *out)
+{
+    IntegrateSurfaceForce(&g_space, &g_model);
+    for (int n = 0; n < g_space.geo.totN; ++n) {
+        const Polyhedron *P = g_space.geo.poly + n;
+        for (int s = 0; s < 3; ++s) {
+            out[9 * n + s] = P->Fp[s];
+            out[9 * n + 3 + s] = P->Fv[s];
+            out[9 * n + 6 + s] = P->Tt[s];
+        }
+    }
+}
+
+/* The contact list that ApplyCollision builds for body p before its
+ * velocity update (the node scan of solid_dynamics.c:242-256, calling the
+ * reference's DetectColState); returns the list length, gid/N receive the
+ * entries.  Stationary bodies have no list. */
+int ref_collision_scan(int p, int *gid, int *N)
+{
+    Space *space = &g_space;
+    const Partition *part = &space->part;
+    Geometry *geo = &space->geo;
+    const Polyhedron *P = geo->poly + p;
+    if (1 == P->state) {
+        return 0;
+    }
+    geo->colN = 0;
+    int box[DIMS][LIMIT];
+    for (int s = 0; s < DIMS; ++s) {
+        box[s][MIN] = ConfineSpace(MapNode(P->box[s][MIN], part->domain[s][MIN], part->dd[s], part->ng[s]),
+                part->ns[PIN][s][MIN], part->ns[PIN][s][MAX]);
+        box[s][MAX] = ConfineSpace(MapNode(P->box[s][MAX], part->domain[s][MIN], part->dd[s], part->ng[s]),
+                part->ns[PIN][s][MIN], part->ns[PIN][s][MAX]) + 1;
+    }
+    for (int k = box[Z][MIN]; k < box[Z][MAX]; ++k) {
+        for (int j = box[Y][MIN]; j < box[Y][MAX]; ++j) {
+            for (int i = box[X][MIN]; i < box[X][MAX]; ++i) {
+                const int idx = IndexNode(k, j, i, part->n[Y], part->n[X]);
+                if ((1 != space->node[idx].lid) || (p + 1 != space->node[idx].did)) {
+                    continue;
+                }
+                DetectColState(k, j, i, p + 1, part->pathSep[1], part->path, space->node, part, geo);
+            }
+        }
+    }
+    for (int c = 0; c < geo->colN; ++c) {
+        gid[c] = geo->col[c].gid;
+        for (int s = 0; s < DIMS; ++s) {
+            N[3 * c + s] = geo->col[c].N[s];
+        }
+    }
+    const int count = geo->colN;
+    geo->colN = 0;
+    return count;
 }
 
 /* One pass of the loop body of EvolveSolution (solve.c:65-89) without output:

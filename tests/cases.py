@@ -45,6 +45,32 @@ def spheres(n=24, count=2, analytic=1, level=2) -> CaseSpec:
     return configs.ib_spheres(n=n, count=count, analytic=analytic, level=level, stepN=0)
 
 
+def contact_spheres(n=32, viscous=True) -> CaseSpec:
+    """Three moving spheres (one analytical, two 320-facet icospheres) of
+    radius 0.15 in the unit cube, closing on one another with surface gaps
+    below a cell, in a crossflow: their nodes meet on the collision search
+    paths of the rigid-body step."""
+    d = 1.0 / n
+    c0 = (0.3, 0.5, 0.5)
+    c1 = (0.6 + 0.3 * d, 0.5, 0.5)
+    # the third sphere rests on the first two, 0.3 cells from each
+    c2 = (0.45 + 0.15 * d, 0.5 + float(np.sqrt((0.3 + 0.3 * d) ** 2 - (0.15 + 0.15 * d) ** 2)), 0.5)
+    refT = 1.0 / (0.3 * 0.3 * 1.4 * 287.058)
+    p0 = 1.0 / (1.4 * 0.09)
+    bodies = [Body(O=c0, r=0.15, V=(0.2, 0.01, 0.0), W=(0.0, 0.0, 0.5), rho=2.0, T=-1.0, cf=1.0),
+              Body(O=c1, r=0.15, V=(-0.2, 0.0, 0.02), rho=3.0, T=-1.0, cf=1.0, stl="s1.stl",
+                   triangles=icosphere(c1, 0.15, level=2)),
+              Body(O=c2, r=0.15, V=(0.0, -0.2, 0.0), W=(0.3, 0.0, 0.0), rho=2.5, T=-1.0, cf=0.0, stl="s2.stl",
+                   triangles=icosphere(c2, 0.15, level=2))]
+    P = Boundary(abi.PERIODIC)
+    return CaseSpec(
+        domain_lo=(0.0, 0.0, 0.0), domain_hi=(1.0, 1.0, 1.0), m=(n, n, n), end=1.0e6, cfl=0.5, stepN=0,
+        psi=2, ibmLayer=1, refMu=((0.3 / 200.0) / configs.sutherland(refT)) if viscous else 0.0, refT=refT,
+        init=("1", "0.6", "0.1*sin(6*y)", "0", "%.17g" % p0),
+        boundaries=[Boundary(abi.INFLOW, (1.0, 0.6, 0.0, 0.0, p0)), Boundary(abi.OUTFLOW), P, P, P, P],
+        bodies=bodies)
+
+
 def cylinder2d(m=(64, 32, 1)) -> CaseSpec:
     spec = configs.shock_cylinder(m=m, segments=24)
     return spec
@@ -59,6 +85,12 @@ SMALL = {
     "gravity_box": gravity_box,
     "cylinder2d": cylinder2d,
     "spheres": spheres,
+}
+
+SOLID = {
+    "spheres48": lambda: configs.ib_spheres(n=48, count=2, analytic=1, level=2, stepN=0),
+    "contact_spheres": contact_spheres,
+    "contact_spheres_inviscid": lambda: contact_spheres(viscous=False),
 }
 
 

@@ -85,6 +85,41 @@ def test_dropin_fast_mode_close_to_reference(tmp_path, name):
 
 
 @needs
+@pytest.mark.parametrize("solid", ["device", "host"])
+def test_dropin_exact_mode_moving_bodies_with_contacts(tmp_path, solid):
+    """Three inviscid moving spheres resting on one another in a crossflow:
+    with the rigid-body step's node scans on the device (surface forces,
+    contact lists, remapping and ghost values; the node array stays on the
+    GPU) or on the host, the exact mode writes the reference's files."""
+    spec = cases.contact_spheres(viscous=False)
+    spec.stepN = 5
+    a, b = _pair(tmp_path, spec)
+    _run(REFBIN, "serial", a)
+    _run(DROPIN, "gpu", b, {"ACFD_MODE": "exact", "ACFD_SOLID": solid})
+    sa, fa = _last_fields(a)
+    sb, fb = _last_fields(b)
+    assert sa == sb
+    for f in FIELDS:
+        assert np.array_equal(fa[f], fb[f]), (f, np.abs(fa[f] - fb[f]).max())
+
+
+@needs
+def test_dropin_viscous_contacts_close_to_reference(tmp_path):
+    spec = cases.contact_spheres(viscous=True)
+    spec.stepN = 5
+    a, b = _pair(tmp_path, spec)
+    _run(REFBIN, "serial", a)
+    _run(DROPIN, "gpu", b, {"ACFD_MODE": "fp64"})
+    sa, fa = _last_fields(a)
+    sb, fb = _last_fields(b)
+    assert sa == sb
+    assert np.array_equal(fa["did"], fb["did"])
+    for f in FIELDS[:-1]:
+        scale = max(np.abs(fa[f]).max(), np.abs(fa["rho"]).max() * 1e-3)
+        assert np.abs(fa[f] - fb[f]).max() <= 1e-5 * scale, f
+
+
+@needs
 def test_dropin_serial_mode_is_the_reference(tmp_path):
     spec = configs.sod(m=(32, 4, 4), stepN=3)
     a, b = _pair(tmp_path, spec)

@@ -48,3 +48,34 @@ def test_ib_spheres_192_remap_bit_exact(tmp_path):
         assert bad.size == 0, (f, bad[:10], got[f][bad[:10]], want[f][bad[:10]])
     assert (want["gst"] > 0).sum() > 5000  # the ghost layers of all eight spheres
     assert np.array_equal(got["U"][:, 0, :], want["U"][:, 0, :])
+
+
+@pytest.mark.skipif(not reference_available(), reason="reference harness oracle/_ref not built")
+def test_ib_spheres_192_surface_force(tmp_path):
+    """IntegrateSurfaceForce of the eight spheres on a perturbed state (the
+    loaded state is uniform, whose forces the variance test zeroes): pressure
+    forces bitwise, shear forces and torques (pow() in the viscosity) to
+    1e-13."""
+    spec = configs.ib_spheres(n=192)
+    path = os.path.join(str(tmp_path), "ib192")
+    spec.write(path)
+    ref = Reference()
+    ref.load(path)
+    part, model = ref.partition(), ref.model()
+    node = ref.nodes()
+    rng = np.random.default_rng(3)
+    U = node["U"][:, 0, :]
+    U[:, 4] *= 1.0 + 0.01 * rng.standard_normal(U.shape[0])
+    U[:, 1] += 0.05 * rng.standard_normal(U.shape[0]) * U[:, 0]
+    node["U"][:, 0, :] = U
+    ref.set_nodes(node)
+    geo = ref.geometry()
+    want = ref.integrate_surface_force()
+    with Solver(part, model, abi.FP64_EXACT) as s:
+        s.upload(node)
+        s.geo_upload(geo)
+        got = s.integrate_surface_force()
+    assert np.abs(want[:, 0:6]).min() > 0.0
+    assert np.array_equal(got[:, 0:3], want[:, 0:3])
+    scale = np.abs(want).max(axis=0)
+    assert np.all(np.abs(got - want) <= 1e-13 * scale), np.abs(got - want) / scale

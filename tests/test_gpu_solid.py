@@ -1,0 +1,90 @@
+"""The node scans of the rigid-body step on the device against the
+reference's own functions on the same state (the harness in oracle/_ref):
+
+* IntegrateSurfaceForce (solid_dynamics.c:51-171): pressure force, shear
+  force and torque of every body, summed over its ghost nodes of layer 2 in
+  the reference's node order and calibrated by area / interfacial node
+  count.  The pressure force takes IEEE +, -, *, / only and is bitwise equal;
+  the shear force (and the torque it enters) of no-slip bodies in a viscous
+  fluid goes through pow() in Sutherland's law, whose last bit the device
+  library may round differently, so those agree to 1e-13;
+* the contact scan of ApplyCollision (DetectColState / AddColObject,
+  solid_dynamics.c:242-256, 327-357): the same contact lists, in the same
+  order, with the same lines of impact.
+
+The states are those of the reference after a few of its own time steps
+(moving spheres in a crossflow, three of them resting on one another).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from artracfd_b200 import abi
+from artracfd_b200.solver import Solver
+from oracle.oracle import Reference, reference_available
+
+import cases
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not reference_available(), reason="reference harness oracle/_ref not built")]
+
+BUILDERS = dict(cases.SMALL, **cases.SOLID)
+
+
+def _load(tmp_path, name, steps):
+    spec = BUILDERS[name]()
+    spec.stepN = steps + 1
+    path = os.path.join(str(tmp_path), name)
+    spec.write(path)
+    ref = Reference()
+    ref.load(path)
+    for _ in range(steps):
+        assert ref.lib.ref_step() > 0.0
+    return ref
+
+
+def _device(ref):
+    s = Solver(ref.partition(), ref.model(), abi.FP64_EXACT)
+    s.upload(ref.nodes())
+    s.geo_upload(ref.geometry())
+    return s
+
+
+@pytest.mark.parametrize("name", ["spheres48", "contact_spheres", "contact_spheres_inviscid"])
+def test_surface_force_matches_reference(tmp_path, name):
+    ref = _load(tmp_path, name, 3)
+    model, geo = ref.model(), ref.geometry()
+    with _device(ref) as s:
+        got = s.integrate_surface_force()
+    want = ref.integrate_surface_force()
+    assert np.abs(want[:, 0:3]).max() > 0.0
+    assert np.array_equal(got[:, 0:3], want[:, 0:3]), np.abs(got - want).max()
+    if model.refMu > 0.0 and any(g.cf > 0.0 for g in geo):
+        assert np.abs(want[:, 3:6]).max() > 0.0
+        scale = np.abs(want).max(axis=0)
+        assert np.all(np.abs(got - want) <= 1e-13 * scale), np.abs(got - want) / scale
+    else:
+        assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("steps", [0, 3])
+def test_collision_scan_matches_reference(tmp_path, steps):
+    ref = _load(tmp_path, "contact_spheres", steps)
+    with _device(ref) as s:
+        got = s.collision_scan()
+    want = ref.collision_scan()
+    assert all(len(c) == 2 for c in want), want  # every sphere touches the other two
+    assert got == want
+
+
+def test_collision_scan_skips_stationary_bodies(tmp_path):
+    ref = _load(tmp_path, "contact_spheres", 0)
+    geo = ref.geometry()
+    geo[0].state = 1
+    with Solver(ref.partition(), ref.model(), abi.FP64_EXACT) as s:
+        s.upload(ref.nodes())
+        s.geo_upload(geo)
+        got = s.collision_scan()
+    assert got[0] == []
+    assert got[1] == ref.collision_scan()[1]
