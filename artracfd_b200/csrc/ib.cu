@@ -1,7 +1,9 @@
 // Immersed boundaries on the device: node mapping (ComputeGeometricField,
 // immersed_boundary.c:65-264, with the point-in-polyhedron test of
-// computational_geometry.c:463-783) and the ghost-node reconstruction
-// (TreatImmersedBoundary, immersed_boundary.c:270-487).
+// computational_geometry.c:463-783), the ghost-node reconstruction
+// (TreatImmersedBoundary, immersed_boundary.c:270-487) and the node scans of
+// the rigid-body step (IntegrateSurfaceForce and the contact search of
+// ApplyCollision, solid_dynamics.c:51-171, 213-357).
 //
 // Compiled with --fmad=false and written in the reference's evaluation
 // order: node flags (did, fid, lid, gst), image-point node indices and IDW
@@ -10,13 +12,19 @@
 // Parallel structure:
 //  * domain mapping: one launch per body in body order (first body wins, as
 //    the reference's body loop); a block stages the body's facets
-//    (v0, e01, e02 per facet) in shared memory and each thread scans them for
-//    its node;
+//    (v0, e01, e02 per facet) in shared memory and a warp scans them for a
+//    node, 32 facets at a time;
 //  * interfacial field: newly uncovered nodes are marked first, so that the
 //    reconstruction reads only nodes that stay fluid (the reference's TYPEF
 //    selection) and never a value written in the same pass;
-//  * ghost layers: one launch per layer over all bodies' boxes (layer r reads
-//    fluid nodes or layer r-1 only; bodies do not read each other).
+//  * ghost layers: the ghost nodes of all bodies are listed once per
+//    treatment, then one launch per layer (layer r reads fluid nodes or
+//    layer r-1 only; bodies do not read each other) gives each listed node of
+//    the layer a warp, whose lanes share the inverse-distance searches;
+//  * rigid-body step: surface-force terms per ghost node of layer 2 with the
+//    sums taken in the reference's node order by one warp per body, and the
+//    contact scan of the collision step with atomics that keep the order in
+//    which the reference's node loop meets each contact.
 #include <algorithm>
 #include <cfloat>
 #include <climits>
@@ -690,39 +698,54 @@ __global__ void sf_terms(IbGrid G, ModelParams mp, const DevBody *bodies, BoxLis
 }
 
 // Ordered sums and calibration of IntegrateSurfaceForce (solid_dynamics.c:
-// 139-168), one warp per body: the warp walks the body's node box 32 nodes at
-// a time; lanes 0..8 add Fp, Fv, Tt and lanes 9, 10 the pressure offset sums
-// of the variance test, each over the ghost nodes in box order.
-__global__ void sf_sum(const DevBody *bodies, int totN, const long long *off, const double *terms,
-                       const unsigned char *valid, const int *lidN, double *force)
+// 139-168), one warp (block) per body: the warp walks the body's node box 128
+// nodes at a time, stages the terms of the ghost nodes among them in shared
+// memory, and lanes 0..8 add Fp, Fv, Tt and lanes 9, 10 the pressure offset
+// sums of the variance test, each over the ghost nodes in box order.
+constexpr int kSumChunks = 4;
+__global__ void __launch_bounds__(32) sf_sum(const DevBody *bodies, const long long *off, const double *terms,
+                                             const unsigned char *valid, const int *lidN, double *force)
 {
-    const int lane = threadIdx.x & 31;
-    const int n = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    if (n >= totN) return;
+    __shared__ double rows[32 * kSumChunks][10];
+    const int lane = threadIdx.x;
+    const int n = blockIdx.x;
     const DevBody &B = bodies[n];
     if (0 < B.state) return;
     const long long a = off[n], b = off[n + 1];
     double acc = 0.0, p0 = 0.0;
     int gstN = 0;
-    for (long long base = a; base < b; base += 32) {
-        const long long t = base + lane;
-        const bool v = (t < b) && valid[t];
-        const unsigned mask = __ballot_sync(0xffffffffu, v);
-        if (!mask) continue;
-        if (0 == gstN) p0 = terms[10 * (base + __ffs(mask) - 1) + 9];
-        gstN += __popc(mask);
-        if (lane < 11) {
-            for (unsigned m = mask; m; m &= m - 1) {
-                const double *row = terms + 10 * (base + __ffs(m) - 1);
-                if (lane < 9) {
-                    acc = acc + row[lane];
-                } else if (lane == 9) {
-                    acc = acc + row[9] - p0;
-                } else {
-                    acc = acc + (row[9] - p0) * (row[9] - p0);
+    for (long long base = a; base < b; base += 32 * kSumChunks) {
+        unsigned mask[kSumChunks];
+#pragma unroll
+        for (int c = 0; c < kSumChunks; ++c) {
+            const long long t = base + 32 * c + lane;
+            const bool v = (t < b) && valid[t];
+            if (v) {
+#pragma unroll
+                for (int q = 0; q < 10; ++q) rows[32 * c + lane][q] = terms[10 * t + q];
+            }
+            mask[c] = __ballot_sync(0xffffffffu, v);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int c = 0; c < kSumChunks; ++c) {
+            if (!mask[c]) continue;
+            if (0 == gstN) p0 = rows[32 * c + __ffs(mask[c]) - 1][9];
+            gstN += __popc(mask[c]);
+            if (lane < 11) {
+                for (unsigned m = mask[c]; m; m &= m - 1) {
+                    const double *row = rows[32 * c + __ffs(m) - 1];
+                    if (lane < 9) {
+                        acc = acc + row[lane];
+                    } else if (lane == 9) {
+                        acc = acc + row[9] - p0;
+                    } else {
+                        acc = acc + (row[9] - p0) * (row[9] - p0);
+                    }
                 }
             }
         }
+        __syncwarp();
     }
     const double f1 = __shfl_sync(0xffffffffu, acc, 9);
     const double f2 = __shfl_sync(0xffffffffu, acc, 10);
@@ -804,7 +827,7 @@ __global__ void map_init(Grid g, const DevBody *bodies, int *flags)
     if (flags[2 * nn + id] > 0) flags[id] = 0;
 }
 
-constexpr int kMapThreads = 128;
+constexpr int kMapThreads = 256;
 constexpr int kMaxSmemFacets = 2048;  // 9 doubles each: 144 KB
 
 __global__ void __launch_bounds__(kMapThreads) map_body(IbGrid G, const DevBody *bodies, int n, BoxList bl,
@@ -817,52 +840,68 @@ __global__ void __launch_bounds__(kMapThreads) map_body(IbGrid G, const DevBody 
         for (int q = threadIdx.x; q < 9 * B.faceN; q += blockDim.x) stri[q] = B.tri[q];
         __syncthreads();
     }
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= bl.start[1]) return;
-    const int i = bl.lo[0][0] + (int)(t % bl.ext[0][0]);
-    const long long rest = t / bl.ext[0][0];
-    const int j = bl.lo[0][1] + (int)(rest % bl.ext[0][1]);
-    const int k = bl.lo[0][2] + (int)(rest / bl.ext[0][1]);
+    const double *tri = staged ? stri : B.tri;
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
     const Grid &g = G.g;
     const long long nn = g.nn;
-    const long long id = node_of(g, i, j, k);
-    if (0 != flags[id]) return;
-    double p[3];
-    node_point(G, k, j, i, p);
-    if (0 >= B.faceN) {
-        if (B.r * B.r >= dist2(B.O, p)) {
+    // one warp per node of the body's box
+    for (long long t = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < bl.start[1];
+         t += warps) {
+        const int i = bl.lo[0][0] + (int)(t % bl.ext[0][0]);
+        const long long rest = t / bl.ext[0][0];
+        const int j = bl.lo[0][1] + (int)(rest % bl.ext[0][1]);
+        const int k = bl.lo[0][2] + (int)(rest / bl.ext[0][1]);
+        const long long id = node_of(g, i, j, k);
+        if (0 != flags[id]) continue;
+        double p[3];
+        node_point(G, k, j, i, p);
+        if (0 >= B.faceN) {
+            if (lane == 0 && B.r * B.r >= dist2(B.O, p)) {
+                flags[id] = n + 1;
+                flags[nn + id] = 0;
+            }
+            continue;
+        }
+        // nearest facet, first minimum wins (computational_geometry.c:463-494):
+        // each lane keeps the first minimum of its facets f = lane (mod 32),
+        // the warp takes the smallest distance and, among equal ones, the
+        // smallest facet index
+        double best = FLT_MAX;
+        int cid = 0;
+        for (int f = lane; f < B.faceN; f += 32) {
+            const double *T = tri + 9 * f;
+            const double v0[3] = {T[0], T[1], T[2]};
+            const double e01[3] = {T[3], T[4], T[5]};
+            const double e02[3] = {T[6], T[7], T[8]};
+            double para[3];
+            const double q = point_triangle(p, v0, e01, e02, para);
+            if (best > q) {
+                best = q;
+                cid = f;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int oc = __shfl_xor_sync(0xffffffffu, cid, o);
+            if (ob < best || (ob == best && oc < cid)) {
+                best = ob;
+                cid = oc;
+            }
+        }
+        double pi[3], N[3];
+        if (!closest_on_facet(p, cid, B, pi, N)) {
+            if (lane == 0) atomicExch(status, 2);
+            continue;
+        }
+        pi[0] = p[0] - pi[0];
+        pi[1] = p[1] - pi[1];
+        pi[2] = p[2] - pi[2];
+        if (lane == 0 && !(0.0 < dot3(pi, N))) {
             flags[id] = n + 1;
-            flags[nn + id] = 0;
+            flags[nn + id] = cid;
         }
-        return;
-    }
-    // nearest facet, first minimum wins (computational_geometry.c:463-494)
-    const double *tri = staged ? stri : B.tri;
-    double best = FLT_MAX;
-    int cid = 0;
-    for (int f = 0; f < B.faceN; ++f) {
-        const double *T = tri + 9 * f;
-        const double v0[3] = {T[0], T[1], T[2]};
-        const double e01[3] = {T[3], T[4], T[5]};
-        const double e02[3] = {T[6], T[7], T[8]};
-        double para[3];
-        const double q = point_triangle(p, v0, e01, e02, para);
-        if (best > q) {
-            best = q;
-            cid = f;
-        }
-    }
-    double pi[3], N[3];
-    if (!closest_on_facet(p, cid, B, pi, N)) {
-        atomicExch(status, 2);
-        return;
-    }
-    pi[0] = p[0] - pi[0];
-    pi[1] = p[1] - pi[1];
-    pi[2] = p[2] - pi[2];
-    if (!(0.0 < dot3(pi, N))) {
-        flags[id] = n + 1;
-        flags[nn + id] = cid;
     }
 }
 
@@ -1266,8 +1305,7 @@ int ib_surface_force(IbState *ib, const Grid &g, const ModelParams &m, const acf
                                                          ib->sf_valid, ib->sf_lid, ib->status);
         ACFD_CUDA(cudaGetLastError());
     }
-    sf_sum<<<blocks_for(32LL * totN, 128), 128, 0, st>>>(ib->dev, totN, ib->sf_off, ib->sf_terms, ib->sf_valid,
-                                                         ib->sf_lid, ib->sf_force);
+    sf_sum<<<totN, 32, 0, st>>>(ib->dev, ib->sf_off, ib->sf_terms, ib->sf_valid, ib->sf_lid, ib->sf_force);
     ACFD_CUDA(cudaGetLastError());
     std::vector<double> h((size_t)9 * totN);
     ACFD_CUDA(cudaMemcpyAsync(h.data(), ib->sf_force, sizeof(double) * 9 * totN, cudaMemcpyDeviceToHost, st));
@@ -1362,8 +1400,10 @@ int ib_compute_geometric_field(IbState *ib, const Grid &g, const ModelParams &m,
         bl.start[1] = (long long)bl.ext[0][0] * bl.ext[0][1] * bl.ext[0][2];
         if (bl.start[1] == 0) continue;
         const size_t smem = (B.faceN > 0 && B.faceN <= kMaxSmemFacets) ? sizeof(double) * 9 * B.faceN : 0;
-        map_body<<<blocks_for(bl.start[1], kMapThreads), kMapThreads, smem, st>>>(G, ib->dev, n, bl, flags,
-                                                                                  ib->status);
+        // a warp per node, at most two resident blocks per SM (staged facets)
+        const long long want = (bl.start[1] + kMapThreads / 32 - 1) / (kMapThreads / 32);
+        const unsigned blocks = (unsigned)std::min<long long>(want, 2LL * 148);
+        map_body<<<blocks, kMapThreads, smem, st>>>(G, ib->dev, n, bl, flags, ib->status);
         ACFD_CUDA(cudaGetLastError());
     }
     map_interface<<<blocks_for(pin, 256), 256, 0, st>>>(G, flags, ib->joined);
