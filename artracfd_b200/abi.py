@@ -23,6 +23,7 @@ ACFD_ERR_STATE = 3
 ACFD_ERR_DEVICE = 4
 ACFD_ERR_NOMEM = 5
 ACFD_ERR_NOT_FOUND = 6
+ACFD_ERR_IO = 7
 # levels / operators
 TO, TN, TM = 0, 1, 2
 X, Y, Z, DIMS, PHI = 0, 1, 2, 3, 4
@@ -193,6 +194,11 @@ def load_library(path: str | None = None):
         "acfd_compute_geometric_field": [vp],
         "acfd_treat_ib": [vp, i],
         "acfd_integrate_surface_force": [vp, dp],
+        "acfd_snapshot_begin": [vp],
+        "acfd_snapshot_nodes": [vp, vp],
+        "acfd_snapshot_save": [vp, ctypes.c_char_p, vp, sz],
+        "acfd_checkpoint_save": [vp, ctypes.c_char_p, vp, sz],
+        "acfd_checkpoint_load": [vp, ctypes.c_char_p, vp, sz, ctypes.POINTER(sz)],
         "acfd_collision_scan": [vp, vp, vp, vp],
         "acfd_weno_batch": [i, i, vp, vp, i],
         "acfd_fhat_batch": [ctypes.POINTER(Model), i, i, vp, vp, i],

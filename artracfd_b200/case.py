@@ -68,6 +68,8 @@ class CaseSpec:
     end: float = 1.0
     cfl: float = 0.6
     stepN: int = 0
+    restart: int = 0   # data output to restart from (0: none)
+    dataW: int = 1     # space data outputs over the run
     tScheme: int = 1
     sScheme: int = 1
     multidim: int = 0
@@ -95,8 +97,8 @@ class CaseSpec:
         L = []
         L += ["space begin", "%.17g, %.17g, %.17g" % tuple(self.domain_lo),
               "%.17g, %.17g, %.17g" % tuple(self.domain_hi), "%d, %d, %d" % tuple(self.m), "space end"]
-        L += ["time begin", "0", "%.17g" % self.end, "%.17g" % self.cfl, "%d" % self.stepN,
-              "%d" % 1, "1", "time end"]
+        L += ["time begin", "%d" % self.restart, "%.17g" % self.end, "%.17g" % self.cfl, "%d" % self.stepN,
+              "%d" % self.dataW, "1", "time end"]
         L += ["numerical begin"] + ["%d" % v for v in (self.tScheme, self.sScheme, self.multidim,
                                                        self.jacobMean, self.fluxSplit, self.psi,
                                                        self.ibmLayer)] + ["numerical end"]

@@ -116,6 +116,12 @@ struct acfd_case {
     double *cfl_out = nullptr;
     double *h_cfl = nullptr;   // pinned
     acfd_node_t *staging = nullptr;
+    // asynchronous snapshot of the node records (output and checkpoints)
+    acfd_node_t *snap_dev = nullptr;   // device copy in the node layout
+    acfd_node_t *snap_host = nullptr;  // pinned host copy
+    cudaStream_t snap_stream = nullptr;
+    cudaEvent_t snap_gathered = nullptr, snap_copied = nullptr;
+    bool snap_pending = false;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     std::vector<std::vector<FaceBox>> bc_groups;  // ordered, each group independent inside
@@ -781,6 +787,12 @@ int acfd_finalize(acfd_case_t *cs)
     cudaFree(cs->sensor_rp);
     cudaFree(cs->sensor_count);
     cudaFree(cs->staging);
+    if (cs->snap_pending && cs->snap_copied) cudaEventSynchronize(cs->snap_copied);
+    cudaFree(cs->snap_dev);
+    if (cs->snap_host) cudaFreeHost(cs->snap_host);
+    if (cs->snap_gathered) cudaEventDestroy(cs->snap_gathered);
+    if (cs->snap_copied) cudaEventDestroy(cs->snap_copied);
+    if (cs->snap_stream) cudaStreamDestroy(cs->snap_stream);
     if (cs->h_cfl) cudaFreeHost(cs->h_cfl);
     if (cs->own_stream && cs->stream) cudaStreamDestroy(cs->stream);
     delete cs;
@@ -1155,6 +1167,167 @@ int acfd_treat_ib(acfd_case_t *cs, int tn)
         return ACFD_ERR_ARG;
     }
     return ib_treat(cs->ib, cs->grid, cs->mp, cs->part, cs->U, cs->flags, tn, cs->stream);
+}
+
+// ---- snapshots and FP64 checkpoints ------------------------------------
+// File layout of a checkpoint (little-endian): a 64-byte header, the
+// caller's block, then the node records of every node (ghosts included) in
+// the reference's Node layout, so that the state round-trips bit for bit.
+struct CheckpointHeader {
+    char magic[8];        // "ACFDCKP1"
+    int32_t version;      // 1
+    int32_t node_bytes;   // sizeof(acfd_node_t)
+    int32_t n[3];         // allocated nodes per axis
+    int32_t pad;
+    int64_t count;        // n[0] * n[1] * n[2]
+    int64_t user_bytes;   // size of the caller's block
+    int64_t reserved[2];
+};
+static_assert(sizeof(CheckpointHeader) == 64, "checkpoint header layout");
+static const char kCheckpointMagic[8] = {'A', 'C', 'F', 'D', 'C', 'K', 'P', '1'};
+
+static size_t node_count(const acfd_case *cs)
+{
+    return (size_t)cs->grid.n[0] * cs->grid.n[1] * cs->grid.n[2];
+}
+
+int acfd_snapshot_begin(acfd_case_t *cs)
+{
+    TRY(check_case(cs));
+    const size_t total = node_count(cs);
+    if (!cs->snap_dev) {
+        ACFD_CUDA(cudaMalloc(&cs->snap_dev, total * sizeof(acfd_node_t)));
+        ACFD_CUDA(cudaMallocHost(&cs->snap_host, total * sizeof(acfd_node_t)));
+        ACFD_CUDA(cudaStreamCreateWithFlags(&cs->snap_stream, cudaStreamNonBlocking));
+        ACFD_CUDA(cudaEventCreateWithFlags(&cs->snap_gathered, cudaEventDisableTiming));
+        ACFD_CUDA(cudaEventCreateWithFlags(&cs->snap_copied, cudaEventDisableTiming));
+    }
+    if (cs->snap_pending) {
+        // the previous snapshot's copy still reads snap_dev
+        ACFD_CUDA(cudaStreamWaitEvent(cs->stream, cs->snap_copied, 0));
+    }
+    // the state as the case's stream has it now: node records on the device,
+    // then copied to pinned memory on a stream of their own, overlapping the
+    // work queued on the case's stream after this call
+    TRY(launch_gather_nodes(cs->grid, cs->U, cs->flags, cs->snap_dev, ACFD_SYNC_ALL, cs->stream));
+    ACFD_CUDA(cudaEventRecord(cs->snap_gathered, cs->stream));
+    ACFD_CUDA(cudaStreamWaitEvent(cs->snap_stream, cs->snap_gathered, 0));
+    ACFD_CUDA(cudaMemcpyAsync(cs->snap_host, cs->snap_dev, total * sizeof(acfd_node_t), cudaMemcpyDeviceToHost,
+                              cs->snap_stream));
+    ACFD_CUDA(cudaEventRecord(cs->snap_copied, cs->snap_stream));
+    cs->snap_pending = true;
+    return ACFD_OK;
+}
+
+static int snapshot_wait(acfd_case *cs, const char *who)
+{
+    if (!cs->snap_pending) {
+        set_error("%s: no snapshot taken (acfd_snapshot_begin)", who);
+        return ACFD_ERR_STATE;
+    }
+    ACFD_CUDA(cudaEventSynchronize(cs->snap_copied));
+    return ACFD_OK;
+}
+
+int acfd_snapshot_nodes(acfd_case_t *cs, acfd_node_t *node)
+{
+    TRY(check_case(cs));
+    if (!node) {
+        set_error("acfd_snapshot_nodes: null node array");
+        return ACFD_ERR_ARG;
+    }
+    TRY(snapshot_wait(cs, "acfd_snapshot_nodes"));
+    memcpy(node, cs->snap_host, node_count(cs) * sizeof(acfd_node_t));
+    return ACFD_OK;
+}
+
+static int write_checkpoint(const acfd_case *cs, const char *path, const void *user, size_t user_bytes,
+                            const acfd_node_t *nodes)
+{
+    if (!path || (user_bytes && !user)) {
+        set_error("checkpoint: null path or user block");
+        return ACFD_ERR_ARG;
+    }
+    CheckpointHeader h;
+    memset(&h, 0, sizeof(h));
+    memcpy(h.magic, kCheckpointMagic, 8);
+    h.version = 1;
+    h.node_bytes = (int32_t)sizeof(acfd_node_t);
+    for (int s = 0; s < 3; ++s) h.n[s] = cs->grid.n[s];
+    h.count = (int64_t)node_count(cs);
+    h.user_bytes = (int64_t)user_bytes;
+    FILE *fp = fopen(path, "wb");
+    if (!fp) {
+        set_error("checkpoint: cannot open %s for writing", path);
+        return ACFD_ERR_IO;
+    }
+    bool ok = fwrite(&h, sizeof(h), 1, fp) == 1;
+    if (ok && user_bytes) ok = fwrite(user, 1, user_bytes, fp) == user_bytes;
+    if (ok) ok = fwrite(nodes, sizeof(acfd_node_t), (size_t)h.count, fp) == (size_t)h.count;
+    ok = (fclose(fp) == 0) && ok;
+    if (!ok) {
+        set_error("checkpoint: writing %s failed", path);
+        return ACFD_ERR_IO;
+    }
+    return ACFD_OK;
+}
+
+int acfd_snapshot_save(acfd_case_t *cs, const char *path, const void *user, size_t user_bytes)
+{
+    TRY(check_case(cs));
+    TRY(snapshot_wait(cs, "acfd_snapshot_save"));
+    return write_checkpoint(cs, path, user, user_bytes, cs->snap_host);
+}
+
+int acfd_checkpoint_save(acfd_case_t *cs, const char *path, const void *user, size_t user_bytes)
+{
+    TRY(acfd_snapshot_begin(cs));
+    return acfd_snapshot_save(cs, path, user, user_bytes);
+}
+
+int acfd_checkpoint_load(acfd_case_t *cs, const char *path, void *user, size_t user_cap, size_t *user_bytes)
+{
+    TRY(check_case(cs));
+    if (!path) {
+        set_error("acfd_checkpoint_load: null path");
+        return ACFD_ERR_ARG;
+    }
+    FILE *fp = fopen(path, "rb");
+    if (!fp) {
+        set_error("acfd_checkpoint_load: cannot open %s", path);
+        return ACFD_ERR_IO;
+    }
+    CheckpointHeader h;
+    int st = ACFD_OK;
+    if (fread(&h, sizeof(h), 1, fp) != 1 || memcmp(h.magic, kCheckpointMagic, 8) != 0 || h.version != 1 ||
+        h.node_bytes != (int32_t)sizeof(acfd_node_t)) {
+        set_error("acfd_checkpoint_load: %s is not a version-1 checkpoint", path);
+        st = ACFD_ERR_IO;
+    } else if (h.n[0] != cs->grid.n[0] || h.n[1] != cs->grid.n[1] || h.n[2] != cs->grid.n[2] ||
+               h.count != (int64_t)node_count(cs)) {
+        set_error("acfd_checkpoint_load: %s holds %d x %d x %d nodes, the case %d x %d x %d", path, h.n[0], h.n[1],
+                  h.n[2], cs->grid.n[0], cs->grid.n[1], cs->grid.n[2]);
+        st = ACFD_ERR_ARG;
+    } else if (h.user_bytes < 0 || (size_t)h.user_bytes > user_cap || (h.user_bytes && !user)) {
+        set_error("acfd_checkpoint_load: user block of %lld bytes, room for %zu", (long long)h.user_bytes, user_cap);
+        st = ACFD_ERR_ARG;
+    }
+    if (user_bytes) *user_bytes = (st == ACFD_OK || st == ACFD_ERR_ARG) ? (size_t)std::max<int64_t>(0, h.user_bytes) : 0;
+    if (st == ACFD_OK && h.user_bytes && fread(user, 1, (size_t)h.user_bytes, fp) != (size_t)h.user_bytes) {
+        set_error("acfd_checkpoint_load: %s is truncated", path);
+        st = ACFD_ERR_IO;
+    }
+    std::vector<acfd_node_t> nodes;
+    if (st == ACFD_OK) {
+        nodes.resize((size_t)h.count);
+        if (fread(nodes.data(), sizeof(acfd_node_t), nodes.size(), fp) != nodes.size()) {
+            set_error("acfd_checkpoint_load: %s is truncated", path);
+            st = ACFD_ERR_IO;
+        }
+    }
+    fclose(fp);
+    if (st != ACFD_OK) return st;
+    return acfd_sync_to_device(cs, nodes.data(), ACFD_SYNC_ALL);
 }
 
 int acfd_integrate_surface_force(acfd_case_t *cs, double *force)

@@ -18,7 +18,11 @@
  *
  * Environment: ACFD_MODE = fp64 (default) | exact | fp32, ACFD_GRAPH = 1
  * (default, replay each step as a CUDA graph) | 0, ACFD_SOLID = device
- * (default) | host.
+ * (default) | host, ACFD_ASYNC_OUTPUT = 1 (default: the outputs of a step
+ * come from a device snapshot and are written while the next step runs, when
+ * no body moves) | 0, ACFD_CHECKPOINT = 0 (default) | 1 (an FP64 checkpoint
+ * artracfd.ckpt.<n> with every space data output; a restart from output n
+ * uses it when it exists).
  */
 #include "acfd_shim.h"
 
@@ -47,6 +51,17 @@ static int g_host_current = 1;   /* host node array holds the latest state */
 static int g_dev_current = 0;    /* device holds the latest state */
 static int g_use_graph = 1;
 static int g_solid_host = 0;   /* ACFD_SOLID=host: rigid-body step on the host */
+static int g_async_output = 1; /* ACFD_ASYNC_OUTPUT=0: output from a synchronous download */
+static int g_checkpoint = 0;   /* ACFD_CHECKPOINT=1: FP64 checkpoint with every space data output */
+
+/* outputs of one step written from a device snapshot while the next step runs */
+typedef struct {
+    int pending;
+    int count;
+    int which[NPROBE];
+    Time time;
+} PendingOutput;
+static PendingOutput g_out;
 
 static void Check(int status, const char *what)
 {
@@ -174,6 +189,10 @@ static void EnsureCase(Space *space, const Model *model)
     g_use_graph = !(env && 0 == strcmp(env, "0"));
     env = getenv("ACFD_SOLID");
     g_solid_host = (env && 0 == strcmp(env, "host"));
+    env = getenv("ACFD_ASYNC_OUTPUT");
+    g_async_output = !(env && 0 == strcmp(env, "0"));
+    env = getenv("ACFD_CHECKPOINT");
+    g_checkpoint = (env && 0 == strcmp(env, "1"));
     AcfdUploadGeometry(space);
     g_dev_current = 0;
     g_host_current = 1;
@@ -284,6 +303,169 @@ static void GpuSolidStep(const Real now, const Real dt, Space *space, const Mode
     AcfdUploadGeometry(space);
 }
 
+/* ---- FP64 checkpoints ----------------------------------------------------
+ * artracfd.ckpt.<dataC> beside the data files of the same output: the node
+ * records of the device state (libacfd_gpu writes them) and, as the caller's
+ * block, the time and every body's motion state and transformed surface, so
+ * that a restart from output dataC continues bit for bit (the reference
+ * restarts from its float32 / %.6g files, ReadData, data_stream.c:71-90). */
+#define CKPT_BODY_REALS 64
+
+static void CheckpointName(int dataC, char *name, size_t len)
+{
+    snprintf(name, len, "artracfd.ckpt.%05d", dataC);
+}
+
+static size_t CheckpointUserBytes(const Geometry *geo)
+{
+    size_t bytes = 3 * sizeof(double) + sizeof(int) * (1 + geo->totN);
+    for (int n = 0; n < geo->totN; ++n) {
+        const Polyhedron *P = geo->poly + n;
+        bytes += CKPT_BODY_REALS * sizeof(double);
+        if (0 < P->faceN) {
+            bytes += 3 * sizeof(double) * (size_t)(2 * P->vertN + P->faceN + P->edgeN);
+        }
+    }
+    return bytes;
+}
+
+/* the body members that change in a run, in one fixed order: pack (to the
+ * block) or unpack (from it) */
+static unsigned char *CheckpointBody(Polyhedron *P, unsigned char *q, int pack)
+{
+    double *r = (double *)q;
+    /* the reference's restart re-reads r, rho, T, cf, area and volume from
+     * the %.6g body file and recomputes the mass properties: kept here too */
+    double *members[] = {P->O, &P->I[0][0], &P->V[0][0], &P->W[0][0], &P->at[0][0], &P->ar[0][0],
+        P->Fp, P->Fv, P->Tt, &P->to, &P->box[0][0], &P->r, &P->rho, &P->T, &P->cf, &P->area, &P->volume};
+    const int sizes[] = {3, 9, 3 * DIMTK, 3 * DIMTK, 3 * DIMTK, 3 * DIMTK, 3, 3, 3, 1, 2 * DIMS, 1, 1, 1, 1, 1, 1};
+    int k = 0;
+    for (int m = 0; m < (int)(sizeof(sizes) / sizeof(sizes[0])); ++m) {
+        for (int c = 0; c < sizes[m]; ++c, ++k) {
+            if (pack) {
+                r[k] = members[m][c];
+            } else {
+                members[m][c] = r[k];
+            }
+        }
+    }
+    for (; k < CKPT_BODY_REALS; ++k) {
+        if (pack) {
+            r[k] = 0.0;
+        }
+    }
+    q += CKPT_BODY_REALS * sizeof(double);
+    if (0 < P->faceN) {
+        Real *arrays[] = {&P->v[0][0], &P->Nv[0][0], &P->Nf[0][0], &P->Ne[0][0]};
+        const size_t counts[] = {(size_t)P->vertN, (size_t)P->vertN, (size_t)P->faceN, (size_t)P->edgeN};
+        for (int m = 0; m < 4; ++m) {
+            const size_t bytes = 3 * sizeof(double) * counts[m];
+            if (pack) {
+                memcpy(q, arrays[m], bytes);
+            } else {
+                memcpy(arrays[m], q, bytes);
+            }
+            q += bytes;
+        }
+    }
+    return q;
+}
+
+static unsigned char *CheckpointUser(const Time *time, const Space *space, size_t *bytes)
+{
+    const Geometry *geo = &(space->geo);
+    *bytes = CheckpointUserBytes(geo);
+    unsigned char *user = AssignStorage(*bytes);
+    unsigned char *q = user;
+    double t[3] = {time->now, (double)time->stepC, (double)time->dataC};
+    memcpy(q, t, sizeof(t));
+    q += sizeof(t);
+    int *ids = (int *)q;
+    ids[0] = geo->totN;
+    for (int n = 0; n < geo->totN; ++n) {
+        ids[1 + n] = geo->poly[n].state;
+    }
+    q += sizeof(int) * (1 + geo->totN);
+    for (int n = 0; n < geo->totN; ++n) {
+        q = CheckpointBody(geo->poly + n, q, 1);
+    }
+    return user;
+}
+
+/* restart from the checkpoint of output time->restart, when there is one */
+static void RestoreCheckpoint(Time *time, Space *space)
+{
+    char name[64];
+    CheckpointName(time->restart, name, sizeof(name));
+    FILE *fp = fopen(name, "rb");
+    if (NULL == fp) {
+        ShowInfo("  no FP64 checkpoint %s: restarting from the data files\n", name);
+        return;
+    }
+    fclose(fp);
+    Geometry *geo = &(space->geo);
+    size_t cap = CheckpointUserBytes(geo), got = 0;
+    unsigned char *user = AssignStorage(cap);
+    Check(acfd_checkpoint_load(g_case, name, user, cap, &got), "acfd_checkpoint_load");
+    if (got != cap || ((int *)(user + 3 * sizeof(double)))[0] != geo->totN) {
+        ShowError("checkpoint %s does not match the case's bodies", name);
+    }
+    const unsigned char *q = user;
+    double t[3];
+    memcpy(t, q, sizeof(t));
+    q += sizeof(t) + sizeof(int) * (1 + geo->totN);
+    time->now = t[0];
+    time->stepC = (int)t[1];
+    time->dataC = (int)t[2];
+    const int *states = (const int *)(user + sizeof(t)) + 1;
+    for (int n = 0; n < geo->totN; ++n) {
+        geo->poly[n].state = states[n];
+        q = CheckpointBody(geo->poly + n, (unsigned char *)q, 0);
+    }
+    RetrieveStorage(user);
+    AcfdUploadGeometry(space);
+    g_dev_current = 1;
+    g_host_current = 0;
+    ShowInfo("  restarted from the FP64 checkpoint %s\n", name);
+}
+
+static void WriteCheckpoint(const Time *time, const Space *space, int from_snapshot)
+{
+    char name[64];
+    CheckpointName(time->dataC, name, sizeof(name));
+    size_t bytes = 0;
+    unsigned char *user = CheckpointUser(time, space, &bytes);
+    if (from_snapshot) {
+        Check(acfd_snapshot_save(g_case, name, user, bytes), "acfd_snapshot_save");
+    } else {
+        Check(acfd_checkpoint_save(g_case, name, user, bytes), "acfd_checkpoint_save");
+    }
+    RetrieveStorage(user);
+}
+
+/* the outputs of the snapshot step, written while the device runs on */
+static void FlushOutput(Space *space, const Model *model)
+{
+    if (!g_out.pending) {
+        return;
+    }
+    Check(acfd_snapshot_nodes(g_case, (acfd_node_t *)space->node), "acfd_snapshot_nodes");
+    for (int q = 0; q < g_out.count; ++q) {
+        const int n = g_out.which[q];
+        if (PROFC == n) {
+            IntegrateSurfaceForce(space, model);
+        }
+        if (PROSD == n) {
+            ShowInfo("  writing data...\n");
+        }
+        WriteData(n, &(g_out.time), space, model);
+        if (PROSD == n && g_checkpoint) {
+            WriteCheckpoint(&(g_out.time), space, 1);
+        }
+    }
+    g_out.pending = 0;
+}
+
 /* EvolveSolution (solve.c:48-107) with the fluid step on the device */
 static void GpuEvolveSolution(Time *time, Space *space, const Model *model)
 {
@@ -323,27 +505,48 @@ static void GpuEvolveSolution(Time *time, Space *space, const Model *model)
             GpuSolidStep(time->now, 0.5 * dt, space, model);
         }
         EvolveFluidDynamics(dt, space, model);
+        /* the previous step's outputs, while the device computes this one */
+        FlushOutput(space, model);
         if (0 != model->psi) {
             GpuSolidStep(time->now, 0.5 * dt, space, model);
         }
         Check(acfd_synchronize(g_case), "acfd_synchronize");
         ShowInfo("  elapsed: %.6gs\n", TockTime(&tm));
+        /* outputs: from a snapshot written during the next step when the
+         * bodies do not move (the data files also hold the bodies), else at once */
+        const int deferred = g_async_output && (0 == model->psi);
         for (int n = 0; n < NPROBE; ++n) {
             rcData[n] = rcData[n] + dt;
             if ((rcData[n] >= dtData[n]) || (time->now == time->end) || (time->stepC == time->stepN)) {
+                if (PROSD == n) {
+                    ++(time->dataC);
+                }
+                rcData[n] = zero;
+                if (deferred) {
+                    if (!g_out.pending) {
+                        Check(acfd_snapshot_begin(g_case), "acfd_snapshot_begin");
+                        g_out.pending = 1;
+                        g_out.count = 0;
+                    }
+                    g_out.which[g_out.count++] = n;
+                    g_out.time = *time;
+                    continue;
+                }
                 EnsureHost(space);
                 if (PROFC == n) {
                     IntegrateSurfaceForce(space, model);
                 }
                 if (PROSD == n) {
                     ShowInfo("  writing data...\n");
-                    ++(time->dataC);
                 }
                 WriteData(n, time, space, model);
-                rcData[n] = zero;
+                if (PROSD == n && g_checkpoint) {
+                    WriteCheckpoint(time, space, 0);
+                }
             }
         }
     }
+    FlushOutput(space, model);
     EnsureHost(space);
 }
 
@@ -356,6 +559,10 @@ int Solve(Time *time, Space *space, const Model *model)
     ShowInfo("Solving (B200, libacfd_gpu)...\n");
     ShowInfo("  initializing...\n");
     InitializeComputeDomain(time, space, model);
+    if (0 != time->restart) {
+        EnsureCase(space, model);
+        RestoreCheckpoint(time, space);
+    }
     ShowInfo("  time marching...\n");
     GpuEvolveSolution(time, space, model);
     ShowInfo("Session");

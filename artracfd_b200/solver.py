@@ -107,6 +107,31 @@ class Solver:
         check(self.lib.acfd_sync_to_host(self.h, node.ctypes.data_as(ctypes.c_void_p), mask), self.lib)
         return node
 
+    # snapshots and FP64 checkpoints ----------------------------------
+    def snapshot_begin(self):
+        """Queue a copy of the node records (returns at once; later work
+        overlaps the copy)."""
+        check(self.lib.acfd_snapshot_begin(self.h), self.lib)
+
+    def snapshot_nodes(self) -> np.ndarray:
+        node = np.zeros(self.node_count, dtype=abi.NODE_DTYPE)
+        check(self.lib.acfd_snapshot_nodes(self.h, node.ctypes.data_as(ctypes.c_void_p)), self.lib)
+        return node
+
+    def snapshot_save(self, path: str, user: bytes = b""):
+        buf = ctypes.create_string_buffer(user, len(user)) if user else None
+        check(self.lib.acfd_snapshot_save(self.h, path.encode(), buf, len(user)), self.lib)
+
+    def checkpoint_save(self, path: str, user: bytes = b""):
+        buf = ctypes.create_string_buffer(user, len(user)) if user else None
+        check(self.lib.acfd_checkpoint_save(self.h, path.encode(), buf, len(user)), self.lib)
+
+    def checkpoint_load(self, path: str, user_cap: int = 1 << 20) -> bytes:
+        buf = ctypes.create_string_buffer(max(user_cap, 1))
+        n = ctypes.c_size_t()
+        check(self.lib.acfd_checkpoint_load(self.h, path.encode(), buf, user_cap, ctypes.byref(n)), self.lib)
+        return buf.raw[:n.value]
+
     def device_state(self):
         U = ctypes.POINTER(ctypes.c_double)()
         F = ctypes.POINTER(ctypes.c_int)()

@@ -36,6 +36,7 @@ extern "C" {
 #define ACFD_ERR_DEVICE 4     /* a kernel reported an error through the device status word */
 #define ACFD_ERR_NOMEM 5      /* device allocation failed */
 #define ACFD_ERR_NOT_FOUND 6  /* e.g. edge search failed (computational_geometry.c:158-160) */
+#define ACFD_ERR_IO 7         /* a checkpoint file could not be read or written */
 
 /* time levels and operators (commons.h:27-48) */
 #define ACFD_TO 0
@@ -266,6 +267,33 @@ int acfd_integrate_surface_force(acfd_case_t *cs, double *force);
  * first body), N[totN * totN * 3]; contact c of body p is gid[p*totN + c],
  * N[(p*totN + c)*3 + 0..2]. */
 int acfd_collision_scan(acfd_case_t *cs, int *counts, int *gid, int *N);
+
+/* ---- output snapshots and FP64 checkpoints -----------------------------
+ * The reference writes its fields as float32 (EnSight) or %.6g text
+ * (ParaView) and restarts from those files (ReadData, data_stream.c:71-90),
+ * losing precision.  A checkpoint holds the node records of every node
+ * (ghosts included, all three levels and the flags, the reference's Node
+ * layout) in FP64, after a 64-byte header {"ACFDCKP1", version 1, node
+ * bytes, n[3], node count, size of the caller's block} and the caller's
+ * block (e.g. time and body state), so a restart continues bit for bit.
+ *
+ * acfd_snapshot_begin queues, on the case's stream, a copy of the node
+ * records into device memory and from there, on a stream of its own, into
+ * pinned host memory, and returns at once: work queued afterwards overlaps
+ * the copy.  acfd_snapshot_nodes / acfd_snapshot_save wait for that copy and
+ * give the records (as acfd_sync_to_host with ACFD_SYNC_ALL would have at the
+ * time of acfd_snapshot_begin) or write them as a checkpoint.  A new
+ * snapshot replaces the previous one. */
+int acfd_snapshot_begin(acfd_case_t *cs);
+int acfd_snapshot_nodes(acfd_case_t *cs, acfd_node_t *node);
+int acfd_snapshot_save(acfd_case_t *cs, const char *path, const void *user, size_t user_bytes);
+/* Synchronous checkpoint of the current state (a snapshot written at once). */
+int acfd_checkpoint_save(acfd_case_t *cs, const char *path, const void *user, size_t user_bytes);
+/* Restore a checkpoint of a case with the same node counts: every node
+ * record goes to the device; the caller's block (at most user_cap bytes) is
+ * copied to user and its size to *user_bytes (also when it does not fit:
+ * ACFD_ERR_ARG). */
+int acfd_checkpoint_load(acfd_case_t *cs, const char *path, void *user, size_t user_cap, size_t *user_bytes);
 
 /* ---- learned smoothness sensor (no counterpart in the reference) ------- */
 

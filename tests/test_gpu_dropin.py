@@ -119,6 +119,59 @@ def test_dropin_viscous_contacts_close_to_reference(tmp_path):
         assert np.abs(fa[f] - fb[f]).max() <= 1e-5 * scale, f
 
 
+def _fields_of(case_dir, index):
+    stem = "field%05d" % index
+    return {f: _field(os.path.join(case_dir, f"{stem}.{f}")) for f in FIELDS}
+
+
+@needs
+@pytest.mark.parametrize("name", ["sod", "contact_spheres"])
+def test_dropin_fp64_checkpoint_restart_continues_bit_for_bit(tmp_path, name):
+    """Two space data outputs; the run restarted from the first one (restart
+    tag 1) with its FP64 checkpoint writes the second one exactly as the
+    uninterrupted run (the reference restarts from its float32 files).  With
+    moving, touching bodies the checkpoint also carries their motion state
+    and transformed surfaces."""
+    if name == "sod":
+        spec = configs.sod(m=(32, 4, 4))
+    else:
+        spec = cases.contact_spheres(viscous=False)
+        spec.end = 0.03
+    spec.stepN = 0
+    spec.dataW = 2
+    a = tmp_path / "a"
+    spec.write(str(a))
+    _run(DROPIN, "gpu", str(a), {"ACFD_MODE": "exact", "ACFD_CHECKPOINT": "1"})
+    assert (a / "artracfd.ckpt.00001").exists() and (a / "artracfd.ckpt.00002").exists()
+    b = tmp_path / "b"
+    shutil.copytree(a, b)
+    for f in b.glob("field00002.*"):
+        f.unlink()
+    spec.restart = 1
+    spec.write(str(b))
+    r = _run(DROPIN, "gpu", str(b), {"ACFD_MODE": "exact"})
+    assert "restarted from the FP64 checkpoint" in r.stdout
+    fa, fb = _fields_of(str(a), 2), _fields_of(str(b), 2)
+    for f in FIELDS:
+        assert np.array_equal(fa[f], fb[f]), f
+
+
+@needs
+def test_dropin_async_output_equals_synchronous_output(tmp_path):
+    """Outputs written from a device snapshot while the next step runs are
+    the outputs of a synchronous download."""
+    spec = configs.sod(m=(32, 4, 4))
+    spec.stepN = 0
+    spec.dataW = 4
+    a, b = _pair(tmp_path, spec)
+    _run(DROPIN, "gpu", a, {"ACFD_MODE": "fp64", "ACFD_ASYNC_OUTPUT": "0"})
+    _run(DROPIN, "gpu", b, {"ACFD_MODE": "fp64"})
+    for q in range(5):
+        fa, fb = _fields_of(a, q), _fields_of(b, q)
+        for f in FIELDS:
+            assert np.array_equal(fa[f], fb[f]), (q, f)
+
+
 @needs
 def test_dropin_serial_mode_is_the_reference(tmp_path):
     spec = configs.sod(m=(32, 4, 4), stepN=3)
