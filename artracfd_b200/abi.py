@@ -173,6 +173,7 @@ def load_library(path: str | None = None):
         "acfd_set_tiles": [vp, ctypes.POINTER(ctypes.c_int)],
         "acfd_mlp_param_count": [],
         "acfd_sensor_load": [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_float],
+        "acfd_sensor_load_file": [vp, ctypes.c_char_p],
         "acfd_sensor_update": [vp, ctypes.POINTER(ctypes.c_ulonglong)],
         "acfd_sensor_flags": [vp, ctypes.POINTER(vp)],
         "acfd_sensor_features": [vp, i, vp, vp],

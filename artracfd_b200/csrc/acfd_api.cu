@@ -1043,6 +1043,35 @@ int acfd_sensor_load(acfd_case_t *cs, const float *params, float threshold)
     return ACFD_OK;
 }
 
+int acfd_sensor_load_file(acfd_case_t *cs, const char *path)
+{
+    TRY(check_case(cs));
+    if (!path) {
+        set_error("acfd_sensor_load_file: null path");
+        return ACFD_ERR_ARG;
+    }
+    FILE *fp = fopen(path, "rb");
+    if (!fp) {
+        set_error("acfd_sensor_load_file: cannot open %s", path);
+        return ACFD_ERR_IO;
+    }
+    char magic[8];
+    int32_t count = 0;
+    float threshold = 0.0f;
+    const int np = sensor_param_count();
+    std::vector<float> params((size_t)np);
+    const bool ok = fread(magic, 1, 8, fp) == 8 && memcmp(magic, "ACFDSNS1", 8) == 0 &&
+                    fread(&count, sizeof(count), 1, fp) == 1 && count == np &&
+                    fread(&threshold, sizeof(threshold), 1, fp) == 1 &&
+                    fread(params.data(), sizeof(float), (size_t)np, fp) == (size_t)np;
+    fclose(fp);
+    if (!ok) {
+        set_error("acfd_sensor_load_file: %s is not a sensor file of %d parameters", path, np);
+        return ACFD_ERR_IO;
+    }
+    return acfd_sensor_load(cs, params.data(), threshold);
+}
+
 int acfd_sensor_update(acfd_case_t *cs, unsigned long long *flagged)
 {
     TRY(check_case(cs));

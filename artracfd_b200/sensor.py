@@ -201,9 +201,24 @@ def predict(params, X):
     return out
 
 
+WEIGHTS_BIN = os.path.join(HERE, "sensor_weights.bin")
+
+
 def save(path, params, threshold, meta):
     np.savez(path, params=np.asarray(params, dtype=np.float32), threshold=np.float32(threshold),
              meta=json.dumps(meta))
+    save_bin(os.path.splitext(path)[0] + ".bin", params, threshold)
+
+
+def save_bin(path, params, threshold):
+    """The weights in the file format of acfd_sensor_load_file: "ACFDSNS1",
+    int32 parameter count, float32 threshold, float32 parameters."""
+    p = np.asarray(params, dtype="<f4")
+    with open(path, "wb") as fh:
+        fh.write(b"ACFDSNS1")
+        fh.write(np.int32(p.size).astype("<i4").tobytes())
+        fh.write(np.float32(threshold).astype("<f4").tobytes())
+        fh.write(p.tobytes())
 
 
 def load(path=WEIGHTS):

@@ -16,7 +16,10 @@
  * host (ACFD_SOLID=host); by default its node scans run on the device
  * (solid_gpu.c).
  *
- * Environment: ACFD_MODE = fp64 (default) | exact | fp32, ACFD_GRAPH = 1
+ * Environment: ACFD_MODE = fp64 (default) | exact | fp32 | hybrid (the
+ * learned-sensor form; ACFD_SENSOR = weights file, default the shipped
+ * sensor_weights.bin), ACFD_TILES = stage-kernel variants per axis (e.g.
+ * 7,7,7), ACFD_AUTOTUNE = 1 (time the variants at the first step), ACFD_GRAPH = 1
  * (default, replay each step as a CUDA graph) | 0, ACFD_SOLID = device
  * (default) | host, ACFD_ASYNC_OUTPUT = 1 (default: the outputs of a step
  * come from a device snapshot and are written while the next step runs, when
@@ -24,6 +27,7 @@
  * artracfd.ckpt.<n> with every space data output; a restart from output n
  * uses it when it exists).
  */
+#define _POSIX_C_SOURCE 200809L /* readlink */
 #include "acfd_shim.h"
 
 #include <math.h>
@@ -31,6 +35,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <limits.h>
+#include <unistd.h>
 
 #include "commons.h"
 #include "cfd_commons.h"
@@ -53,6 +58,7 @@ static int g_use_graph = 1;
 static int g_solid_host = 0;   /* ACFD_SOLID=host: rigid-body step on the host */
 static int g_async_output = 1; /* ACFD_ASYNC_OUTPUT=0: output from a synchronous download */
 static int g_checkpoint = 0;   /* ACFD_CHECKPOINT=1: FP64 checkpoint with every space data output */
+static int g_autotune = 0;     /* ACFD_AUTOTUNE=1: time the stage-kernel variants at the first step */
 
 /* outputs of one step written from a device snapshot while the next step runs */
 typedef struct {
@@ -183,8 +189,37 @@ static void EnsureCase(Space *space, const Model *model)
         mode = ACFD_FP64_EXACT;
     } else if (env && 0 == strcmp(env, "fp32")) {
         mode = ACFD_FP32_BULK;
+    } else if (env && 0 == strcmp(env, "hybrid")) {
+        mode = ACFD_FP32_HYBRID;
+        /* the trained sensor: ACFD_SENSOR, else the weights shipped beside
+         * the library (artracfd_b200/sensor_weights.bin) */
+        char path[4096] = {0};
+        const char *given = getenv("ACFD_SENSOR");
+        if (given) {
+            snprintf(path, sizeof(path), "%s", given);
+        } else {
+            char exe[4096] = {0};
+            const ssize_t len = readlink("/proc/self/exe", exe, sizeof(exe) - 1);
+            char *slash = (len > 0) ? strrchr(exe, '/') : NULL;
+            if (NULL == slash) {
+                ShowError("ACFD_MODE=hybrid: set ACFD_SENSOR to the sensor weights file");
+            }
+            *slash = '\0';
+            snprintf(path, sizeof(path), "%s/../../sensor_weights.bin", exe);
+        }
+        Check(acfd_sensor_load_file(g_case, path), "acfd_sensor_load_file");
     }
     Check(acfd_set_precision(g_case, mode), "acfd_set_precision");
+    env = getenv("ACFD_TILES");
+    if (env) {
+        int tiles[3];
+        if (3 != sscanf(env, "%d,%d,%d", tiles, tiles + 1, tiles + 2)) {
+            ShowError("ACFD_TILES: three variants, e.g. 7,7,7");
+        }
+        Check(acfd_set_tiles(g_case, tiles), "acfd_set_tiles");
+    }
+    env = getenv("ACFD_AUTOTUNE");
+    g_autotune = (env && 0 == strcmp(env, "1"));
     env = getenv("ACFD_GRAPH");
     g_use_graph = !(env && 0 == strcmp(env, "0"));
     env = getenv("ACFD_SOLID");
@@ -247,6 +282,12 @@ void EvolveFluidDynamics(const Real dt, Space *space, const Model *model)
     }
     EnsureCase(space, model);
     EnsureDevice(space);
+    if (g_autotune) {
+        int tiles[3];
+        Check(acfd_autotune(g_case, tiles), "acfd_autotune");
+        ShowInfo("  stage kernels (autotuned): %d %d %d\n", tiles[0], tiles[1], tiles[2]);
+        g_autotune = 0;
+    }
     if (g_use_graph) {
         Check(acfd_evolve_fluid_graph(g_case, dt), "acfd_evolve_fluid_graph");
     } else {
@@ -443,6 +484,16 @@ static void WriteCheckpoint(const Time *time, const Space *space, int from_snaps
     RetrieveStorage(user);
 }
 
+/* Does output n read the node array?  The probe writers (data_probe.c:23-197)
+ * return at once when the case defines no probe of their kind, and a case
+ * without a probe section leaves their frequencies at INT_MAX, which makes
+ * them fire at every step of a long run; only the space data and defined
+ * probes need the state on the host. */
+static int OutputNeedsNodes(int n, const Time *time)
+{
+    return (PROSD == n) || (0 < time->dataN[n]);
+}
+
 /* the outputs of the snapshot step, written while the device runs on */
 static void FlushOutput(Space *space, const Model *model)
 {
@@ -522,6 +573,9 @@ static void GpuEvolveSolution(Time *time, Space *space, const Model *model)
                     ++(time->dataC);
                 }
                 rcData[n] = zero;
+                if (!OutputNeedsNodes(n, time)) {
+                    continue;  /* its writer has nothing to write */
+                }
                 if (deferred) {
                     if (!g_out.pending) {
                         Check(acfd_snapshot_begin(g_case), "acfd_snapshot_begin");

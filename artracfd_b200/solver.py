@@ -77,6 +77,10 @@ class Solver:
         check(self.lib.acfd_sensor_load(self.h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(threshold)),
               self.lib)
 
+    def sensor_load_file(self, path: str):
+        """The sensor from a weights file (acfd_sensor_load_file)."""
+        check(self.lib.acfd_sensor_load_file(self.h, path.encode()), self.lib)
+
     def sensor_update(self) -> int:
         """Evaluate the sensor on U[TO]; returns the number of flags set."""
         n = ctypes.c_ulonglong()

@@ -304,6 +304,10 @@ int acfd_mlp_param_count(void);
  * threshold above which a node keeps the full WENO5 reconstruction; enables
  * acfd_set_precision(ACFD_FP32_HYBRID). */
 int acfd_sensor_load(acfd_case_t *cs, const float *params, float threshold);
+/* The same from a file: "ACFDSNS1", int32 parameter count, float32
+ * threshold, float32 parameters (artracfd_b200/sensor_weights.bin holds the
+ * trained sensor). */
+int acfd_sensor_load_file(acfd_case_t *cs, const char *path);
 /* Evaluate the sensor on U[TO] for the three sweep axes (the hybrid step does
  * this itself at its start); *flagged (optional) = number of flags set. */
 int acfd_sensor_update(acfd_case_t *cs, unsigned long long *flagged);

@@ -173,6 +173,26 @@ def test_dropin_async_output_equals_synchronous_output(tmp_path):
 
 
 @needs
+def test_dropin_hybrid_mode_within_stated_error(tmp_path):
+    """ACFD_MODE=hybrid: the learned-sensor form through the drop-in program
+    (the shipped sensor weights) on a reduced shock-cylinder case stays within
+    L1 density error 1e-3 of the unmodified reference program."""
+    spec = configs.shock_cylinder(m=(128, 64, 4), segments=48)
+    spec.stepN = 20
+    a, b = _pair(tmp_path, spec)
+    _run(REFBIN, "serial", a)
+    r = _run(DROPIN, "gpu", b, {"ACFD_MODE": "hybrid", "ACFD_AUTOTUNE": "1"})
+    assert "autotuned" in r.stdout
+    sa, fa = _last_fields(a)
+    sb, fb = _last_fields(b)
+    assert sa == sb
+    assert np.array_equal(fa["did"], fb["did"])
+    fluid = fa["did"] == 0
+    l1 = np.abs(fb["rho"][fluid] - fa["rho"][fluid]).sum() / np.abs(fa["rho"][fluid]).sum()
+    assert l1 <= 1e-3, l1
+
+
+@needs
 def test_dropin_serial_mode_is_the_reference(tmp_path):
     spec = configs.sod(m=(32, 4, 4), stepN=3)
     a, b = _pair(tmp_path, spec)

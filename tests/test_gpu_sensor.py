@@ -228,3 +228,30 @@ def test_trained_sensor_gain_on_shock_cylinder():
     e_hyb, e_lin = l1(hyb), l1(lin)
     assert e_hyb <= 1e-3, e_hyb
     assert e_lin > 3 * e_hyb, (e_lin, e_hyb)
+
+
+@pytest.mark.skipif(not os.path.exists(sensor.WEIGHTS_BIN), reason="no trained sensor weights")
+def test_sensor_file_is_the_trained_sensor(tmp_path):
+    """acfd_sensor_load_file reads the shipped weights file: the same flags as
+    the parameters given directly; a damaged file is refused."""
+    spec = configs.shock_cylinder(m=(64, 32, 4), segments=24)
+    spec.bodies = []
+    part, model = spec.descriptors()
+    node = spec.initial_nodes(part, model)
+    params, thr, _ = sensor.load(sensor.WEIGHTS)
+    counts = []
+    for how in ("params", "file"):
+        with Solver(part, model, abi.FP64) as s:
+            s.upload(node)
+            s.treat_boundary(abi.TO)
+            if how == "params":
+                s.sensor_load(params, thr)
+            else:
+                s.sensor_load_file(sensor.WEIGHTS_BIN)
+            counts.append(s.sensor_update())
+    assert counts[0] == counts[1] > 0
+    bad = tmp_path / "bad.bin"
+    bad.write_bytes(open(sensor.WEIGHTS_BIN, "rb").read()[:100])
+    with Solver(part, model, abi.FP64) as s:
+        with pytest.raises(abi.AcfdError):
+            s.sensor_load_file(str(bad))
