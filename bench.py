@@ -191,6 +191,22 @@ FORM_NAMES = {0: "fp64_exact", 1: "fp64", 2: "fp32", 3: "hybrid"}
 DTYPES = {"fp64": "f64", "fp64_exact": "f64", "fp32": "f32/f64", "hybrid": "f32/f64"}
 
 
+def max_over_ranks(torch, dist, x: float, device="cuda") -> float:
+    """The largest of the ranks' values of x (x itself on one rank): every
+    multi-rank time in the JSON line is the slowest rank's."""
+    if not dist:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world: int, nodes_per_rank: int, steps: int, seconds: float) -> float:
+    """Whole-job Mcell-steps/s of N independent replicas (weak scaling: every
+    rank advances its own copy of the workload) timed by the slowest rank."""
+    return world * nodes_per_rank * steps / seconds / 1e6
+
+
 def _solver(part, model, form, stream):
     from artracfd_b200 import abi
     from artracfd_b200.solver import Solver
@@ -231,9 +247,7 @@ def _timed_steps(torch, s, spec, steps, warmup, dist, stream, clock_index):
     torch.cuda.synchronize()
     sec = e0.elapsed_time(e1) / 1e3
     if dist:
-        t = torch.tensor([sec], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        sec = float(t.item())
+        sec = max_over_ranks(torch, dist, sec)
         dist.barrier()
     return sec, s.launches() - launches0, clk.summary()
 
@@ -346,7 +360,7 @@ def run_ours(args, rank, world, local_rank):
         sec64, _, clk64 = _timed_steps(torch, s, spec, args.steps, args.warmup, dist, stream, local_rank)
         st64, bc64, by64 = _stage_profile(torch, s, spec, nodes_pin, stream)
         s.close()
-        plain = {"value": world * nodes_pin * args.steps / sec64 / 1e6, "ms_per_step": sec64 / args.steps * 1e3,
+        plain = {"value": job_rate(world, nodes_pin, args.steps, sec64), "ms_per_step": sec64 / args.steps * 1e3,
                  "stage_ms": {"sweep_mean": st64, "ghost_fill_mean": bc64},
                  "hbm_frac": by64 / (st64 / 1e3) / 1e9 / hbm_peak, "tiles": tiles64, "clocks": clk64}
 
@@ -360,7 +374,7 @@ def run_ours(args, rank, world, local_rank):
         flagged = s.sensor_update()
         sensor_info = {"flagged_fraction_at_start": flagged / (3.0 * nodes_pin)}
     sec, gpu_launches, clocks = _timed_steps(torch, s, spec, args.steps, args.warmup, dist, stream, local_rank)
-    value = world * nodes_pin * args.steps / sec / 1e6
+    value = job_rate(world, nodes_pin, args.steps, sec)
     if args.mode == "hybrid":
         sensor_info["flagged_fraction_after_timed_steps"] = s.sensor_update() / (3.0 * nodes_pin)
     per_axis = {}
@@ -397,10 +411,7 @@ def run_ours(args, rank, world, local_rank):
         s.evolve(s.time_step(spec.cfl), graph=True)
     s.download(host)
     e2e_sec = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_sec], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_sec = float(t.item())
+    e2e_sec = max_over_ranks(torch, dist, e2e_sec)
     node_bytes = host.nbytes
     s.close()
     accuracy = None
@@ -447,7 +458,7 @@ def run_ours(args, rank, world, local_rank):
                               "note": "reference FP64 flop count; meaningful as a fraction for the FP64 forms"}},
         "stage_ms": {"sweep_mean": stage_mean, "ghost_fill_mean": bc_mean},
         "clocks": clocks,
-        "e2e": {"value": world * nodes_pin * args.steps / e2e_sec / 1e6, "unit": UNIT,
+        "e2e": {"value": job_rate(world, nodes_pin, args.steps, e2e_sec), "unit": UNIT,
                 "h2d_bytes_per_step": (node_bytes + 8 * args.steps) / args.steps,
                 "d2h_bytes_per_step": (node_bytes + 24 * args.steps) / args.steps,
                 "what": "C-ABI loop with host node arrays: acfd_sync_to_device, K x (acfd_cfl + host dt + "
