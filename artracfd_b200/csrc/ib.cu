@@ -406,10 +406,11 @@ struct BoxList {
     int nb;
 };
 
-// Ghost list: every ghost node of layers 1..gl of every body, as
-// (i, j, k, body | layer << 24).  The flags do not change during a boundary
-// treatment and a node belongs to one body only, so a node is listed once;
-// the order of the list is free (nodes of one layer are independent).
+// Ghost lists: every ghost node of layers 1..gl of every body, as
+// (i, j, k, body | layer << 24), in the list of its layer (cap entries each).
+// The flags do not change during a boundary treatment and a node belongs to
+// one body only, so a node is listed once; the order of a list is free
+// (nodes of one layer are independent).
 __global__ void ib_list(IbGrid G, BoxList bl, const int *flags, int4 *ghosts, int *nghost, int cap, int *status)
 {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -426,12 +427,12 @@ __global__ void ib_list(IbGrid G, BoxList bl, const int *flags, int4 *ghosts, in
     const long long id = node_of(g, i, j, k);
     const int gst = flags[3 * g.nn + id];
     if (gst < 1 || gst > G.gl || n + 1 != flags[id]) return;
-    const int slot = atomicAdd(nghost, 1);
+    const int slot = atomicAdd(nghost + gst - 1, 1);
     if (slot >= cap) {
         atomicExch(status, 4);
         return;
     }
-    ghosts[slot] = make_int4(i, j, k, n | (gst << 24));
+    ghosts[(long long)(gst - 1) * cap + slot] = make_int4(i, j, k, n | (gst << 24));
 }
 
 constexpr int kGhostWarps = 4;    // warps per block of ib_ghost
@@ -541,7 +542,8 @@ __global__ void __launch_bounds__(kGhostWarps * 32) ib_ghost(IbGrid G, ModelPara
     __shared__ double scratch[kGhostWarps][32 * kIdwBatch][8];
     const int lane = threadIdx.x & 31;
     double (*sp)[8] = scratch[threadIdx.x >> 5];
-    const int count = min(*nghost, cap);  // an overflowing list has set the status
+    const int count = min(nghost[r - 1], cap);  // an overflowing list has set the status
+    ghosts += (long long)(r - 1) * cap;
     const Grid &g = G.g;
     const long long nn = g.nn;
     double *Ut = U + (long long)tn * 5 * nn;
@@ -1181,8 +1183,8 @@ int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, const acfd_p
     }
     ACFD_CUDA(cudaMalloc(&ib->dev, sizeof(DevBody) * totN));
     ACFD_CUDA(cudaMemcpy(ib->dev, ib->host.data(), sizeof(DevBody) * totN, cudaMemcpyHostToDevice));
-    // ghost list: a node is listed at most once, so the smaller of the
-    // bodies' node boxes and the computed nodes bounds it
+    // ghost lists, one per layer: a node is listed at most once, so the
+    // smaller of the bodies' node boxes and the computed nodes bounds each
     if (totN >= (1 << 24) || part.gl >= 128) {
         set_error("immersed boundary: %d bodies, %d ghost layers (at most %d, 127)", totN, part.gl, (1 << 24) - 1);
         return ACFD_ERR_ARG;
@@ -1201,9 +1203,10 @@ int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, const acfd_p
         return ACFD_ERR_ARG;
     }
     void *gl_buf = nullptr, *cnt = nullptr;
-    ACFD_CUDA(cudaMalloc(&gl_buf, sizeof(int4) * (size_t)cap));
+    const int layers = std::max(1, part.gl);
+    ACFD_CUDA(cudaMalloc(&gl_buf, sizeof(int4) * (size_t)cap * layers));
     ib->buffers.push_back(gl_buf);
-    ACFD_CUDA(cudaMalloc(&cnt, sizeof(int)));
+    ACFD_CUDA(cudaMalloc(&cnt, sizeof(int) * layers));
     ib->buffers.push_back(cnt);
     ib->ghosts = (int4 *)gl_buf;
     ib->nghost = (int *)cnt;
@@ -1230,7 +1233,8 @@ int ib_treat(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partit
 {
     if (!ib || ib->count == 0) return ACFD_OK;
     const IbGrid G = make_ibgrid(g, part, m.ibmLayer);
-    ACFD_CUDA(cudaMemsetAsync(ib->nghost, 0, sizeof(int), st));
+    if (part.gl < 1) return ACFD_OK;
+    ACFD_CUDA(cudaMemsetAsync(ib->nghost, 0, sizeof(int) * part.gl, st));
     for (int n0 = 0; n0 < ib->count; n0 += 8) {
         BoxList bl;
         boxes_of(ib, part, n0, bl);
