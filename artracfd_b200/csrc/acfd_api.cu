@@ -57,7 +57,7 @@ struct IbState;
 int ib_create(IbState **out);
 void ib_destroy(IbState *ib);
 int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, const acfd_partition_t &part,
-              cudaStream_t st);
+              cudaStream_t st, bool *relayout);
 int ib_treat_launches(const IbState *ib, const acfd_partition_t &part);
 int ib_surface_force(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partition_t &part,
                      const double *U, const int *flags, double *force, cudaStream_t st);
@@ -1177,8 +1177,11 @@ int acfd_geo_upload(acfd_case_t *cs, const acfd_polyhedron_t *poly, int totN)
         set_error("acfd_geo_upload: bad body list");
         return ACFD_ERR_ARG;
     }
-    TRY(ib_upload(cs->ib, poly, totN, cs->part, cs->stream));
-    release_graph(cs);
+    bool relayout = true;
+    TRY(ib_upload(cs->ib, poly, totN, cs->part, cs->stream, &relayout));
+    // bodies moved in place keep every device pointer and launch shape of a
+    // captured step; a new body list does not
+    if (relayout) release_graph(cs);
     return ACFD_OK;
 }
 

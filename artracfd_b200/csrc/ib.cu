@@ -48,6 +48,15 @@ struct DevBody {
     const double *tri;  // faceN x 9: v0, e01, e02
 };
 
+// node boxes of up to 8 bodies (body0 ..), flattened in (k, j, i) order
+struct BoxList {
+    int lo[8][3];
+    int ext[8][3];
+    long long start[9];
+    int body0;
+    int nb;
+};
+
 struct IbState {
     std::vector<DevBody> host;
     DevBody *dev = nullptr;
@@ -59,6 +68,8 @@ struct IbState {
     int4 *ghosts = nullptr;  // ghost list of a boundary treatment
     int *nghost = nullptr;
     int ghost_cap = 0;
+    BoxList *groups = nullptr;  // device: node boxes of the bodies, 8 per entry
+    int ngroups = 0;
     // surface-force integration and collision scan (allocated on first use)
     double *sf_terms = nullptr;        // [box node][10]: Fp, Fv, Tt, p of ghost nodes of layer 2
     unsigned char *sf_valid = nullptr; // [box node]: 1 = ghost node of layer 2 of the box's body
@@ -398,41 +409,39 @@ __device__ void orthogonal_space(const double N[3], double Ta[3], double Tb[3])
 // ---------------------------------------------------------------------------
 // ghost layer r of every body (immersed_boundary.c:294-338)
 // ---------------------------------------------------------------------------
-struct BoxList {
-    int lo[8][3];
-    int ext[8][3];
-    long long start[9];
-    int body0;
-    int nb;
-};
 
 // Ghost lists: every ghost node of layers 1..gl of every body, as
 // (i, j, k, body | layer << 24), in the list of its layer (cap entries each).
 // The flags do not change during a boundary treatment and a node belongs to
 // one body only, so a node is listed once; the order of a list is free
 // (nodes of one layer are independent).
-__global__ void ib_list(IbGrid G, BoxList bl, const int *flags, int4 *ghosts, int *nghost, int cap, int *status)
+__global__ void ib_list(IbGrid G, const BoxList *groups, int gidx, const int *flags, int4 *ghosts, int *nghost,
+                        int cap, int *status)
 {
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= bl.start[bl.nb]) return;
-    int q = 0;
-    while (t >= bl.start[q + 1]) ++q;
-    t -= bl.start[q];
-    const int n = bl.body0 + q;
-    const int i = bl.lo[q][0] + (int)(t % bl.ext[q][0]);
-    const long long rest = t / bl.ext[q][0];
-    const int j = bl.lo[q][1] + (int)(rest % bl.ext[q][1]);
-    const int k = bl.lo[q][2] + (int)(rest / bl.ext[q][1]);
-    const Grid &g = G.g;
-    const long long id = node_of(g, i, j, k);
-    const int gst = flags[3 * g.nn + id];
-    if (gst < 1 || gst > G.gl || n + 1 != flags[id]) return;
-    const int slot = atomicAdd(nghost + gst - 1, 1);
-    if (slot >= cap) {
-        atomicExch(status, 4);
-        return;
+    const BoxList &bl = groups[gidx];
+    const long long total = bl.start[bl.nb];
+    for (long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; t0 < total;
+         t0 += (long long)gridDim.x * blockDim.x) {
+        long long t = t0;
+        int q = 0;
+        while (t >= bl.start[q + 1]) ++q;
+        t -= bl.start[q];
+        const int n = bl.body0 + q;
+        const int i = bl.lo[q][0] + (int)(t % bl.ext[q][0]);
+        const long long rest = t / bl.ext[q][0];
+        const int j = bl.lo[q][1] + (int)(rest % bl.ext[q][1]);
+        const int k = bl.lo[q][2] + (int)(rest / bl.ext[q][1]);
+        const Grid &g = G.g;
+        const long long id = node_of(g, i, j, k);
+        const int gst = flags[3 * g.nn + id];
+        if (gst < 1 || gst > G.gl || n + 1 != flags[id]) continue;
+        const int slot = atomicAdd(nghost + gst - 1, 1);
+        if (slot >= cap) {
+            atomicExch(status, 4);
+            continue;
+        }
+        ghosts[(long long)(gst - 1) * cap + slot] = make_int4(i, j, k, n | (gst << 24));
     }
-    ghosts[(long long)(gst - 1) * cap + slot] = make_int4(i, j, k, n | (gst << 24));
 }
 
 constexpr int kGhostWarps = 4;    // warps per block of ib_ghost
@@ -1085,6 +1094,9 @@ static void ib_release_geometry(IbState *ib)
     ib->ghosts = nullptr;
     ib->nghost = nullptr;
     ib->ghost_cap = 0;
+    cudaFree(ib->groups);
+    ib->groups = nullptr;
+    ib->ngroups = 0;
 }
 
 static void ib_release_solid(IbState *ib)
@@ -1122,8 +1134,111 @@ int ib_count(const IbState *ib)
     return ib ? ib->count : 0;
 }
 
-int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, const acfd_partition_t &part, cudaStream_t st)
+static void body_scalars(DevBody &B, const acfd_polyhedron_t &P)
 {
+    B.faceN = P.faceN;
+    B.edgeN = P.edgeN;
+    B.vertN = P.vertN;
+    B.state = P.state;
+    B.r = P.r;
+    B.T = P.T;
+    B.cf = P.cf;
+    B.area = P.area;
+    for (int s = 0; s < 3; ++s) {
+        B.O[s] = P.O[s];
+        B.V[s] = P.V[s];
+        B.W[s] = P.W[s];
+        B.box[s][0] = P.box[s][0];
+        B.box[s][1] = P.box[s][1];
+    }
+}
+
+static int boxes_of(IbState *ib, const acfd_partition_t &part, int n0, BoxList &bl);
+
+// the per-layer ghost capacity the bodies' node boxes need
+static long long ghost_need(const IbState *ib, const acfd_partition_t &part)
+{
+    long long cap = 0;
+    for (int n = 0; n < ib->count; ++n) {
+        int lo[3], ext[3];
+        body_box(part, ib->host[n], lo, ext);
+        cap += (long long)ext[0] * ext[1] * ext[2];
+    }
+    long long pin = 1;
+    for (int s = 0; s < 3; ++s) pin *= std::max(0, part.ns[0][s][1] - part.ns[0][s][0]);
+    return std::max(1LL, std::min(cap, pin));
+}
+
+// the node boxes of all bodies to the device (the ghost list reads them there,
+// so that a captured step stays valid while the bodies move)
+static int upload_groups(IbState *ib, const acfd_partition_t &part, cudaStream_t st)
+{
+    std::vector<BoxList> h((size_t)ib->ngroups);
+    for (int g = 0; g < ib->ngroups; ++g) boxes_of(ib, part, 8 * g, h[(size_t)g]);
+    ACFD_CUDA(cudaMemcpyAsync(ib->groups, h.data(), sizeof(BoxList) * h.size(), cudaMemcpyHostToDevice, st));
+    return ACFD_OK;
+}
+
+// A moved body list of the same bodies (same counts of faces, edges and
+// vertices) whose ghost lists still fit: new positions, velocities and
+// surfaces go into the device buffers in place, in stream order, so that
+// the device pointers and launch shapes of a captured step stay valid.
+static int update_in_place(IbState *ib, const acfd_polyhedron_t *poly, int totN, const acfd_partition_t &part,
+                           cudaStream_t st, bool *done)
+{
+    *done = false;
+    if (totN != ib->count || !ib->dev || !ib->groups) return ACFD_OK;
+    for (int n = 0; n < totN; ++n) {
+        const DevBody &B = ib->host[n];
+        if (B.faceN != poly[n].faceN || B.edgeN != poly[n].edgeN || B.vertN != poly[n].vertN) return ACFD_OK;
+        if (poly[n].faceN > 0 && (!poly[n].f || !poly[n].Nf || !poly[n].e || !poly[n].Ne || !poly[n].v ||
+                                  !poly[n].Nv)) {
+            return ACFD_OK;
+        }
+    }
+    std::vector<DevBody> prev = ib->host;
+    for (int n = 0; n < totN; ++n) body_scalars(ib->host[n], poly[n]);
+    if (ghost_need(ib, part) > ib->ghost_cap) {
+        ib->host = prev;
+        return ACFD_OK;
+    }
+    for (int n = 0; n < totN; ++n) {
+        const acfd_polyhedron_t &P = poly[n];
+        const DevBody &B = ib->host[n];
+        if (P.faceN <= 0) continue;
+        auto put = [&](const void *dst, const void *src, size_t bytes) {
+            return cudaMemcpyAsync(const_cast<void *>(dst), src, bytes, cudaMemcpyHostToDevice, st);
+        };
+        cudaError_t e = put(B.f, P.f, sizeof(int) * 3 * P.faceN);
+        if (e == cudaSuccess) e = put(B.Nf, P.Nf, sizeof(double) * 3 * P.faceN);
+        if (e == cudaSuccess) e = put(B.e, P.e, sizeof(int) * 4 * P.edgeN);
+        if (e == cudaSuccess) e = put(B.Ne, P.Ne, sizeof(double) * 3 * P.edgeN);
+        if (e == cudaSuccess) e = put(B.v, P.v, sizeof(double) * 3 * P.vertN);
+        if (e == cudaSuccess) e = put(B.Nv, P.Nv, sizeof(double) * 3 * P.vertN);
+        if (e != cudaSuccess) return cuda_status(e, "acfd_geo_upload");
+        build_tri<<<blocks_for(P.faceN, 128), 128, 0, st>>>(B.f, B.v, const_cast<double *>(B.tri), P.faceN);
+        ACFD_CUDA(cudaGetLastError());
+    }
+    ACFD_CUDA(cudaMemcpyAsync(ib->dev, ib->host.data(), sizeof(DevBody) * totN, cudaMemcpyHostToDevice, st));
+    int rc = upload_groups(ib, part, st);
+    if (rc != ACFD_OK) return rc;
+    *done = true;
+    return ACFD_OK;
+}
+
+int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, const acfd_partition_t &part, cudaStream_t st,
+              bool *relayout)
+{
+    *relayout = true;
+    if (totN > 0) {
+        bool done = false;
+        const int rc = update_in_place(ib, poly, totN, part, st, &done);
+        if (rc != ACFD_OK) return rc;
+        if (done) {
+            *relayout = false;
+            return ACFD_OK;
+        }
+    }
     ACFD_CUDA(cudaStreamSynchronize(st));
     ib_release_geometry(ib);
     if (totN == 0) return ACFD_OK;
@@ -1143,21 +1258,7 @@ int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, const acfd_p
     for (int n = 0; n < totN; ++n) {
         const acfd_polyhedron_t &P = poly[n];
         DevBody &B = ib->host[n];
-        B.faceN = P.faceN;
-        B.edgeN = P.edgeN;
-        B.vertN = P.vertN;
-        B.state = P.state;
-        B.r = P.r;
-        B.T = P.T;
-        B.cf = P.cf;
-        B.area = P.area;
-        for (int s = 0; s < 3; ++s) {
-            B.O[s] = P.O[s];
-            B.V[s] = P.V[s];
-            B.W[s] = P.W[s];
-            B.box[s][0] = P.box[s][0];
-            B.box[s][1] = P.box[s][1];
-        }
+        body_scalars(B, P);
         B.f = nullptr; B.Nf = nullptr; B.e = nullptr; B.Ne = nullptr; B.v = nullptr; B.Nv = nullptr; B.tri = nullptr;
         if (P.faceN > 0) {
             void *f, *Nf, *e, *Ne, *v, *Nv, *tri;
@@ -1189,15 +1290,12 @@ int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, const acfd_p
         set_error("immersed boundary: %d bodies, %d ghost layers (at most %d, 127)", totN, part.gl, (1 << 24) - 1);
         return ACFD_ERR_ARG;
     }
-    long long cap = 0;
-    for (int n = 0; n < totN; ++n) {
-        int lo[3], ext[3];
-        body_box(part, ib->host[n], lo, ext);
-        cap += (long long)ext[0] * ext[1] * ext[2];
-    }
+    ib->count = totN;
     long long pin = 1;
     for (int s = 0; s < 3; ++s) pin *= std::max(0, part.ns[0][s][1] - part.ns[0][s][0]);
-    cap = std::max(1LL, std::min(cap, pin));
+    // a margin for bodies that move into larger boxes (kept in place then)
+    long long cap = ghost_need(ib, part);
+    cap = std::max(1LL, std::min(cap + cap / 4 + 64, pin));
     if (cap > INT_MAX) {
         set_error("immersed boundary: ghost list of %lld nodes", cap);
         return ACFD_ERR_ARG;
@@ -1211,8 +1309,12 @@ int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, const acfd_p
     ib->ghosts = (int4 *)gl_buf;
     ib->nghost = (int *)cnt;
     ib->ghost_cap = (int)cap;
+    ib->ngroups = (totN + 7) / 8;
+    ACFD_CUDA(cudaMalloc(&ib->groups, sizeof(BoxList) * ib->ngroups));
     ACFD_CUDA(cudaDeviceSynchronize());
-    ib->count = totN;
+    int rc = upload_groups(ib, part, st);
+    if (rc != ACFD_OK) return rc;
+    ACFD_CUDA(cudaStreamSynchronize(st));
     return ACFD_OK;
 }
 
@@ -1235,13 +1337,12 @@ int ib_treat(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partit
     const IbGrid G = make_ibgrid(g, part, m.ibmLayer);
     if (part.gl < 1) return ACFD_OK;
     ACFD_CUDA(cudaMemsetAsync(ib->nghost, 0, sizeof(int) * part.gl, st));
-    for (int n0 = 0; n0 < ib->count; n0 += 8) {
-        BoxList bl;
-        boxes_of(ib, part, n0, bl);
-        const long long total = bl.start[bl.nb];
-        if (total == 0) continue;
-        ib_list<<<blocks_for(total, 256), 256, 0, st>>>(G, bl, flags, ib->ghosts, ib->nghost, ib->ghost_cap,
-                                                        ib->status);
+    // the boxes come from device memory and the grid is fixed (grid-stride):
+    // a captured step replays correctly after the bodies moved
+    const unsigned lblocks = (unsigned)std::min<long long>(blocks_for(ib->ghost_cap, 256), 148LL * 4);
+    for (int gi = 0; gi < ib->ngroups; ++gi) {
+        ib_list<<<lblocks, 256, 0, st>>>(G, ib->groups, gi, flags, ib->ghosts, ib->nghost, ib->ghost_cap,
+                                         ib->status);
         ACFD_CUDA(cudaGetLastError());
     }
     // one warp per listed node, at most a few waves of resident warps

@@ -88,3 +88,29 @@ def test_collision_scan_skips_stationary_bodies(tmp_path):
         got = s.collision_scan()
     assert got[0] == []
     assert got[1] == ref.collision_scan()[1]
+
+
+def test_moved_bodies_update_in_place(tmp_path):
+    """A moved body list of the same bodies is written into the device
+    buffers in place (no new allocation, a captured step stays valid): the
+    node mapping and ghost values afterwards equal those of a case given the
+    moved bodies as a new list."""
+    ref = _load(tmp_path, "contact_spheres", 0)
+    part, model, node = ref.partition(), ref.model(), ref.nodes()
+    before = ref.geometry()
+    before_copy = [abi.copy_struct(g, abi.Polyhedron) for g in before]
+    ref.lib.ref_step()  # moves the bodies (the arrays behind `before` are the reference's own)
+    after = ref.geometry()
+    outs = []
+    for lists in ([before_copy, after], [after]):
+        with Solver(part, model, abi.FP64_EXACT) as s:
+            s.upload(node)
+            for geo in lists:
+                s.geo_upload(geo)
+            s.compute_geometric_field()
+            s.treat_ib(abi.TO)
+            outs.append(s.download())
+    for f in ("did", "fid", "lid", "gst"):
+        assert np.array_equal(outs[0][f], outs[1][f]), f
+    assert np.array_equal(outs[0]["U"], outs[1]["U"])
+    assert not np.array_equal(np.array([g.O[0] for g in before_copy]), np.array([g.O[0] for g in after]))
