@@ -175,9 +175,11 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
     }
     const uint8_t *__restrict__ fl = HYB ? a.flags + (long long)(pt.swap ? 2 : 1) * nn : nullptr;
     unsigned fw = 0;
+    unsigned fl_ahead = 0;  // flag of node p+2, loaded one plane ahead of its use
     if (HYB && active) {
         fw = (unsigned)fl[base + (long long)(p0 - 2) * st] | ((unsigned)fl[base + (long long)(p0 - 1) * st] << 1) |
              ((unsigned)fl[base + (long long)p0 * st] << 2);
+        fl_ahead = fl[base + (long long)(p0 + 1) * st];
     }
     Real Fl[5];
     for (int p = p0 - 1; p < p1; ++p) {
@@ -195,7 +197,8 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
         }
         bool full_w = true;
         if (HYB) {
-            if (active) fw |= (unsigned)fl[id + 2 * st] << 3;
+            fw |= fl_ahead << 3;
+            if (active) fl_ahead = fl[id + 3 * st];  // node p+3 <= p1+2, inside the march's planes
             full_w = (fw != 0u);
         }
         if (!wait_plane(qf)) return;
