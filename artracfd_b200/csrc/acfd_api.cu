@@ -29,6 +29,10 @@ void set_error(const char *fmt, ...)
 int cuda_status(cudaError_t e, const char *what)
 {
     set_error("%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+    // a failed call that leaves the context usable (an allocation that did
+    // not fit, an invalid argument) also sets the runtime's last error: clear
+    // it, or the next launch check of this thread would report it again
+    (void)cudaGetLastError();
     return (e == cudaErrorMemoryAllocation) ? ACFD_ERR_NOMEM : ACFD_ERR_CUDA;
 }
 
@@ -716,9 +720,9 @@ int acfd_init(const acfd_partition_t *part, const acfd_model_t *model, acfd_case
     if ((e = cudaMalloc(&cs->U, ubytes)) != cudaSuccess ||
         (e = cudaMalloc(&cs->flags, fbytes)) != cudaSuccess ||
         (e = cudaMalloc(&cs->d_dt, sizeof(double))) != cudaSuccess ||
-        (e = cudaMalloc(&cs->cfl_part, sizeof(double) * 3 * kCflBlocks)) != cudaSuccess ||
-        (e = cudaMalloc(&cs->cfl_out, sizeof(double) * 3)) != cudaSuccess ||
-        (e = cudaMallocHost(&cs->h_cfl, sizeof(double) * 3)) != cudaSuccess ||
+        (e = cudaMalloc(&cs->cfl_part, sizeof(double) * 4 * kCflBlocks)) != cudaSuccess ||
+        (e = cudaMalloc(&cs->cfl_out, sizeof(double) * 4)) != cudaSuccess ||
+        (e = cudaMallocHost(&cs->h_cfl, sizeof(double) * 4)) != cudaSuccess ||
         (e = cudaMalloc(&cs->dstatus, sizeof(int))) != cudaSuccess ||
         (e = cudaMalloc(&cs->bcbar, 2 * sizeof(unsigned))) != cudaSuccess) {
         st = cuda_status(e, "acfd_init allocation");
@@ -890,10 +894,15 @@ int acfd_cfl(acfd_case_t *cs, double vmax[3])
     }
     TRY(launch_cfl(cs->grid, cs->mp, cs->U, cs->flags, cs->cfl_part, cs->cfl_out, cs->stream));
     cs->launches += 2;
-    ACFD_CUDA(cudaMemcpyAsync(cs->h_cfl, cs->cfl_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, cs->stream));
+    ACFD_CUDA(cudaMemcpyAsync(cs->h_cfl, cs->cfl_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, cs->stream));
     ACFD_CUDA(cudaStreamSynchronize(cs->stream));
     for (int s = 0; s < 3; ++s) {
         vmax[s] = cs->h_cfl[s];
+    }
+    if (cs->h_cfl[3] != 0.0) {
+        set_error("acfd_cfl: a fluid node of U[TO] has a non-finite wave speed (NaN or Inf in the state); "
+                  "the maxima exclude it");
+        return ACFD_ERR_DEVICE;
     }
     TRY(check_device_status(cs));
     return ib_check(cs->ib, cs->stream);

@@ -238,7 +238,8 @@ int launch_domain_boundary_fused(const Grid &g, const ModelParams &m, const acfd
                                  const FaceBox *const *groups, const int *sizes, int ngroups, double *U,
                                  unsigned *bar, int *status, cudaStream_t st);
 
-// CFL wave-speed maximum: partials (>= kCflBlocks*3 doubles) then out[3]
+// CFL wave-speed maximum: partials (>= kCflBlocks*4 doubles) then out[4]: the
+// three maxima and the count of blocks that met a non-finite wave speed
 constexpr int kCflBlocks = 296;
 int launch_cfl(const Grid &g, const ModelParams &m, const double *U, const int *did,
                double *partials, double *out, cudaStream_t st);

@@ -239,6 +239,7 @@ __global__ void cfl_partial(Grid g, ModelParams mp, const double *U, const int *
     const int Lx = g.hi[0] - g.lo[0], Ly = g.hi[1] - g.lo[1], Lz = g.hi[2] - g.lo[2];
     const long long total = (long long)Lx * Ly * Lz;
     double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+    bool bad = false;  // a fluid node whose wave speed is not finite
     auto visit = [&](long long id) {
         if (did[id] != 0) {
             return;
@@ -247,9 +248,13 @@ __global__ void cfl_partial(Grid g, ModelParams mp, const double *U, const int *
         load5(U, g.nn, id, Uc);
         to_primitive(mp.gamma, mp.gasR, Uc, Uo);
         const double c = sqrt(mp.gamma * mp.gasR * Uo[5]);
-        m0 = vmax_of(m0, fabs(Uo[1]) + c);
-        m1 = vmax_of(m1, fabs(Uo[2]) + c);
-        m2 = vmax_of(m2, fabs(Uo[3]) + c);
+        const double v0 = fabs(Uo[1]) + c, v1 = fabs(Uo[2]) + c, v2 = fabs(Uo[3]) + c;
+        m0 = vmax_of(m0, v0);
+        m1 = vmax_of(m1, v1);
+        m2 = vmax_of(m2, v2);
+        // the maximum passes over a NaN as the reference's does; it is
+        // reported beside it (a blown-up or corrupted state)
+        bad = bad || !isfinite(v0 + v1 + v2);
     };
     if (total < (long long)INT32_MAX / 2 && g.nn < (long long)INT32_MAX) {
         // 32-bit work indices: 64-bit divisions would cost more than the loads
@@ -282,13 +287,16 @@ __global__ void cfl_partial(Grid g, ModelParams mp, const double *U, const int *
         sm[1][warp] = m1;
         sm[2][warp] = m2;
     }
-    __syncthreads();
+    const int any_bad = __syncthreads_or(bad);
     if (threadIdx.x < 3) {
         double m = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
             m = vmax_of(m, sm[threadIdx.x][w]);
         }
         part[3 * blockIdx.x + threadIdx.x] = m;
+    }
+    if (threadIdx.x == 3) {
+        part[3 * gridDim.x + blockIdx.x] = any_bad ? 1.0 : 0.0;
     }
 }
 
@@ -300,11 +308,20 @@ __global__ void cfl_final(const double *part, int nblocks, double *out)
     pdl_wait();
     const int lane = threadIdx.x & 31;
     double m[3] = {0.0, 0.0, 0.0};
+    double nbad = 0.0;
     for (int b = lane; b < nblocks; b += 32) {
 #pragma unroll
         for (int s = 0; s < 3; ++s) {
             m[s] = vmax_of(m[s], part[3 * b + s]);
         }
+        nbad += part[3 * nblocks + b];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        nbad += __shfl_xor_sync(0xffffffffu, nbad, o);
+    }
+    if (lane == 0) {
+        out[3] = nbad;  // blocks that met a fluid node with a non-finite wave speed
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
