@@ -204,7 +204,10 @@ int acfd_device_state(acfd_case_t *cs, double **U, int **flags, int *pitch, size
 
 /* Fluid part of ComputeTimeStep (solve.c:132-151): per-direction maximum of
  * |u_s| + c over PIN nodes with did == 0 of U[TO].  The body-speed part and
- * dt = CFL * min(d/Vmax) stay with the caller. */
+ * dt = CFL * min(d/Vmax) stay with the caller.  A fluid node with a
+ * non-finite wave speed (NaN or Inf in the state) is passed over by the
+ * maxima, as in the reference, and reported: vmax is written and the call
+ * returns ACFD_ERR_DEVICE. */
 int acfd_cfl(acfd_case_t *cs, double vmax[3]);
 /* The same maximum for callers that must not allocate device memory (hosts
  * whose device memory belongs to a pool allocator, or whose memory budget is
