@@ -7,6 +7,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include <cudaTypedefs.h>
@@ -631,6 +634,123 @@ int check_case(const acfd_case *cs)
     return ACFD_OK;
 }
 
+// ---- host <-> device copies of the node array --------------------------
+// The node array of a caller is pageable memory; the runtime copies such
+// memory through its own small pinned buffers at a fraction of PCIe speed.
+// Instead the array goes through two pinned bounce chunks, filled and
+// drained by several host threads while the other chunk is in flight.  The
+// chunks are shared by every case of the process (one copy at a time).
+constexpr size_t kPinChunk = (size_t)32 << 20;
+
+struct PinnedBounce {
+    std::mutex lock;
+    unsigned char *buf = nullptr;  // 2 x kPinChunk, pinned and portable
+};
+
+// completion events of the two chunks, on the calling thread's device
+struct ChunkEvents {
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    cudaError_t create()
+    {
+        cudaError_t e = cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming);
+        return e;
+    }
+    ~ChunkEvents()
+    {
+        for (int q = 0; q < 2; ++q) {
+            if (done[q]) {
+                cudaEventSynchronize(done[q]);
+                cudaEventDestroy(done[q]);
+            }
+        }
+    }
+};
+
+PinnedBounce &bounce()
+{
+    static PinnedBounce b;
+    return b;
+}
+
+void parallel_memcpy(void *dst, const void *src, size_t bytes)
+{
+    const size_t kPart = (size_t)4 << 20;
+    unsigned T = std::thread::hardware_concurrency();
+    T = std::min<unsigned>(T == 0 ? 1u : T, 8u);
+    T = (unsigned)std::min<size_t>(T, bytes / kPart);
+    if (T < 2) {
+        memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t part = ((bytes + T - 1) / T + 63) & ~(size_t)63;
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < T; ++t) {
+        const size_t off = t * part;
+        if (off >= bytes) break;
+        const size_t len = std::min(part, bytes - off);
+        pool.emplace_back([=] { memcpy((char *)dst + off, (const char *)src + off, len); });
+    }
+    memcpy(dst, src, std::min(part, bytes));
+    for (auto &th : pool) th.join();
+}
+
+int ensure_bounce(PinnedBounce &b)
+{
+    if (b.buf) return ACFD_OK;
+    ACFD_CUDA(cudaHostAlloc(&b.buf, 2 * kPinChunk, cudaHostAllocPortable));
+    return ACFD_OK;
+}
+
+// host array -> device buffer, on the case's stream (returns with the copies
+// queued; the bounce chunks are free again when the stream reaches them)
+int upload_host(acfd_case *cs, void *dev, const void *host, size_t bytes)
+{
+    PinnedBounce &b = bounce();
+    std::lock_guard<std::mutex> guard(b.lock);
+    TRY(ensure_bounce(b));
+    ChunkEvents ev;
+    ACFD_CUDA(ev.create());
+    int c = 0;
+    for (size_t off = 0; off < bytes; off += kPinChunk, ++c) {
+        const size_t len = std::min(kPinChunk, bytes - off);
+        unsigned char *slot = b.buf + (size_t)(c & 1) * kPinChunk;
+        ACFD_CUDA(cudaEventSynchronize(ev.done[c & 1]));  // the copy that last read this chunk
+        parallel_memcpy(slot, (const char *)host + off, len);
+        ACFD_CUDA(cudaMemcpyAsync((char *)dev + off, slot, len, cudaMemcpyHostToDevice, cs->stream));
+        ACFD_CUDA(cudaEventRecord(ev.done[c & 1], cs->stream));
+    }
+    // the chunks must not be refilled by another case before these copies
+    // ran: the events are waited for when they go out of scope, under the lock
+    return ACFD_OK;
+}
+
+// device buffer -> host array (waits for the case's stream)
+int download_host(acfd_case *cs, void *host, const void *dev, size_t bytes)
+{
+    PinnedBounce &b = bounce();
+    std::lock_guard<std::mutex> guard(b.lock);
+    TRY(ensure_bounce(b));
+    ChunkEvents ev;
+    ACFD_CUDA(ev.create());
+    const size_t n = (bytes + kPinChunk - 1) / kPinChunk;
+    auto issue = [&](size_t c) -> int {
+        const size_t off = c * kPinChunk, len = std::min(kPinChunk, bytes - off);
+        ACFD_CUDA(cudaMemcpyAsync(b.buf + (c & 1) * kPinChunk, (const char *)dev + off, len,
+                                  cudaMemcpyDeviceToHost, cs->stream));
+        ACFD_CUDA(cudaEventRecord(ev.done[c & 1], cs->stream));
+        return ACFD_OK;
+    };
+    for (size_t c = 0; c < n && c < 2; ++c) TRY(issue(c));
+    for (size_t c = 0; c < n; ++c) {
+        ACFD_CUDA(cudaEventSynchronize(ev.done[c & 1]));
+        const size_t off = c * kPinChunk, len = std::min(kPinChunk, bytes - off);
+        parallel_memcpy((char *)host + off, b.buf + (c & 1) * kPinChunk, len);
+        if (c + 2 < n) TRY(issue(c + 2));
+    }
+    return ACFD_OK;
+}
+
 int ensure_staging(acfd_case *cs)
 {
     if (cs->staging) {
@@ -848,7 +968,7 @@ int acfd_sync_to_device(acfd_case_t *cs, const acfd_node_t *node, unsigned mask)
     }
     TRY(ensure_staging(cs));
     const size_t total = (size_t)cs->grid.n[0] * cs->grid.n[1] * cs->grid.n[2];
-    ACFD_CUDA(cudaMemcpyAsync(cs->staging, node, total * sizeof(acfd_node_t), cudaMemcpyHostToDevice, cs->stream));
+    TRY(upload_host(cs, cs->staging, node, total * sizeof(acfd_node_t)));
     TRY(launch_scatter_nodes(cs->grid, cs->staging, cs->U, cs->flags, mask, cs->stream));
     ACFD_CUDA(cudaStreamSynchronize(cs->stream));
     return ACFD_OK;
@@ -865,11 +985,10 @@ int acfd_sync_to_host(acfd_case_t *cs, acfd_node_t *node, unsigned mask)
     const size_t total = (size_t)cs->grid.n[0] * cs->grid.n[1] * cs->grid.n[2];
     // keep host members that are not selected: start from the host copy
     if ((mask & ACFD_SYNC_ALL) != ACFD_SYNC_ALL) {
-        ACFD_CUDA(cudaMemcpyAsync(cs->staging, node, total * sizeof(acfd_node_t), cudaMemcpyHostToDevice,
-                                  cs->stream));
+        TRY(upload_host(cs, cs->staging, node, total * sizeof(acfd_node_t)));
     }
     TRY(launch_gather_nodes(cs->grid, cs->U, cs->flags, cs->staging, mask, cs->stream));
-    ACFD_CUDA(cudaMemcpyAsync(node, cs->staging, total * sizeof(acfd_node_t), cudaMemcpyDeviceToHost, cs->stream));
+    TRY(download_host(cs, node, cs->staging, total * sizeof(acfd_node_t)));
     ACFD_CUDA(cudaStreamSynchronize(cs->stream));
     TRY(check_device_status(cs));
     return ib_check(cs->ib, cs->stream);
