@@ -575,11 +575,23 @@ def run_batch(args, rank, world, local_rank):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    procs = os.cpu_count() or 1
-    procs = max(1, min(procs, args.ref_procs))
+    # every host thread this process may use (one reference process each; the
+    # reference is serial), at most one process per GB of available memory
+    # (a TGV 128^3 reference process holds ~0.5 GB); --ref-procs caps it
+    procs = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    try:
+        import psutil
+        procs = min(procs, max(1, int(psutil.virtual_memory().available // (1 << 30))))
+    except Exception:
+        pass
+    if args.ref_procs > 0:
+        procs = min(procs, args.ref_procs)
+    procs = max(1, procs)
     t0 = time.perf_counter()
     rates = []
-    rate, det = cpu_baseline_reference(args.n, steps=max(1, args.steps), procs=procs)
+    # a bounded sample: two reference time steps per process whatever --steps
+    # (one step of TGV 128^3 takes ~15 s on one core)
+    rate, det = cpu_baseline_reference(args.n, steps=max(1, min(args.steps, 2)), procs=procs)
     if rate is None:
         print(json.dumps({"impl": "reference", "unavailable": "reference harness oracle/_ref not built"}))
         return
@@ -608,7 +620,7 @@ def main():
     ap.add_argument("--accuracy-steps", type=int, default=200)
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ref-procs", type=int, default=16)
+    ap.add_argument("--ref-procs", type=int, default=0, help="reference processes (0: every usable host thread)")
     ap.add_argument("--workload", default="tgv", choices=["tgv", "batch"],
                     help="tgv: the headline line (TGV 128^3); batch: the 48-case batched sweep")
     ap.add_argument("--batch-cases", type=int, default=48)
