@@ -240,7 +240,7 @@ int launch_domain_boundary_fused(const Grid &g, const ModelParams &m, const acfd
 
 // CFL wave-speed maximum: partials (>= kCflBlocks*4 doubles) then out[4]: the
 // three maxima and the count of blocks that met a non-finite wave speed
-constexpr int kCflBlocks = 296;
+constexpr int kCflBlocks = 1184;  // 148 SMs x 8 blocks of 256 threads: enough warps to hide the loads
 int launch_cfl(const Grid &g, const ModelParams &m, const double *U, const int *did,
                double *partials, double *out, cudaStream_t st);
 
