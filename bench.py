@@ -125,10 +125,14 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def fp64_peak_tflops(torch):
-    """Measured FP64 reference: cuBLAS DGEMM 8192^3, best of 5."""
-    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
-    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+def fp64_peak_tflops(torch, dtype=None):
+    """Measured FP64 (or FP32) reference: cuBLAS DGEMM (SGEMM without TF32)
+    8192^3, best of 5."""
+    dtype = dtype or torch.float64
+    tf32 = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    a = torch.randn(8192, 8192, dtype=dtype, device="cuda")
+    b = torch.randn(8192, 8192, dtype=dtype, device="cuda")
     torch.matmul(a, b)
     torch.cuda.synchronize()
     best = 1e9
@@ -140,6 +144,7 @@ def fp64_peak_tflops(torch):
         e1.synchronize()
         best = min(best, e0.elapsed_time(e1) / 1e3)
     del a, b
+    torch.backends.cuda.matmul.allow_tf32 = tf32
     return 2.0 * 8192 ** 3 / best / 1e12
 
 
@@ -400,6 +405,7 @@ def run_ours(args, rank, world, local_rank):
     traffic = tr2 * (dom_bytes / (STAGE_BYTES[1] * nodes_pin)) if tr2 else None
     flop_rate = FLOP_PER_NODE_STAGE_VISCOUS * nodes_pin / (stage_mean / 1e3) / 1e12
     fp64_peak = fp64_peak_tflops(torch) if rank == 0 else None
+    fp32_peak = fp64_peak_tflops(torch, torch.float32) if rank == 0 and args.mode in ("fp32", "hybrid") else None
     # e2e through the C ABI with host buffers: upload of the host node array,
     # K steps (CFL read back each step), download of the result
     host = node.copy()
@@ -455,7 +461,13 @@ def run_ours(args, rank, world, local_rank):
                               "frac": (flop_rate / fp64_peak) if fp64_peak else None,
                               "peak_kind": "measured cuBLAS DGEMM 8192^3 in this run",
                               "flop_per_node_stage": FLOP_PER_NODE_STAGE_VISCOUS,
-                              "note": "reference FP64 flop count; meaningful as a fraction for the FP64 forms"}},
+                              "note": "reference FP64 flop count; meaningful as a fraction for the FP64 forms"},
+                     "fp32": ({"achieved_tflops": flop_rate, "peak_tflops": fp32_peak,
+                               "frac": (flop_rate / fp32_peak) if fp32_peak else None,
+                               "peak_kind": "measured cuBLAS SGEMM 8192^3 (no TF32) in this run",
+                               "note": "the reference's flop count of the same stages over the FP32 form's stage time "
+                                       "(reference-equivalent work: the hybrid computes fewer flops on smooth "
+                                       "interfaces)"} if fp32_peak else None)},
         "stage_ms": {"sweep_mean": stage_mean, "ghost_fill_mean": bc_mean},
         "clocks": clocks,
         "e2e": {"value": job_rate(world, nodes_pin, args.steps, e2e_sec), "unit": UNIT,
