@@ -32,7 +32,9 @@ FP64_EXACT, FP64, FP32_BULK, FP32_HYBRID = 0, 1, 2, 3
 # stage-kernel variants (acfd_set_tiles): bricks below BRICK_VARIANTS, then
 # the line-march kernels with 1, 2, 4 waves, then from PLANE_VARIANT the
 # plane-march kernels (Y/Z sweeps) with 1, 2, 4 waves
-BRICK_VARIANTS, PLANE_VARIANT, STAGE_VARIANTS = 2, 5, 8
+BRICK_VARIANTS, PLANE_VARIANT, STAGE_VARIANTS = 2, 5, 11
+# the plane march with equal shares of all tiles' planes per block (Y/Z)
+PLANE_SHARE_VARIANT = PLANE_VARIANT + 3
 # stage kernel of a batch (acfd_batch_set_kernel)
 BATCH_BRICK, BATCH_PLANE = 0, 1
 # sync masks

@@ -88,11 +88,13 @@ bool pdl_enabled()
 
 // Stage-kernel variants: the brick tile shapes (0 .. kTileVariants-1), the
 // line-march kernels and the plane-march kernels, each launched with 1, 2 or
-// 4 waves
+// 4 waves; the plane march twice: lines cut into equal segments per tile,
+// then (Y and Z sweeps) equal shares of all tiles' planes per block
 constexpr int kMarchVariants = 3;
 constexpr int kMarchWaves[kMarchVariants] = {1, 2, 4};
-constexpr int kPlaneVariants = 3;
-constexpr int kPlaneWaves[kPlaneVariants] = {1, 2, 4};
+constexpr int kPlaneVariants = 6;
+constexpr int kPlaneWaves[kPlaneVariants] = {1, 2, 4, 1, 2, 4};
+constexpr bool kPlaneShare[kPlaneVariants] = {false, false, false, true, true, true};
 constexpr int kPlaneFirst = kTileVariants + kMarchVariants;
 constexpr int kStageVariants = kPlaneFirst + kPlaneVariants;
 static_assert(ACFD_BRICK_VARIANTS == kTileVariants && ACFD_STAGE_VARIANTS == kStageVariants &&
@@ -507,7 +509,7 @@ int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int 
         const int target32 = waves * cs->sms * 16, target64 = waves * cs->sms * 8;
         PlaneTile pt = {};
         if (plane) {
-            pt = plane_tile(cs->grid, s, visc, waves, cs->sms);
+            pt = plane_tile(cs->grid, s, visc, waves, cs->sms, kPlaneShare[var - kPlaneFirst]);
             if (pt.BXp != cs->pbox[s][0] || pt.BC != cs->pbox[s][1]) {
                 set_error("plane tile (%d x %d) does not match the encoded box (%d x %d) of axis %d", pt.BXp, pt.BC,
                           cs->pbox[s][0], cs->pbox[s][1], s);
@@ -1848,7 +1850,7 @@ int acfd_batch_init(int ncase, const acfd_partition_t *parts, const acfd_model_t
                     b->plane_ok = false;
                 }
                 hpm[(size_t)c * 3 + s] = cs->pmaps[s];
-                const long long nb = (long long)P.pt.ntx * P.pt.ntc * P.pt.nseg;
+                const long long nb = P.pt.nblk;
                 pprefix[(size_t)s * (ncase + 1) + c + 1] = pprefix[(size_t)s * (ncase + 1) + c] + nb;
                 b->pthreads[s] = std::max(b->pthreads[s], (P.pt.ncw + 1) * 32);
                 b->psmem[s] = std::max(b->psmem[s], plane_smem_bytes(P.pt, s));

@@ -114,7 +114,9 @@ struct PlaneTile {
     int WX, NR;    // tile: nodes updated along x and rows of the row axis
     int TR;        // consumer threads per row (WX; WX + 1 interfaces on X sweeps)
     int ntx, ntc;  // tiles along x and along the rows
-    int nseg;      // segments along the march axis
+    int nseg;      // X kernel: segments along the march axis
+    int nblk;      // blocks of a launch: tiles x segments, or (Y/Z, share) equal shares of all tiles' planes
+    int share;     // Y/Z kernel: 1 = a block marches an equal share of the tiles' planes
     int BXp, BC;   // plane box: x extent (even, covers the x halo) and rows with halo
     int ncw;       // consumer warps (the producer is warp ncw)
     int swap;      // Y/Z kernel: 1 = a Z sweep run with axes 1 and 2 exchanged
@@ -125,7 +127,7 @@ struct PlaneTile {
 // with rows along the other transverse axis; X sweeps march along y with rows
 // along z and an x halo of three nodes (the WENO5 stencil).  `waves` scales
 // the number of blocks (segments of the march axis, each at least 8 planes).
-inline PlaneTile plane_tile(const Grid &g, int s, bool visc, int waves, int sms)
+inline PlaneTile plane_tile(const Grid &g, int s, bool visc, int waves, int sms, bool share = false)
 {
     PlaneTile pt = {};
     const int T2 = (s == 1) ? 2 : (s == 2 ? 1 : 2);  // row axis
@@ -156,6 +158,15 @@ inline PlaneTile plane_tile(const Grid &g, int s, bool visc, int waves, int sms)
     if (nseg > cap) nseg = cap;
     if (nseg < 1) nseg = 1;
     pt.nseg = (int)nseg;
+    pt.share = (share && s != 0) ? 1 : 0;
+    if (!pt.share) {
+        pt.nblk = (int)(tiles * nseg);
+    } else {
+        // every block the same number of planes (at least 8): no partial
+        // last wave, one fill of the ring per item
+        long long nb = std::min<long long>(target, tiles * Ls / 8);
+        pt.nblk = (int)std::max<long long>(1, nb);
+    }
     return pt;
 }
 

@@ -39,7 +39,7 @@ constexpr long long kPlaneWaitLimit = 1LL << 22;
 // (blk) so that the batched kernel runs the same code for a block of any case;
 // warps beyond the case's producer warp (a batch launch sized for its largest
 // tile) leave after the barrier set-up.
-template <int NP, bool VISC, bool HYB>
+template <int NP, bool VISC, bool HYB, bool SHARE = false>
 __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams &mp, const StageArgs &a,
                                                const PlaneTile &pt, const CUtensorMap *mapp, int blk,
                                                unsigned char *smem)
@@ -69,47 +69,84 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
         return;
     }
 
-    int b = blk;
-    const int tx = b % pt.ntx;
-    b /= pt.ntx;
-    const int tc = b % pt.ntc;
-    const int seg = b / pt.ntc;
+    // With shares (pt.share) a block marches planes [r0, r1) of the
+    // tile-major list of all tiles' lines (tile T holds planes T*Ls ..
+    // T*Ls+Ls-1): every block of the launch gets the same number of planes;
+    // a share that crosses a tile boundary is two items, marched one after
+    // the other through the same ring (the plane sequence q runs on).
+    // Without shares (pt.share == 0) a block marches segment seg of one tile.
     const int Ls = g.hi[S] - g.lo[S];
-    const int x0 = g.lo[0] + tx * pt.WX;
-    const int c0 = g.lo[T2] + tc * pt.NR;
-    const int p0 = g.lo[S] + (int)((long long)seg * Ls / pt.nseg);
-    const int p1 = g.lo[S] + (int)((long long)(seg + 1) * Ls / pt.nseg);
-    const int xs = (x0 - hv) & ~1;
-    const int cs = c0 - hv;
-    const int NQ = p1 - p0 + 2 * H;  // planes p0-H .. p1+H-1
+    const long long tiles = (long long)pt.ntx * pt.ntc;
+    const long long work = tiles * Ls;
+    long long r0 = 0, r1 = 0, T0, T1;
+    int seg = 0;
+    if constexpr (SHARE) {
+        r0 = (long long)blk * work / pt.nblk;
+        r1 = (long long)(blk + 1) * work / pt.nblk;
+        if (r1 <= r0) return;
+        T0 = r0 / Ls;
+        T1 = (r1 - 1) / Ls;
+    } else {
+        T0 = blk % tiles;
+        T1 = T0;
+        seg = (int)(blk / tiles);
+    }
+    // item T: its tile origin and its planes [p0, p1) along s
+    auto item = [&](long long T, int &x0, int &c0, int &p0, int &p1) {
+        x0 = g.lo[0] + (int)(T % pt.ntx) * pt.WX;
+        c0 = g.lo[T2] + (int)(T / pt.ntx) * pt.NR;
+        if constexpr (SHARE) {
+            const long long a0 = T * Ls, a1 = (T + 1) * Ls;
+            p0 = g.lo[S] + (int)((r0 > a0 ? r0 : a0) - a0);
+            p1 = g.lo[S] + (int)((r1 < a1 ? r1 : a1) - a0);
+        } else {
+            p0 = g.lo[S] + (int)((long long)seg * Ls / pt.nseg);
+            p1 = g.lo[S] + (int)((long long)(seg + 1) * Ls / pt.nseg);
+        }
+    };
 
     if (warp == pt.ncw) {
-        // producer: plane q (node p0-H+q along s) into slot q % NS
+        // producer: plane q of the block's sequence into slot q % NS
         if (lane == 0) {
-            int issued = 0;
-            for (int q = 0; q < NQ; ++q) {
-                const int slot = q % NS;
-                if (q >= NS && !tma::mbar_wait_bounded(empty + slot, ((q / NS) - 1) & 1, a.status, 5,
-                                                       kPlaneWaitLimit)) {
-                    break;
+            int q = 0, issued = 0;
+            bool ok = true;
+            for (long long T = T0; T <= T1 && ok; ++T) {
+                int x0, c0, p0, p1;
+                item(T, x0, c0, p0, p1);
+                const int xs = (x0 - hv) & ~1, cs = c0 - hv;
+                const int NQ = p1 - p0 + 2 * H;  // planes p0-H .. p1+H-1
+                for (int ql = 0; ql < NQ; ++ql, ++q) {
+                    const int slot = q % NS;
+                    if (q >= NS && !tma::mbar_wait_bounded(empty + slot, ((q / NS) - 1) & 1, a.status, 5,
+                                                           kPlaneWaitLimit)) {
+                        ok = false;
+                        break;
+                    }
+                    tma::mbar_expect_tx(full + slot, plane_bytes);
+                    const int pos = p0 - H + ql;
+                    double *dst = ring + (size_t)slot * slot_doubles;
+                    if (!pt.swap) {
+                        tma::load_5d(dst, mapp, xs, pos, cs, 0, a.tn, full + slot);
+                    } else {
+                        tma::load_5d(dst, mapp, xs, cs, pos, 0, a.tn, full + slot);
+                    }
+                    issued = q + 1;
                 }
-                tma::mbar_expect_tx(full + slot, plane_bytes);
-                const int pos = p0 - H + q;
-                double *dst = ring + (size_t)slot * slot_doubles;
-                if (!pt.swap) {
-                    tma::load_5d(dst, mapp, xs, pos, cs, 0, a.tn, full + slot);
-                } else {
-                    tma::load_5d(dst, mapp, xs, cs, pos, 0, a.tn, full + slot);
-                }
-                issued = q + 1;
             }
             // the block must not end with copies in flight
-            for (int q = issued - NS > 0 ? issued - NS : 0; q < issued; ++q) {
-                tma::mbar_wait_bounded(full + q % NS, (q / NS) & 1, a.status, 5, kPlaneWaitLimit);
+            for (int qq = issued - NS > 0 ? issued - NS : 0; qq < issued; ++qq) {
+                tma::mbar_wait_bounded(full + qq % NS, (qq / NS) & 1, a.status, 5, kPlaneWaitLimit);
             }
         }
         return;
     }
+
+    int qbase = 0;  // first plane of the item in the block's sequence
+    for (long long T = T0; T <= T1; ++T) {
+    int x0, c0, p0, p1;
+    item(T, x0, c0, p0, p1);
+    const int xs = (x0 - hv) & ~1;
+    const int NQ = p1 - p0 + 2 * H;
 
     // consumer thread: line (i, c)
     const int t = threadIdx.x;
@@ -128,14 +165,16 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
     const Real cvinv = Real(1.0 / mp.cv);
     const bool same_o = (a.Uo == a.Un);
     const double rdt = (a.dt_scale * a.dt[0]) * g.dd[S];
-    auto plane = [&](int q) { return ring + (size_t)(q % NS) * slot_doubles; };
+    // plane q of the item is plane qbase + q of the block's sequence
+    auto plane = [&](int q) { return ring + (size_t)((qbase + q) % NS) * slot_doubles; };
     auto wait_plane = [&](int q) {
-        const bool ok = tma::mbar_wait_bounded(full + q % NS, (q / NS) & 1, a.status, 5, kPlaneWaitLimit);
+        const int qq = qbase + q;
+        const bool ok = tma::mbar_wait_bounded(full + qq % NS, (qq / NS) & 1, a.status, 5, kPlaneWaitLimit);
         return __all_sync(kAll, ok);
     };
     auto release = [&](int q) {
         __syncwarp();
-        if (lane == 0) tma::mbar_arrive(empty + q % NS);
+        if (lane == 0) tma::mbar_arrive(empty + (qbase + q) % NS);
     };
     auto node_of_plane = [&](const double *P, Real w[5]) {
 #pragma unroll
@@ -248,14 +287,23 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
         }
         fw >>= 1;
     }
+    if constexpr (SHARE) {
+        // planes p1 .. p1+H-1 were read for the last time: free their slots
+        // for the next item's planes
+        for (int q = NQ - H; q < NQ; ++q) {
+            release(q);
+        }
+    }
+    qbase += NQ;
+    }
 }
 
-template <int NP, bool VISC, bool HYB>
+template <int NP, bool VISC, bool HYB, bool SHARE>
 __global__ void __launch_bounds__(kPlaneMaxThreads, sizeof(Real) == sizeof(float) ? 2 : 1)
 stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_constant__ CUtensorMap map)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    plane_yz_block<NP, VISC, HYB>(g, mp, a, pt, &map, (int)blockIdx.x, smem);
+    plane_yz_block<NP, VISC, HYB, SHARE>(g, mp, a, pt, &map, (int)blockIdx.x, smem);
 }
 
 // ---------------------------------------------------------------------------
@@ -490,13 +538,13 @@ static int launch_plane_x(const Grid &g, const ModelParams &m, const StageArgs &
         set_error("plane tile needs %d bytes of shared memory", smem);
         return ACFD_ERR_ARG;
     }
-    const unsigned blocks = (unsigned)pt.ntx * pt.ntc * pt.nseg;
+    const unsigned blocks = (unsigned)pt.nblk;
     cudaError_t e = launch_k(stage_plane_x<NP, VISC, HYB>, dim3(blocks), dim3((pt.ncw + 1) * 32), smem, st, g, m, a,
                              pt, map);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "stage_plane_x launch");
 }
 
-template <int NP, bool VISC, bool HYB>
+template <int NP, bool VISC, bool HYB, bool SHARE>
 static int launch_plane_yz(const Grid &g, const ModelParams &m, const StageArgs &a, int s, const PlaneTile &pt0,
                            const CUtensorMap &map, cudaStream_t st)
 {
@@ -505,7 +553,7 @@ static int launch_plane_yz(const Grid &g, const ModelParams &m, const StageArgs 
     cudaGetDevice(&dev);
     const int smem = plane_smem_bytes(pt0, s);
     if (dev >= 0 && dev < 64 && !configured[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(stage_plane_yz<NP, VISC, HYB>,
+        cudaError_t e = cudaFuncSetAttribute(stage_plane_yz<NP, VISC, HYB, SHARE>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, kPlaneSmemMax);
         if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(stage_plane_yz)");
         configured[dev] = true;
@@ -531,9 +579,9 @@ static int launch_plane_yz(const Grid &g, const ModelParams &m, const StageArgs 
         std::swap(gk.hi[1], gk.hi[2]);
         std::swap(gk.dd[1], gk.dd[2]);
     }
-    const unsigned blocks = (unsigned)pt.ntx * pt.ntc * pt.nseg;
-    cudaError_t e = launch_k(stage_plane_yz<NP, VISC, HYB>, dim3(blocks), dim3((pt.ncw + 1) * 32), smem, st, gk, m, a,
-                             pt, map);
+    const unsigned blocks = (unsigned)pt.nblk;
+    cudaError_t e = launch_k(stage_plane_yz<NP, VISC, HYB, SHARE>, dim3(blocks), dim3((pt.ncw + 1) * 32), smem, st, gk,
+                             m, a, pt, map);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "stage_plane_yz launch");
 }
 
@@ -542,7 +590,8 @@ static int launch_plane_s(const Grid &g, const ModelParams &m, const StageArgs &
                           const CUtensorMap &map, cudaStream_t st)
 {
     if (s == 0) return launch_plane_x<NP, VISC, HYB>(g, m, a, pt, map, st);
-    return launch_plane_yz<NP, VISC, HYB>(g, m, a, s, pt, map, st);
+    return pt.share ? launch_plane_yz<NP, VISC, HYB, true>(g, m, a, s, pt, map, st)
+                    : launch_plane_yz<NP, VISC, HYB, false>(g, m, a, s, pt, map, st);
 }
 
 // `map` is the state map with box (BXp, 1, BC) (X and Y sweeps) or

@@ -212,6 +212,14 @@ def job_rate(world: int, nodes_per_rank: int, steps: int, seconds: float) -> flo
     return world * nodes_per_rank * steps / seconds / 1e6
 
 
+def _tune(s, spec, steps=3):
+    """The stage-kernel variants timed on the state after a few steps (the
+    sensor flags of the initial field are not those of the timed steps)."""
+    for _ in range(steps):
+        s.evolve(s.time_step(spec.cfl))
+    return s.autotune()
+
+
 def _solver(part, model, form, stream):
     from artracfd_b200 import abi
     from artracfd_b200.solver import Solver
@@ -361,7 +369,7 @@ def run_ours(args, rank, world, local_rank):
         s = _solver(part, model, "fp64", stream)
         s.upload(node)
         s.treat_boundary(abi.TO)
-        tiles64 = s.autotune()
+        tiles64 = _tune(s, spec)
         sec64, _, clk64 = _timed_steps(torch, s, spec, args.steps, args.warmup, dist, stream, local_rank)
         st64, bc64, by64 = _stage_profile(torch, s, spec, nodes_pin, stream)
         s.close()
@@ -373,7 +381,7 @@ def run_ours(args, rank, world, local_rank):
     s = _solver(part, model, args.mode, stream)
     s.upload(node)
     s.treat_boundary(abi.TO)
-    tiles = s.autotune()
+    tiles = _tune(s, spec)
     sensor_info = None
     if args.mode == "hybrid":
         flagged = s.sensor_update()

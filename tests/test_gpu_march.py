@@ -29,7 +29,8 @@ CASES = golden_io.names()
 BRICK = [0, 0, 0]
 MARCH = [abi.BRICK_VARIANTS] * 3
 PLANE = [abi.PLANE_VARIANT] * 3
-FAMILIES = {"march": MARCH, "plane": PLANE}
+SHARE = [abi.PLANE_VARIANT, abi.PLANE_SHARE_VARIANT, abi.PLANE_SHARE_VARIANT]
+FAMILIES = {"march": MARCH, "plane": PLANE, "share": SHARE}
 # FP32 stencil arithmetic in two operation orders, after two steps (relative
 # to the magnitude of each conservative variable)
 TOL_FP32_ORDER = 2e-5
@@ -121,8 +122,11 @@ def test_march_launch_size_does_not_change_results(mode, family):
     dts = [b.dt[0]] * 2
     first = FAMILIES[family][0]
     ref = run(b, mode, [first] * 3, 2, dts=dts)[-1]
-    for v in (first + 1, first + 2):
-        got = run(b, mode, [v] * 3, 2, dts=dts)[-1]
+    others = [first + 1, first + 2]
+    if family == "plane":  # the same kernel with equal shares of planes per block
+        others += [abi.PLANE_SHARE_VARIANT + q for q in range(3)]
+    for v in others:
+        got = run(b, mode, [first, v, v] if v >= abi.PLANE_SHARE_VARIANT else [v] * 3, 2, dts=dts)[-1]
         assert np.array_equal(got, ref), v
 
 
