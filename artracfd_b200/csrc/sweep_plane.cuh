@@ -143,158 +143,158 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
 
     int qbase = 0;  // first plane of the item in the block's sequence
     for (long long T = T0; T <= T1; ++T) {
-    int x0, c0, p0, p1;
-    item(T, x0, c0, p0, p1);
-    const int xs = (x0 - hv) & ~1;
-    const int NQ = p1 - p0 + 2 * H;
+        int x0, c0, p0, p1;
+        item(T, x0, c0, p0, p1);
+        const int xs = (x0 - hv) & ~1;
+        const int NQ = p1 - p0 + 2 * H;
 
-    // consumer thread: line (i, c)
-    const int t = threadIdx.x;
-    const int xl = t % pt.WX, rl = t / pt.WX;
-    const int i = x0 + xl, c = c0 + rl;
-    const bool active = (rl < pt.NR) && (i < g.hi[0]) && (c < g.hi[T2]);
-    // element of (i, c) in a plane (inactive threads: the tile's first node,
-    // whose halo neighbours exist)
-    const int e0 = active ? (rl + hv) * pt.BXp + (i - xs) : hv * pt.BXp + (x0 - xs);
-    const long long nn = g.nn;
-    const long long st = pt.st;                      // node stride along the line
-    const long long base = (long long)c * pt.rs + i;  // node (i, c) at position 0
-    // variable v of the kernel's frame is variable vg(v) of the state
-    const int o2 = pt.swap ? 3 : 2, o3 = pt.swap ? 2 : 3;
-    auto vg = [&](int v) { return v == 2 ? o2 : (v == 3 ? o3 : v); };
-    const Real cvinv = Real(1.0 / mp.cv);
-    const bool same_o = (a.Uo == a.Un);
-    const double rdt = (a.dt_scale * a.dt[0]) * g.dd[S];
-    // plane q of the item is plane qbase + q of the block's sequence
-    auto plane = [&](int q) { return ring + (size_t)((qbase + q) % NS) * slot_doubles; };
-    auto wait_plane = [&](int q) {
-        const int qq = qbase + q;
-        const bool ok = tma::mbar_wait_bounded(full + qq % NS, (qq / NS) & 1, a.status, 5, kPlaneWaitLimit);
-        return __all_sync(kAll, ok);
-    };
-    auto release = [&](int q) {
-        __syncwarp();
-        if (lane == 0) tma::mbar_arrive(empty + (qbase + q) % NS);
-    };
-    auto node_of_plane = [&](const double *P, Real w[5]) {
-#pragma unroll
-        for (int v = 0; v < 5; ++v) w[v] = Real(P[vg(v) * pe + e0]);
-    };
-    // transverse differences at the plane's node from its halo neighbours:
-    // axis 0 (x, element stride 1) and axis T2 (rows, element stride BXp)
-    auto tdiff = [&](const double *P, Real (&D)[2][2]) {
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int tax = q == 0 ? 0 : T2;
-            const int es = q == 0 ? 1 : pt.BXp;
-            const int ep = e0 + es, em = e0 - es;
-            const Real rp = fast::rcp<Real>(Real(P[ep])), rm = fast::rcp<Real>(Real(P[em]));
-            const int ot = vg(1 + tax) * pe, os = vg(1 + S) * pe;
-            const Real tp = Real(P[ot + ep]), tm = Real(P[ot + em]);
-            const Real sp = Real(P[os + ep]), sm = Real(P[os + em]);
-            D[q][0] = tp * rp - tm * rm;
-            D[q][1] = sp * rp - sm * rm;
-        }
-    };
-
-    Real W[NP][5];
-#pragma unroll
-    for (int m = 0; m < NP - 1; ++m) {
-        if (!wait_plane(m)) return;
-        node_of_plane(plane(m), W[m]);
-    }
-    Real Pc[4] = {Real(0), Real(0), Real(0), Real(0)};
-    Real Dc[2][2] = {{Real(0), Real(0)}, {Real(0), Real(0)}};
-    if (VISC) {
-        march_prims(W[H - 1], cvinv, Pc);
-        tdiff(plane(H - 1), Dc);
-    }
-    for (int q = 0; q < H; ++q) {
-        release(q);  // nodes p0-H .. p0-1 have no update
-    }
-    const uint8_t *__restrict__ fl = HYB ? a.flags + (long long)(pt.swap ? 2 : 1) * nn : nullptr;
-    unsigned fw = 0;
-    unsigned fl_ahead = 0;  // flag of node p+2, loaded one plane ahead of its use
-    if (HYB && active) {
-        fw = (unsigned)fl[base + (long long)(p0 - 2) * st] | ((unsigned)fl[base + (long long)(p0 - 1) * st] << 1) |
-             ((unsigned)fl[base + (long long)p0 * st] << 2);
-        fl_ahead = fl[base + (long long)(p0 + 1) * st];
-    }
-    Real Fl[5];
-    for (int p = p0 - 1; p < p1; ++p) {
-        const int qf = p - p0 + 2 * H;  // front node p+H
-        const int q0 = p - p0 + H;      // node p
-        const long long id = base + (long long)p * st;
-        int did = 1;
-        double uo[5];
-        if (active && p >= p0) {
-            did = a.did[id];
-            if (!same_o && !a.accumulate) {
-#pragma unroll
-                for (int v = 0; v < 5; ++v) uo[v] = a.Uo[vg(v) * nn + id];
+        // consumer thread: line (i, c)
+        const int t = threadIdx.x;
+        const int xl = t % pt.WX, rl = t / pt.WX;
+        const int i = x0 + xl, c = c0 + rl;
+        const bool active = (rl < pt.NR) && (i < g.hi[0]) && (c < g.hi[T2]);
+        // element of (i, c) in a plane (inactive threads: the tile's first node,
+        // whose halo neighbours exist)
+        const int e0 = active ? (rl + hv) * pt.BXp + (i - xs) : hv * pt.BXp + (x0 - xs);
+        const long long nn = g.nn;
+        const long long st = pt.st;                      // node stride along the line
+        const long long base = (long long)c * pt.rs + i;  // node (i, c) at position 0
+        // variable v of the kernel's frame is variable vg(v) of the state
+        const int o2 = pt.swap ? 3 : 2, o3 = pt.swap ? 2 : 3;
+        auto vg = [&](int v) { return v == 2 ? o2 : (v == 3 ? o3 : v); };
+        const Real cvinv = Real(1.0 / mp.cv);
+        const bool same_o = (a.Uo == a.Un);
+        const double rdt = (a.dt_scale * a.dt[0]) * g.dd[S];
+        // plane q of the item is plane qbase + q of the block's sequence
+        auto plane = [&](int q) { return ring + (size_t)((qbase + q) % NS) * slot_doubles; };
+        auto wait_plane = [&](int q) {
+            const int qq = qbase + q;
+            const bool ok = tma::mbar_wait_bounded(full + qq % NS, (qq / NS) & 1, a.status, 5, kPlaneWaitLimit);
+            return __all_sync(kAll, ok);
+        };
+        auto release = [&](int q) {
+            __syncwarp();
+            if (lane == 0) tma::mbar_arrive(empty + (qbase + q) % NS);
+        };
+        auto node_of_plane = [&](const double *P, Real w[5]) {
+    #pragma unroll
+            for (int v = 0; v < 5; ++v) w[v] = Real(P[vg(v) * pe + e0]);
+        };
+        // transverse differences at the plane's node from its halo neighbours:
+        // axis 0 (x, element stride 1) and axis T2 (rows, element stride BXp)
+        auto tdiff = [&](const double *P, Real (&D)[2][2]) {
+    #pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int tax = q == 0 ? 0 : T2;
+                const int es = q == 0 ? 1 : pt.BXp;
+                const int ep = e0 + es, em = e0 - es;
+                const Real rp = fast::rcp<Real>(Real(P[ep])), rm = fast::rcp<Real>(Real(P[em]));
+                const int ot = vg(1 + tax) * pe, os = vg(1 + S) * pe;
+                const Real tp = Real(P[ot + ep]), tm = Real(P[ot + em]);
+                const Real sp = Real(P[os + ep]), sm = Real(P[os + em]);
+                D[q][0] = tp * rp - tm * rm;
+                D[q][1] = sp * rp - sm * rm;
             }
+        };
+
+        Real W[NP][5];
+    #pragma unroll
+        for (int m = 0; m < NP - 1; ++m) {
+            if (!wait_plane(m)) return;
+            node_of_plane(plane(m), W[m]);
         }
-        bool full_w = true;
-        if (HYB) {
-            fw |= fl_ahead << 3;
-            if (active) fl_ahead = fl[id + 3 * st];  // node p+3 <= p1+2, inside the march's planes
-            full_w = (fw != 0u);
-        }
-        if (!wait_plane(qf)) return;
-        node_of_plane(plane(qf), W[NP - 1]);
-        Real Pn[4], Dn[2][2];
+        Real Pc[4] = {Real(0), Real(0), Real(0), Real(0)};
+        Real Dc[2][2] = {{Real(0), Real(0)}, {Real(0), Real(0)}};
         if (VISC) {
-            march_prims(W[H], cvinv, Pn);
-            tdiff(plane(q0 + 1), Dn);
+            march_prims(W[H - 1], cvinv, Pc);
+            tdiff(plane(H - 1), Dc);
         }
-        Real F[5];
-        march_flux<S, NP, HYB>(mp, W, full_w, F);
-        if (VISC) {
-            march_visc<S>(g, mp, Pc, Pn, Dc, Dn, F);
+        for (int q = 0; q < H; ++q) {
+            release(q);  // nodes p0-H .. p0-1 have no update
         }
-        if (p >= p0) {
-            if (active && did == 0) {
-                const double *P = plane(q0);
-#pragma unroll
-                for (int v = 0; v < 5; ++v) {
-                    const double phi = double(Fl[v]) - double(F[v]);
-                    const long long qv = vg(v) * nn + id;
-                    const double un = P[vg(v) * pe + e0];
-                    if (a.accumulate) {
-                        a.Um[qv] = a.Um[qv] + a.coeB * rdt * phi;
-                    } else {
-                        a.Um[qv] = a.coeA * (same_o ? un : uo[v]) + a.coeB * (un + rdt * phi);
-                    }
+        const uint8_t *__restrict__ fl = HYB ? a.flags + (long long)(pt.swap ? 2 : 1) * nn : nullptr;
+        unsigned fw = 0;
+        unsigned fl_ahead = 0;  // flag of node p+2, loaded one plane ahead of its use
+        if (HYB && active) {
+            fw = (unsigned)fl[base + (long long)(p0 - 2) * st] | ((unsigned)fl[base + (long long)(p0 - 1) * st] << 1) |
+                 ((unsigned)fl[base + (long long)p0 * st] << 2);
+            fl_ahead = fl[base + (long long)(p0 + 1) * st];
+        }
+        Real Fl[5];
+        for (int p = p0 - 1; p < p1; ++p) {
+            const int qf = p - p0 + 2 * H;  // front node p+H
+            const int q0 = p - p0 + H;      // node p
+            const long long id = base + (long long)p * st;
+            int did = 1;
+            double uo[5];
+            if (active && p >= p0) {
+                did = a.did[id];
+                if (!same_o && !a.accumulate) {
+    #pragma unroll
+                    for (int v = 0; v < 5; ++v) uo[v] = a.Uo[vg(v) * nn + id];
                 }
             }
-            release(q0);
+            bool full_w = true;
+            if (HYB) {
+                fw |= fl_ahead << 3;
+                if (active) fl_ahead = fl[id + 3 * st];  // node p+3 <= p1+2, inside the march's planes
+                full_w = (fw != 0u);
+            }
+            if (!wait_plane(qf)) return;
+            node_of_plane(plane(qf), W[NP - 1]);
+            Real Pn[4], Dn[2][2];
+            if (VISC) {
+                march_prims(W[H], cvinv, Pn);
+                tdiff(plane(q0 + 1), Dn);
+            }
+            Real F[5];
+            march_flux<S, NP, HYB>(mp, W, full_w, F);
+            if (VISC) {
+                march_visc<S>(g, mp, Pc, Pn, Dc, Dn, F);
+            }
+            if (p >= p0) {
+                if (active && did == 0) {
+                    const double *P = plane(q0);
+    #pragma unroll
+                    for (int v = 0; v < 5; ++v) {
+                        const double phi = double(Fl[v]) - double(F[v]);
+                        const long long qv = vg(v) * nn + id;
+                        const double un = P[vg(v) * pe + e0];
+                        if (a.accumulate) {
+                            a.Um[qv] = a.Um[qv] + a.coeB * rdt * phi;
+                        } else {
+                            a.Um[qv] = a.coeA * (same_o ? un : uo[v]) + a.coeB * (un + rdt * phi);
+                        }
+                    }
+                }
+                release(q0);
+            }
+    #pragma unroll
+            for (int v = 0; v < 5; ++v) Fl[v] = F[v];
+    #pragma unroll
+            for (int m = 0; m < NP - 1; ++m) {
+    #pragma unroll
+                for (int v = 0; v < 5; ++v) W[m][v] = W[m + 1][v];
+            }
+            if (VISC) {
+    #pragma unroll
+                for (int q = 0; q < 4; ++q) Pc[q] = Pn[q];
+    #pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    Dc[q][0] = Dn[q][0];
+                    Dc[q][1] = Dn[q][1];
+                }
+            }
+            fw >>= 1;
         }
-#pragma unroll
-        for (int v = 0; v < 5; ++v) Fl[v] = F[v];
-#pragma unroll
-        for (int m = 0; m < NP - 1; ++m) {
-#pragma unroll
-            for (int v = 0; v < 5; ++v) W[m][v] = W[m + 1][v];
-        }
-        if (VISC) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) Pc[q] = Pn[q];
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                Dc[q][0] = Dn[q][0];
-                Dc[q][1] = Dn[q][1];
+        if constexpr (SHARE) {
+            // planes p1 .. p1+H-1 were read for the last time: free their slots
+            // for the next item's planes
+            for (int q = NQ - H; q < NQ; ++q) {
+                release(q);
             }
         }
-        fw >>= 1;
-    }
-    if constexpr (SHARE) {
-        // planes p1 .. p1+H-1 were read for the last time: free their slots
-        // for the next item's planes
-        for (int q = NQ - H; q < NQ; ++q) {
-            release(q);
-        }
-    }
-    qbase += NQ;
+        qbase += NQ;
     }
 }
 
