@@ -77,3 +77,61 @@ def test_batch_cases_are_seeded_and_cover_the_stated_ranges():
     for s in a[:4]:
         part, model = s.descriptors()
         assert model.refMu > 0.0 and part.collapse == 0
+
+
+def test_sensor_weights_file_holds_the_trained_sensor(tmp_path):
+    """sensor_weights.bin (read by acfd_sensor_load_file and the drop-in
+    program's hybrid mode) holds the parameters and threshold of
+    sensor_weights.npz in the stated layout; save_bin writes that layout."""
+    from artracfd_b200 import sensor
+    params, thr, _ = sensor.load(sensor.WEIGHTS)
+
+    def parse(path):
+        raw = open(path, "rb").read()
+        assert raw[:8] == b"ACFDSNS1"
+        count = int(np.frombuffer(raw[8:12], dtype="<i4")[0])
+        t = float(np.frombuffer(raw[12:16], dtype="<f4")[0])
+        p = np.frombuffer(raw[16:], dtype="<f4")
+        assert p.size == count
+        return p, t
+
+    p, t = parse(sensor.WEIGHTS_BIN)
+    assert p.size == load_library().acfd_mlp_param_count()
+    assert np.array_equal(p, params) and t == np.float32(thr)
+    out = str(tmp_path / "w.bin")
+    sensor.save_bin(out, params[::-1], 0.25)
+    p2, t2 = parse(out)
+    assert np.array_equal(p2, params[::-1]) and t2 == 0.25
+
+
+@pytest.mark.skipif(not __import__("oracle.oracle", fromlist=["x"]).reference_available(),
+                    reason="reference harness oracle/_ref not built")
+def test_case_files_carry_restart_and_output_count(tmp_path):
+    """CaseSpec writes the restart tag and the space-data output count where
+    the reference's loader reads them (case_loader.c:68-72): the reference
+    loaded from the file starts its data count at the restart tag."""
+    from oracle.oracle import Reference
+    spec = configs.sod(m=(32, 4, 4))
+    spec.restart, spec.dataW = 0, 3
+    path = str(tmp_path / "sod")
+    spec.write(path)
+    text = open(os.path.join(path, "artracfd.case")).read().split("time begin")[1].split("time end")[0].split()
+    assert text[0] == "0" and text[4] == "3"
+    ref = Reference()
+    ref.load(path)
+    assert ref.time()["stepC"] == 0
+
+
+@pytest.mark.skipif(not __import__("oracle.oracle", fromlist=["x"]).reference_available(),
+                    reason="reference harness oracle/_ref not built")
+def test_contact_case_has_touching_spheres(tmp_path):
+    """The rigid-body tests' contact case is what it claims: the reference's
+    own contact search finds every sphere touching the other two."""
+    from oracle.oracle import Reference
+    spec = cases.contact_spheres(viscous=False)
+    path = str(tmp_path / "contact")
+    spec.write(path)
+    ref = Reference()
+    ref.load(path)
+    lists = ref.collision_scan()
+    assert [sorted(g for g, _ in c) for c in lists] == [[2, 3], [1, 3], [1, 2]]
