@@ -163,9 +163,15 @@ inline PlaneTile plane_tile(const Grid &g, int s, bool visc, int waves, int sms,
         pt.nblk = (int)(tiles * nseg);
     } else {
         // every block the same number of planes (at least 8): no partial
-        // last wave, one fill of the ring per item
+        // last wave, one fill of the ring per item; the lines are cut into
+        // about one chunk per block of a tile (the chunk-major order of the
+        // shares)
         long long nb = std::min<long long>(target, tiles * Ls / 8);
         pt.nblk = (int)std::max<long long>(1, nb);
+        long long nch = (pt.nblk + tiles / 2) / tiles;
+        if (nch > cap) nch = cap;
+        if (nch < 1) nch = 1;
+        pt.nseg = (int)nch;
     }
     return pt;
 }

@@ -69,40 +69,52 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
         return;
     }
 
-    // With shares (pt.share) a block marches planes [r0, r1) of the
-    // tile-major list of all tiles' lines (tile T holds planes T*Ls ..
-    // T*Ls+Ls-1): every block of the launch gets the same number of planes;
-    // a share that crosses a tile boundary is two items, marched one after
-    // the other through the same ring (the plane sequence q runs on).
-    // Without shares (pt.share == 0) a block marches segment seg of one tile.
+    // With shares (pt.share) a block marches planes [r0, r1) of the list of
+    // all tiles' lines in chunk-major order: the lines are cut into pt.nseg
+    // chunks, and chunk c of every tile comes before chunk c+1 of any tile, so
+    // that blocks of neighbouring tiles march the same planes at the same
+    // time (their halo rows are shared in L2) while every block of the launch
+    // gets the same number of planes.  A share that crosses the end of a
+    // (chunk, tile) piece is two items, marched one after the other through
+    // the same ring (the plane sequence q runs on).  Without shares
+    // (pt.share == 0) a block marches segment blk / tiles of tile blk % tiles.
     const int Ls = g.hi[S] - g.lo[S];
     const long long tiles = (long long)pt.ntx * pt.ntc;
-    const long long work = tiles * Ls;
-    long long r0 = 0, r1 = 0, T0, T1;
-    int seg = 0;
+    long long r0 = 0, r1 = 1;
     if constexpr (SHARE) {
+        const long long work = tiles * Ls;
         r0 = (long long)blk * work / pt.nblk;
         r1 = (long long)(blk + 1) * work / pt.nblk;
         if (r1 <= r0) return;
-        T0 = r0 / Ls;
-        T1 = (r1 - 1) / Ls;
-    } else {
-        T0 = blk % tiles;
-        T1 = T0;
-        seg = (int)(blk / tiles);
     }
-    // item T: its tile origin and its planes [p0, p1) along s
-    auto item = [&](long long T, int &x0, int &c0, int &p0, int &p1) {
+    const int nch = pt.nseg;
+    auto plo = [&](int c) { return (int)((long long)c * Ls / nch); };  // first plane of chunk c
+    // the item at list position w: tile origin, planes [p0, p1); w moves past it
+    auto next_item = [&](long long &w, int &x0, int &c0, int &p0, int &p1) {
+        if (w >= r1) return false;
+        long long T;
+        if constexpr (SHARE) {
+            int c = (int)((w / tiles) * nch / Ls);
+            while (c + 1 < nch && tiles * plo(c + 1) <= w) ++c;
+            while (c > 0 && tiles * plo(c) > w) --c;
+            const int len = plo(c + 1) - plo(c);
+            const long long rel = w - tiles * plo(c);
+            T = rel / len;
+            const int o = (int)(rel - T * len);
+            const int n = (int)((r1 - w < (long long)(len - o)) ? r1 - w : (long long)(len - o));
+            p0 = g.lo[S] + plo(c) + o;
+            p1 = p0 + n;
+            w += n;
+        } else {
+            T = blk % tiles;
+            const int seg = (int)(blk / tiles);
+            p0 = g.lo[S] + (int)((long long)seg * Ls / nch);
+            p1 = g.lo[S] + (int)((long long)(seg + 1) * Ls / nch);
+            w = r1;
+        }
         x0 = g.lo[0] + (int)(T % pt.ntx) * pt.WX;
         c0 = g.lo[T2] + (int)(T / pt.ntx) * pt.NR;
-        if constexpr (SHARE) {
-            const long long a0 = T * Ls, a1 = (T + 1) * Ls;
-            p0 = g.lo[S] + (int)((r0 > a0 ? r0 : a0) - a0);
-            p1 = g.lo[S] + (int)((r1 < a1 ? r1 : a1) - a0);
-        } else {
-            p0 = g.lo[S] + (int)((long long)seg * Ls / pt.nseg);
-            p1 = g.lo[S] + (int)((long long)(seg + 1) * Ls / pt.nseg);
-        }
+        return true;
     };
 
     if (warp == pt.ncw) {
@@ -110,9 +122,9 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
         if (lane == 0) {
             int q = 0, issued = 0;
             bool ok = true;
-            for (long long T = T0; T <= T1 && ok; ++T) {
-                int x0, c0, p0, p1;
-                item(T, x0, c0, p0, p1);
+            long long w = r0;
+            int x0, c0, p0, p1;
+            while (ok && next_item(w, x0, c0, p0, p1)) {
                 const int xs = (x0 - hv) & ~1, cs = c0 - hv;
                 const int NQ = p1 - p0 + 2 * H;  // planes p0-H .. p1+H-1
                 for (int ql = 0; ql < NQ; ++ql, ++q) {
@@ -142,9 +154,9 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
     }
 
     int qbase = 0;  // first plane of the item in the block's sequence
-    for (long long T = T0; T <= T1; ++T) {
-        int x0, c0, p0, p1;
-        item(T, x0, c0, p0, p1);
+    long long wi = r0;
+    int x0, c0, p0, p1;
+    while (next_item(wi, x0, c0, p0, p1)) {
         const int xs = (x0 - hv) & ~1;
         const int NQ = p1 - p0 + 2 * H;
 
