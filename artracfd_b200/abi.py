@@ -203,6 +203,8 @@ def load_library(path: str | None = None):
         "acfd_checkpoint_save": [vp, ctypes.c_char_p, vp, sz],
         "acfd_checkpoint_load": [vp, ctypes.c_char_p, vp, sz, ctypes.POINTER(sz)],
         "acfd_collision_scan": [vp, vp, vp, vp],
+        "acfd_transform_polyhedron": [vp, i, dp, dp, dp, dp, dp, dp, dp],
+        "acfd_geo_fetch": [vp, i, vp, vp, vp, vp],
         "acfd_weno_batch": [i, i, vp, vp, i],
         "acfd_fhat_batch": [ctypes.POINTER(Model), i, i, vp, vp, i],
         "acfd_batch_init": [i, ctypes.POINTER(Partition), ctypes.POINTER(Model), pp],

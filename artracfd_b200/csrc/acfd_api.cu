@@ -76,6 +76,9 @@ int ib_compute_geometric_field(IbState *ib, const Grid &g, const ModelParams &m,
 int ib_treat(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partition_t &part, double *U,
              int *flags, int tn, cudaStream_t st);
 int ib_check(IbState *ib, cudaStream_t st);
+int ib_transform(IbState *ib, int n, const double O[3], const double scale[3], const double angle[3],
+                 const double offset[3], double centroid[3], double inertia[9], double box[6], cudaStream_t st);
+int ib_fetch(IbState *ib, int n, double *v, double *Nf, double *Ne, double *Nv, cudaStream_t st);
 
 bool pdl_enabled()
 {
@@ -1313,6 +1316,24 @@ int acfd_geo_upload(acfd_case_t *cs, const acfd_polyhedron_t *poly, int totN)
     // captured step; a new body list does not
     if (relayout) release_graph(cs);
     return ACFD_OK;
+}
+
+int acfd_transform_polyhedron(acfd_case_t *cs, int n, const double O[3], const double scale[3],
+                              const double angle[3], const double offset[3], double centroid[3],
+                              double inertia[9], double box[6])
+{
+    TRY(check_case(cs));
+    if (!O || !scale || !angle || !offset || !centroid || !inertia || !box) {
+        set_error("acfd_transform_polyhedron: null argument");
+        return ACFD_ERR_ARG;
+    }
+    return ib_transform(cs->ib, n, O, scale, angle, offset, centroid, inertia, box, cs->stream);
+}
+
+int acfd_geo_fetch(acfd_case_t *cs, int n, double *v, double *Nf, double *Ne, double *Nv)
+{
+    TRY(check_case(cs));
+    return ib_fetch(cs->ib, n, v, Nf, Ne, Nv, cs->stream);
 }
 
 int acfd_compute_geometric_field(acfd_case_t *cs)

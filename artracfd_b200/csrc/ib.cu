@@ -57,6 +57,14 @@ struct BoxList {
     int nb;
 };
 
+// box extremes of a block of vertices: (min x, max x, min y, ...) with the
+// index of the vertex that gave each
+struct BoxPart {
+    double v[6];
+    int i[6];
+};
+constexpr int kMotionBlocks = 148;
+
 struct IbState {
     std::vector<DevBody> host;
     DevBody *dev = nullptr;
@@ -80,6 +88,7 @@ struct IbState {
     unsigned long long *col_key = nullptr;  // [totN][totN] first meeting (node order x path length + path index)
     int *col_N = nullptr;              // [totN][totN][3] summed path offsets
     int col_n = 0;
+    BoxPart *motion_part = nullptr;  // [kMotionBlocks] box extremes of a surface motion
 };
 
 namespace {
@@ -104,7 +113,7 @@ __device__ __forceinline__ long long node_of(const Grid &g, int i, int j, int k)
     return ((long long)k * g.n[1] + j) * g.pitch + i;
 }
 
-__device__ __forceinline__ double dot3(const double *a, const double *b)
+__host__ __device__ __forceinline__ double dot3(const double *a, const double *b)
 {
     return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
 }
@@ -1005,6 +1014,117 @@ __global__ void build_tri(const int *f, const double *v, double *tri, int faceN)
     }
 }
 
+// ---- surface motion (TransformPolyhedron, computational_geometry.c:162-246) ----
+// rot is the point rotation matrix of the angles; a point is moved relative
+// to the reference point O: shifted to it, scaled, rotated, offset and
+// shifted back, each product and sum rounded on its own in the reference's
+// order (this unit is compiled without contraction).  Normals are rotated.
+struct SurfaceMotion {
+    double rot[3][3];
+    double O[3], scale[3], offset[3];
+};
+
+__host__ __device__ inline void move_point(const SurfaceMotion &M, double p[3])
+{
+    double t[3];
+    for (int s = 0; s < 3; ++s) t[s] = (p[s] - M.O[s]) * M.scale[s];
+    for (int s = 0; s < 3; ++s) p[s] = dot3(M.rot[s], t) + M.offset[s] + M.O[s];
+}
+
+// The reference updates the box vertex by vertex with box = (box < v) ? box : v
+// (and > for the maximum), starting from FLT_MAX and FLT_MIN: the result is
+// the extreme value, and among equal values (+0 and -0) the last one in
+// vertex order.  Extremes are therefore reduced as (value, vertex index)
+// pairs, the larger index winning ties; the start values carry index -1.
+__host__ __device__ inline void take_lo(double &v, int &i, double x, int j)
+{
+    if (x < v || (x == v && j > i)) {
+        v = x;
+        i = j;
+    }
+}
+
+__host__ __device__ inline void take_hi(double &v, int &i, double x, int j)
+{
+    if (x > v || (x == v && j > i)) {
+        v = x;
+        i = j;
+    }
+}
+
+constexpr int kMotionThreads = 256;
+
+__global__ void __launch_bounds__(kMotionThreads) move_surface(SurfaceMotion M, double *v, double *Nf, double *Ne,
+                                                               double *Nv, int vertN, int faceN, int edgeN,
+                                                               BoxPart *part)
+{
+    double lo[3], hi[3];
+    int loi[3], hii[3];
+    for (int s = 0; s < 3; ++s) {
+        lo[s] = FLT_MAX;
+        hi[s] = FLT_MIN;
+        loi[s] = -1;
+        hii[s] = -1;
+    }
+    const long long total = 2LL * vertN + faceN + edgeN;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x) {
+        if (q < vertN) {
+            double p[3] = {v[3 * q], v[3 * q + 1], v[3 * q + 2]};
+            move_point(M, p);
+            for (int s = 0; s < 3; ++s) {
+                v[3 * q + s] = p[s];
+                take_lo(lo[s], loi[s], p[s], (int)q);
+                take_hi(hi[s], hii[s], p[s], (int)q);
+            }
+        } else {
+            long long k = q - vertN;
+            double *N;
+            if (k < faceN) {
+                N = Nf + 3 * k;
+            } else if ((k -= faceN) < edgeN) {
+                N = Ne + 3 * k;
+            } else {
+                N = Nv + 3 * (k - edgeN);
+            }
+            const double t[3] = {N[0], N[1], N[2]};
+            for (int s = 0; s < 3; ++s) N[s] = dot3(M.rot[s], t);
+        }
+    }
+    // block extremes: lanes, then warps
+    for (int off = 16; off > 0; off >>= 1) {
+        for (int s = 0; s < 3; ++s) {
+            const double a = __shfl_down_sync(0xffffffffu, lo[s], off);
+            const int ai = __shfl_down_sync(0xffffffffu, loi[s], off);
+            const double b = __shfl_down_sync(0xffffffffu, hi[s], off);
+            const int bi = __shfl_down_sync(0xffffffffu, hii[s], off);
+            take_lo(lo[s], loi[s], a, ai);
+            take_hi(hi[s], hii[s], b, bi);
+        }
+    }
+    __shared__ BoxPart warps[kMotionThreads / 32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        for (int s = 0; s < 3; ++s) {
+            warps[warp].v[2 * s] = lo[s];
+            warps[warp].i[2 * s] = loi[s];
+            warps[warp].v[2 * s + 1] = hi[s];
+            warps[warp].i[2 * s + 1] = hii[s];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        BoxPart r = warps[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            for (int s = 0; s < 3; ++s) {
+                take_lo(r.v[2 * s], r.i[2 * s], warps[w].v[2 * s], warps[w].i[2 * s]);
+                take_hi(r.v[2 * s + 1], r.i[2 * s + 1], warps[w].v[2 * s + 1], warps[w].i[2 * s + 1]);
+            }
+        }
+        part[blockIdx.x] = r;
+    }
+}
+
 IbGrid make_ibgrid(const Grid &g, const acfd_partition_t &part, int ibmLayer)
 {
     IbGrid G;
@@ -1108,6 +1228,8 @@ static void ib_release_solid(IbState *ib)
     cudaFree(ib->sf_force);
     cudaFree(ib->col_key);
     cudaFree(ib->col_N);
+    cudaFree(ib->motion_part);
+    ib->motion_part = nullptr;
     ib->sf_terms = nullptr;
     ib->sf_valid = nullptr;
     ib->sf_off = nullptr;
@@ -1179,6 +1301,14 @@ static int upload_groups(IbState *ib, const acfd_partition_t &part, cudaStream_t
     return ACFD_OK;
 }
 
+// A triangulated body given without vertices and normals keeps the surface
+// it has on the device (moved there by acfd_transform_polyhedron); its face
+// and edge lists are kept too.
+static bool keeps_surface(const acfd_polyhedron_t &P)
+{
+    return P.faceN > 0 && !P.v && !P.Nv && !P.Nf && !P.Ne;
+}
+
 // A moved body list of the same bodies (same counts of faces, edges and
 // vertices) whose ghost lists still fit: new positions, velocities and
 // surfaces go into the device buffers in place, in stream order, so that
@@ -1191,8 +1321,8 @@ static int update_in_place(IbState *ib, const acfd_polyhedron_t *poly, int totN,
     for (int n = 0; n < totN; ++n) {
         const DevBody &B = ib->host[n];
         if (B.faceN != poly[n].faceN || B.edgeN != poly[n].edgeN || B.vertN != poly[n].vertN) return ACFD_OK;
-        if (poly[n].faceN > 0 && (!poly[n].f || !poly[n].Nf || !poly[n].e || !poly[n].Ne || !poly[n].v ||
-                                  !poly[n].Nv)) {
+        if (poly[n].faceN > 0 && !keeps_surface(poly[n]) &&
+            (!poly[n].f || !poly[n].Nf || !poly[n].e || !poly[n].Ne || !poly[n].v || !poly[n].Nv)) {
             return ACFD_OK;
         }
     }
@@ -1205,7 +1335,7 @@ static int update_in_place(IbState *ib, const acfd_polyhedron_t *poly, int totN,
     for (int n = 0; n < totN; ++n) {
         const acfd_polyhedron_t &P = poly[n];
         const DevBody &B = ib->host[n];
-        if (P.faceN <= 0) continue;
+        if (P.faceN <= 0 || keeps_surface(P)) continue;
         auto put = [&](const void *dst, const void *src, size_t bytes) {
             return cudaMemcpyAsync(const_cast<void *>(dst), src, bytes, cudaMemcpyHostToDevice, st);
         };
@@ -1240,6 +1370,37 @@ int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, const acfd_p
         }
     }
     ACFD_CUDA(cudaStreamSynchronize(st));
+    // bodies that keep their device surface through a new layout: the
+    // surface comes back to the host first and is uploaded with the list
+    std::vector<acfd_polyhedron_t> listed;
+    std::vector<std::vector<double>> reals;
+    std::vector<std::vector<int>> ints;
+    for (int n = 0; n < totN; ++n) {
+        if (!keeps_surface(poly[n])) continue;
+        if (n >= ib->count || ib->host[n].faceN != poly[n].faceN || ib->host[n].edgeN != poly[n].edgeN ||
+            ib->host[n].vertN != poly[n].vertN || !ib->host[n].v) {
+            set_error("acfd_geo_upload: body %d has no surface on the device to keep", n);
+            return ACFD_ERR_ARG;
+        }
+        if (listed.empty()) listed.assign(poly, poly + totN);
+        const DevBody &B = ib->host[n];
+        acfd_polyhedron_t &P = listed[n];
+        const size_t sizes[4] = {3 * (size_t)B.vertN, 3 * (size_t)B.vertN, 3 * (size_t)B.faceN, 3 * (size_t)B.edgeN};
+        const double *from[4] = {B.v, B.Nv, B.Nf, B.Ne};
+        const double **to[4] = {&P.v, &P.Nv, &P.Nf, &P.Ne};
+        for (int a = 0; a < 4; ++a) {
+            reals.emplace_back(sizes[a]);
+            ACFD_CUDA(cudaMemcpy(reals.back().data(), from[a], sizeof(double) * sizes[a], cudaMemcpyDeviceToHost));
+            *to[a] = reals.back().data();
+        }
+        ints.emplace_back(3 * (size_t)B.faceN);
+        ACFD_CUDA(cudaMemcpy(ints.back().data(), B.f, sizeof(int) * 3 * B.faceN, cudaMemcpyDeviceToHost));
+        P.f = ints.back().data();
+        ints.emplace_back(4 * (size_t)B.edgeN);
+        ACFD_CUDA(cudaMemcpy(ints.back().data(), B.e, sizeof(int) * 4 * B.edgeN, cudaMemcpyDeviceToHost));
+        P.e = ints.back().data();
+    }
+    if (!listed.empty()) poly = listed.data();
     ib_release_geometry(ib);
     if (totN == 0) return ACFD_OK;
     ib->host.resize(totN);
@@ -1465,6 +1626,110 @@ int ib_collision_scan(IbState *ib, const Grid &g, const ModelParams &m, const ac
             for (int s = 0; s < 3; ++s) N[3 * ((size_t)p * totN + c) + s] = cn[3 * slot + s];
         }
     }
+    return ACFD_OK;
+}
+
+// TransformPolyhedron (computational_geometry.c:162-208) of body n: its
+// device surface is moved (move_surface, then the facet table), and the
+// reference point O, the centroid, the inertia tensor and the box follow on
+// the host in the reference's order.  The host part uses the C library's
+// sin, cos and sqrt, as the reference does.
+int ib_transform(IbState *ib, int n, const double O[3], const double scale[3], const double angle[3],
+                 const double offset[3], double centroid[3], double inertia[9], double box[6], cudaStream_t st)
+{
+    if (!ib || n < 0 || n >= ib->count) {
+        set_error("acfd_transform_polyhedron: body %d of %d", n, ib ? ib->count : 0);
+        return ACFD_ERR_ARG;
+    }
+    const DevBody &B = ib->host[n];
+    if (B.faceN <= 0 || !B.v) {
+        set_error("acfd_transform_polyhedron: body %d is not triangulated", n);
+        return ACFD_ERR_ARG;
+    }
+    SurfaceMotion M;
+    for (int s = 0; s < 3; ++s) {
+        M.O[s] = O[s];
+        M.scale[s] = scale[s];
+        M.offset[s] = offset[s];
+    }
+    const double Sx = sin(angle[0]), Sy = sin(angle[1]), Sz = sin(angle[2]);
+    const double Cx = cos(angle[0]), Cy = cos(angle[1]), Cz = cos(angle[2]);
+    // rotation about x, then y, then z (the reference's point rotation matrix)
+    const double R[3][3] = {{Cy * Cz, -Cx * Sz + Sx * Sy * Cz, Sx * Sz + Cx * Sy * Cz},
+                            {Cy * Sz, Cx * Cz + Sx * Sy * Sz, -Sx * Cz + Cx * Sy * Sz},
+                            {-Sy, Sx * Cy, Cx * Cy}};
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) M.rot[a][b] = R[a][b];
+    if (!ib->motion_part) ACFD_CUDA(cudaMalloc(&ib->motion_part, sizeof(BoxPart) * kMotionBlocks));
+    const long long total = 2LL * B.vertN + B.faceN + B.edgeN;
+    const int nblk = (int)std::min<long long>(kMotionBlocks, (total + kMotionThreads - 1) / kMotionThreads);
+    move_surface<<<nblk, kMotionThreads, 0, st>>>(M, const_cast<double *>(B.v), const_cast<double *>(B.Nf),
+                                                  const_cast<double *>(B.Ne), const_cast<double *>(B.Nv), B.vertN,
+                                                  B.faceN, B.edgeN, ib->motion_part);
+    ACFD_CUDA(cudaGetLastError());
+    build_tri<<<blocks_for(B.faceN, 128), 128, 0, st>>>(B.f, B.v, const_cast<double *>(B.tri), B.faceN);
+    ACFD_CUDA(cudaGetLastError());
+    std::vector<BoxPart> part((size_t)nblk);
+    ACFD_CUDA(cudaMemcpyAsync(part.data(), ib->motion_part, sizeof(BoxPart) * nblk, cudaMemcpyDeviceToHost, st));
+    ACFD_CUDA(cudaStreamSynchronize(st));
+    BoxPart r;
+    for (int s = 0; s < 3; ++s) {
+        r.v[2 * s] = FLT_MAX;
+        r.v[2 * s + 1] = FLT_MIN;
+        r.i[2 * s] = r.i[2 * s + 1] = -1;
+    }
+    for (const BoxPart &p : part) {
+        for (int s = 0; s < 3; ++s) {
+            take_lo(r.v[2 * s], r.i[2 * s], p.v[2 * s], p.i[2 * s]);
+            take_hi(r.v[2 * s + 1], r.i[2 * s + 1], p.v[2 * s + 1], p.i[2 * s + 1]);
+        }
+    }
+    // inertia tensor: moments about the six axes xx, yy, zz, xy, yz, zx seen
+    // in the rotated frame
+    const double num = 1.0 / sqrt(2.0);
+    const double axe[6][3] = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 1.0},
+                              {num, num, 0.0}, {0.0, num, num}, {num, 0.0, num}};
+    const double inv[3][3] = {{R[0][0], R[1][0], R[2][0]}, {R[0][1], R[1][1], R[2][1]}, {R[0][2], R[1][2], R[2][2]}};
+    const double *I = inertia;  // rows xx xy xz / yx yy yz / zx zy zz
+    double m[6];
+    for (int q = 0; q < 6; ++q) {
+        const double ax = dot3(inv[0], axe[q]), ay = dot3(inv[1], axe[q]), az = dot3(inv[2], axe[q]);
+        m[q] = I[0] * ax * ax + I[4] * ay * ay + I[8] * az * az + 2.0 * I[1] * ax * ay + 2.0 * I[5] * ay * az +
+               2.0 * I[6] * az * ax;
+    }
+    const double It[9] = {m[0], -m[3], -m[5], -m[3], m[1], -m[4], -m[5], -m[4], m[2]};
+    for (int q = 0; q < 9; ++q) inertia[q] = It[q];
+    // the centroid last, entering the box after the vertices
+    double c[3] = {centroid[0], centroid[1], centroid[2]};
+    move_point(M, c);
+    for (int s = 0; s < 3; ++s) {
+        centroid[s] = c[s];
+        box[2 * s] = (r.v[2 * s] < c[s]) ? r.v[2 * s] : c[s];
+        box[2 * s + 1] = (r.v[2 * s + 1] > c[s]) ? r.v[2 * s + 1] : c[s];
+    }
+    return ACFD_OK;
+}
+
+// the device surface of body n to the host (null outputs are skipped)
+int ib_fetch(IbState *ib, int n, double *v, double *Nf, double *Ne, double *Nv, cudaStream_t st)
+{
+    if (!ib || n < 0 || n >= ib->count) {
+        set_error("acfd_geo_fetch: body %d of %d", n, ib ? ib->count : 0);
+        return ACFD_ERR_ARG;
+    }
+    const DevBody &B = ib->host[n];
+    if (B.faceN <= 0 || !B.v) {
+        set_error("acfd_geo_fetch: body %d is not triangulated", n);
+        return ACFD_ERR_ARG;
+    }
+    const double *from[4] = {B.v, B.Nf, B.Ne, B.Nv};
+    double *to[4] = {v, Nf, Ne, Nv};
+    const int rows[4] = {B.vertN, B.faceN, B.edgeN, B.vertN};
+    for (int a = 0; a < 4; ++a) {
+        if (!to[a]) continue;
+        ACFD_CUDA(cudaMemcpyAsync(to[a], from[a], sizeof(double) * 3 * rows[a], cudaMemcpyDeviceToHost, st));
+    }
+    ACFD_CUDA(cudaStreamSynchronize(st));
     return ACFD_OK;
 }
 

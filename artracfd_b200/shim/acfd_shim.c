@@ -21,7 +21,10 @@
  * sensor_weights.bin), ACFD_TILES = stage-kernel variants per axis (e.g.
  * 7,7,7), ACFD_AUTOTUNE = 1 (time the variants at the first step), ACFD_GRAPH = 1
  * (default, replay each step as a CUDA graph) | 0, ACFD_SOLID = device
- * (default) | host, ACFD_ASYNC_OUTPUT = 1 (default: the outputs of a step
+ * (default) | host, ACFD_MOTION = device (default: the surfaces of moving
+ * triangulated bodies are transformed on the device and come back to the
+ * host only for output) | host (the reference's ApplyMotion on the host;
+ * with ACFD_SOLID=device), ACFD_ASYNC_OUTPUT = 1 (default: the outputs of a step
  * come from a device snapshot and are written while the next step runs, when
  * no body moves) | 0, ACFD_CHECKPOINT = 0 (default) | 1 (an FP64 checkpoint
  * artracfd.ckpt.<n> with every space data output; a restart from output n
@@ -59,6 +62,8 @@ static int g_solid_host = 0;   /* ACFD_SOLID=host: rigid-body step on the host *
 static int g_async_output = 1; /* ACFD_ASYNC_OUTPUT=0: output from a synchronous download */
 static int g_checkpoint = 0;   /* ACFD_CHECKPOINT=1: FP64 checkpoint with every space data output */
 static int g_autotune = 0;     /* ACFD_AUTOTUNE=1: time the stage-kernel variants at the first step */
+static int g_motion_host = 0;  /* ACFD_MOTION=host: surfaces moved on the host */
+static unsigned char *g_surface_on_device = NULL; /* per body: the host's surface is older */
 
 /* outputs of one step written from a device snapshot while the next step runs */
 typedef struct {
@@ -161,13 +166,16 @@ void AcfdUploadGeometry(const Space *space)
             o->box[s][0] = P->box[s][MIN];
             o->box[s][1] = P->box[s][MAX];
         }
+        o->area = P->area;
+        if (g_surface_on_device && g_surface_on_device[n]) {
+            continue; /* NULL arrays: the device keeps the moved surface */
+        }
         o->f = (const int *)P->f;
         o->Nf = (const double *)P->Nf;
         o->e = (const int *)P->e;
         o->Ne = (const double *)P->Ne;
         o->v = (const double *)P->v;
         o->Nv = (const double *)P->Nv;
-        o->area = P->area;
     }
     Check(acfd_geo_upload(g_case, list, geo->totN), "acfd_geo_upload");
     RetrieveStorage(list);
@@ -224,6 +232,14 @@ static void EnsureCase(Space *space, const Model *model)
     g_use_graph = !(env && 0 == strcmp(env, "0"));
     env = getenv("ACFD_SOLID");
     g_solid_host = (env && 0 == strcmp(env, "host"));
+    env = getenv("ACFD_MOTION");
+    g_motion_host = (env && 0 == strcmp(env, "host"));
+    if (0 < space->geo.totN) {
+        g_surface_on_device = calloc((size_t)space->geo.totN, 1);
+        if (NULL == g_surface_on_device) {
+            ShowError("out of memory");
+        }
+    }
     env = getenv("ACFD_ASYNC_OUTPUT");
     g_async_output = !(env && 0 == strcmp(env, "0"));
     env = getenv("ACFD_CHECKPOINT");
@@ -241,8 +257,33 @@ static void EnsureDevice(Space *space)
     }
 }
 
+int AcfdMotionOnDevice(void)
+{
+    return !g_motion_host;
+}
+
+void AcfdMarkSurfaceOnDevice(int n)
+{
+    g_surface_on_device[n] = 1;
+}
+
+/* the surfaces moved on the device back into the host's polyhedra */
+static void FetchSurfaces(Space *space)
+{
+    Geometry *geo = &(space->geo);
+    for (int n = 0; g_surface_on_device && n < geo->totN; ++n) {
+        if (!g_surface_on_device[n]) {
+            continue;
+        }
+        Polyhedron *P = geo->poly + n;
+        Check(acfd_geo_fetch(g_case, n, &P->v[0][0], &P->Nf[0][0], &P->Ne[0][0], &P->Nv[0][0]), "acfd_geo_fetch");
+        g_surface_on_device[n] = 0;
+    }
+}
+
 static void EnsureHost(Space *space)
 {
+    FetchSurfaces(space);
     if (!g_host_current) {
         Check(acfd_sync_to_host(g_case, (acfd_node_t *)space->node, ACFD_SYNC_ALL), "acfd_sync_to_host");
         g_host_current = 1;
@@ -255,6 +296,8 @@ void AcfdShimFinalize(void)
         acfd_finalize(g_case);
         g_case = NULL;
     }
+    free(g_surface_on_device);
+    g_surface_on_device = NULL;
 }
 
 /* TreatBoundary (boundary_treatment.c:28) */
@@ -464,6 +507,9 @@ static void RestoreCheckpoint(Time *time, Space *space)
         q = CheckpointBody(geo->poly + n, (unsigned char *)q, 0);
     }
     RetrieveStorage(user);
+    if (g_surface_on_device) {
+        memset(g_surface_on_device, 0, (size_t)geo->totN);
+    }
     AcfdUploadGeometry(space);
     g_dev_current = 1;
     g_host_current = 0;

@@ -20,6 +20,10 @@ void AcfdShimFinalize(void);
 
 /* send the bodies as they are on the host to the device */
 void AcfdUploadGeometry(const Space *);
+/* 1 unless ACFD_MOTION=host: moving triangulated surfaces stay on the device */
+int AcfdMotionOnDevice(void);
+/* body n's surface was moved on the device (the host fetches it when needed) */
+void AcfdMarkSurfaceOnDevice(int n);
 /* the rigid-body half step with the node scans on the device (solid_gpu.c) */
 void AcfdDeviceSolidStep(acfd_case_t *, const Real now, const Real dt, Space *, const Model *);
 

@@ -10,6 +10,9 @@
  *   IntegrateSurfaceForce  -> acfd_integrate_surface_force
  *   the contact scan of ApplyCollision (DetectColState / AddColObject)
  *                          -> acfd_collision_scan
+ *   TransformPolyhedron of ApplyMotion
+ *                          -> acfd_transform_polyhedron (ACFD_MOTION=host
+ *                             keeps the reference's ApplyMotion)
  *   ComputeGeometricField  -> acfd_compute_geometric_field
  *   TreatImmersedBoundary  -> acfd_treat_ib
  * and the velocity exchange of ApplyCollision (solid_dynamics.c:262-318)
@@ -142,6 +145,46 @@ static void DeviceCollision(acfd_case_t *cs, Space *space)
     RetrieveStorage(counts);
 }
 
+/* ApplyMotion (solid_dynamics.c:380-410) with the surfaces of triangulated
+ * bodies transformed on the device (acfd_transform_polyhedron, the
+ * reference's TransformPolyhedron): the host receives their centroid,
+ * inertia tensor and box, and fetches the surface only for output */
+static void DeviceMotion(acfd_case_t *cs, const Real dt, Space *space)
+{
+    Geometry *const geo = &(space->geo);
+    const RealVec scale = {1.0, 1.0, 1.0};
+    for (int n = 0; n < geo->totN; ++n) {
+        Polyhedron *poly = geo->poly + n;
+        if (1 == poly->state) {
+            continue;
+        }
+        RealVec offset, angle;
+        for (int s = 0; s < DIMS; ++s) {
+            offset[s] = poly->V[TN][s] * dt;
+            angle[s] = poly->W[TN][s] * dt;
+        }
+        if (0 >= poly->faceN) {
+            for (int s = 0; s < DIMS; ++s) {
+                poly->O[s] = poly->O[s] + offset[s];
+            }
+            for (int s = 0; s < DIMS; ++s) {
+                poly->box[s][MIN] = poly->O[s] - poly->r;
+                poly->box[s][MAX] = poly->O[s] + poly->r;
+            }
+            continue;
+        }
+        const RealVec O = {poly->O[X], poly->O[Y], poly->O[Z]};
+        double box[6];
+        SolidCheck(acfd_transform_polyhedron(cs, n, O, scale, angle, offset, poly->O, &poly->I[0][0], box),
+                "acfd_transform_polyhedron");
+        for (int s = 0; s < DIMS; ++s) {
+            poly->box[s][MIN] = box[2 * s];
+            poly->box[s][MAX] = box[2 * s + 1];
+        }
+        AcfdMarkSurfaceOnDevice(n);
+    }
+}
+
 void AcfdDeviceSolidStep(acfd_case_t *cs, const Real now, const Real dt, Space *space, const Model *model)
 {
     DeviceSurfaceForce(cs, space);
@@ -149,7 +192,11 @@ void AcfdDeviceSolidStep(acfd_case_t *cs, const Real now, const Real dt, Space *
     if (1 != model->psi) {
         DeviceCollision(cs, space);
     }
-    ApplyMotion(dt, space);
+    if (AcfdMotionOnDevice()) {
+        DeviceMotion(cs, dt, space);
+    } else {
+        ApplyMotion(dt, space);
+    }
     AcfdUploadGeometry(space);
     SolidCheck(acfd_compute_geometric_field(cs), "acfd_compute_geometric_field");
     SolidCheck(acfd_treat_ib(cs, TO), "acfd_treat_ib");

@@ -225,6 +225,33 @@ class Solver:
                  for c in range(counts[p])] for p in range(n)]
 
 
+    def transform_polyhedron(self, n, O, scale, angle, offset, centroid, inertia):
+        """TransformPolyhedron (computational_geometry.c:162-208) of
+        triangulated body n with its surface on the device.  Returns the moved
+        centroid (3), the rotated inertia tensor (3, 3) and the box (3, 2) of
+        the moved vertices and centroid."""
+        def vec(x, k):
+            return np.ascontiguousarray(np.array(x, dtype=np.float64).reshape(k))
+        args = [vec(O, 3), vec(scale, 3), vec(angle, 3), vec(offset, 3)]
+        c = vec(centroid, 3).copy()
+        inert = vec(inertia, 9).copy()
+        box = np.zeros(6)
+        ptr = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        check(self.lib.acfd_transform_polyhedron(self.h, n, *[ptr(a) for a in args], ptr(c), ptr(inert), ptr(box)),
+              self.lib)
+        return c, inert.reshape(3, 3), box.reshape(3, 2)
+
+    def geo_fetch(self, n):
+        """The device surface of triangulated body n: dict of v, Nf, Ne, Nv
+        as (rows, 3) arrays."""
+        g = self.geo[n]
+        out = {"v": np.zeros((g.vertN, 3)), "Nf": np.zeros((g.faceN, 3)), "Ne": np.zeros((g.edgeN, 3)),
+               "Nv": np.zeros((g.vertN, 3))}
+        check(self.lib.acfd_geo_fetch(self.h, n, out["v"].ctypes.data, out["Nf"].ctypes.data, out["Ne"].ctypes.data,
+                                      out["Nv"].ctypes.data), self.lib)
+        return out
+
+
 def run(solver: Solver, numCFL: float, end: float, steps: int, now: float = 0.0):
     """The fluid part of EvolveSolution's loop (solve.c:65-89) without output
     or solid dynamics: dt from the CFL condition, rectified to end exactly at

@@ -245,8 +245,29 @@ int acfd_evolve_fluid_graph(acfd_case_t *cs, double dt);
 
 /* ---- immersed boundaries ---------------------------------------------- */
 
-/* Upload (or replace after host-side motion) the body list. */
+/* Upload (or replace after host-side motion) the body list.  On an update of
+ * the same bodies, a triangulated body given with v, Nv, Nf and Ne all NULL
+ * keeps the surface it has on the device (moved there by
+ * acfd_transform_polyhedron); its f and e are then ignored. */
 int acfd_geo_upload(acfd_case_t *cs, const acfd_polyhedron_t *poly, int totN);
+/* TransformPolyhedron (computational_geometry.c:162-208) of triangulated
+ * body n of the last acfd_geo_upload, with its surface on the device: the
+ * vertices are shifted to the reference point O, scaled by scale, rotated by
+ * angle (about x, then y, then z), offset by offset and shifted back; the
+ * face, edge and vertex normals are rotated.  On the host: centroid[3] (in,
+ * out) is moved like a vertex, inertia[9] (in, out; row-major I) is rotated,
+ * and box[6] (out: min x, max x, min y, max y, min z, max z) receives the
+ * reference's bounding box of the moved vertices and centroid.  Bitwise
+ * equal to the reference.  The body list on the device keeps its old
+ * centroid and box until the next acfd_geo_upload, which passes NULL surface
+ * arrays to keep the moved surface.  ApplyMotion (solid_dynamics.c:380-410)
+ * calls it with O = the centroid and scale = 1. */
+int acfd_transform_polyhedron(acfd_case_t *cs, int n, const double O[3], const double scale[3],
+                              const double angle[3], const double offset[3], double centroid[3],
+                              double inertia[9], double box[6]);
+/* The device surface of triangulated body n to host arrays: v[vertN*3],
+ * Nf[faceN*3], Ne[edgeN*3], Nv[vertN*3]; a NULL output is skipped. */
+int acfd_geo_fetch(acfd_case_t *cs, int n, double *v, double *Nf, double *Ne, double *Nv);
 /* ComputeGeometricField (immersed_boundary.c:65-264): did, fid, lid, gst and
  * the reconstruction of newly uncovered fluid nodes on U[TO]. */
 int acfd_compute_geometric_field(acfd_case_t *cs);

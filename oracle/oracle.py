@@ -168,6 +168,8 @@ class Reference:
             "ref_evolve_solid": (None, [d, d]),
             "ref_integrate_surface_force": (None, [_dp]),
             "ref_collision_scan": (i, [i, _ip, _ip]),
+            "ref_transform_polyhedron": (None, [i, _dp, _dp, _dp, _dp]),
+            "ref_get_inertia": (None, [i, _dp]),
             "ref_step": (d, []),
             "ref_weno5": (None, [_vp, _dp]),
             "ref_weno3": (None, [_vp, _dp]),
@@ -270,6 +272,22 @@ class Reference:
             c = self.lib.ref_collision_scan(p, gid.ctypes.data_as(_ip), N.ctypes.data_as(_ip))
             res.append([(int(gid[q]), tuple(int(v) for v in N[3 * q:3 * q + 3])) for q in range(c)])
         return res
+
+    def transform_polyhedron(self, n, O, scale, angle, offset) -> None:
+        args = [np.ascontiguousarray(np.array(a, dtype=np.float64).reshape(3)) for a in (O, scale, angle, offset)]
+        self.lib.ref_transform_polyhedron(n, *[a.ctypes.data_as(_dp) for a in args])
+
+    def inertia(self, n) -> np.ndarray:
+        out = np.zeros(9)
+        self.lib.ref_get_inertia(n, out.ctypes.data_as(_dp))
+        return out.reshape(3, 3)
+
+    def surface(self, n):
+        """Copies of body n's vertices and normals: dict of v, Nf, Ne, Nv."""
+        p = self.geometry()[n]
+        rows = {"v": p.vertN, "Nf": p.faceN, "Ne": p.edgeN, "Nv": p.vertN}
+        return {k: np.ctypeslib.as_array(getattr(p, k), shape=(rows[k] * 3,)).reshape(rows[k], 3).copy()
+                for k in rows}
 
     def compute_geometric_field(self) -> None:
         self.lib.ref_compute_geometric_field()

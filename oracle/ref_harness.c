@@ -228,6 +228,22 @@ void ref_integrate_surface_force(double *out)
     }
 }
 
+/* TransformPolyhedron (computational_geometry.c:162-208) of body n, the
+ * reference point O given apart from the body's centroid (ApplyMotion passes
+ * the centroid itself). */
+void ref_transform_polyhedron(int n, const double O[3], const double scale[3], const double angle[3],
+        const double offset[3])
+{
+    const RealVec Oc = {O[0], O[1], O[2]};
+    TransformPolyhedron(Oc, scale, angle, offset, g_space.geo.poly + n);
+}
+
+/* the inertia tensor of body n, row-major */
+void ref_get_inertia(int n, double out[9])
+{
+    memcpy(out, g_space.geo.poly[n].I, 9 * sizeof(double));
+}
+
 /* The contact list that ApplyCollision builds for body p before its
  * velocity update (the node scan of solid_dynamics.c:242-256, calling the
  * reference's DetectColState); returns the list length, gid/N receive the

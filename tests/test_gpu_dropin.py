@@ -85,17 +85,22 @@ def test_dropin_fast_mode_close_to_reference(tmp_path, name):
 
 
 @needs
-@pytest.mark.parametrize("solid", ["device", "host"])
+@pytest.mark.parametrize("solid", ["device", "device_host_motion", "host"])
 def test_dropin_exact_mode_moving_bodies_with_contacts(tmp_path, solid):
     """Three inviscid moving spheres resting on one another in a crossflow:
     with the rigid-body step's node scans on the device (surface forces,
     contact lists, remapping and ghost values; the node array stays on the
-    GPU) or on the host, the exact mode writes the reference's files."""
+    GPU) and the surfaces moved there too (default) or on the host
+    (ACFD_MOTION=host), or with the whole step on the host, the exact mode
+    writes the reference's files."""
     spec = cases.contact_spheres(viscous=False)
     spec.stepN = 5
     a, b = _pair(tmp_path, spec)
     _run(REFBIN, "serial", a)
-    _run(DROPIN, "gpu", b, {"ACFD_MODE": "exact", "ACFD_SOLID": solid})
+    env = {"ACFD_MODE": "exact", "ACFD_SOLID": "host" if solid == "host" else "device"}
+    if solid == "device_host_motion":
+        env["ACFD_MOTION"] = "host"
+    _run(DROPIN, "gpu", b, env)
     sa, fa = _last_fields(a)
     sb, fb = _last_fields(b)
     assert sa == sb

@@ -11,6 +11,9 @@ reference's own functions on the same state (the harness in oracle/_ref):
 * the contact scan of ApplyCollision (DetectColState / AddColObject,
   solid_dynamics.c:242-256, 327-357): the same contact lists, in the same
   order, with the same lines of impact.
+* TransformPolyhedron (computational_geometry.c:162-208), the surface motion
+  of ApplyMotion: vertices, normals, centroid, inertia tensor and box
+  bitwise; a moved surface kept on the device through a new body list.
 
 The states are those of the reference after a few of its own time steps
 (moving spheres in a crossflow, three of them resting on one another).
@@ -114,3 +117,87 @@ def test_moved_bodies_update_in_place(tmp_path):
         assert np.array_equal(outs[0][f], outs[1][f]), f
     assert np.array_equal(outs[0]["U"], outs[1]["U"])
     assert not np.array_equal(np.array([g.O[0] for g in before_copy]), np.array([g.O[0] for g in after]))
+
+
+MOTIONS = {"rotate": ((1.0, 1.0, 1.0), (0.3, -0.2, 0.7), (0.01, -0.02, 0.005)),
+           "scale": ((1.5, 0.75, 2.0), (1e-3, 2e-3, -5e-4), (0.0, 0.0, 0.0)),
+           "shift": ((1.0, 1.0, 1.0), (0.0, 0.0, 0.0), (-0.5, -0.5, -0.5))}
+
+
+def _rows(box):
+    return np.array([list(b) for b in box])
+
+
+@pytest.mark.parametrize("motion", MOTIONS)
+def test_transform_polyhedron_matches_reference(tmp_path, motion):
+    """The device transform of each triangulated body against the
+    reference's TransformPolyhedron on the same body: moved vertices, rotated
+    face, edge and vertex normals, centroid, inertia tensor and box."""
+    scale, angle, offset = MOTIONS[motion]
+    ref = _load(tmp_path, "contact_spheres", 0)
+    tri = [n for n, g in enumerate(ref.geometry()) if g.faceN > 0]
+    assert tri
+    with _device(ref) as s:
+        for n in tri:
+            g = ref.geometry()[n]
+            O = list(g.O)
+            c, inertia, box = s.transform_polyhedron(n, O, scale, angle, offset, O, ref.inertia(n))
+            got = s.geo_fetch(n)
+            ref.transform_polyhedron(n, O, scale, angle, offset)
+            want = ref.surface(n)
+            moved = ref.geometry()[n]
+            for k in ("v", "Nf", "Ne", "Nv"):
+                assert np.array_equal(got[k], want[k]), (n, k)
+            assert np.array_equal(c, np.array(list(moved.O))), n
+            assert np.array_equal(inertia, ref.inertia(n)), n
+            assert np.array_equal(box, _rows(moved.box)), n
+
+
+@pytest.mark.parametrize("motion", ["rotate", "scale"])
+def test_transformed_surface_stays_on_device(tmp_path, motion):
+    """Bodies moved on the device and listed again without surface arrays
+    (the drop-in program's device motion) map the nodes and fill the ghost
+    nodes as a case given the reference's moved bodies.  The anisotropic
+    scale grows the node boxes past the ghost lists, so the list takes a new
+    layout, which brings the kept surfaces along."""
+    scale, angle, offset = MOTIONS[motion]
+    ref = _load(tmp_path, "contact_spheres", 0)
+    with _device(ref) as s:
+        for n, g in enumerate(ref.geometry()):
+            if g.faceN > 0:
+                O = list(g.O)
+                s.transform_polyhedron(n, O, scale, angle, offset, O, ref.inertia(n))
+                ref.transform_polyhedron(n, O, scale, angle, offset)
+        moved = ref.geometry()
+        kept = []
+        for g in moved:
+            p = abi.copy_struct(g, abi.Polyhedron)
+            if p.faceN > 0:
+                p.f, p.Nf, p.e, p.Ne, p.v, p.Nv = None, None, None, None, None, None
+            kept.append(p)
+        s.geo_upload(kept)
+        s.compute_geometric_field()
+        s.treat_ib(abi.TO)
+        got = s.download()
+        for n, g in enumerate(moved):
+            if g.faceN > 0:
+                surf, want = s.geo_fetch(n), ref.surface(n)
+                for k in want:
+                    assert np.array_equal(surf[k], want[k]), (n, k)
+    with _device(ref) as s:
+        s.compute_geometric_field()
+        s.treat_ib(abi.TO)
+        want = s.download()
+    for f in ("did", "fid", "lid", "gst"):
+        assert np.array_equal(got[f], want[f]), f
+    assert np.array_equal(got["U"], want["U"])
+
+
+def test_transform_rejects_analytical_and_missing_bodies(tmp_path):
+    ref = _load(tmp_path, "contact_spheres", 0)
+    sphere = [n for n, g in enumerate(ref.geometry()) if g.faceN <= 0][0]
+    with _device(ref) as s:
+        one = [1.0, 1.0, 1.0]
+        for n in (sphere, len(ref.geometry()), -1):
+            with pytest.raises(abi.AcfdError):
+                s.transform_polyhedron(n, [0.0] * 3, one, [0.0] * 3, [0.0] * 3, [0.0] * 3, np.eye(3))
