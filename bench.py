@@ -72,18 +72,64 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region: NVML polled from a thread every 5 ms when it answers (a timed
+    region of ~0.1 s still gets tens of samples), else nvidia-smi every
+    100 ms.  Read-only: no GPU setting is touched."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                   "hw_thermal_slowdown": 0x40}
+    PERIOD_S = 0.005
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
         self.lines = []
+        self.nvml = None
+        self.samples = []  # NVML: (sm MHz, max sm MHz, reason bits)
+        self.stop = threading.Event()
+        self.thread = None
+
+    def _start_nvml(self) -> bool:
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+        except Exception:
+            return False
+        try:
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+            smax = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            first = (float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)), smax, int(reasons(h)))
+        except Exception:
+            try:
+                pynvml.nvmlShutdown()
+            except Exception:
+                pass
+            return False
+        self.nvml = (pynvml, h, reasons, smax)
+        self.samples.append(first)
+        self.thread = threading.Thread(target=self._poll, daemon=True)
+        self.thread.start()
+        return True
+
+    def _poll(self):
+        pynvml, h, reasons, smax = self.nvml
+        while not self.stop.wait(self.PERIOD_S):
+            try:
+                self.samples.append((float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)), smax,
+                                     int(reasons(h))))
+            except Exception:
+                return
 
     def __enter__(self):
+        if self._start_nvml():
+            return self
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
@@ -99,6 +145,13 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        if self.nvml:
+            self.stop.set()
+            self.thread.join(timeout=2)
+            try:
+                self.nvml[0].nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -108,6 +161,13 @@ class ClockSampler:
 
     def summary(self):
         sm, smax, reasons = [], None, set()
+        if self.nvml:
+            for mhz, mx, bits in list(self.samples):
+                sm.append(mhz)
+                smax = mx
+                reasons.update(nm for nm, b in self.REASON_BITS.items() if bits & b)
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                    "reasons": sorted(reasons), "samples": len(sm), "source": "nvml"}
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.lines:
             f = [x.strip() for x in line.split(",")]
@@ -122,7 +182,7 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
 def fp64_peak_tflops(torch, dtype=None):

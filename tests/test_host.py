@@ -135,3 +135,69 @@ def test_contact_case_has_touching_spheres(tmp_path):
     ref.load(path)
     lists = ref.collision_scan()
     assert [sorted(g for g, _ in c) for c in lists] == [[2, 3], [1, 3], [1, 2]]
+
+
+def _bench():
+    import importlib.util
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    spec = importlib.util.spec_from_file_location("acfd_bench", os.path.join(root, "bench.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+class _FakeNvml:
+    """The NVML calls the clock sampler makes, answering like a GPU held at
+    1965 MHz under its power cap."""
+    NVML_CLOCK_SM = 1
+
+    def __init__(self, fail_init=False):
+        self.fail_init = fail_init
+        self.calls = 0
+        self.shut = False
+
+    def nvmlInit(self):
+        if self.fail_init:
+            raise RuntimeError("no NVML")
+
+    def nvmlShutdown(self):
+        self.shut = True
+
+    def nvmlDeviceGetHandleByIndex(self, i):
+        return ("gpu", i)
+
+    def nvmlDeviceGetMaxClockInfo(self, h, clock):
+        return 1965
+
+    def nvmlDeviceGetClockInfo(self, h, clock):
+        self.calls += 1
+        return 1965 if self.calls % 4 else 1950
+
+    def nvmlDeviceGetCurrentClocksEventReasons(self, h):
+        return 0x4 | 0x1  # power cap (and the idle bit, which is not reported)
+
+
+def test_clock_sampler_polls_nvml_during_a_short_region(monkeypatch):
+    import sys
+    import time
+    bench = _bench()
+    fake = _FakeNvml()
+    monkeypatch.setitem(sys.modules, "pynvml", fake)
+    with bench.ClockSampler(0) as clk:
+        time.sleep(0.1)
+    got = clk.summary()
+    assert got["source"] == "nvml" and fake.shut
+    assert got["samples"] >= 5
+    assert got["sm_mhz"] == 1965.0 and got["sm_max_mhz"] == 1965.0
+    assert got["reasons"] == ["sw_power_cap"]
+
+
+def test_clock_sampler_without_nvml_falls_back_quietly(monkeypatch):
+    import sys
+    bench = _bench()
+    monkeypatch.setitem(sys.modules, "pynvml", _FakeNvml(fail_init=True))
+    monkeypatch.setenv("PATH", "/nonexistent")
+    with bench.ClockSampler(0) as clk:
+        pass
+    got = clk.summary()
+    assert got["source"] == "nvidia-smi" and got["samples"] == 0 and got["sm_mhz"] is None
