@@ -114,9 +114,9 @@ struct PlaneTile {
     int WX, NR;    // tile: nodes updated along x and rows of the row axis
     int TR;        // consumer threads per row (WX; WX + 1 interfaces on X sweeps)
     int ntx, ntc;  // tiles along x and along the rows
-    int nseg;      // X kernel: segments along the march axis
+    int nseg;      // segments of each line (with shares: the chunks of the chunk-major plane order)
     int nblk;      // blocks of a launch: tiles x segments, or (Y/Z, share) equal shares of all tiles' planes
-    int share;     // Y/Z kernel: 1 = a block marches an equal share of the tiles' planes
+    int share;     // Y/Z kernel: 1 = a block marches an equal share of the tiles' planes, chunk-major
     int BXp, BC;   // plane box: x extent (even, covers the x halo) and rows with halo
     int ncw;       // consumer warps (the producer is warp ncw)
     int swap;      // Y/Z kernel: 1 = a Z sweep run with axes 1 and 2 exchanged
