@@ -2,7 +2,8 @@
  * acfd_oracle_ib.c -- TEST INFRASTRUCTURE ONLY (the parity checker).
  *
  * CPU restatement of the immersed-boundary node mapping and ghost-node
- * reconstruction of ArtraCFD (immersed_boundary.c, computational_geometry.c).
+ * reconstruction of ArtraCFD (immersed_boundary.c, computational_geometry.c)
+ * and of the surface motion of a triangulated body (TransformPolyhedron).
  * Same evaluation order as the reference; build with -ffp-contract=off.
  */
 #include "acfd_oracle.h"
@@ -608,4 +609,93 @@ void orc_compute_geometric_field(acfd_node_t *node, const acfd_partition_t *part
             }
         }
     }
+}
+
+/* TransformPolyhedron (computational_geometry.c:162-208, with TransformVertex,
+ * TransformNormal and TransformInertia :209-261): the surface of one body
+ * moved about the reference point O (shift to O, scale, rotate about x, then
+ * y, then z, offset, shift back), its normals rotated, its inertia tensor
+ * restated on the rotated axes, its box rebuilt from FLT_MAX / FLT_MIN over
+ * the vertices and then the centroid, vertex by vertex. */
+static void orc_move_point(const double O[3], const double scale[3], const double R[3][3],
+        const double offset[3], double p[3])
+{
+    double t[3];
+    for (int s = 0; s < 3; ++s) {
+        t[s] = p[s] - O[s];
+    }
+    for (int s = 0; s < 3; ++s) {
+        t[s] = t[s] * scale[s];
+    }
+    for (int s = 0; s < 3; ++s) {
+        p[s] = dot3(R[s], t);
+    }
+    for (int s = 0; s < 3; ++s) {
+        p[s] = p[s] + offset[s] + O[s];
+    }
+}
+
+static void orc_grow_box(double box[6], const double p[3])
+{
+    for (int s = 0; s < 3; ++s) {
+        box[2 * s] = (box[2 * s] < p[s]) ? box[2 * s] : p[s];
+        box[2 * s + 1] = (box[2 * s + 1] > p[s]) ? box[2 * s + 1] : p[s];
+    }
+}
+
+void orc_transform_polyhedron(const double O[3], const double scale[3], const double angle[3],
+        const double offset[3], int vertN, int faceN, int edgeN, double *v, double *Nf, double *Ne,
+        double *Nv, double centroid[3], double inertia[9], double box[6])
+{
+    const double Sx = sin(angle[0]), Sy = sin(angle[1]), Sz = sin(angle[2]);
+    const double Cx = cos(angle[0]), Cy = cos(angle[1]), Cz = cos(angle[2]);
+    const double R[3][3] = {
+        {Cy * Cz, -Cx * Sz + Sx * Sy * Cz, Sx * Sz + Cx * Sy * Cz},
+        {Cy * Sz, Cx * Cz + Sx * Sy * Sz, -Sx * Cz + Cx * Sy * Sz},
+        {-Sy, Sx * Cy, Cx * Cy}};
+    const double Oref[3] = {O[0], O[1], O[2]};
+    for (int s = 0; s < 3; ++s) {
+        box[2 * s] = FLT_MAX;
+        box[2 * s + 1] = FLT_MIN;
+    }
+    for (int n = 0; n < vertN; ++n) {
+        orc_move_point(Oref, scale, R, offset, v + 3 * n);
+        orc_grow_box(box, v + 3 * n);
+    }
+    double *normals[3] = {Nf, Ne, Nv};
+    const int counts[3] = {faceN, edgeN, vertN};
+    for (int a = 0; a < 3; ++a) {
+        for (int n = 0; n < counts[a]; ++n) {
+            double *N = normals[a] + 3 * n;
+            const double t[3] = {N[0], N[1], N[2]};
+            for (int s = 0; s < 3; ++s) {
+                N[s] = dot3(R[s], t);
+            }
+        }
+    }
+    /* moments about the axes xx, yy, zz, xy, yz, zx of the rotated frame */
+    const double h = 1.0 / sqrt(2.0);
+    const double axes[6][3] = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 1.0},
+        {h, h, 0.0}, {0.0, h, h}, {h, 0.0, h}};
+    double m[6];
+    for (int q = 0; q < 6; ++q) {
+        double a[3];
+        for (int s = 0; s < 3; ++s) {
+            const double col[3] = {R[0][s], R[1][s], R[2][s]};
+            a[s] = dot3(col, axes[q]);
+        }
+        m[q] = inertia[0] * a[0] * a[0] + inertia[4] * a[1] * a[1] + inertia[8] * a[2] * a[2] +
+            2.0 * inertia[1] * a[0] * a[1] + 2.0 * inertia[5] * a[1] * a[2] + 2.0 * inertia[6] * a[2] * a[0];
+    }
+    inertia[0] = m[0];
+    inertia[1] = -m[3];
+    inertia[2] = -m[5];
+    inertia[3] = -m[3];
+    inertia[4] = m[1];
+    inertia[5] = -m[4];
+    inertia[6] = -m[5];
+    inertia[7] = -m[4];
+    inertia[8] = m[2];
+    orc_move_point(Oref, scale, R, offset, centroid);
+    orc_grow_box(box, centroid);
 }

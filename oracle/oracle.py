@@ -65,6 +65,7 @@ class Oracle:
             "orc_compute_geometric_field": (None, [_vp, _PP, _MP, _GP, i]),
             "orc_treat_ib": (None, [i, _vp, _PP, _MP, _GP, i]),
             "orc_point_in_polyhedron": (i, [_dp, _GP, _ip]),
+            "orc_transform_polyhedron": (None, [_dp, _dp, _dp, _dp, i, i, i, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
             "orc_set_node_number": (None, [_PP, _MP]),
             "orc_partition_domain": (None, [_PP]),
         }
@@ -126,6 +127,19 @@ class Oracle:
     def treat_ib(self, node, part, model, tn, geo):
         g, n = _geo(geo)
         self.lib.orc_treat_ib(tn, _ptr(node), ctypes.byref(part), ctypes.byref(model), g, n)
+
+
+    def transform_polyhedron(self, O, scale, angle, offset, surface, centroid, inertia):
+        """TransformPolyhedron on copies: returns (surface dict of v, Nf, Ne,
+        Nv; centroid; inertia (3, 3); box (3, 2))."""
+        vec = lambda a, k: np.ascontiguousarray(np.array(a, dtype=np.float64).reshape(k))
+        surf = {k: np.ascontiguousarray(np.array(surface[k], dtype=np.float64)) for k in ("v", "Nf", "Ne", "Nv")}
+        c, inert, box = vec(centroid, 3).copy(), vec(inertia, 9).copy(), np.zeros(6)
+        p = lambda a: a.ctypes.data_as(_dp)
+        self.lib.orc_transform_polyhedron(p(vec(O, 3)), p(vec(scale, 3)), p(vec(angle, 3)), p(vec(offset, 3)),
+                                          len(surf["v"]), len(surf["Nf"]), len(surf["Ne"]),
+                                          *[p(surf[k]) for k in ("v", "Nf", "Ne", "Nv")], p(c), p(inert), p(box))
+        return surf, c, inert.reshape(3, 3), box.reshape(3, 2)
 
 
 def _geo(geo):

@@ -112,3 +112,11 @@ def pin_mask(part) -> np.ndarray:
     ns = np.array(part.ns)
     mask[ns[0, 2, 0]:ns[0, 2, 1], ns[0, 1, 0]:ns[0, 1, 1], ns[0, 0, 0]:ns[0, 0, 1]] = True
     return mask.ravel()
+
+
+# rigid motions of a triangulated body (scale, angle, offset) for the
+# TransformPolyhedron parity tests: a rotation with a shift, an anisotropic
+# scale with a small rotation, a pure shift towards negative coordinates
+MOTIONS = {"rotate": ((1.0, 1.0, 1.0), (0.3, -0.2, 0.7), (0.01, -0.02, 0.005)),
+           "scale": ((1.5, 0.75, 2.0), (1e-3, 2e-3, -5e-4), (0.0, 0.0, 0.0)),
+           "shift": ((1.0, 1.0, 1.0), (0.0, 0.0, 0.0), (-0.5, -0.5, -0.5))}

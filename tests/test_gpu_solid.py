@@ -119,9 +119,7 @@ def test_moved_bodies_update_in_place(tmp_path):
     assert not np.array_equal(np.array([g.O[0] for g in before_copy]), np.array([g.O[0] for g in after]))
 
 
-MOTIONS = {"rotate": ((1.0, 1.0, 1.0), (0.3, -0.2, 0.7), (0.01, -0.02, 0.005)),
-           "scale": ((1.5, 0.75, 2.0), (1e-3, 2e-3, -5e-4), (0.0, 0.0, 0.0)),
-           "shift": ((1.0, 1.0, 1.0), (0.0, 0.0, 0.0), (-0.5, -0.5, -0.5))}
+MOTIONS = cases.MOTIONS
 
 
 def _rows(box):

@@ -71,6 +71,35 @@ def test_per_point_functions_match_reference():
         assert np.array_equal(orc.weno3(F[:3]), ref.weno3(F[:3]))
 
 
+@pytest.mark.skipif(not reference_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("motion", ["rotate", "scale", "shift"])
+def test_oracle_transform_polyhedron_matches_reference(tmp_path, motion):
+    """The restated TransformPolyhedron against the reference's on every
+    triangulated body of the contact case: surface, centroid, inertia tensor
+    and box bitwise."""
+    import cases
+    scale, angle, offset = cases.MOTIONS[motion]
+    spec = cases.contact_spheres()
+    spec.stepN = 1
+    path = str(tmp_path / "case")
+    spec.write(path)
+    ref = Reference()
+    ref.load(path)
+    orc = Oracle()
+    bodies = [n for n, g in enumerate(ref.geometry()) if g.faceN > 0]
+    assert bodies
+    for n in bodies:
+        O = list(ref.geometry()[n].O)
+        surf, c, inertia, box = orc.transform_polyhedron(O, scale, angle, offset, ref.surface(n), O, ref.inertia(n))
+        ref.transform_polyhedron(n, O, scale, angle, offset)
+        want, moved = ref.surface(n), ref.geometry()[n]
+        for k in want:
+            assert np.array_equal(surf[k], want[k]), (n, k)
+        assert np.array_equal(c, np.array(list(moved.O)))
+        assert np.array_equal(inertia, ref.inertia(n))
+        assert np.array_equal(box, np.array([list(b) for b in moved.box]))
+
+
 def _sod_exact_plateaus():
     # exact Riemann solution of the Sod problem (gamma = 1.4)
     return 0.42632, 0.26557
