@@ -255,6 +255,14 @@ void orc_weno3(const double F[3][5], double Fhat[5])
     }
 }
 
+/* the left and right eigenvectors of direction s at the averaged state Uo
+ * (rows of L, columns of R; EigenvectorL / EigenvectorR, cfd_commons.c:149-246) */
+void orc_eigenvectors(int s, double gamma, const double Uo[6], double L[5][5], double R[5][5])
+{
+    left_eigenvectors(s, gamma, Uo, L);
+    right_eigenvectors(s, Uo, R);
+}
+
 /* ------------------------------------------------------------------------
  * convective numerical flux at i+1/2: convective_flux.c:48-124
  * Ust holds U at the stencil points sL..sR along s (6 points for WENO5,

@@ -22,6 +22,7 @@ extern "C" {
 /* per-point functions */
 void orc_symmetric_average(int averager, double gamma, const double UL[5],
         const double UR[5], double Uo[6]);
+void orc_eigenvectors(int s, double gamma, const double Uo[6], double L[5][5], double R[5][5]);
 void orc_weno5(const double F[5][5], double Fhat[5]);
 void orc_weno3(const double F[3][5], double Fhat[5]);
 void orc_fhat_stencil(const acfd_model_t *model, int s, const double Ust[6][5], double Fhat[5]);

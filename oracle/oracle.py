@@ -50,6 +50,7 @@ class Oracle:
         d, i = ctypes.c_double, ctypes.c_int
         sig = {
             "orc_symmetric_average": (None, [i, d, _dp, _dp, _dp]),
+            "orc_eigenvectors": (None, [i, d, _dp, _dp, _dp]),
             "orc_weno5": (None, [_vp, _dp]),
             "orc_weno3": (None, [_vp, _dp]),
             "orc_fhat_stencil": (None, [_MP, i, _vp, _dp]),
@@ -81,6 +82,14 @@ class Oracle:
         out = np.zeros(5)
         self.lib.orc_weno5(_ptr(F), out.ctypes.data_as(_dp))
         return out
+
+    def eigenvectors(self, s, gamma, Uo):
+        """(L, R) of direction s at the averaged state Uo (u, v, w, h_T, c
+        after the unused first entry)."""
+        Uo = np.ascontiguousarray(np.array(Uo, dtype=np.float64).reshape(6))
+        L, R = np.zeros((5, 5)), np.zeros((5, 5))
+        self.lib.orc_eigenvectors(s, gamma, Uo.ctypes.data_as(_dp), L.ctypes.data_as(_dp), R.ctypes.data_as(_dp))
+        return L, R
 
     def weno3(self, F: np.ndarray) -> np.ndarray:
         F = np.ascontiguousarray(F, dtype=np.float64).reshape(3, 5)
@@ -182,6 +191,7 @@ class Reference:
             "ref_evolve_solid": (None, [d, d]),
             "ref_integrate_surface_force": (None, [_dp]),
             "ref_collision_scan": (i, [i, _ip, _ip]),
+            "ref_eigenvectors": (None, [i, ctypes.c_double, _dp, _dp, _dp]),
             "ref_transform_polyhedron": (None, [i, _dp, _dp, _dp, _dp]),
             "ref_get_inertia": (None, [i, _dp]),
             "ref_step": (d, []),
@@ -286,6 +296,12 @@ class Reference:
             c = self.lib.ref_collision_scan(p, gid.ctypes.data_as(_ip), N.ctypes.data_as(_ip))
             res.append([(int(gid[q]), tuple(int(v) for v in N[3 * q:3 * q + 3])) for q in range(c)])
         return res
+
+    def eigenvectors(self, s, gamma, Uo):
+        Uo = np.ascontiguousarray(np.array(Uo, dtype=np.float64).reshape(6))
+        L, R = np.zeros((5, 5)), np.zeros((5, 5))
+        self.lib.ref_eigenvectors(s, gamma, Uo.ctypes.data_as(_dp), L.ctypes.data_as(_dp), R.ctypes.data_as(_dp))
+        return L, R
 
     def transform_polyhedron(self, n, O, scale, angle, offset) -> None:
         args = [np.ascontiguousarray(np.array(a, dtype=np.float64).reshape(3)) for a in (O, scale, angle, offset)]

@@ -228,6 +228,13 @@ void ref_integrate_surface_force(double *out)
     }
 }
 
+/* the reference's EigenvectorL / EigenvectorR (cfd_commons.c:149-246) */
+void ref_eigenvectors(int s, double gamma, const double Uo[6], double L[25], double R[25])
+{
+    EigenvectorL(s, gamma, Uo, (Real (*)[DIMU])L);
+    EigenvectorR(s, Uo, (Real (*)[DIMU])R);
+}
+
 /* TransformPolyhedron (computational_geometry.c:162-208) of body n, the
  * reference point O given apart from the body's centroid (ApplyMotion passes
  * the centroid itself). */

@@ -100,6 +100,51 @@ def test_oracle_transform_polyhedron_matches_reference(tmp_path, motion):
         assert np.array_equal(box, np.array([list(b) for b in moved.box]))
 
 
+def _roe_states(count, seed):
+    """Roe-averaged interface states of random left/right states drawn from
+    the sensor-training ranges (rho in [0.1, 10], |u_i| <= 2, p in [0.1, 100])."""
+    import ctypes
+    orc = Oracle()
+    rng = np.random.default_rng(seed)
+    gamma = 1.4
+    out = []
+    for _ in range(count):
+        sides = []
+        for _side in range(2):
+            rho, p = rng.uniform(0.1, 10.0), rng.uniform(0.1, 100.0)
+            vel = rng.uniform(-2.0, 2.0, size=3)
+            sides.append(np.array([rho, *(rho * vel), p / (gamma - 1.0) + 0.5 * rho * vel @ vel]))
+        Uo = np.zeros(6)
+        dp = ctypes.POINTER(ctypes.c_double)
+        orc.lib.orc_symmetric_average(1, gamma, sides[0].ctypes.data_as(dp), sides[1].ctypes.data_as(dp),
+                                      Uo.ctypes.data_as(dp))
+        out.append(Uo)
+    return gamma, out
+
+
+def test_eigenvectors_are_inverse_to_each_other():
+    """Known answer: the left eigenvectors are the inverse of the right ones,
+    L R = I, in every direction, to the rounding bound of a 5x5 product."""
+    orc = Oracle()
+    gamma, states = _roe_states(300, 3)
+    eps = np.finfo(np.float64).eps
+    for Uo in states:
+        for s in range(3):
+            L, R = orc.eigenvectors(s, gamma, Uo)
+            bound = 10 * eps * (np.abs(L) @ np.abs(R)) + 1e-300
+            assert np.all(np.abs(L @ R - np.eye(5)) <= bound), (s, Uo)
+
+
+@pytest.mark.skipif(not reference_available(), reason="oracle/_ref not built")
+def test_oracle_eigenvectors_match_reference():
+    orc, ref = Oracle(), Reference()
+    gamma, states = _roe_states(100, 5)
+    for Uo in states:
+        for s in range(3):
+            for a, b in zip(orc.eigenvectors(s, gamma, Uo), ref.eigenvectors(s, gamma, Uo)):
+                assert np.array_equal(a, b), s
+
+
 def _sod_exact_plateaus():
     # exact Riemann solution of the Sod problem (gamma = 1.4)
     return 0.42632, 0.26557
