@@ -201,3 +201,49 @@ def test_clock_sampler_without_nvml_falls_back_quietly(monkeypatch):
         pass
     got = clk.summary()
     assert got["source"] == "nvidia-smi" and got["samples"] == 0 and got["sm_mhz"] is None
+
+
+_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+_DROPIN = os.path.join(_ROOT, "artracfd_b200", "shim", "_build", "artracfd_gpu")
+_REFBIN = os.path.join(_ROOT, "oracle", "_ref", "artracfd")
+
+
+def _ensight(path):
+    raw = open(path, "rb").read()
+    return np.frombuffer(raw[80 + 80 + 4 + 80:], dtype=np.float32)
+
+
+@pytest.mark.skipif(not (os.path.exists(_DROPIN) and os.path.exists(_REFBIN)), reason="programs not built")
+def test_dropin_serial_mode_writes_the_reference_files(tmp_path):
+    """The drop-in program in `-m serial` mode is the reference program: the
+    renamed Solve / EvolveFluidDynamics / TreatBoundary route to the
+    reference's own functions (no device is touched)."""
+    import subprocess
+    spec = configs.sod(m=(32, 4, 4), stepN=4)
+    outs = []
+    for name, binary in (("ref", _REFBIN), ("dropin", _DROPIN)):
+        d = str(tmp_path / name)
+        spec.write(d)
+        r = subprocess.run([binary, "-m", "serial"], cwd=d, capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stderr[-2000:]
+        outs.append(d)
+    names = sorted(f for f in os.listdir(outs[0]) if f.startswith("field0") and not f.endswith(".case"))
+    assert names
+    for f in names:
+        assert np.array_equal(_ensight(os.path.join(outs[0], f)), _ensight(os.path.join(outs[1], f))), f
+
+
+@pytest.mark.skipif(not os.path.exists(_DROPIN), reason="drop-in program not built")
+def test_dropin_gpu_mode_fails_loudly_without_a_device(tmp_path):
+    """No CPU fallback: `-m gpu` on a machine without a usable GPU stops with
+    the library's error instead of computing on the host."""
+    import subprocess
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    d = str(tmp_path / "case")
+    configs.sod(m=(32, 4, 4), stepN=2).write(d)
+    r = subprocess.run([_DROPIN, "-m", "gpu"], cwd=d, capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0
+    assert "acfd_init failed" in r.stderr
+    assert not any(f.startswith("field00001") for f in os.listdir(d))
