@@ -247,3 +247,28 @@ def test_dropin_gpu_mode_fails_loudly_without_a_device(tmp_path):
     assert r.returncode != 0
     assert "acfd_init failed" in r.stderr
     assert not any(f.startswith("field00001") for f in os.listdir(d))
+
+
+def _header_prototypes():
+    """name -> parameter count of every function declared in include/acfd.h."""
+    header = open(os.path.join(ROOT, "include", "acfd.h")).read()
+    header = re.sub(r"/\*.*?\*/", "", header, flags=re.S)
+    out = {}
+    for m in re.finditer(r"^(?:int|void|double|const char\s*\*)\s*\**\s*(acfd_\w+)\s*\(([^)]*)\)\s*;", header,
+                         re.M | re.S):
+        params = " ".join(m.group(2).split())
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_ctypes_binding_matches_every_prototype():
+    """The ctypes binding declares every function of the header with the
+    header's number of parameters (a drifted binding would pass wrong
+    arguments without any error)."""
+    protos = _header_prototypes()
+    assert len(protos) >= 40
+    lib = load_library()
+    for name, count in protos.items():
+        fn = getattr(lib, name)
+        assert fn.argtypes is not None, name
+        assert len(fn.argtypes) == count, (name, len(fn.argtypes), count)
