@@ -272,3 +272,21 @@ def test_ctypes_binding_matches_every_prototype():
         fn = getattr(lib, name)
         assert fn.argtypes is not None, name
         assert len(fn.argtypes) == count, (name, len(fn.argtypes), count)
+
+
+@pytest.mark.skipif(not os.path.exists(_DROPIN), reason="drop-in program not built")
+def test_dropin_bad_case_file_stops_before_the_device(tmp_path):
+    """A bad case file (zero cells along x) stops the drop-in program in the
+    reference's own case check (CheckCaseSettingData, case_loader.c:509-544)
+    with its message, before any device work."""
+    import subprocess
+    d = str(tmp_path / "case")
+    configs.sod(m=(32, 4, 4), stepN=2).write(d)
+    path = os.path.join(d, "artracfd.case")
+    text = open(path).read()
+    assert "\n32, 4, 4\n" in text
+    open(path, "w").write(text.replace("\n32, 4, 4\n", "\n0, 4, 4\n", 1))
+    r = subprocess.run([_DROPIN, "-m", "gpu"], cwd=d, capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0
+    assert "mesh number should be positive" in r.stderr
+    assert "Solving" not in r.stdout
