@@ -699,3 +699,101 @@ void orc_transform_polyhedron(const double O[3], const double scale[3], const do
     orc_move_point(Oref, scale, R, offset, centroid);
     orc_grow_box(box, centroid);
 }
+
+/* IntegrateSurfaceForce (solid_dynamics.c:50-171): for every body with
+ * state <= 0, the pressure force, shear force and torque summed over its
+ * ghost nodes of layer 2 in node order (k, j, i), then scaled by -area over
+ * its interfacial nodes of layer 2 (zero when the pressure samples are
+ * uniform to FLT_EPSILON^2 of their mean).  force: totN x 9 (Fp, Fv, Tt);
+ * rows of bodies with state > 0 are left as given.  The bodies' V and W are
+ * their velocities at level TO. */
+static void cross3(const double a[3], const double b[3], double c[3])
+{
+    /* cfd_commons.c:424-430 */
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+void orc_integrate_surface_force(const acfd_node_t *node, const acfd_partition_t *part,
+        const acfd_model_t *model, const acfd_polyhedron_t *poly, int totN, double *force)
+{
+    const double percent = (double)(FLT_EPSILON * FLT_EPSILON);
+    for (int n = 0; n < totN; ++n) {
+        const acfd_polyhedron_t *P = poly + n;
+        if (0 < P->state) {
+            continue;
+        }
+        double sumP[3] = {0.0, 0.0, 0.0}, sumV[3] = {0.0, 0.0, 0.0}, sumT[3] = {0.0, 0.0, 0.0};
+        double first = 0.0, shift = 0.0, square = 0.0; /* pressure samples: first, sums of offsets */
+        int lidN = 0, gstN = 0;
+        int box[3][2];
+        body_box(part, P, box);
+        for (int k = box[2][0]; k < box[2][1]; ++k) {
+            for (int j = box[1][0]; j < box[1][1]; ++j) {
+                for (int i = box[0][0]; i < box[0][1]; ++i) {
+                    const acfd_node_t *q = node + nidx(part, k, j, i);
+                    if ((2 == q->lid) && (n + 1 == q->did)) {
+                        ++lidN;
+                    }
+                    if ((2 != q->gst) || (n + 1 != q->did)) {
+                        continue;
+                    }
+                    ++gstN;
+                    double pG[3], pO[3], pI[3], N[3], Uo[6];
+                    node_point(part, k, j, i, pG);
+                    surface_data(pG, q->fid, P, pO, pI, N);
+                    const double r[3] = {pO[0] - P->O[0], pO[1] - P->O[1], pO[2] - P->O[2]};
+                    to_primitive(model->gamma, model->gasR, q->U[0], Uo);
+                    const double Fp[3] = {Uo[4] * N[0], Uo[4] * N[1], Uo[4] * N[2]};
+                    if (1 == gstN) {
+                        first = Uo[4];
+                    }
+                    shift = shift + Uo[4] - first;
+                    square = square + (Uo[4] - first) * (Uo[4] - first);
+                    double Fv[3] = {0.0, 0.0, 0.0};
+                    if ((0.0 < model->refMu) && (0.0 < P->cf)) {
+                        const double T = Uo[5] * model->refT;
+                        const double mu = model->refMu * (1.458e-6 * pow(T, 1.5) / (T + 110.4));
+                        double V[3];
+                        cross3(P->W, r, V);
+                        for (int s = 0; s < 3; ++s) {
+                            V[s] = Uo[1 + s] - (P->V[s] + V[s]);
+                        }
+                        const double Vn = dot3(V, N);
+                        for (int s = 0; s < 3; ++s) {
+                            Fv[s] = mu * (V[s] - Vn * N[s]) / sqrt(dist2(pG, pO));
+                        }
+                    }
+                    const double Fs[3] = {Fp[0] + Fv[0], Fp[1] + Fv[1], Fp[2] + Fv[2]};
+                    double Tt[3];
+                    cross3(r, Fs, Tt);
+                    for (int s = 0; s < 3; ++s) {
+                        sumP[s] = sumP[s] + Fp[s];
+                        sumV[s] = sumV[s] + Fv[s];
+                        sumT[s] = sumT[s] + Tt[s];
+                    }
+                }
+            }
+        }
+        double *out = force + 9 * (size_t)n;
+        if ((0 == lidN) || (0 == gstN)) {
+            /* the reference leaves the zeroed sums */
+            for (int s = 0; s < 9; ++s) {
+                out[s] = (s < 3) ? sumP[s] : ((s < 6) ? sumV[s - 3] : sumT[s - 6]);
+            }
+            continue;
+        }
+        double ds = P->area / lidN;
+        const double variance = (square - shift * shift / gstN) / gstN;
+        const double mean = shift / gstN + first;
+        if (percent * mean * mean > variance) {
+            ds = 0.0;
+        }
+        for (int s = 0; s < 3; ++s) {
+            out[s] = -sumP[s] * ds;
+            out[3 + s] = -sumV[s] * ds;
+            out[6 + s] = -sumT[s] * ds;
+        }
+    }
+}

@@ -66,6 +66,7 @@ class Oracle:
             "orc_compute_geometric_field": (None, [_vp, _PP, _MP, _GP, i]),
             "orc_treat_ib": (None, [i, _vp, _PP, _MP, _GP, i]),
             "orc_point_in_polyhedron": (i, [_dp, _GP, _ip]),
+            "orc_integrate_surface_force": (None, [_vp, _PP, _MP, _GP, i, _dp]),
             "orc_transform_polyhedron": (None, [_dp, _dp, _dp, _dp, i, i, i, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
             "orc_set_node_number": (None, [_PP, _MP]),
             "orc_partition_domain": (None, [_PP]),
@@ -137,6 +138,15 @@ class Oracle:
         g, n = _geo(geo)
         self.lib.orc_treat_ib(tn, _ptr(node), ctypes.byref(part), ctypes.byref(model), g, n)
 
+
+    def integrate_surface_force(self, node, part, model, geo, force=None):
+        """IntegrateSurfaceForce: (totN, 9) array of Fp, Fv, Tt per body; rows
+        of bodies with state > 0 keep ``force`` (zeros when not given)."""
+        g, n = _geo(geo)
+        out = np.zeros((n, 9)) if force is None else np.array(force, dtype=np.float64).reshape(n, 9)
+        self.lib.orc_integrate_surface_force(_ptr(node), ctypes.byref(part), ctypes.byref(model), g, n,
+                                             out.ctypes.data_as(_dp))
+        return out
 
     def transform_polyhedron(self, O, scale, angle, offset, surface, centroid, inertia):
         """TransformPolyhedron on copies: returns (surface dict of v, Nf, Ne,

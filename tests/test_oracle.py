@@ -100,6 +100,30 @@ def test_oracle_transform_polyhedron_matches_reference(tmp_path, motion):
         assert np.array_equal(box, np.array([list(b) for b in moved.box]))
 
 
+@pytest.mark.skipif(not reference_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("name", ["spheres48", "contact_spheres", "contact_spheres_inviscid"])
+def test_oracle_surface_force_matches_reference(tmp_path, name):
+    """The restated IntegrateSurfaceForce against the reference's on the
+    state the reference reaches after three of its own steps (moving spheres
+    in a crossflow, viscous and inviscid, some resting on one another):
+    pressure force, shear force and torque of every body, bitwise."""
+    import cases
+    spec = dict(cases.SMALL, **cases.SOLID)[name]()
+    spec.stepN = 4
+    path = str(tmp_path / name)
+    spec.write(path)
+    ref = Reference()
+    ref.load(path)
+    for _ in range(3):
+        assert ref.lib.ref_step() > 0.0
+    node, part, model, geo = ref.nodes(), ref.partition(), ref.model(), ref.geometry()
+    got = Oracle().integrate_surface_force(node, part, model, geo)
+    want = ref.integrate_surface_force()
+    moving = [n for n, g in enumerate(geo) if g.state <= 0]
+    assert moving and np.any(want[moving] != 0.0)
+    assert np.array_equal(got[moving], want[moving])
+
+
 def _roe_states(count, seed):
     """Roe-averaged interface states of random left/right states drawn from
     the sensor-training ranges (rho in [0.1, 10], |u_i| <= 2, p in [0.1, 100])."""
