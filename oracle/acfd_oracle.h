@@ -53,6 +53,8 @@ void orc_compute_geometric_field(acfd_node_t *node, const acfd_partition_t *part
 void orc_treat_ib(int tn, acfd_node_t *node, const acfd_partition_t *part,
         const acfd_model_t *model, const acfd_polyhedron_t *poly, int totN);
 int orc_point_in_polyhedron(const double p[3], const acfd_polyhedron_t *poly, int *fid);
+int orc_collision_scan(const acfd_node_t *node, const acfd_partition_t *part, const acfd_polyhedron_t *poly,
+        int totN, int p, int *gid, int *N);
 void orc_integrate_surface_force(const acfd_node_t *node, const acfd_partition_t *part,
         const acfd_model_t *model, const acfd_polyhedron_t *poly, int totN, double *force);
 void orc_transform_polyhedron(const double O[3], const double scale[3], const double angle[3],

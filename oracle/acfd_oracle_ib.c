@@ -797,3 +797,56 @@ void orc_integrate_surface_force(const acfd_node_t *node, const acfd_partition_t
         }
     }
 }
+
+/* The contact list ApplyCollision builds for body p (the node scan of
+ * solid_dynamics.c:242-256 with DetectColState / AddColObject :327-379):
+ * every interfacial node of layer 1 of body p, in node order, looks along
+ * the first pathSep[1] steps of the search path; a node of another body met
+ * on the way adds that body to the list (in the order first met) or adds the
+ * step to its line of impact.  Returns the list length; gid[c] (body ids,
+ * 1 = first body) and N[3c..3c+2] receive the entries.  A stationary body
+ * (state 1) has no list. */
+int orc_collision_scan(const acfd_node_t *node, const acfd_partition_t *part, const acfd_polyhedron_t *poly,
+        int totN, int p, int *gid, int *N)
+{
+    if ((p < 0) || (p >= totN) || (1 == poly[p].state)) {
+        return 0;
+    }
+    int count = 0;
+    int box[3][2];
+    body_box(part, poly + p, box);
+    for (int k = box[2][0]; k < box[2][1]; ++k) {
+        for (int j = box[1][0]; j < box[1][1]; ++j) {
+            for (int i = box[0][0]; i < box[0][1]; ++i) {
+                const acfd_node_t *q = node + nidx(part, k, j, i);
+                if ((1 != q->lid) || (p + 1 != q->did)) {
+                    continue;
+                }
+                for (int m = 0; m < part->pathSep[1]; ++m) {
+                    const int *step = part->path[m];
+                    const int kh = k + step[2], jh = j + step[1], ih = i + step[0];
+                    if (!in_pin(part, kh, jh, ih)) {
+                        continue;
+                    }
+                    const int did = node[nidx(part, kh, jh, ih)].did;
+                    if ((0 == did) || (p + 1 == did)) {
+                        continue;
+                    }
+                    int c = 0;
+                    while ((c < count) && (gid[c] != did)) {
+                        ++c;
+                    }
+                    if (c == count) {
+                        gid[c] = did;
+                        N[3 * c] = N[3 * c + 1] = N[3 * c + 2] = 0;
+                        ++count;
+                    }
+                    for (int s = 0; s < 3; ++s) {
+                        N[3 * c + s] = N[3 * c + s] + step[s];
+                    }
+                }
+            }
+        }
+    }
+    return count;
+}

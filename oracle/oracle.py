@@ -67,6 +67,7 @@ class Oracle:
             "orc_treat_ib": (None, [i, _vp, _PP, _MP, _GP, i]),
             "orc_point_in_polyhedron": (i, [_dp, _GP, _ip]),
             "orc_integrate_surface_force": (None, [_vp, _PP, _MP, _GP, i, _dp]),
+            "orc_collision_scan": (i, [_vp, _PP, _GP, i, i, _ip, _ip]),
             "orc_transform_polyhedron": (None, [_dp, _dp, _dp, _dp, i, i, i, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
             "orc_set_node_number": (None, [_PP, _MP]),
             "orc_partition_domain": (None, [_PP]),
@@ -147,6 +148,19 @@ class Oracle:
         self.lib.orc_integrate_surface_force(_ptr(node), ctypes.byref(part), ctypes.byref(model), g, n,
                                              out.ctypes.data_as(_dp))
         return out
+
+    def collision_scan(self, node, part, geo):
+        """Contact list of every body: [(body id, line of impact)] in the
+        reference's list order."""
+        g, n = _geo(geo)
+        res = []
+        for p in range(n):
+            gid = np.zeros(max(n, 1), dtype=np.int32)
+            N = np.zeros(3 * max(n, 1), dtype=np.int32)
+            c = self.lib.orc_collision_scan(_ptr(node), ctypes.byref(part), g, n, p, gid.ctypes.data_as(_ip),
+                                            N.ctypes.data_as(_ip))
+            res.append([(int(gid[q]), tuple(int(v) for v in N[3 * q:3 * q + 3])) for q in range(c)])
+        return res
 
     def transform_polyhedron(self, O, scale, angle, offset, surface, centroid, inertia):
         """TransformPolyhedron on copies: returns (surface dict of v, Nf, Ne,

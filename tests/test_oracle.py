@@ -124,6 +124,27 @@ def test_oracle_surface_force_matches_reference(tmp_path, name):
     assert np.array_equal(got[moving], want[moving])
 
 
+@pytest.mark.skipif(not reference_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("steps", [0, 2])
+def test_oracle_collision_scan_matches_reference(tmp_path, steps):
+    """The restated contact scan against the reference's DetectColState
+    lists on the touching-spheres case: same bodies, same order, same lines
+    of impact."""
+    import cases
+    spec = cases.contact_spheres(viscous=False)
+    spec.stepN = steps + 1
+    path = str(tmp_path / "case")
+    spec.write(path)
+    ref = Reference()
+    ref.load(path)
+    for _ in range(steps):
+        assert ref.lib.ref_step() > 0.0
+    got = Oracle().collision_scan(ref.nodes(), ref.partition(), ref.geometry())
+    want = ref.collision_scan()
+    assert any(want), "the case has no contact"
+    assert got == want
+
+
 def _roe_states(count, seed):
     """Roe-averaged interface states of random left/right states drawn from
     the sensor-training ranges (rho in [0.1, 10], |u_i| <= 2, p in [0.1, 100])."""
