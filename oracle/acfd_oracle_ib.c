@@ -2,8 +2,10 @@
  * acfd_oracle_ib.c -- TEST INFRASTRUCTURE ONLY (the parity checker).
  *
  * CPU restatement of the immersed-boundary node mapping and ghost-node
- * reconstruction of ArtraCFD (immersed_boundary.c, computational_geometry.c)
- * and of the surface motion of a triangulated body (TransformPolyhedron).
+ * reconstruction of ArtraCFD (immersed_boundary.c, computational_geometry.c),
+ * and of the node scans and surface motion of the rigid-body step
+ * (IntegrateSurfaceForce and the contact scan of ApplyCollision,
+ * solid_dynamics.c; TransformPolyhedron, computational_geometry.c).
  * Same evaluation order as the reference; build with -ffp-contract=off.
  */
 #include "acfd_oracle.h"
