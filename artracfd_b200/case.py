@@ -444,3 +444,47 @@ def extruded_cylinder(center_xy, radius, z0, z1, segments=64) -> np.ndarray:
         tris.append(((cx, cy, z0), B0, A0))
         tris.append(((cx, cy, z1), A1, B1))
     return np.array(tris, dtype=np.float32)
+
+
+# ----------------------------------------------------------------------
+# preprocessed bodies
+# ----------------------------------------------------------------------
+
+def load_polyhedra(z, prefix: str = "geo_"):
+    """Body descriptors (abi.Polyhedron) from arrays saved with the given key
+    prefix: ``<prefix>count`` bodies, each with ``scal`` (faceN, edgeN, vertN,
+    state), ``real`` (r, O, V, W, T, cf, box) and, for triangulated bodies,
+    the surface arrays f, Nf, e, Ne, v, Nv of the reference's Polyhedron
+    (commons.h:203-243) after its load-time preprocessing.  Returns
+    (bodies, keep): ``keep`` holds the arrays the descriptors point into and
+    must outlive them."""
+    import ctypes
+    keep = []
+    geo = []
+    if prefix + "count" not in z:
+        return geo, keep
+    for q in range(int(z[prefix + "count"])):
+        p = f"{prefix}{q}_"
+        P = abi.Polyhedron()
+        P.faceN, P.edgeN, P.vertN, P.state = (int(v) for v in z[p + "scal"])
+        real = z[p + "real"]
+        P.r = real[0]
+        for s in range(3):
+            P.O[s] = real[1 + s]
+            P.V[s] = real[4 + s]
+            P.W[s] = real[7 + s]
+        P.T = real[10]
+        P.cf = real[11]
+        for s in range(3):
+            for m in range(2):
+                P.box[s][m] = real[12 + 2 * s + m]
+        if P.faceN > 0:
+            arrs = {}
+            for key, ct in (("f", ctypes.c_int), ("Nf", ctypes.c_double), ("e", ctypes.c_int),
+                            ("Ne", ctypes.c_double), ("v", ctypes.c_double), ("Nv", ctypes.c_double)):
+                a = np.ascontiguousarray(z[p + key], dtype=np.int32 if ct is ctypes.c_int else np.float64)
+                arrs[key] = a
+                setattr(P, key, a.ctypes.data_as(ctypes.POINTER(ct)))
+            keep.append(arrs)
+        geo.append(P)
+    return geo, keep

@@ -43,23 +43,27 @@ FLOP_PER_NODE_STAGE_VISCOUS = 1535.0  # ComputeFhat 1380 + ComputeFvhat 115 + LU
 STAGE_BYTES = (80.0, 120.0, 120.0)
 
 
-def profiled_traffic(mode: str, axes=(0, 1, 2)):
-    """DRAM bytes per RK-stage-2 launch from the committed ncu summary of the
-    stage kernels (mean over the captured launches of the given sweep axes),
-    or None."""
-    name = {"fp64": "stage_sweep_fp64_tgv128.md", "fp32": "stage_sweep_fp32_tgv128.md",
-            "hybrid": "stage_sweep_hybrid_tgv128.md"}.get(mode)
-    if not name:
-        return None
-    p = os.path.join(ROOT, "profiles", name)
+def profiled_traffic(mode: str, tiles, axes=(0, 1, 2)):
+    """DRAM bytes per RK-stage-2 launch of this form's stage kernels, mean over
+    the given sweep axes, from the committed ncu record profiles/dram_traffic.json
+    (dram__bytes_read.sum + dram__bytes_write.sum of one capture per axis, the
+    stage-kernel variant of each axis recorded beside it).  Returns (bytes,
+    source) or (None, reason) when the record does not hold this form with
+    these variants."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if not os.path.exists(p):
-        return None
-    for line in open(p):
-        if line.startswith("| DRAM traffic per launch (MB)"):
-            vals = [float(c.strip().strip("*")) for c in line.split("|")[2:] if c.strip()]
-            vals = [vals[a] for a in axes if a < len(vals)]
-            return sum(vals) / len(vals) * 1e6 if vals else None
-    return None
+        return None, "no profiles/dram_traffic.json"
+    with open(p) as fh:
+        rec = json.load(fh).get(mode)
+    if not rec:
+        return None, f"no capture of the {mode} form"
+    vals = []
+    for a in axes:
+        ax = rec["axes"].get(str(a))
+        if ax is None or int(tiles[a]) not in [int(v) for v in ax["variants"]]:
+            return None, f"no capture of variant {tiles[a]} on axis {a}"
+        vals.append(float(ax["dram_bytes"]))
+    return sum(vals) / len(vals), rec["source"]
 
 
 def load_peaks():
@@ -368,30 +372,42 @@ def _pin_mask(part):
     return m.ravel()
 
 
-def _accuracy(part, model, node, spec, form, steps, stream):
+def _start(part, model, node, form, stream, geo=None):
+    """A solver of the given form on the case's initial state: the node
+    array uploaded, the bodies (if any) uploaded and mapped onto the nodes
+    (ComputeGeometricField), then TreatBoundary on U[TO] -- the steps of
+    InitializeComputeDomain (initialization.c:38-55)."""
+    from artracfd_b200 import abi
+    s = _solver(part, model, form, stream)
+    s.upload(node)
+    if geo:
+        s.geo_upload(geo)
+        s.compute_geometric_field()
+    s.treat_boundary(abi.TO)
+    return s
+
+
+def _accuracy(part, model, node, spec, form, steps, stream, geo=None):
     """The form against the plain FP64 path on the same initial state and
     the same dt sequence: relative L1 and Linf errors of density, pressure
-    and momentum over the computed nodes after `steps` steps."""
+    and momentum over the computed fluid nodes after `steps` steps."""
     import numpy as np
-    from artracfd_b200 import abi
-    ref = _solver(part, model, "fp64", stream)
-    ref.upload(node)
-    ref.treat_boundary(abi.TO)
+    ref = _start(part, model, node, "fp64", stream, geo)
     dts = []
     for _ in range(steps):
         dt = ref.time_step(spec.cfl)
         ref.evolve(dt, graph=True)
         dts.append(dt)
-    a = ref.download()["U"][:, 0, :].copy()
+    got = ref.download()
+    a = got["U"][:, 0, :].copy()
+    fluid = got["did"] == 0
     ref.close()
-    s = _solver(part, model, form, stream)
-    s.upload(node)
-    s.treat_boundary(abi.TO)
+    s = _start(part, model, node, form, stream, geo)
     for dt in dts:
         s.evolve(dt, graph=True)
     b = s.download()["U"][:, 0, :].copy()
     s.close()
-    pin = _pin_mask(part)
+    pin = _pin_mask(part) & fluid
     a, b = a[pin], b[pin]
     gm1 = model.gamma - 1.0
 
@@ -404,6 +420,62 @@ def _accuracy(part, model, node, spec, form, steps, stream):
         out["l1_" + name] = float(d.sum() / np.abs(fa).sum()) if np.isfinite(d).all() else float("inf")
         out["linf_" + name] = float(d.max() / np.abs(fa).max()) if np.isfinite(d).all() else float("inf")
     return out
+
+
+def _form_block(torch, part, model, node, spec, form, nodes_pin, args, dist, stream, local_rank, geo=None,
+                hbm_peak=None, profile=True):
+    """One arithmetic form on one case: autotuned variants, W warm-up and K
+    device-timed steps (CFL read back + host dt + graph replay each step),
+    and optionally one profiled eager step (mean stage and ghost-fill
+    times)."""
+    s = _start(part, model, node, form, stream, geo)
+    tiles = _tune(s, spec)
+    sec, launches, clk = _timed_steps(torch, s, spec, args.steps, args.warmup, dist, stream, local_rank)
+    out = {"value": job_rate(int(os.environ.get("WORLD_SIZE", "1")), nodes_pin, args.steps, sec),
+           "ms_per_step": sec / args.steps * 1e3, "tiles": tiles, "clocks": clk, "gpu_launches": launches}
+    if profile:
+        st, bc, by = _stage_profile(torch, s, spec, nodes_pin, stream)
+        out["stage_ms"] = {"sweep_mean": st, "ghost_fill_mean": bc}
+        if hbm_peak:
+            out["hbm_frac"] = by / (st / 1e3) / 1e9 / hbm_peak
+        out["_stage_mean_ms"] = st
+    s.close()
+    return out
+
+
+def shock_cylinder_block(torch, args, dist, stream, local_rank):
+    """The learned sensor's own configuration: a Ma 2.81 planar shock over an
+    extruded cylinder, [0,16]x[0,8]x[0,0.0625] at 1024x512x4 cells (1023 x
+    511 x 5 = 2,613,765 computed nodes), inviscid, WENO5/LLF/Roe, RK3, CFL
+    0.5.  The cylinder is the reference's own preprocessed surface
+    (tests/golden/bodies_shock_cylinder.npz, made by make_bodies.py); the
+    initial field follows the case file.  Hybrid and plain FP64 rates, and
+    the hybrid's L1/Linf errors against the plain FP64 path after 100 steps
+    on the same dt sequence."""
+    import numpy as np
+    from artracfd_b200 import configs
+    from artracfd_b200.case import load_polyhedra
+
+    path = os.path.join(ROOT, "tests", "golden", "bodies_shock_cylinder.npz")
+    if not os.path.exists(path):
+        return {"unavailable": "tests/golden/bodies_shock_cylinder.npz missing"}
+    spec = configs.shock_cylinder()
+    part, model = spec.descriptors()
+    z = np.load(path)
+    geo, keep = load_polyhedra(z)
+    node = spec.initial_nodes(part, model)
+    pin = int(np.prod(np.array(part.ns)[0, :, 1] - np.array(part.ns)[0, :, 0]))
+    f64 = _form_block(torch, part, model, node, spec, "fp64", pin, args, dist, stream, local_rank, geo, profile=False)
+    hyb = _form_block(torch, part, model, node, spec, "hybrid", pin, args, dist, stream, local_rank, geo,
+                      profile=False)
+    acc = None
+    if args.sc_accuracy_steps > 0:
+        acc = _accuracy(part, model, node, spec, "hybrid", args.sc_accuracy_steps, stream, geo)
+    del keep
+    return {"workload": "Ma 2.81 shock over an extruded cylinder (256 facets), 1024x512x4 cells "
+                        "(2,613,765 computed nodes), inviscid WENO5/LLF/Roe, RK3, CFL 0.5",
+            "nodes": pin, "hybrid": hyb, "plain_fp64": f64,
+            "speedup_vs_plain_fp64": hyb["value"] / f64["value"], "accuracy": acc}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -426,16 +498,13 @@ def run_ours(args, rank, world, local_rank):
     # the plain FP64 path, timed first (the comparison of the headline)
     plain = None
     if args.mode != "fp64":
-        s = _solver(part, model, "fp64", stream)
-        s.upload(node)
-        s.treat_boundary(abi.TO)
-        tiles64 = _tune(s, spec)
-        sec64, _, clk64 = _timed_steps(torch, s, spec, args.steps, args.warmup, dist, stream, local_rank)
-        st64, bc64, by64 = _stage_profile(torch, s, spec, nodes_pin, stream)
-        s.close()
-        plain = {"value": job_rate(world, nodes_pin, args.steps, sec64), "ms_per_step": sec64 / args.steps * 1e3,
-                 "stage_ms": {"sweep_mean": st64, "ghost_fill_mean": bc64},
-                 "hbm_frac": by64 / (st64 / 1e3) / 1e9 / hbm_peak, "tiles": tiles64, "clocks": clk64}
+        plain = _form_block(torch, part, model, node, spec, "fp64", nodes_pin, args, dist, stream, local_rank,
+                            hbm_peak=hbm_peak)
+    # the FP32-bulk form without the sensor: what the sensor itself adds
+    fp32 = None
+    if args.mode == "hybrid":
+        fp32 = _form_block(torch, part, model, node, spec, "fp32", nodes_pin, args, dist, stream, local_rank,
+                           hbm_peak=hbm_peak)
 
     # the form named by --mode (default: the learned-sensor hybrid)
     s = _solver(part, model, args.mode, stream)
@@ -469,11 +538,14 @@ def run_ours(args, rank, world, local_rank):
     dom_share = sum(dom["ms"]) / sum(sum(d["ms"]) for d in fams.values())
     # ncu traffic of RK stage 2 (120 B algorithmic per node), scaled to the
     # mean RK-stage mix of one step (106.7 B per node)
-    tr2 = profiled_traffic(args.mode, tuple(sorted(dom["axes"])))
+    tr2, tr_src = profiled_traffic(args.mode, tiles, tuple(sorted(dom["axes"])))
     traffic = tr2 * (dom_bytes / (STAGE_BYTES[1] * nodes_pin)) if tr2 else None
     flop_rate = FLOP_PER_NODE_STAGE_VISCOUS * nodes_pin / (stage_mean / 1e3) / 1e12
     fp64_peak = fp64_peak_tflops(torch) if rank == 0 else None
     fp32_peak = fp64_peak_tflops(torch, torch.float32) if rank == 0 and args.mode in ("fp32", "hybrid") else None
+    # the FP64 pipe fraction belongs to the plain FP64 path's own stage time
+    st64 = plain["_stage_mean_ms"] if plain else stage_mean
+    flop_rate64 = FLOP_PER_NODE_STAGE_VISCOUS * nodes_pin / (st64 / 1e3) / 1e12
     # e2e through the C ABI with host buffers: upload of the host node array,
     # K steps (CFL read back each step), download of the result
     host = node.copy()
@@ -491,6 +563,12 @@ def run_ours(args, rank, world, local_rank):
     accuracy = None
     if args.mode in ("fp32", "hybrid") and args.accuracy_steps > 0:
         accuracy = _accuracy(part, model, node, spec, args.mode, args.accuracy_steps, stream)
+    shock_cyl = None
+    if args.mode == "hybrid" and not args.no_shock_cylinder:
+        shock_cyl = shock_cylinder_block(torch, args, dist, stream, local_rank)
+    for blk in (plain, fp32):
+        if blk:
+            blk.pop("_stage_mean_ms", None)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -513,11 +591,14 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "state 295 MB > 126 MB L2, no flush", "parallelism": f"replicas x{world}"},
         "plain_fp64": plain,
         "speedup_vs_plain_fp64": (value / plain["value"]) if plain else None,
+        "fp32_bulk": fp32,
+        "speedup_vs_fp32_bulk": (value / fp32["value"]) if fp32 else None,
         "accuracy": accuracy,
+        "shock_cylinder": shock_cyl,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": traffic,
                      "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of an RK-stage-2 launch "
-                                     "of this kernel (profiles/stage_sweep_<form>_tgv128.md), scaled to the mean "
+                                     f"of this kernel ({tr_src}), scaled to the mean "
                                      f"RK-stage mix; algorithmic bytes per launch = {dom_bytes:.4g}",
                      "kernel": f"{dom_name} stage kernel of sweep axes {sorted(dom['axes'])} "
                                f"({dom_share * 100:.0f}% of the stage time), mean over its launches in one step",
@@ -525,11 +606,13 @@ def run_ours(args, rank, world, local_rank):
                                            "frac": bytes_per_stage / (stage_mean / 1e3) / 1e9 / hbm_peak},
                      "per_axis_ms": {str(ax): sum(d["ms"]) / len(d["ms"]) for ax, d in sorted(per_axis.items())},
                      "peak_kind": peak_kind,
-                     "fp64": {"achieved_tflops": flop_rate, "peak_tflops": fp64_peak,
-                              "frac": (flop_rate / fp64_peak) if fp64_peak else None,
+                     "fp64": {"achieved_tflops": flop_rate64, "peak_tflops": fp64_peak,
+                              "frac": (flop_rate64 / fp64_peak) if fp64_peak else None,
                               "peak_kind": "measured cuBLAS DGEMM 8192^3 in this run",
                               "flop_per_node_stage": FLOP_PER_NODE_STAGE_VISCOUS,
-                              "note": "reference FP64 flop count; meaningful as a fraction for the FP64 forms"},
+                              "stage_ms": st64,
+                              "note": "the plain FP64 path's mean stage time against the reference's FP64 flop "
+                                      "count of a stage (1,535 flop per node)"},
                      "fp32": ({"achieved_tflops": flop_rate, "peak_tflops": fp32_peak,
                                "frac": (flop_rate / fp32_peak) if fp32_peak else None,
                                "peak_kind": "measured cuBLAS SGEMM 8192^3 (no TF32) in this run",
@@ -677,7 +760,11 @@ def run_reference(args, rank, world):
         return
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": 0, "ms_per_step": det["seconds_per_step"] * 1e3,
+        # the steps each process ran (a bounded sample; --steps/--warmup asked for more)
+        "steps": det["steps"], "warmup": 0, "steps_requested": args.steps, "warmup_requested": args.warmup,
+        "ms_per_step": det["seconds_per_step"] * 1e3,
+        "ms_per_step_note": "seconds per time step of one process while all processes run (slowest process)",
+        "per_core_value": rate / det["procs"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (analytic TGV initial field)",
         "config": {"workload": WORKLOAD, "form": "reference CPU (serial C99)", "procs": det["procs"]},
@@ -700,6 +787,9 @@ def main():
     ap.add_argument("--accuracy-steps", type=int, default=200)
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-shock-cylinder", action="store_true", help="leave out the shock-cylinder block")
+    ap.add_argument("--sc-accuracy-steps", type=int, default=100,
+                    help="steps of the shock-cylinder accuracy comparison (0: none)")
     ap.add_argument("--ref-procs", type=int, default=0, help="reference processes (0: every usable host thread)")
     ap.add_argument("--workload", default="tgv", choices=["tgv", "batch"],
                     help="tgv: the headline line (TGV 128^3); batch: the 48-case batched sweep")

@@ -218,11 +218,15 @@ int acfd_cfl(acfd_case_t *cs, double vmax[3]);
  * U_to: device pointer to the five U[TO] planes (plane stride pitch*n[Y]*n[Z]),
  * did: device pointer to the did plane, vmax_dev: device pointer to 3 doubles
  * (written), stream: cudaStream_t or NULL.  Allocates nothing: its scratch is
- * a fixed 96 KiB device array in the library (4096 partial maxima), held on
- * every GPU that loads the library until exit, which limits a case to
- * 33,554,432 computed nodes (larger cases: ACFD_ERR_ARG).  The first call on a
- * device looks up that array's address, so make it before any stream capture.
- * All calls share the array: calls that overlap on the GPU race. */
+ * a fixed 128 KiB device array in the library (4096 blocks' partial maxima and
+ * non-finite flags), held on every GPU that loads the library until exit,
+ * which limits a case to 33,554,432 computed nodes (larger cases, and PIN
+ * ranges outside the node array: ACFD_ERR_ARG).  The call is asynchronous on
+ * `stream`: when a fluid node has a non-finite wave speed (the condition for
+ * which acfd_cfl returns ACFD_ERR_DEVICE) all three outputs are NaN.  The
+ * first call on a device, and the first after its context changed (a device
+ * reset), looks up that array's address, so make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race. */
 int acfd_cfl_noalloc(const acfd_partition_t *part, const acfd_model_t *model, const double *U_to,
         const int *did, int pitch, double *vmax_dev, void *stream);
 /* EvolveFluidDynamics (fluid_dynamics.c:55-116): one time step of size dt on

@@ -7,13 +7,15 @@ import os
 import numpy as np
 
 from artracfd_b200 import abi
+from artracfd_b200.case import load_polyhedra
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 JUNK = np.frombuffer(b"\x01" * 8, dtype="<f8")[0]  # the reference's memset(U, 1) value
 
 
 def names():
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+    """The golden cases (bodies_*.npz hold preprocessed bodies, not cases)."""
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith("bodies_"))
 
 
 def _struct(cls, raw):
@@ -24,35 +26,7 @@ def _struct(cls, raw):
 
 
 def _geo(z, prefix):
-    keep = []
-    geo = []
-    if prefix + "count" not in z:
-        return geo, keep
-    for q in range(int(z[prefix + "count"])):
-        p = f"{prefix}{q}_"
-        P = abi.Polyhedron()
-        P.faceN, P.edgeN, P.vertN, P.state = (int(v) for v in z[p + "scal"])
-        real = z[p + "real"]
-        P.r = real[0]
-        for s in range(3):
-            P.O[s] = real[1 + s]
-            P.V[s] = real[4 + s]
-            P.W[s] = real[7 + s]
-        P.T = real[10]
-        P.cf = real[11]
-        for s in range(3):
-            for m in range(2):
-                P.box[s][m] = real[12 + 2 * s + m]
-        if P.faceN > 0:
-            arrs = {}
-            for key, ct in (("f", ctypes.c_int), ("Nf", ctypes.c_double), ("e", ctypes.c_int),
-                            ("Ne", ctypes.c_double), ("v", ctypes.c_double), ("Nv", ctypes.c_double)):
-                a = np.ascontiguousarray(z[p + key], dtype=np.int32 if ct is ctypes.c_int else np.float64)
-                arrs[key] = a
-                setattr(P, key, a.ctypes.data_as(ctypes.POINTER(ct)))
-            keep.append(arrs)
-        geo.append(P)
-    return geo, keep
+    return load_polyhedra(z, prefix)
 
 
 def nodes_from(U, flags):
@@ -82,6 +56,14 @@ class Bundle:
 
     def U_after(self, k):
         return self.z[f"U{k}"]
+
+    def nodes_after(self, k):
+        """The reference's own state after k fluid steps (k = 0: the initial
+        state); the bodies do not move in these steps, so the flags are the
+        initial ones."""
+        if k == 0:
+            return self.initial_nodes()
+        return nodes_from(self.U_after(k), self.z["flags0"])
 
     @property
     def has_motion(self):

@@ -26,6 +26,31 @@ def test_python_descriptors_equal_reference(name):
     assert bytes(model) == bytes(b.model)
 
 
+def test_shock_cylinder_body_fixture_belongs_to_the_named_case(tmp_path):
+    """tests/golden/bodies_shock_cylinder.npz (the cylinder as the reference
+    preprocesses it, read by bench.py) holds the partition and model of
+    configs.shock_cylinder() at its full size; where the reference harness is
+    built, its preprocessing of the same case gives the same surface."""
+    from artracfd_b200.case import load_polyhedra
+    z = np.load(os.path.join(ROOT, "tests", "golden", "bodies_shock_cylinder.npz"))
+    part, model = configs.shock_cylinder().descriptors()
+    assert bytes(part) == bytes(z["part"])
+    assert bytes(model) == bytes(z["model"])
+    geo, keep = load_polyhedra(z)
+    assert len(geo) == 1 and geo[0].faceN > 0 and geo[0].state == 1
+    from oracle.oracle import Reference, reference_available
+    if not reference_available():
+        return
+    ref = Reference()
+    path = str(tmp_path / "sc")
+    configs.shock_cylinder(m=(64, 32, 4)).write(path)  # same body file, small mesh
+    ref.load(path)
+    P = ref.geometry()[0]
+    for key, rows in (("v", P.vertN), ("Nv", P.vertN), ("Nf", P.faceN), ("Ne", P.edgeN)):
+        got = np.ctypeslib.as_array(getattr(P, key), (rows * 3,))
+        assert np.array_equal(got, keep[0][key]), key
+
+
 def test_node_record_layout():
     # acfd_node_t has the reference Node layout: 4 ints, U[3][5] doubles
     assert abi.NODE_DTYPE.itemsize == 136

@@ -17,11 +17,43 @@ from artracfd_b200.solver import Solver
 pytestmark = pytest.mark.gpu
 
 
-def _noalloc(lib, s, out_ptr):
+def _noalloc(lib, s, out_ptr, stream=None):
     U, F, pitch, plane = s.device_state()
     st = lib.acfd_cfl_noalloc(ctypes.byref(s.part), ctypes.byref(s.model), ctypes.c_void_p(U),
-                              ctypes.c_void_p(F), pitch, ctypes.c_void_p(out_ptr), None)
+                              ctypes.c_void_p(F), pitch, ctypes.c_void_p(out_ptr),
+                              ctypes.c_void_p(stream) if stream else None)
     assert st == abi.ACFD_OK, abi.last_error(lib)
+
+
+def _two_calls_equal(spec, stream=None, steps_between=1):
+    """acfd_cfl_noalloc against acfd_cfl on two calls in a row, with the state
+    advanced between them; returns the last result."""
+    import torch
+
+    part, model = spec.descriptors()
+    node = spec.initial_nodes(part, model)
+    out = torch.full((3,), -1.0, dtype=torch.float64, device="cuda")
+    with Solver(part, model, abi.FP64) as s:
+        lib = s.lib
+        s.upload(node)
+        if spec.bodies:
+            s.compute_geometric_field()
+        s.treat_boundary(abi.TO)
+        got = None
+        for call in range(2):
+            expect = s.cfl()  # existing entry point (synchronizes its stream)
+            _noalloc(lib, s, out.data_ptr(), stream.cuda_stream if stream is not None else None)
+            if stream is not None:
+                stream.synchronize()
+            torch.cuda.synchronize()
+            got = out.cpu().numpy()
+            # same reduction of the same values: equal bit for bit (tolerance 0)
+            assert np.array_equal(got, expect), (call, got, expect)
+            assert np.all(got > 0)
+            for _ in range(steps_between):
+                s.evolve(s.time_step(spec.cfl))
+            s.download()
+        return got
 
 
 def test_cfl_noalloc_matches_cfl_on_two_calls():
@@ -46,6 +78,64 @@ def test_cfl_noalloc_matches_cfl_on_two_calls():
             # change the state between the two calls
             s.evolve(s.time_step(spec.cfl))
             s.download()
+
+
+def test_cfl_noalloc_skips_solid_nodes_like_cfl():
+    """Immersed bodies: nodes inside them (did != 0) are left out of the
+    maximum by both entry points."""
+    spec = configs.ib_spheres(n=32, count=2, analytic=1, level=2, stepN=0)
+    _two_calls_equal(spec)
+
+
+def test_cfl_noalloc_many_blocks_on_a_side_stream():
+    """TGV 128^3 (2.1 M computed nodes, over 2,000 blocks of partial maxima)
+    on a caller's stream that is not the default one."""
+    import torch
+
+    side = torch.cuda.Stream()
+    _two_calls_equal(configs.tgv(n=128), stream=side, steps_between=1)
+
+
+def test_cfl_noalloc_reports_a_non_finite_state_as_nan():
+    """A NaN planted in one fluid node's energy: acfd_cfl returns
+    ACFD_ERR_DEVICE; the allocation-free call, which does not wait for its
+    kernels, writes NaN to all three outputs instead.  The next call on a
+    clean state gives acfd_cfl's maxima again (the shared scratch keeps no
+    stale flag)."""
+    import torch
+
+    spec = configs.tgv(n=16)
+    part, model = spec.descriptors()
+    node = spec.initial_nodes(part, model)
+    out = torch.full((3,), -1.0, dtype=torch.float64, device="cuda")
+    with Solver(part, model, abi.FP64) as s:
+        s.upload(node)
+        s.treat_boundary(abi.TO)
+        good = s.cfl()
+        bad = s.download()
+        fluid = np.flatnonzero(bad["did"] == 0)
+        bad["U"][fluid[len(fluid) // 3], 0, 4] = np.nan
+        s.upload(bad)
+        _noalloc(s.lib, s, out.data_ptr())
+        torch.cuda.synchronize()
+        assert np.all(np.isnan(out.cpu().numpy()))
+        s.upload(node)
+        s.treat_boundary(abi.TO)
+        _noalloc(s.lib, s, out.data_ptr())
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy(), good)
+
+
+def test_cfl_noalloc_rejects_an_inverted_pin_range():
+    lib = abi.load_library()
+    part, model = configs.tgv(n=16).descriptors()
+    bad = abi.copy_struct(part, abi.Partition)
+    bad.ns[0][0][0], bad.ns[0][0][1] = bad.ns[0][0][1], bad.ns[0][0][0]
+    bad.ns[0][1][0], bad.ns[0][1][1] = bad.ns[0][1][1], bad.ns[0][1][0]
+    dummy = ctypes.c_void_p(16)  # never dereferenced: the range check comes first
+    st = lib.acfd_cfl_noalloc(ctypes.byref(bad), ctypes.byref(model), dummy, dummy, part.n[0], dummy, None)
+    assert st == abi.ACFD_ERR_ARG
+    assert "not inside" in abi.last_error(lib)
 
 
 def test_cfl_noalloc_rejects_cases_beyond_its_scratch():
