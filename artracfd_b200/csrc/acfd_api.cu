@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <mutex>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include <cudaTypedefs.h>
@@ -66,6 +67,8 @@ void ib_destroy(IbState *ib);
 int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, const acfd_partition_t &part,
               cudaStream_t st, bool *relayout);
 int ib_treat_launches(const IbState *ib, const acfd_partition_t &part);
+int ib_flags_changed(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partition_t &part,
+                     const int *flags, cudaStream_t st);
 int ib_surface_force(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partition_t &part,
                      const double *U, const int *flags, double *force, cudaStream_t st);
 int ib_collision_scan(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partition_t &part,
@@ -159,9 +162,13 @@ struct acfd_case {
     bool plain_kernels = false;    // use the global-memory stage kernels instead of the bricks
     bool bc_multi = false;         // one launch per ghost-fill phase instead of the fused launch
     unsigned *bcbar = nullptr;     // grid-barrier words of the fused ghost fill
-    int2 *bc_pairs = nullptr;      // ghost fill as one gather (all faces copies)
+    int2 *bc_pairs = nullptr;      // ghost fill as one launch: copies (dst, src) -- base of the allocation
     int bc_npairs = 0;
-    bool bc_gather = false;
+    int4 *bc_progs = nullptr;      // ... and formula programs (dst, first op, op count)
+    int bc_nprog = 0;
+    int2 *bc_ops = nullptr;
+    GhostFaces bc_faces;
+    bool bc_gather = false;        // the one-launch fill replaces the ordered launches
     std::vector<const FaceBox *> bc_ptrs;
     std::vector<int> bc_sizes;
     // learned sensor of the hybrid form
@@ -335,98 +342,219 @@ void build_bc_plan(acfd_case *cs)
     }
 }
 
-// Ghost fill of copy-only cases as one gather.  The reference fills the faces
-// in order (boundary_treatment.c:51-63); when every face is periodic or
-// outflow, every write copies one node into another, so replaying the
-// ordered fill on node indices instead of values gives, for each node the
-// fill changes, the node whose value (from before the fill) it ends with.
-// When no such source node is itself changed, one gather reproduces the
-// ordered fill bit for bit.  Returns false (keep the ordered launches) for any
-// other boundary kind or overlap.
-bool build_bc_gather(acfd_case *cs)
+// Ghost fill as one launch.  The reference fills the faces in order, layer
+// by layer (boundary_treatment.c:51-63), and every write is one of: a copy of
+// another node (outflow, periodic, the outer layers of inflow), the given
+// inflow state (inflow boundary node), the wall formula of a boundary node
+// from its inner neighbour (slip / no-slip wall, :148-177) or the method of
+// images of a wall ghost node from its boundary point and image node
+// (:105-115).  Replaying the ordered fill on formulas instead of values gives,
+// for every node the fill changes, one formula over values from before the
+// fill (a write that reads a node changed earlier in the fill takes that
+// node's formula).  When no node that a final formula reads is itself changed
+// by the fill, one launch evaluating every formula reproduces the ordered
+// fill bit for bit: the operations and their order are the reference's.  Pure
+// copies are kept as (destination, source) pairs, the other formulas as short
+// postfix programs.  Returns false (keep the ordered launches) when a formula
+// reads a changed node, a program is longer than kGhostMaxOps, or the node
+// count does not fit 32-bit indices.
+namespace {
+
+struct GhostExpr {
+    int op, a, b, face;  // a, b: references (>= 0 expression, < 0 LOAD of node -ref-1)
+    bool operator==(const GhostExpr &o) const { return op == o.op && a == o.a && b == o.b && face == o.face; }
+};
+struct GhostExprHash {
+    size_t operator()(const GhostExpr &e) const
+    {
+        unsigned long long h = (unsigned long long)(unsigned)e.a * 0x9E3779B97F4A7C15ULL;
+        h ^= ((unsigned long long)(unsigned)e.b + 0x632BE59BD9B4E019ULL) * 0xC2B2AE3D27D4EB4FULL;
+        h ^= (unsigned long long)(e.op * 8 + e.face) * 0x165667B19E3779F9ULL;
+        return (size_t)(h ^ (h >> 29));
+    }
+};
+
+}  // namespace
+
+bool build_bc_program(acfd_case *cs)
 {
     const acfd_partition_t &p = cs->part;
     const Grid &g = cs->grid;
-    for (int face = 1; face <= 6; ++face) {
-        if (p.typeBC[face] != 1 && p.typeBC[face] != 4) {
-            return false;
-        }
-    }
     if (g.nn * 5 > (long long)INT32_MAX) {
         return false;
     }
-    std::vector<int> sym((size_t)g.nn);
-    for (long long q = 0; q < g.nn; ++q) {
-        sym[(size_t)q] = (int)q;
-    }
+    const int kUnset = INT32_MIN;
+    std::vector<int> def((size_t)g.nn, kUnset);
+    std::vector<GhostExpr> ex;
+    std::unordered_map<GhostExpr, int, GhostExprHash> memo;
+    auto make = [&](const GhostExpr &e) {
+        auto it = memo.find(e);
+        if (it != memo.end()) {
+            return it->second;
+        }
+        const int id = (int)ex.size();
+        ex.push_back(e);
+        memo.emplace(e, id);
+        return id;
+    };
+    auto ref_of = [&](long long q) { return def[(size_t)q] != kUnset ? def[(size_t)q] : -(int)q - 1; };
     auto idx = [&](int i, int j, int k) { return ((long long)k * g.n[1] + j) * g.pitch + i; };
+    auto inside = [&](int i, int j, int k) {
+        return i >= 0 && j >= 0 && k >= 0 && i < g.n[0] && j < g.n[1] && k < g.n[2];
+    };
     for (const auto &grp : cs->bc_groups) {
         for (const FaceBox &b : grp) {
-            const int *N = p.N[b.face];
-            const int periodic = (p.typeBC[b.face] == 4);
-            int off[3];
-            for (int s = 0; s < 3; ++s) {
-                off[s] = (b.r != 0 && periodic) ? p.m[s] * N[s] : N[s];
-            }
+            const int face = b.face, r = b.r, type = p.typeBC[face];
+            const int *N = p.N[face];
             for (int k = b.box[2][0]; k < b.box[2][1]; ++k) {
                 for (int j = b.box[1][0]; j < b.box[1][1]; ++j) {
                     for (int i = b.box[0][0]; i < b.box[0][1]; ++i) {
-                        const int si = i - off[0], sj = j - off[1], sk = k - off[2];
-                        if (si < 0 || sj < 0 || sk < 0 || si >= g.n[0] || sj >= g.n[1] || sk >= g.n[2]) {
-                            return false;
+                        const long long q = idx(i, j, k);
+                        int e;
+                        if (r != 0) {
+                            if (type == 2 || type == 3) {
+                                const int oi = i - r * N[0], oj = j - r * N[1], ok = k - r * N[2];
+                                const int ii = i - 2 * r * N[0], ij = j - 2 * r * N[1], ik = k - 2 * r * N[2];
+                                if (!inside(oi, oj, ok) || !inside(ii, ij, ik)) return false;
+                                e = make(GhostExpr{kGhostImage, ref_of(idx(oi, oj, ok)), ref_of(idx(ii, ij, ik)), 0});
+                            } else {
+                                const int per = (type == 4);
+                                const int si = i - (per ? p.m[0] * N[0] : N[0]);
+                                const int sj = j - (per ? p.m[1] * N[1] : N[1]);
+                                const int sk = k - (per ? p.m[2] * N[2] : N[2]);
+                                if (!inside(si, sj, sk)) return false;
+                                e = ref_of(idx(si, sj, sk));
+                            }
+                        } else if (type == 0) {
+                            e = make(GhostExpr{kGhostInflow, 0, 0, face});
+                        } else if (type == 1 || type == 2 || type == 3) {
+                            const int si = i - N[0], sj = j - N[1], sk = k - N[2];
+                            if (!inside(si, sj, sk)) return false;
+                            e = ref_of(idx(si, sj, sk));
+                            if (type != 1) {
+                                e = make(GhostExpr{kGhostWall, e, 0, face});
+                            }
+                        } else {
+                            continue;  // periodic boundary plane: computed like an interior node
                         }
-                        sym[(size_t)idx(i, j, k)] = sym[(size_t)idx(si, sj, sk)];
+                        def[(size_t)q] = e;
                     }
                 }
             }
         }
     }
+    // final formulas: copies and programs; no node a formula reads may change
     std::vector<int2> pairs;
+    std::vector<int4> progs;
+    std::vector<int2> ops;
     std::vector<char> changed((size_t)g.nn, 0);
     for (long long q = 0; q < g.nn; ++q) {
-        if (sym[(size_t)q] != (int)q) {
-            pairs.push_back(make_int2((int)q, sym[(size_t)q]));
+        const int d = def[(size_t)q];
+        if (d != kUnset && d != -(int)q - 1) {
             changed[(size_t)q] = 1;
         }
     }
-    for (const int2 &pr : pairs) {
-        if (changed[(size_t)pr.y]) {
-            return false;  // a source is itself rewritten: order matters
+    std::vector<int> first((size_t)ex.size(), -1), count((size_t)ex.size(), 0), depth((size_t)ex.size(), 0);
+    bool ok = true;
+    // postfix flattening of expression e into ops (memoized: a shared
+    // sub-formula is copied, not referenced)
+    std::vector<int2> tmp;
+    auto emit = [&](auto &&self, int ref, std::vector<int2> &out, int &dep) -> void {
+        if (!ok) return;
+        if (ref < 0) {
+            const int node = -ref - 1;
+            if (changed[(size_t)node]) ok = false;
+            out.push_back(make_int2(kGhostLoad, node));
+            dep = 1;
+            return;
         }
+        const GhostExpr &e = ex[(size_t)ref];
+        if (e.op == kGhostInflow) {
+            out.push_back(make_int2(kGhostInflow | (e.face << 3), 0));
+            dep = 1;
+        } else if (e.op == kGhostWall) {
+            int d0 = 0;
+            self(self, e.a, out, d0);
+            out.push_back(make_int2(kGhostWall | (e.face << 3), 0));
+            dep = d0;
+        } else {
+            int d0 = 0, d1 = 0;
+            self(self, e.a, out, d0);
+            self(self, e.b, out, d1);
+            out.push_back(make_int2(kGhostImage, 0));
+            dep = std::max(d0, d1 + 1);
+        }
+    };
+    for (long long q = 0; q < g.nn && ok; ++q) {
+        if (!changed[(size_t)q]) continue;
+        const int d = def[(size_t)q];
+        if (d < 0) {
+            const int src = -d - 1;
+            if (changed[(size_t)src]) ok = false;
+            pairs.push_back(make_int2((int)q, src));
+            continue;
+        }
+        if (first[(size_t)d] < 0) {
+            tmp.clear();
+            int dep = 0;
+            emit(emit, d, tmp, dep);
+            if ((int)tmp.size() > kGhostMaxOps || dep > kGhostStack) ok = false;
+            first[(size_t)d] = (int)ops.size();
+            count[(size_t)d] = (int)tmp.size();
+            ops.insert(ops.end(), tmp.begin(), tmp.end());
+        }
+        progs.push_back(make_int4((int)q, first[(size_t)d], count[(size_t)d], 0));
     }
-    if (pairs.empty()) {
+    if (!ok || (pairs.empty() && progs.empty())) {
         return false;
     }
-    if (cudaMalloc(&cs->bc_pairs, pairs.size() * sizeof(int2)) != cudaSuccess) {
+    for (int f = 0; f < 7; ++f) {
+        cs->bc_faces.type[f] = p.typeBC[f];
+        for (int s = 0; s < 3; ++s) cs->bc_faces.N[f][s] = p.N[f][s];
+        for (int v = 0; v < 6; ++v) cs->bc_faces.given[f][v] = p.varBC[f][v];
+    }
+    const size_t b_pairs = pairs.size() * sizeof(int2), b_progs = progs.size() * sizeof(int4);
+    const size_t off_progs = (b_pairs + 255) / 256 * 256, off_ops = off_progs + (b_progs + 255) / 256 * 256;
+    const size_t total = off_ops + ops.size() * sizeof(int2);
+    char *base = nullptr;
+    if (cudaMalloc(&base, total) != cudaSuccess) {
         cudaGetLastError();
-        cs->bc_pairs = nullptr;
         return false;
     }
-    if (cudaMemcpy(cs->bc_pairs, pairs.data(), pairs.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess) {
+    bool copied = cudaMemcpy(base, pairs.data(), b_pairs, cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(base + off_progs, progs.data(), b_progs, cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(base + off_ops, ops.data(), ops.size() * sizeof(int2), cudaMemcpyHostToDevice) ==
+                      cudaSuccess;
+    if (!copied) {
         cudaGetLastError();
-        cudaFree(cs->bc_pairs);
-        cs->bc_pairs = nullptr;
+        cudaFree(base);
         return false;
     }
+    cs->bc_pairs = reinterpret_cast<int2 *>(base);
     cs->bc_npairs = (int)pairs.size();
+    cs->bc_progs = reinterpret_cast<int4 *>(base + off_progs);
+    cs->bc_nprog = (int)progs.size();
+    cs->bc_ops = reinterpret_cast<int2 *>(base + off_ops);
     return true;
 }
 
 int treat_boundary(acfd_case *cs, int tn)
 {
     if (cs->ib && ib_count(cs->ib) > 0) {
+        cs->launches += ib_treat_launches(cs->ib, cs->part);
         int st = ib_treat(cs->ib, cs->grid, cs->mp, cs->part, cs->U, cs->flags, tn, cs->stream);
         if (st != ACFD_OK) {
             return st;
         }
     }
-    if (cs->ib && ib_count(cs->ib) > 0) {
-        cs->launches += ib_treat_launches(cs->ib, cs->part);
-    }
     double *U = level(cs, tn);
     if (cs->bc_gather) {
         ++cs->launches;
-        return launch_ghost_gather(cs->grid, cs->bc_pairs, cs->bc_npairs, U, cs->stream);
+        if (cs->bc_nprog == 0) {
+            return launch_ghost_gather(cs->grid, cs->bc_pairs, cs->bc_npairs, U, cs->stream);
+        }
+        return launch_ghost_program(cs->grid, cs->mp, cs->bc_faces, cs->bc_pairs, cs->bc_npairs, cs->bc_progs,
+                                    cs->bc_nprog, cs->bc_ops, U, cs->stream);
     }
     if (!cs->bc_multi) {
         if (cs->bc_groups.empty()) {
@@ -882,7 +1010,7 @@ int acfd_init(const acfd_partition_t *part, const acfd_model_t *model, acfd_case
             acfd_finalize(cs);
             return st;
         }
-        cs->bc_gather = build_bc_gather(cs);
+        cs->bc_gather = build_bc_program(cs);
     }
     if ((e = cudaStreamSynchronize(cs->stream)) != cudaSuccess) {
         st = cuda_status(e, "acfd_init");
@@ -975,6 +1103,9 @@ int acfd_sync_to_device(acfd_case_t *cs, const acfd_node_t *node, unsigned mask)
     const size_t total = (size_t)cs->grid.n[0] * cs->grid.n[1] * cs->grid.n[2];
     TRY(upload_host(cs, cs->staging, node, total * sizeof(acfd_node_t)));
     TRY(launch_scatter_nodes(cs->grid, cs->staging, cs->U, cs->flags, mask, cs->stream));
+    if (mask & ACFD_SYNC_FLAGS) {
+        TRY(ib_flags_changed(cs->ib, cs->grid, cs->mp, cs->part, cs->flags, cs->stream));
+    }
     ACFD_CUDA(cudaStreamSynchronize(cs->stream));
     return ACFD_OK;
 }
@@ -1820,7 +1951,7 @@ int acfd_batch_init(int ncase, const acfd_partition_t *parts, const acfd_model_t
         vmax[c] = cs->cfl_out;
         lv[c].U = cs->U;
         lv[c].nn = cs->grid.nn;
-        if (cs->bc_gather) {
+        if (cs->bc_gather && cs->bc_nprog == 0) {
             std::vector<int2> hp(cs->bc_npairs);
             if ((e = cudaMemcpy(hp.data(), cs->bc_pairs, sizeof(int2) * hp.size(), cudaMemcpyDeviceToHost)) !=
                 cudaSuccess) {

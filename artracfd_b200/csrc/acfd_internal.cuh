@@ -249,6 +249,23 @@ int launch_domain_boundary(const Grid &g, const ModelParams &m, const acfd_parti
 // ghost fill as one gather: U[dst] = U[src] for every (dst, src) pair, all
 // five variables of the level U
 int launch_ghost_gather(const Grid &g, const int2 *pairs, int count, double *U, cudaStream_t st);
+// ghost fill as one launch of formulas: per-face constants of the programs
+// (type, outward normal, given primitive state of faces 1..6), op codes
+// (low 3 bits; the face in the bits above), the value-stack depth
+struct GhostFaces {
+    int type[7];
+    int N[7][3];
+    double given[7][6];
+};
+constexpr int kGhostLoad = 0;    // push U[arg]
+constexpr int kGhostInflow = 1;  // push the given inflow state of the face
+constexpr int kGhostWall = 2;    // top := wall boundary node from the top (its inner neighbour)
+constexpr int kGhostImage = 3;   // (O, I) := image ghost of boundary point O and image node I
+constexpr int kGhostStack = 6;
+constexpr int kGhostMaxOps = 32;
+// pairs: (dst, src) copies; progs: (dst, first op, op count, 0); ops: (code | face << 3, node)
+int launch_ghost_program(const Grid &g, const ModelParams &m, const GhostFaces &F, const int2 *pairs, int npairs,
+                         const int4 *progs, int nprog, const int2 *ops, double *U, cudaStream_t st);
 // all groups of one TreatBoundary in one cooperative launch with grid barriers;
 // bar: two device words (arrival count, generation), zero at first use
 int launch_domain_boundary_fused(const Grid &g, const ModelParams &m, const acfd_partition_t &part,

@@ -157,6 +157,46 @@ __global__ void __launch_bounds__(1024) domain_fill_fused(Grid g, ModelParams mp
     }
 }
 
+// method of images of a wall ghost node from its boundary point O and image
+// node I (boundary_treatment.c:105-115 with DoMethodOfImage,
+// immersed_boundary.c:341-356)
+__device__ __forceinline__ void image_ghost(const ModelParams &mp, const double UO[5], const double UI[5],
+                                            double Ut[5])
+{
+    double UoO[6], UoI[6], UoG[6];
+    to_primitive(mp.gamma, mp.gasR, UO, UoO);
+    to_primitive(mp.gamma, mp.gasR, UI, UoI);
+    UoG[1] = UoO[1] + UoO[1] - UoI[1];
+    UoG[2] = UoO[2] + UoO[2] - UoI[2];
+    UoG[3] = UoO[3] + UoO[3] - UoI[3];
+    UoG[4] = UoI[4];
+    UoG[5] = UoI[5];
+    UoG[0] = UoG[4] / (UoG[5] * mp.gasR);
+    to_conservative(mp.gamma, UoG, Ut);
+}
+
+// slip (type 2) or no-slip (type 3) wall boundary node from its inner
+// neighbour h (boundary_treatment.c:148-177); given5 < 0: adiabatic
+__device__ __forceinline__ void wall_node(const ModelParams &mp, int type, const int N[3], double given5,
+                                          const double Uh[5], double Ut[5])
+{
+    double Uoh[6], UoO[6];
+    to_primitive(mp.gamma, mp.gasR, Uh, Uoh);
+    if (type == 2) {
+        UoO[1] = (double)(!N[0]) * Uoh[1];
+        UoO[2] = (double)(!N[1]) * Uoh[2];
+        UoO[3] = (double)(!N[2]) * Uoh[3];
+    } else {
+        UoO[1] = 0.0;
+        UoO[2] = 0.0;
+        UoO[3] = 0.0;
+    }
+    UoO[4] = Uoh[4];
+    UoO[5] = (0.0 > given5) ? Uoh[5] : given5;
+    UoO[0] = UoO[4] / (UoO[5] * mp.gasR);
+    to_conservative(mp.gamma, UoO, Ut);
+}
+
 __device__ void fill_node(const Grid &g, const ModelParams &mp, const FaceJob &J, long long t, double *U)
 {
     const int i = J.lo[0] + (int)(t % J.ext[0]);
@@ -171,19 +211,10 @@ __device__ void fill_node(const Grid &g, const ModelParams &mp, const FaceJob &J
     if (r != 0) {
         // ghost layer r
         if (J.type == 2 || J.type == 3) {
-            double UO[5], UI[5], UoO[6], UoI[6], UoG[6];
+            double UO[5], UI[5];
             load5(U, nn, node_of(g, i - r * N[0], j - r * N[1], k - r * N[2]), UO);
             load5(U, nn, node_of(g, i - 2 * r * N[0], j - 2 * r * N[1], k - 2 * r * N[2]), UI);
-            to_primitive(mp.gamma, mp.gasR, UO, UoO);
-            to_primitive(mp.gamma, mp.gasR, UI, UoI);
-            // method of images (immersed_boundary.c:341-356)
-            UoG[1] = UoO[1] + UoO[1] - UoI[1];
-            UoG[2] = UoO[2] + UoO[2] - UoI[2];
-            UoG[3] = UoO[3] + UoO[3] - UoI[3];
-            UoG[4] = UoI[4];
-            UoG[5] = UoI[5];
-            UoG[0] = UoG[4] / (UoG[5] * mp.gasR);
-            to_conservative(mp.gamma, UoG, Ut);
+            image_ghost(mp, UO, UI, Ut);
         } else if (J.type == 4) {
             load5(U, nn, node_of(g, i - J.LN[0], j - J.LN[1], k - J.LN[2]), Ut);
         } else {
@@ -202,22 +233,9 @@ __device__ void fill_node(const Grid &g, const ModelParams &mp, const FaceJob &J
             break;
         case 2:  // slip wall
         case 3: {  // no-slip wall
-            double Uh[5], Uoh[6], UoO[6];
+            double Uh[5];
             load5(U, nn, node_of(g, i - N[0], j - N[1], k - N[2]), Uh);
-            to_primitive(mp.gamma, mp.gasR, Uh, Uoh);
-            if (J.type == 2) {
-                UoO[1] = (double)(!N[0]) * Uoh[1];
-                UoO[2] = (double)(!N[1]) * Uoh[2];
-                UoO[3] = (double)(!N[2]) * Uoh[3];
-            } else {
-                UoO[1] = 0.0;
-                UoO[2] = 0.0;
-                UoO[3] = 0.0;
-            }
-            UoO[4] = Uoh[4];
-            UoO[5] = (0.0 > J.given[5]) ? Uoh[5] : J.given[5];
-            UoO[0] = UoO[4] / (UoO[5] * mp.gasR);
-            to_conservative(mp.gamma, UoO, Ut);
+            wall_node(mp, J.type, N, J.given[5], Uh, Ut);
             break;
         }
         default:  // periodic: the boundary plane is computed like an interior node
@@ -461,6 +479,75 @@ int launch_ghost_gather(const Grid &g, const int2 *pairs, int count, double *U, 
     const int blocks = (int)blocks_for(count, 256);
     cudaError_t e = launch_k(ghost_gather, dim3(blocks), dim3(256), 0, st, g.nn, pairs, count, U);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "ghost_gather launch");
+}
+
+// Ghost fill as one launch of formulas (see build_bc_program): threads
+// t < npairs copy U[src] to U[dst]; the others evaluate one postfix program
+// each -- LOAD pushes a node's five values, INFLOW the given inflow state,
+// WALL replaces the top with the wall formula of a boundary node, IMAGE
+// replaces the top two (boundary point O, image node I) with the image
+// ghost -- and store the result.  No node a program or pair reads is written
+// by the launch, so the threads need no ordering among themselves.
+__global__ void __launch_bounds__(256) ghost_program(long long nn, const int2 *__restrict__ pairs, int npairs,
+                                                     const int4 *__restrict__ progs, int nprog,
+                                                     const int2 *__restrict__ ops, GhostFaces F, ModelParams mp,
+                                                     double *U)
+{
+    pdl_wait();
+    const int total = npairs + nprog;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        if (t < npairs) {
+            const int2 q = pairs[t];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+                U[v * nn + q.x] = U[v * nn + q.y];
+            }
+            continue;
+        }
+        const int4 pr = progs[t - npairs];  // dst, first op, op count
+        double st[kGhostStack][5];
+        int sp = 0;
+        for (int o = 0; o < pr.z; ++o) {
+            const int2 op = ops[pr.y + o];
+            const int code = op.x & 7, face = op.x >> 3;
+            if (code == kGhostLoad) {
+                load5(U, nn, op.y, st[sp]);
+                ++sp;
+            } else if (code == kGhostInflow) {
+                to_conservative(mp.gamma, F.given[face], st[sp]);
+                ++sp;
+            } else if (code == kGhostWall) {
+                double Ut[5];
+                wall_node(mp, F.type[face], F.N[face], F.given[face][5], st[sp - 1], Ut);
+#pragma unroll
+                for (int v = 0; v < 5; ++v) {
+                    st[sp - 1][v] = Ut[v];
+                }
+            } else {  // kGhostImage
+                double Ut[5];
+                image_ghost(mp, st[sp - 2], st[sp - 1], Ut);
+                --sp;
+#pragma unroll
+                for (int v = 0; v < 5; ++v) {
+                    st[sp - 1][v] = Ut[v];
+                }
+            }
+        }
+        store5(U, nn, pr.x, st[0]);
+    }
+}
+
+int launch_ghost_program(const Grid &g, const ModelParams &m, const GhostFaces &F, const int2 *pairs, int npairs,
+                         const int4 *progs, int nprog, const int2 *ops, double *U, cudaStream_t st)
+{
+    const int total = npairs + nprog;
+    if (total <= 0) {
+        return ACFD_OK;
+    }
+    const int blocks = (int)blocks_for(total, 256);
+    cudaError_t e = launch_k(ghost_program, dim3(blocks), dim3(256), 0, st, g.nn, pairs, npairs, progs, nprog, ops,
+                             F, m, U);
+    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "ghost_program launch");
 }
 
 // ghost fill of all cases of a batch in one launch (copy-only cases, see

@@ -89,6 +89,11 @@ struct IbState {
     int *col_N = nullptr;              // [totN][totN][3] summed path offsets
     int col_n = 0;
     BoxPart *motion_part = nullptr;  // [kMotionBlocks] box extremes of a surface motion
+    // the ghost lists hold the ghost nodes of the current flags: rebuilt by
+    // every writer of the flags (the geometric field, an upload of node
+    // records), so that a boundary treatment, captured step graphs included,
+    // only reads them
+    bool lists_valid = false;
 };
 
 namespace {
@@ -1360,6 +1365,7 @@ int ib_upload(IbState *ib, const acfd_polyhedron_t *poly, int totN, const acfd_p
               bool *relayout)
 {
     *relayout = true;
+    ib->lists_valid = false;  // new boxes: the next geometric field (or treatment) lists the ghosts
     if (totN > 0) {
         bool done = false;
         const int rc = update_in_place(ib, poly, totN, part, st, &done);
@@ -1491,20 +1497,40 @@ static int boxes_of(IbState *ib, const acfd_partition_t &part, int n0, BoxList &
     return ACFD_OK;
 }
 
+// the ghost lists of every body from the current flags
+static int build_lists(IbState *ib, const IbGrid &G, const acfd_partition_t &part, const int *flags,
+                       cudaStream_t st)
+{
+    ACFD_CUDA(cudaMemsetAsync(ib->nghost, 0, sizeof(int) * part.gl, st));
+    // the boxes come from device memory and the grid is fixed (grid-stride)
+    const unsigned lblocks = (unsigned)std::min<long long>(blocks_for(ib->ghost_cap, 256), 148LL * 4);
+    for (int gi = 0; gi < ib->ngroups; ++gi) {
+        ib_list<<<lblocks, 256, 0, st>>>(G, ib->groups, gi, flags, ib->ghosts, ib->nghost, ib->ghost_cap,
+                                         ib->status);
+        ACFD_CUDA(cudaGetLastError());
+    }
+    ib->lists_valid = true;
+    return ACFD_OK;
+}
+
+int ib_flags_changed(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partition_t &part,
+                     const int *flags, cudaStream_t st)
+{
+    if (!ib || ib->count == 0) return ACFD_OK;
+    ib->lists_valid = false;
+    if (part.gl < 1) return ACFD_OK;
+    return build_lists(ib, make_ibgrid(g, part, m.ibmLayer), part, flags, st);
+}
+
 int ib_treat(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partition_t &part, double *U, int *flags,
              int tn, cudaStream_t st)
 {
     if (!ib || ib->count == 0) return ACFD_OK;
     const IbGrid G = make_ibgrid(g, part, m.ibmLayer);
     if (part.gl < 1) return ACFD_OK;
-    ACFD_CUDA(cudaMemsetAsync(ib->nghost, 0, sizeof(int) * part.gl, st));
-    // the boxes come from device memory and the grid is fixed (grid-stride):
-    // a captured step replays correctly after the bodies moved
-    const unsigned lblocks = (unsigned)std::min<long long>(blocks_for(ib->ghost_cap, 256), 148LL * 4);
-    for (int gi = 0; gi < ib->ngroups; ++gi) {
-        ib_list<<<lblocks, 256, 0, st>>>(G, ib->groups, gi, flags, ib->ghosts, ib->nghost, ib->ghost_cap,
-                                         ib->status);
-        ACFD_CUDA(cudaGetLastError());
+    if (!ib->lists_valid) {
+        const int rc = build_lists(ib, G, part, flags, st);
+        if (rc != ACFD_OK) return rc;
     }
     // one warp per listed node, at most a few waves of resident warps
     const unsigned blocks = (unsigned)std::min<long long>(blocks_for(ib->ghost_cap, kGhostWarps), 148LL * 12);
@@ -1519,7 +1545,7 @@ int ib_treat(IbState *ib, const Grid &g, const ModelParams &m, const acfd_partit
 int ib_treat_launches(const IbState *ib, const acfd_partition_t &part)
 {
     if (!ib || ib->count == 0) return 0;
-    return (ib->count + 7) / 8 + part.gl;
+    return (ib->lists_valid ? 0 : (ib->count + 7) / 8) + part.gl;
 }
 
 // node boxes of all bodies, their offsets and the scratch of the surface
@@ -1780,6 +1806,10 @@ int ib_compute_geometric_field(IbState *ib, const Grid &g, const ModelParams &m,
     ACFD_CUDA(cudaGetLastError());
     map_refill<<<blocks_for(pin, 128), 128, 0, st>>>(G, m, U, flags, ib->joined, ib->status);
     ACFD_CUDA(cudaGetLastError());
+    if (part.gl >= 1) {
+        const int rc = build_lists(ib, G, part, flags, st);
+        if (rc != ACFD_OK) return rc;
+    }
     return read_status(ib, st);
 }
 

@@ -295,7 +295,7 @@ def _solver(part, model, form, stream):
     return s
 
 
-def _timed_steps(torch, s, spec, steps, warmup, dist, stream, clock_index):
+def _timed_steps(torch, s, spec, steps, warmup, dist, stream, clock_index, label=None):
     """W untimed steps, then K steps between CUDA events on the solver's
     stream (barrier + synchronize on both sides); seconds (max over ranks),
     kernel launches and the clocks sampled meanwhile."""
@@ -313,7 +313,7 @@ def _timed_steps(torch, s, spec, steps, warmup, dist, stream, clock_index):
     launches0 = s.launches()
     # NVTX range of the timed steps (an ncu launch list can be limited to it
     # with --nvtx --nvtx-include "timed_<form>/")
-    torch.cuda.nvtx.range_push("timed_" + FORM_NAMES.get(s.mode, "form"))
+    torch.cuda.nvtx.range_push(label or ("timed_" + FORM_NAMES.get(s.mode, "form")))
     with ClockSampler(clock_index) as clk:
         e0.record(stream)
         for _ in range(steps):
@@ -423,14 +423,14 @@ def _accuracy(part, model, node, spec, form, steps, stream, geo=None):
 
 
 def _form_block(torch, part, model, node, spec, form, nodes_pin, args, dist, stream, local_rank, geo=None,
-                hbm_peak=None, profile=True):
+                hbm_peak=None, profile=True, label=None):
     """One arithmetic form on one case: autotuned variants, W warm-up and K
     device-timed steps (CFL read back + host dt + graph replay each step),
     and optionally one profiled eager step (mean stage and ghost-fill
     times)."""
     s = _start(part, model, node, form, stream, geo)
     tiles = _tune(s, spec)
-    sec, launches, clk = _timed_steps(torch, s, spec, args.steps, args.warmup, dist, stream, local_rank)
+    sec, launches, clk = _timed_steps(torch, s, spec, args.steps, args.warmup, dist, stream, local_rank, label)
     out = {"value": job_rate(int(os.environ.get("WORLD_SIZE", "1")), nodes_pin, args.steps, sec),
            "ms_per_step": sec / args.steps * 1e3, "tiles": tiles, "clocks": clk, "gpu_launches": launches}
     if profile:
@@ -465,9 +465,12 @@ def shock_cylinder_block(torch, args, dist, stream, local_rank):
     geo, keep = load_polyhedra(z)
     node = spec.initial_nodes(part, model)
     pin = int(np.prod(np.array(part.ns)[0, :, 1] - np.array(part.ns)[0, :, 0]))
-    f64 = _form_block(torch, part, model, node, spec, "fp64", pin, args, dist, stream, local_rank, geo, profile=False)
+    f64 = _form_block(torch, part, model, node, spec, "fp64", pin, args, dist, stream, local_rank, geo,
+                      label="timed_sc_fp64")
     hyb = _form_block(torch, part, model, node, spec, "hybrid", pin, args, dist, stream, local_rank, geo,
-                      profile=False)
+                      label="timed_sc_hybrid")
+    for blk in (f64, hyb):
+        blk.pop("_stage_mean_ms", None)
     acc = None
     if args.sc_accuracy_steps > 0:
         acc = _accuracy(part, model, node, spec, "hybrid", args.sc_accuracy_steps, stream, geo)

@@ -162,11 +162,14 @@ def test_fused_ghost_fill_equals_phase_launches(name, monkeypatch):
         assert np.array_equal(a, c)
 
 
-@pytest.mark.parametrize("name", ["tgv", "sod", "tgv_weno3_rk2"])
+@pytest.mark.parametrize("name", ["tgv", "sod", "tgv_weno3_rk2", "channel", "gravity_box", "cylinder2d", "spheres"])
 def test_gather_ghost_fill_equals_phase_launches(name, monkeypatch):
-    """Copy-only cases (periodic and outflow faces) fill their ghosts with one
-    gather launch built from a replay of the ordered fill on node indices;
-    it gives the same bits as the ordered per-phase launches."""
+    """The domain ghost fill in one launch, built from a replay of the ordered
+    fill on formulas (copies for periodic and outflow faces, the inflow state,
+    the wall formula of boundary nodes, the image of wall ghosts), gives the
+    same bits as the ordered per-phase launches: copy-only cases, inflow /
+    outflow / slip / no-slip walls, an all-wall box with gravity, a 2D
+    collapsed case with a body."""
     b = golden_io.Bundle(name)
     outs = []
     for phases in (True, False):
@@ -178,6 +181,8 @@ def test_gather_ghost_fill_equals_phase_launches(name, monkeypatch):
         outs.append(o)
     for a, c in zip(*outs):
         assert np.array_equal(a, c)
+    if b.geo:
+        return  # the body's ghost values add their own launches
     with Solver(b.part, b.model, abi.FP64) as s:
         s.upload(b.initial_nodes())
         n0 = s.launches()
