@@ -36,7 +36,7 @@ BRICK_VARIANTS, PLANE_VARIANT, STAGE_VARIANTS = 2, 5, 11
 # the plane march with equal shares of all tiles' planes per block (Y/Z)
 PLANE_SHARE_VARIANT = PLANE_VARIANT + 3
 # stage kernel of a batch (acfd_batch_set_kernel)
-BATCH_BRICK, BATCH_PLANE = 0, 1
+BATCH_BRICK, BATCH_PLANE, BATCH_PERSISTENT = 0, 1, 2
 # sync masks
 SYNC_TO, SYNC_TN, SYNC_TM, SYNC_U, SYNC_FLAGS, SYNC_ALL = 0x1, 0x2, 0x4, 0x7, 0x8, 0xF
 # boundary kinds (commons.h:83-87)
@@ -173,6 +173,7 @@ def load_library(path: str | None = None):
         "acfd_synchronize": [vp],
         "acfd_autotune": [vp, ctypes.POINTER(ctypes.c_int)],
         "acfd_set_tiles": [vp, ctypes.POINTER(ctypes.c_int)],
+        "acfd_set_wait_limit": [vp, ctypes.c_longlong],
         "acfd_mlp_param_count": [],
         "acfd_sensor_load": [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_float],
         "acfd_sensor_load_file": [vp, ctypes.c_char_p],

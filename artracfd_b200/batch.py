@@ -106,8 +106,10 @@ class Batch:
         check(self.lib.acfd_batch_set_precision(self.h, mode), self.lib)
 
     def set_kernel(self, kernel: int):
-        """abi.BATCH_PLANE (plane march, default when the cases allow it) or
-        abi.BATCH_BRICK (persistent brick kernel)."""
+        """abi.BATCH_PERSISTENT (every RK stage of a step of every case in one
+        persistent launch; the default when the cases allow it),
+        abi.BATCH_PLANE (one plane-march launch per RK stage) or
+        abi.BATCH_BRICK (persistent brick kernel, one launch per RK stage)."""
         check(self.lib.acfd_batch_set_kernel(self.h, kernel), self.lib)
 
     def sensor_load(self, params: np.ndarray, threshold: float):

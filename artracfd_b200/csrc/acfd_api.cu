@@ -169,6 +169,11 @@ struct acfd_case {
     int2 *bc_ops = nullptr;
     GhostFaces bc_faces;
     bool bc_gather = false;        // the one-launch fill replaces the ordered launches
+    long long wait_limit = kWaitLimitDefault;  // polls of a plane-march wait (acfd_set_wait_limit)
+    // ACFD_DEBUG=1: every stage and ghost fill is followed by a scan of its
+    // level for non-finite values, checked at once (no step graphs)
+    bool debug = false;
+    int *dbg_word = nullptr;
     std::vector<const FaceBox *> bc_ptrs;
     std::vector<int> bc_sizes;
     // learned sensor of the hybrid form
@@ -538,7 +543,18 @@ bool build_bc_program(acfd_case *cs)
     return true;
 }
 
+int debug_scan(acfd_case *cs, int l, const char *what, int s);
+static int treat_boundary_fill(acfd_case *cs, int tn);
+
 int treat_boundary(acfd_case *cs, int tn)
+{
+    const int st = treat_boundary_fill(cs, tn);
+    return st != ACFD_OK ? st : debug_scan(cs, tn, "ghost fill", -1);
+}
+
+// TreatBoundary (boundary_treatment.c:28-65): the bodies' ghost nodes, then
+// the domain's ghost shells
+static int treat_boundary_fill(acfd_case *cs, int tn)
 {
     if (cs->ib && ib_count(cs->ib) > 0) {
         cs->launches += ib_treat_launches(cs->ib, cs->part);
@@ -574,6 +590,27 @@ int treat_boundary(acfd_case *cs, int tn)
     return ACFD_OK;
 }
 
+// debug mode: scan level l for non-finite values and report `what`
+int debug_scan(acfd_case *cs, int l, const char *what, int s)
+{
+    if (!cs->debug) {
+        return ACFD_OK;
+    }
+    const int st = launch_finite_scan(level(cs, l), (long long)kVars * cs->grid.nn, cs->dbg_word, cs->stream);
+    if (st != ACFD_OK) {
+        return st;
+    }
+    int h = 0;
+    ACFD_CUDA(cudaMemcpyAsync(&h, cs->dbg_word, sizeof(int), cudaMemcpyDeviceToHost, cs->stream));
+    ACFD_CUDA(cudaStreamSynchronize(cs->stream));
+    if (h != 0) {
+        ACFD_CUDA(cudaMemsetAsync(cs->dbg_word, 0, sizeof(int), cs->stream));
+        set_error("ACFD_DEBUG: %d values of U[%d] not finite after the %s of sweep axis %d", h, l, what, s);
+        return ACFD_ERR_DEVICE;
+    }
+    return ACFD_OK;
+}
+
 int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int tn, int tm, int p)
 {
     StageArgs a;
@@ -593,6 +630,7 @@ int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int 
     a.omaps = nullptr;
     a.status = cs->dstatus;
     a.flags = cs->sensor_flags;
+    a.wait_limit = cs->wait_limit;
     for (int s = 0; s < 3; ++s) {
         const int v = cs->tile_var[cs->mode][s];
         a.var[s] = v < kTileVariants ? v : 0;
@@ -674,6 +712,9 @@ int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int 
             return st;
         }
         ++cs->launches;
+        if ((st = debug_scan(cs, tm, "stage", s)) != ACFD_OK) {
+            return st;
+        }
     }
     return ACFD_OK;
 }
@@ -997,6 +1038,18 @@ int acfd_init(const acfd_partition_t *part, const acfd_model_t *model, acfd_case
     if (getenv("ACFD_PLAIN_KERNELS")) {
         cs->plain_kernels = true;
     }
+    {
+        const char *dbg = getenv("ACFD_DEBUG");
+        if (dbg && atoi(dbg) != 0) {
+            if ((e = cudaMalloc(&cs->dbg_word, sizeof(int))) != cudaSuccess ||
+                (e = cudaMemsetAsync(cs->dbg_word, 0, sizeof(int), cs->stream)) != cudaSuccess) {
+                st = cuda_status(e, "acfd_init (debug word)");
+                acfd_finalize(cs);
+                return st;
+            }
+            cs->debug = true;
+        }
+    }
     if ((st = ib_create(&cs->ib)) != ACFD_OK) {
         acfd_finalize(cs);
         return st;
@@ -1039,6 +1092,7 @@ int acfd_finalize(acfd_case_t *cs)
     cudaFree(cs->dstatus);
     cudaFree(cs->bcbar);
     cudaFree(cs->bc_pairs);
+    cudaFree(cs->dbg_word);
     cudaFree(cs->sensor_params);
     cudaFree(cs->sensor_flags);
     cudaFree(cs->sensor_rp);
@@ -1174,6 +1228,9 @@ int acfd_evolve_fluid(acfd_case_t *cs, double dt)
 int acfd_evolve_fluid_graph(acfd_case_t *cs, double dt)
 {
     TRY(check_case(cs));
+    if (cs->debug) {
+        return acfd_evolve_fluid(cs, dt);  // the per-stage checks synchronize: no capture
+    }
     TRY(set_dt(cs, dt));
     if (!cs->graph_exec || cs->graph_mode != cs->mode) {
         release_graph(cs);
@@ -1281,6 +1338,14 @@ int acfd_set_tiles(acfd_case_t *cs, const int tiles[3])
         cs->tile_var[cs->mode][s] = tiles[s];
     }
     release_graph(cs);
+    return ACFD_OK;
+}
+
+int acfd_set_wait_limit(acfd_case_t *cs, long long polls)
+{
+    TRY(check_case(cs));
+    cs->wait_limit = polls < 0 ? kWaitLimitDefault : polls;
+    release_graph(cs);  // a captured step holds the limit of its stage launches
     return ACFD_OK;
 }
 
@@ -1777,6 +1842,14 @@ struct acfd_batch {
     long long *d_pprefix = nullptr;        // [3][ncase + 1] prefix sums of the plane blocks per sweep axis
     long long pblocks[3] = {0, 0, 0};
     int pthreads[3] = {0, 0, 0}, psmem[3] = {0, 0, 0};
+    // persistent step (plane march, copy-only ghost fills): all stages of a
+    // time step of every case in one launch (stage_plane_persistent)
+    bool persist_ok = false, persist = false;
+    int persist_blocks = 0, persist_threads = 0, persist_smem = 0;
+    unsigned long long *d_queue = nullptr;
+    unsigned *d_done = nullptr, *d_filled = nullptr;  // [kMaxStepStages][ncase]
+    int *d_abort = nullptr;
+    long long *d_pair_off = nullptr;                  // [ncase + 1]
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int graph_mode = -1;
@@ -1817,7 +1890,6 @@ int batch_step(acfd_batch *b)
             b->launches += 2;
         }
     }
-    ACFD_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long) * kBatchStagesPerStep, b->stream));
     static const int order[6] = {2, 1, 0, 0, 1, 2};
     struct Coef {
         double a, c;
@@ -1829,6 +1901,41 @@ int batch_step(acfd_batch *b)
     static const Coef rk2[2] = {{0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN}, {1.0 / 2.0, 1.0 / 2.0, ACFD_TO, ACFD_TN, ACFD_TO}};
     const Coef *rk = b->tScheme == 1 ? rk3 : rk2;
     const int nstage = b->tScheme == 1 ? 3 : 2;
+    if (b->persist && b->plane) {
+        // every stage of the step in one launch, cases and stages linked by
+        // per-case counters
+        PersistStep ps;
+        memset(&ps, 0, sizeof(ps));
+        ps.nk = 6 * nstage;
+        ps.kbase[0] = 0;
+        for (int s = 0; s < 3; ++s) {
+            ps.ntile[s] = b->pblocks[s];
+        }
+        for (int h = 0, k = 0; h < 6; ++h) {
+            for (int q = 0; q < nstage; ++q, ++k) {
+                ps.s_of[k] = order[h];
+                ps.sc[k].coeA = rk[q].a;
+                ps.sc[k].coeB = rk[q].c;
+                ps.sc[k].dt_scale = 0.5;
+                ps.sc[k].to = rk[q].to;
+                ps.sc[k].tn = rk[q].tn;
+                ps.sc[k].tm = rk[q].tm;
+                ps.kbase[k + 1] = ps.kbase[k] + b->pblocks[order[h]] + ncase;
+            }
+        }
+        const size_t nflag = (size_t)kMaxStepStages * ncase;
+        ACFD_CUDA(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned long long), b->stream));
+        ACFD_CUDA(cudaMemsetAsync(b->d_done, 0, sizeof(unsigned) * nflag, b->stream));
+        ACFD_CUDA(cudaMemsetAsync(b->d_filled, 0, sizeof(unsigned) * nflag, b->stream));
+        ACFD_CUDA(cudaMemsetAsync(b->d_abort, 0, sizeof(int), b->stream));
+        TRY(launch_stage_plane_persistent(b->d_cases, b->d_planes, b->d_pmaps, b->d_pprefix, ncase, ps, b->d_dts,
+                                          b->d_levels, b->d_pairs, b->d_pair_off, b->d_queue, b->d_done, b->d_filled,
+                                          b->d_abort, b->d_status, b->visc, hybrid, b->persist_blocks,
+                                          b->persist_threads, b->persist_smem, b->stream));
+        ++b->launches;
+        return ACFD_OK;
+    }
+    ACFD_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long) * kBatchStagesPerStep, b->stream));
     int launch = 0;
     for (int h = 0; h < 6; ++h) {
         const int s = order[h];
@@ -2054,6 +2161,34 @@ int acfd_batch_init(int ncase, const acfd_partition_t *parts, const acfd_model_t
             st = cuda_status(e, "acfd_batch_init");
         }
     }
+    // persistent step: plane maps for every case and copy-only ghost fills
+    if (st == ACFD_OK && b->plane_ok && b->ordered_fill.empty()) {
+        std::vector<long long> off((size_t)ncase + 1, 0);
+        for (const int4 &q : pairs) {
+            ++off[(size_t)q.x + 1];
+        }
+        for (int c = 0; c < ncase; ++c) {
+            off[(size_t)c + 1] += off[(size_t)c];
+        }
+        b->persist_threads = std::max(b->pthreads[0], std::max(b->pthreads[1], b->pthreads[2]));
+        b->persist_smem = std::max(b->psmem[0], std::max(b->psmem[1], b->psmem[2]));
+        int bps = 0;
+        const size_t nflag = (size_t)kMaxStepStages * ncase;
+        if (plane_persistent_occupancy(b->visc, true, b->persist_threads, b->persist_smem, &bps) == ACFD_OK &&
+            bps >= 1 && (e = cudaMalloc(&b->d_queue, sizeof(unsigned long long))) == cudaSuccess &&
+            (e = cudaMalloc(&b->d_done, sizeof(unsigned) * nflag)) == cudaSuccess &&
+            (e = cudaMalloc(&b->d_filled, sizeof(unsigned) * nflag)) == cudaSuccess &&
+            (e = cudaMalloc(&b->d_abort, sizeof(int))) == cudaSuccess &&
+            (e = cudaMalloc(&b->d_pair_off, sizeof(long long) * off.size())) == cudaSuccess &&
+            (e = cudaMemcpy(b->d_pair_off, off.data(), sizeof(long long) * off.size(), cudaMemcpyHostToDevice)) ==
+                cudaSuccess) {
+            b->persist_blocks = bps * b->sms;
+            b->persist_ok = true;
+            b->persist = true;
+        } else {
+            cudaGetLastError();  // keep the per-stage launches
+        }
+    }
     if (st != ACFD_OK) {
         acfd_batch_finalize(b);
         return st;
@@ -2089,6 +2224,11 @@ int acfd_batch_finalize(acfd_batch_t *b)
     cudaFree(b->d_planes);
     cudaFree(b->d_pmaps);
     cudaFree(b->d_pprefix);
+    cudaFree(b->d_queue);
+    cudaFree(b->d_done);
+    cudaFree(b->d_filled);
+    cudaFree(b->d_abort);
+    cudaFree(b->d_pair_off);
     if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
     delete b;
     return ACFD_OK;
@@ -2195,15 +2335,20 @@ int acfd_batch_advance(acfd_batch_t *b, const double *cfl, int steps, double *dt
 int acfd_batch_set_kernel(acfd_batch_t *b, int kernel)
 {
     TRY(batch_check(b));
-    if (kernel != ACFD_BATCH_BRICK && kernel != ACFD_BATCH_PLANE) {
+    if (kernel != ACFD_BATCH_BRICK && kernel != ACFD_BATCH_PLANE && kernel != ACFD_BATCH_PERSISTENT) {
         set_error("acfd_batch_set_kernel: unknown kernel %d", kernel);
         return ACFD_ERR_ARG;
     }
-    if (kernel == ACFD_BATCH_PLANE && !b->plane_ok) {
+    if (kernel != ACFD_BATCH_BRICK && !b->plane_ok) {
         set_error("acfd_batch_set_kernel: the plane-march batch needs all cases viscous or all inviscid");
         return ACFD_ERR_STATE;
     }
-    b->plane = (kernel == ACFD_BATCH_PLANE);
+    if (kernel == ACFD_BATCH_PERSISTENT && !b->persist_ok) {
+        set_error("acfd_batch_set_kernel: the persistent step needs copy-only ghost fills in every case");
+        return ACFD_ERR_STATE;
+    }
+    b->plane = (kernel != ACFD_BATCH_BRICK);
+    b->persist = (kernel == ACFD_BATCH_PERSISTENT);
     batch_release_graph(b);
     return ACFD_OK;
 }

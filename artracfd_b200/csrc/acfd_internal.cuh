@@ -52,7 +52,13 @@ struct StageArgs {
     int var[3];               // tile variant of each sweep axis (brick_geometry.cuh)
     int *status;          // device error word of the case
     const uint8_t *flags; // hybrid form: sensor flags [3][node] (1 = full WENO5)
+    long long wait_limit; // polls of a plane-march wait for a TMA plane or a free ring slot
 };
+
+// polls of a bounded device wait before it gives up (kernels then write their
+// status word and leave; the wait for a block's own copies in flight before
+// it ends always uses this default)
+constexpr long long kWaitLimitDefault = 1LL << 22;
 
 // one case of a batch (batch.cu), as the batched kernels see it
 struct BatchCase {
@@ -93,7 +99,11 @@ int launch_batch_dt(const double *const *vmax, const double *d, const double *cf
 // warp streams halo'd planes of U[tn] into a ring of kPlaneSlots slots.
 constexpr int kPlaneSlots = 6;
 constexpr int kPlaneMaxThreads = 256;
-constexpr int kPlaneSmemMax = 110 * 1024;
+constexpr int kPlaneSmemMax = 112 * 1024;  // two blocks per SM (228 KB, 1 KB reserved per block)
+// hybrid form: per consumer warp, the WENO5 inputs of kCoopSlots flagged
+// interfaces (2 sides x 5 fields x 5 points, FP32) shared out over the warp
+constexpr int kCoopSlots = 6;
+constexpr int kCoopBytes = kCoopSlots * 50 * 4;
 
 // bytes of one ring slot: a TMA destination in shared memory starts on a
 // 128-byte boundary, so the slot stride is rounded up to it
@@ -104,10 +114,17 @@ __host__ __device__ inline int plane_slot_bytes(int BXp, int BC)
 
 // shared memory of a plane-march block: the ring, the X sweep's double-
 // buffered interface fluxes (nflux interfaces, five values of at most 8
-// bytes) and the full/empty barriers
-__host__ __device__ inline int plane_smem_total(int BXp, int BC, int nflux)
+// bytes), the hybrid form's per-warp WENO buffers of the ncw consumer warps
+// and the full/empty barriers
+__host__ __device__ inline int plane_flux_bytes(int nflux)
 {
-    return kPlaneSlots * plane_slot_bytes(BXp, BC) + ((2 * nflux * 5 * 8 + 127) & ~127) + 2 * kPlaneSlots * 8;
+    return (2 * nflux * 5 * 8 + 127) & ~127;
+}
+
+__host__ __device__ inline int plane_smem_total(int BXp, int BC, int nflux, int ncw)
+{
+    return kPlaneSlots * plane_slot_bytes(BXp, BC) + plane_flux_bytes(nflux) + ncw * kCoopBytes +
+           2 * kPlaneSlots * 8;
 }
 
 struct PlaneTile {
@@ -145,7 +162,8 @@ inline PlaneTile plane_tile(const Grid &g, int s, bool visc, int waves, int sms,
     if (pt.NR < 1) pt.NR = 1;
     pt.BXp = (pt.WX + 2 * hx + 2) & ~1;
     // the ring of kPlaneSlots planes (and the X sweep's flux exchange) must fit
-    while (pt.NR > 1 && plane_smem_total(pt.BXp, pt.NR + 2 * hv, s == 0 ? pt.TR * pt.NR : 0) > kPlaneSmemMax) {
+    while (pt.NR > 1 && plane_smem_total(pt.BXp, pt.NR + 2 * hv, s == 0 ? pt.TR * pt.NR : 0,
+                                         (pt.TR * pt.NR + 31) / 32) > kPlaneSmemMax) {
         --pt.NR;
     }
     pt.ntc = (Lt + pt.NR - 1) / pt.NR;
@@ -178,7 +196,7 @@ inline PlaneTile plane_tile(const Grid &g, int s, bool visc, int waves, int sms,
 
 inline int plane_smem_bytes(const PlaneTile &pt, int s)
 {
-    return plane_smem_total(pt.BXp, pt.BC, s == 0 ? pt.TR * pt.NR : 0);
+    return plane_smem_total(pt.BXp, pt.BC, s == 0 ? pt.TR * pt.NR : 0, pt.ncw);
 }
 
 // plane-march geometry of one case and sweep axis of a batch: the kernel's
@@ -194,6 +212,35 @@ int launch_stage_plane_batch(const BatchCase *cases, const BatchPlane *planes, c
                              const long long *prefix, long long blocks, int ncase, const StageCoefs &sc,
                              const double *dts, int *status, int s, bool viscous, bool hybrid, int nthreads, int smem,
                              cudaStream_t st);
+
+// Persistent batch step: every RK stage of one time step of every case in
+// one launch.  Work items, in order: for each stage k of the step, the plane
+// blocks of every case (case order) and then one ghost-fill item per case.
+// A plane block of stage k > 0 of case c waits until the fill of stage k-1
+// of case c is done; the fill of stage k of case c waits until all its plane
+// blocks of stage k are done (per-case counters, no grid-wide barrier).
+// Items are taken from a queue in order, so every item a block waits for was
+// taken earlier by a running block.
+constexpr int kMaxStepStages = 18;
+struct PersistStep {
+    int nk;                               // stages of the step
+    int s_of[kMaxStepStages];             // sweep axis of stage k
+    StageCoefs sc[kMaxStepStages];
+    long long kbase[kMaxStepStages + 1];  // first item of stage k
+    long long ntile[3];                   // plane blocks of one stage along axis s, all cases
+};
+// queue: one counter; done, filled: [nk][ncase] (zero at launch); abort: one
+// word set by a block whose wait gave up (status code 7), after which every
+// block leaves; pairs: (case, dst, src) copy pairs of the ghost fill, case
+// by case, pair_off[c] .. pair_off[c + 1] those of case c
+int launch_stage_plane_persistent(const BatchCase *cases, const BatchPlane *planes, const CUtensorMap *pmaps,
+                                  const long long *prefix, int ncase, const PersistStep &ps, const double *dts,
+                                  const BatchLevel *levels, const int4 *pairs, const long long *pair_off,
+                                  unsigned long long *queue, unsigned *done, unsigned *filled, int *abort,
+                                  int *status, bool viscous, bool hybrid, int blocks, int nthreads, int smem,
+                                  cudaStream_t st);
+// resident blocks per SM of the persistent batch kernel
+int plane_persistent_occupancy(bool viscous, bool hybrid, int nthreads, int smem, int *blocks_per_sm);
 
 // learned sensor (sensor.cu)
 // Flags of the PIN nodes (the caller sets the others to 1 once); rho_p:
@@ -249,6 +296,8 @@ int launch_domain_boundary(const Grid &g, const ModelParams &m, const acfd_parti
 // ghost fill as one gather: U[dst] = U[src] for every (dst, src) pair, all
 // five variables of the level U
 int launch_ghost_gather(const Grid &g, const int2 *pairs, int count, double *U, cudaStream_t st);
+// debug mode: add the count of non-finite values among U[0, count) to *word
+int launch_finite_scan(const double *U, long long count, int *word, cudaStream_t st);
 // ghost fill as one launch of formulas: per-face constants of the programs
 // (type, outward normal, given primitive state of faces 1..6), op codes
 // (low 3 bits; the face in the bits above), the value-stack depth

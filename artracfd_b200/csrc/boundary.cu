@@ -244,6 +244,21 @@ __device__ void fill_node(const Grid &g, const ModelParams &mp, const FaceJob &J
     store5(U, nn, id, Ut);
 }
 
+// debug mode: count the non-finite values of one level (all nodes, all five
+// variables; padding and never-written nodes hold finite values)
+__global__ void finite_scan(const double *__restrict__ U, long long count, int *word)
+{
+    int bad = 0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < count;
+         t += (long long)gridDim.x * blockDim.x) {
+        bad += !isfinite(U[t]);
+    }
+    bad = __reduce_add_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0 && bad > 0) {
+        atomicAdd(word, bad);
+    }
+}
+
 // CFL: per-direction max of |u_s| + sqrt(gamma*gasR*T) over PIN nodes with
 // did == 0 (the max is order independent, so the result is the reference's)
 __device__ __forceinline__ double vmax_of(double a, double b)
@@ -456,6 +471,22 @@ unsigned blocks_for(long long n, int bs)
 
 }  // namespace
 
+// U[dst] = U[src], all five variables: the five loads are issued before the
+// first store (U is both read and written, so a store may not be moved above
+// a later load; loads issued first keep five requests in flight)
+__device__ __forceinline__ void copy_node(double *U, long long nn, long long dst, long long src)
+{
+    double u[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        u[v] = U[v * nn + src];
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        U[v * nn + dst] = u[v];
+    }
+}
+
 // Ghost fill of a case whose faces are all copies (periodic, outflow): every
 // changed node takes the value of one unchanged node, so the ordered faces
 // collapse into one gather (pairs: destination, source node index)
@@ -464,10 +495,7 @@ __global__ void ghost_gather(long long nn, const int2 *__restrict__ pairs, int c
     pdl_wait();
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
         const int2 q = pairs[t];
-#pragma unroll
-        for (int v = 0; v < 5; ++v) {
-            U[v * nn + q.x] = U[v * nn + q.y];
-        }
+        copy_node(U, nn, q.x, q.y);
     }
 }
 
@@ -498,10 +526,7 @@ __global__ void __launch_bounds__(256) ghost_program(long long nn, const int2 *_
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         if (t < npairs) {
             const int2 q = pairs[t];
-#pragma unroll
-            for (int v = 0; v < 5; ++v) {
-                U[v * nn + q.x] = U[v * nn + q.y];
-            }
+            copy_node(U, nn, q.x, q.y);
             continue;
         }
         const int4 pr = progs[t - npairs];  // dst, first op, op count
@@ -560,11 +585,7 @@ __global__ void batch_ghost_gather(const BatchLevel *__restrict__ cases, const i
          t += (long long)gridDim.x * blockDim.x) {
         const int4 q = pairs[t];
         const BatchLevel c = cases[q.x];
-        double *U = c.U + (long long)tn * 5 * c.nn;
-#pragma unroll
-        for (int v = 0; v < 5; ++v) {
-            U[v * c.nn + q.y] = U[v * c.nn + q.z];
-        }
+        copy_node(c.U + (long long)tn * 5 * c.nn, c.nn, q.y, q.z);
     }
 }
 
@@ -733,6 +754,14 @@ int launch_cfl(const Grid &g, const ModelParams &m, const double *U, const int *
     cudaError_t e = launch_k(cfl_partial, dim3(kCflBlocks), dim3(256), 0, st, g, m, U, did, partials);
     if (e == cudaSuccess) e = launch_k(cfl_final, dim3(1), dim3(32), 0, st, (const double *)partials, (int)kCflBlocks, out);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "cfl launch");
+}
+
+int launch_finite_scan(const double *U, long long count, int *word, cudaStream_t st)
+{
+    const unsigned blocks = (unsigned)std::min<long long>(blocks_for(count, 256), 148LL * 8);
+    finite_scan<<<blocks, 256, 0, st>>>(U, count, word);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "finite_scan launch");
 }
 
 int launch_stage_phi(const Grid &g, const ModelParams &m, const StageArgs &a, cudaStream_t st)

@@ -558,6 +558,7 @@ stage_batch(const BatchCase *cases, const CUtensorMap *maps, const long long *pr
         a.var[0] = a.var[1] = a.var[2] = 0;
         a.status = status;
         a.flags = C.flags;
+        a.wait_limit = kWaitLimitDefault;
         if (!brick_tile<S, 6, true, HYB, 0>(C.g, C.mp, a, maps + 3 * lo + S, tx, ty, tz, smem, parity)) {
             break;
         }

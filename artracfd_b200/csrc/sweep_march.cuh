@@ -247,6 +247,99 @@ __device__ __forceinline__ void march_flux(const ModelParams &mp, const Real (&W
     back_project<S>(is, G, F);
 }
 
+// The hybrid interface flux with the full WENO5 branch shared out over the
+// warp.  The flagged lanes (full) need ten WENO5 evaluations each (five characteristic fields, two
+// sides).  Taken lane by lane, a warp with one flagged lane runs all ten for
+// that lane alone; here the flagged lanes write their WENO5 inputs to the
+// warp's buffer (kCoopSlots interfaces per round) and every lane of the warp
+// evaluates some of them, so a warp with k flagged lanes spends about
+// ceil(k / kCoopSlots) * ceil(10 kCoopSlots / 32) WENO5 passes instead of
+// ten; the other lanes then take the linear-weight flux.  A warp with more
+// than 16 flagged lanes takes the lane-by-lane branch.
+// The arithmetic of each evaluation is that of march_weno.  All 32 lanes of
+// the warp must call this together (plane-march kernels: every consumer lane
+// runs the same march).
+template <int S>
+__device__ __forceinline__ void march_flux_coop(const ModelParams &mp, const Real (&W)[6][5], bool full, Real F[5],
+                                                Real *wbuf)
+{
+    constexpr unsigned kAll = 0xffffffffu;
+    const IfaceState<Real> is = march_state<S>(mp, W[2], W[3]);
+    Real G[5];
+    unsigned fm = __ballot_sync(kAll, full);
+    if (__popc(fm) > 16) {
+        if (full) {
+            march_weno<S, 6>(is, W, G);
+        } else {
+            march_linear<S>(is, W, G);
+        }
+    } else {
+        const int lane = threadIdx.x & 31;
+        while (fm) {
+            // this round: the lowest kCoopSlots flagged lanes
+            unsigned rest = fm;
+#pragma unroll
+            for (int k = 0; k < kCoopSlots; ++k) rest &= rest - 1;
+            const unsigned chunk = fm & ~rest;
+            fm = rest;
+            const bool mine = (chunk >> lane) & 1u;
+            const int slot = __popc(chunk & ((1u << lane) - 1u));
+            if (mine) {
+                Real A[6], Bv[6];
+#pragma unroll
+                for (int m = 0; m < 6; ++m) {
+                    A[m] = is.qk * W[m][0] - is.V[0] * W[m][1] - is.V[1] * W[m][2] - is.V[2] * W[m][3] + W[m][4];
+                    Bv[m] = is.V[S] * W[m][0] - W[m][S + 1];
+                }
+                Real *o = wbuf + slot * 50;
+#pragma unroll
+                for (int r = 0; r < 5; ++r) {
+                    Real C[6];
+#pragma unroll
+                    for (int m = 0; m < 6; ++m) {
+                        if (r == 0) {
+                            C[m] = is.b * A[m] + is.d * Bv[m];
+                        } else if (r == 4) {
+                            C[m] = is.b * A[m] - is.d * Bv[m];
+                        } else if (r == S + 1) {
+                            C[m] = W[m][0] - is.b2 * A[m];
+                        } else {
+                            C[m] = W[m][r] - is.b2 * is.V[r - 1] * A[m];
+                        }
+                    }
+                    const Real lp = is.lp[r], ln = is.ln[r];
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) {
+                        o[(2 * r) * 5 + m] = lp * C[m];
+                        o[(2 * r + 1) * 5 + m] = ln * C[5 - m];
+                    }
+                }
+            }
+            __syncwarp();
+            // task t = slot * 10 + 2 * field + side reads inputs [5t, 5t+5)
+            // and leaves its result in the first of them
+            const int ntask = __popc(chunk) * 10;
+            for (int t = lane; t < ntask; t += 32) {
+                Real *f = wbuf + t * 5;
+                f[0] = fast::weno5<Real>(f[0], f[1], f[2], f[3], f[4]);
+            }
+            __syncwarp();
+            if (mine) {
+                const Real *o = wbuf + slot * 50;
+#pragma unroll
+                for (int r = 0; r < 5; ++r) {
+                    G[r] = o[(2 * r) * 5] + o[(2 * r + 1) * 5];
+                }
+            }
+            __syncwarp();
+        }
+        if (!full) {
+            march_linear<S>(is, W, G);
+        }
+    }
+    back_project<S>(is, G, F);
+}
+
 // node update from the fluxes of its left and right interfaces
 __device__ __forceinline__ void march_update(const StageArgs &a, long long nn, long long id, double rdt,
                                              const Real Fl[5], const Real Fr[5], bool same_o)

@@ -14,7 +14,10 @@
 //    in shared memory, and the node update reads U[tn] of its node from the
 //    ring.
 // Every plane of U[tn] crosses from L2 once per tile (halo included), and the
-// loads run ahead of the arithmetic without holding registers.
+// loads run ahead of the arithmetic without holding registers.  The direct
+// loads of other levels (U[to] at the node) go to L2 (__ldcg): a block of the
+// persistent batch kernel may read a level that another SM rewrote since this
+// SM last cached it in L1.
 //
 // Included after sweep_march.cuh by sweep_fast.cu and sweep_fp32.cu.
 #pragma once
@@ -26,7 +29,7 @@
 namespace acfd {
 namespace ACFD_NS {
 
-constexpr long long kPlaneWaitLimit = 1LL << 22;
+constexpr long long kPlaneWaitLimit = kWaitLimitDefault;
 
 // One instantiation serves both axes: the kernel is written for the Y sweep
 // (S = 1, rows along z).  A Z sweep runs it on a grid descriptor with axes 1
@@ -54,7 +57,8 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
     const int plane_bytes = pe * 5 * 8;
     const int slot_doubles = plane_slot_bytes(pt.BXp, pt.BC) / 8;  // 128-byte aligned slots
     double *ring = reinterpret_cast<double *>(smem);
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)NS * slot_doubles * 8);
+    Real *coop = reinterpret_cast<Real *>(smem + (size_t)NS * slot_doubles * 8);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)NS * slot_doubles * 8 + (size_t)pt.ncw * kCoopBytes);
     uint64_t *empty = full + NS;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -130,7 +134,7 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
                 for (int ql = 0; ql < NQ; ++ql, ++q) {
                     const int slot = q % NS;
                     if (q >= NS && !tma::mbar_wait_bounded(empty + slot, ((q / NS) - 1) & 1, a.status, 5,
-                                                           kPlaneWaitLimit)) {
+                                                           a.wait_limit)) {
                         ok = false;
                         break;
                     }
@@ -181,7 +185,7 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
         auto plane = [&](int q) { return ring + (size_t)((qbase + q) % NS) * slot_doubles; };
         auto wait_plane = [&](int q) {
             const int qq = qbase + q;
-            const bool ok = tma::mbar_wait_bounded(full + qq % NS, (qq / NS) & 1, a.status, 5, kPlaneWaitLimit);
+            const bool ok = tma::mbar_wait_bounded(full + qq % NS, (qq / NS) & 1, a.status, 5, a.wait_limit);
             return __all_sync(kAll, ok);
         };
         auto release = [&](int q) {
@@ -243,7 +247,7 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
                 did = a.did[id];
                 if (!same_o && !a.accumulate) {
     #pragma unroll
-                    for (int v = 0; v < 5; ++v) uo[v] = a.Uo[vg(v) * nn + id];
+                    for (int v = 0; v < 5; ++v) uo[v] = __ldcg(a.Uo + vg(v) * nn + id);
                 }
             }
             bool full_w = true;
@@ -260,7 +264,11 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
                 tdiff(plane(q0 + 1), Dn);
             }
             Real F[5];
-            march_flux<S, NP, HYB>(mp, W, full_w, F);
+            if constexpr (HYB && NP == 6) {
+                march_flux_coop<S>(mp, W, full_w, F, coop + (size_t)warp * (kCoopBytes / sizeof(Real)));
+            } else {
+                march_flux<S, NP, HYB>(mp, W, full_w, F);
+            }
             if (VISC) {
                 march_visc<S>(g, mp, Pc, Pn, Dc, Dn, F);
             }
@@ -273,7 +281,7 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
                         const long long qv = vg(v) * nn + id;
                         const double un = P[vg(v) * pe + e0];
                         if (a.accumulate) {
-                            a.Um[qv] = a.Um[qv] + a.coeB * rdt * phi;
+                            a.Um[qv] = __ldcg(a.Um + qv) + a.coeB * rdt * phi;
                         } else {
                             a.Um[qv] = a.coeA * (same_o ? un : uo[v]) + a.coeB * (un + rdt * phi);
                         }
@@ -343,8 +351,9 @@ __device__ __forceinline__ void plane_x_block(const Grid &g, const ModelParams &
     const int nflux = pt.TR * pt.NR;
     double *ring = reinterpret_cast<double *>(smem);
     Real *sF = reinterpret_cast<Real *>(smem + (size_t)NS * slot_doubles * 8);
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)NS * slot_doubles * 8 +
-                                                  ((2 * nflux * 5 * 8 + 127) & ~127));
+    Real *coop = reinterpret_cast<Real *>(smem + (size_t)NS * slot_doubles * 8 + plane_flux_bytes(nflux));
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)NS * slot_doubles * 8 + plane_flux_bytes(nflux) +
+                                                  (size_t)pt.ncw * kCoopBytes);
     uint64_t *empty = full + NS;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -379,7 +388,7 @@ __device__ __forceinline__ void plane_x_block(const Grid &g, const ModelParams &
             for (int q = 0; q < NQ; ++q) {
                 const int slot = q % NS;
                 if (q >= NS && !tma::mbar_wait_bounded(empty + slot, ((q / NS) - 1) & 1, a.status, 5,
-                                                       kPlaneWaitLimit)) {
+                                                       a.wait_limit)) {
                     break;
                 }
                 tma::mbar_expect_tx(full + slot, plane_bytes);
@@ -412,7 +421,7 @@ __device__ __forceinline__ void plane_x_block(const Grid &g, const ModelParams &
     const uint8_t *__restrict__ fl = a.flags;  // sweep 0 flags
     auto plane = [&](int q) { return ring + (size_t)(q % NS) * slot_doubles; };
     auto wait_plane = [&](int q) {
-        const bool ok = tma::mbar_wait_bounded(full + q % NS, (q / NS) & 1, a.status, 5, kPlaneWaitLimit);
+        const bool ok = tma::mbar_wait_bounded(full + q % NS, (q / NS) & 1, a.status, 5, a.wait_limit);
         return __all_sync(kAll, ok);
     };
     auto release = [&](int q) {
@@ -459,7 +468,7 @@ __device__ __forceinline__ void plane_x_block(const Grid &g, const ModelParams &
         double uo[5];
         if (upd && !same_o && !a.accumulate) {
 #pragma unroll
-            for (int v = 0; v < 5; ++v) uo[v] = a.Uo[v * nn + id];
+            for (int v = 0; v < 5; ++v) uo[v] = __ldcg(a.Uo + v * nn + id);
         }
         const bool full_w = !HYB || fl_j != 0u;
         ok = ok && wait_plane(q + hv);  // row j+1 (viscous) or j
@@ -471,7 +480,11 @@ __device__ __forceinline__ void plane_x_block(const Grid &g, const ModelParams &
             for (int v = 0; v < 5; ++v) W[m][v] = Real(P[v * pe + e0 - (H - 1) + m]);
         }
         Real F[5];
-        march_flux<0, NP, HYB>(mp, W, full_w, F);
+        if constexpr (HYB && NP == 6) {
+            march_flux_coop<0>(mp, W, full_w, F, coop + (size_t)warp * (kCoopBytes / sizeof(Real)));
+        } else {
+            march_flux<0, NP, HYB>(mp, W, full_w, F);
+        }
         if (VISC) {
             Real Pc[4], Pn[4], Dc[2][2], Dn[2][2];
             march_prims(W[H - 1], cvinv, Pc);
@@ -512,7 +525,7 @@ __device__ __forceinline__ void plane_x_block(const Grid &g, const ModelParams &
                 const long long qv = v * nn + id;
                 const double un = P[v * pe + e0];
                 if (a.accumulate) {
-                    a.Um[qv] = a.Um[qv] + a.coeB * rdt * phi;
+                    a.Um[qv] = __ldcg(a.Um + qv) + a.coeB * rdt * phi;
                 } else {
                     a.Um[qv] = a.coeA * (same_o ? un : uo[v]) + a.coeB * (un + rdt * phi);
                 }
@@ -666,6 +679,7 @@ stage_plane_batch(const BatchCase *__restrict__ cases, const BatchPlane *__restr
     a.var[0] = a.var[1] = a.var[2] = 0;
     a.status = status;
     a.flags = C.flags;
+    a.wait_limit = kWaitLimitDefault;
     const int blk = (int)(item - prefix[lo]);
     if (XS) {
         plane_x_block<NP, VISC, HYB>(P.gk, C.mp, a, P.pt, pmaps + 3 * lo + s, blk, smem);
@@ -716,6 +730,209 @@ static int launch_plane_batch_impl(const BatchCase *cases, const BatchPlane *pla
         if (hybrid) { ACFD_PB(false, true) } else { ACFD_PB(false, false) }
     }
 #undef ACFD_PB
+}
+// ---------------------------------------------------------------------------
+// persistent batch step (see PersistStep)
+// ---------------------------------------------------------------------------
+constexpr long long kPersistWaitLimit = 1LL << 24;  // polls of 64+ ns: about a second or more
+
+// bounded wait until *word >= want (acquire); false when it gave up (status 7,
+// abort set) or another block aborted
+__device__ __forceinline__ bool persist_wait(const unsigned *word, unsigned want, int *abort, int *status)
+{
+    for (long long it = 0; it < kPersistWaitLimit; ++it) {
+        unsigned v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(word) : "memory");
+        if (v >= want) {
+            return true;
+        }
+        if (*reinterpret_cast<volatile int *>(abort) != 0) {
+            return false;
+        }
+        __nanosleep(64);
+    }
+    atomicExch(status, 7);
+    atomicExch(abort, 1);
+    return false;
+}
+
+// the block bodies as calls of their own, so that each keeps the register
+// allocation of its single-case kernel inside the persistent loop
+template <bool VISC, bool HYB>
+__device__ __noinline__ void persist_x_item(const Grid &g, const ModelParams &mp, const StageArgs &a,
+                                            const PlaneTile &pt, const CUtensorMap *mapp, int blk, unsigned char *smem)
+{
+    plane_x_block<6, VISC, HYB>(g, mp, a, pt, mapp, blk, smem);
+}
+
+template <bool VISC, bool HYB>
+__device__ __noinline__ void persist_yz_item(const Grid &g, const ModelParams &mp, const StageArgs &a,
+                                             const PlaneTile &pt, const CUtensorMap *mapp, int blk, unsigned char *smem)
+{
+    plane_yz_block<6, VISC, HYB>(g, mp, a, pt, mapp, blk, smem);
+}
+
+template <bool VISC, bool HYB>
+__global__ void __launch_bounds__(kPlaneMaxThreads, 2)
+stage_plane_persistent(const BatchCase *__restrict__ cases, const BatchPlane *__restrict__ planes,
+                       const CUtensorMap *pmaps, const long long *__restrict__ prefix, int ncase, PersistStep ps,
+                       const double *dts, const BatchLevel *__restrict__ levels, const int4 *__restrict__ pairs,
+                       const long long *__restrict__ pair_off, unsigned long long *queue, unsigned *done,
+                       unsigned *filled, int *abort, int *status)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ long long s_item;
+    __shared__ int s_ok;
+    const long long total = ps.kbase[ps.nk];
+    for (;;) {
+        if (threadIdx.x == 0) {
+            s_item = (*reinterpret_cast<volatile int *>(abort) != 0) ? total : (long long)atomicAdd(queue, 1ULL);
+        }
+        __syncthreads();
+        const long long it = s_item;
+        if (it >= total) {
+            break;
+        }
+        int k = 0;
+        while (it >= ps.kbase[k + 1]) ++k;
+        const int s = ps.s_of[k];
+        const long long local = it - ps.kbase[k];
+        const long long *pre = prefix + (long long)s * (ncase + 1);
+        if (local < ps.ntile[s]) {
+            int lo = 0, hi = ncase - 1;  // the case whose blocks contain this one
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) / 2;
+                if (pre[mid] <= local) lo = mid; else hi = mid - 1;
+            }
+            const int c = lo;
+            if (threadIdx.x == 0) {
+                s_ok = (k == 0) || persist_wait(filled + (long long)(k - 1) * ncase + c, 1u, abort, status);
+            }
+            __syncthreads();
+            if (!s_ok) {
+                break;
+            }
+            // the planes this block's TMA copies read were written by other
+            // blocks' ordinary stores
+            asm volatile("fence.proxy.async.global;" ::: "memory");
+            const BatchCase &C = cases[c];
+            const BatchPlane &P = planes[3 * c + s];
+            const StageCoefs &sc = ps.sc[k];
+            StageArgs a;
+            const long long lv = 5LL * C.g.nn;
+            a.Uo = C.U + sc.to * lv;
+            a.Un = C.U + sc.tn * lv;
+            a.Um = C.U + sc.tm * lv;
+            a.did = C.did;
+            a.dt = dts + c;
+            a.dt_scale = sc.dt_scale;
+            a.coeA = sc.coeA;
+            a.coeB = sc.coeB;
+            a.accumulate = 0;
+            a.to = sc.to;
+            a.tn = sc.tn;
+            a.tm = sc.tm;
+            a.maps = nullptr;
+            a.omaps = nullptr;
+            a.var[0] = a.var[1] = a.var[2] = 0;
+            a.status = status;
+            a.flags = C.flags;
+            a.wait_limit = kWaitLimitDefault;
+            const int blk = (int)(local - pre[c]);
+            if (s == 0) {
+                persist_x_item<VISC, HYB>(P.gk, C.mp, a, P.pt, pmaps + 3 * c + s, blk, smem);
+            } else {
+                persist_yz_item<VISC, HYB>(P.gk, C.mp, a, P.pt, pmaps + 3 * c + s, blk, smem);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();
+                atomicAdd(done + (long long)k * ncase + c, 1u);
+            }
+        } else {
+            const int c = (int)(local - ps.ntile[s]);
+            if (threadIdx.x == 0) {
+                s_ok = persist_wait(done + (long long)k * ncase + c, (unsigned)(pre[c + 1] - pre[c]), abort, status);
+            }
+            __syncthreads();
+            if (!s_ok) {
+                break;
+            }
+            // the ghost fill of case c (copy pairs), reading through L2
+            const BatchLevel L = levels[c];
+            double *U = L.U + (long long)ps.sc[k].tm * 5 * L.nn;
+            for (long long t = pair_off[c] + threadIdx.x; t < pair_off[c + 1]; t += blockDim.x) {
+                const int4 q = pairs[t];
+                double u[5];
+#pragma unroll
+                for (int v = 0; v < 5; ++v) u[v] = __ldcg(U + v * L.nn + q.z);
+#pragma unroll
+                for (int v = 0; v < 5; ++v) U[v * L.nn + q.y] = u[v];
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();
+                atomicExch(filled + (long long)k * ncase + c, 1u);
+            }
+        }
+    }
+}
+
+template <bool VISC, bool HYB>
+static int launch_plane_persistent_one(const BatchCase *cases, const BatchPlane *planes, const CUtensorMap *pmaps,
+                                       const long long *prefix, int ncase, const PersistStep &ps, const double *dts,
+                                       const BatchLevel *levels, const int4 *pairs, const long long *pair_off,
+                                       unsigned long long *queue, unsigned *done, unsigned *filled, int *abort,
+                                       int *status, int blocks, int nthreads, int smem, cudaStream_t st)
+{
+    static bool configured[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(stage_plane_persistent<VISC, HYB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, kPlaneSmemMax);
+        if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(stage_plane_persistent)");
+        configured[dev] = true;
+    }
+    cudaError_t e = launch_k(stage_plane_persistent<VISC, HYB>, dim3((unsigned)blocks), dim3(nthreads), smem, st,
+                             cases, planes, pmaps, prefix, ncase, ps, dts, levels, pairs, pair_off, queue, done, filled,
+                             abort, status);
+    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "stage_plane_persistent launch");
+}
+
+static int launch_plane_persistent_impl(const BatchCase *cases, const BatchPlane *planes, const CUtensorMap *pmaps,
+                                        const long long *prefix, int ncase, const PersistStep &ps, const double *dts,
+                                        const BatchLevel *levels, const int4 *pairs, const long long *pair_off,
+                                        unsigned long long *queue, unsigned *done, unsigned *filled, int *abort,
+                                        int *status, bool viscous, bool hybrid, int blocks, int nthreads, int smem,
+                                        cudaStream_t st)
+{
+    if (smem > kPlaneSmemMax || nthreads > kPlaneMaxThreads || ps.nk < 1 || ps.nk > kMaxStepStages) {
+        set_error("persistent batch launch: %d threads, %d bytes of shared memory, %d stages", nthreads, smem, ps.nk);
+        return ACFD_ERR_ARG;
+    }
+#define ACFD_PP(V_, H_)                                                                                           \
+    return launch_plane_persistent_one<V_, H_>(cases, planes, pmaps, prefix, ncase, ps, dts, levels, pairs, pair_off, \
+                                               queue, done, filled, abort, status, blocks, nthreads, smem, st);
+    if (viscous) {
+        if (hybrid) { ACFD_PP(true, true) } else { ACFD_PP(true, false) }
+    } else {
+        if (hybrid) { ACFD_PP(false, true) } else { ACFD_PP(false, false) }
+    }
+#undef ACFD_PP
+}
+
+static int plane_persistent_occupancy_impl(bool viscous, bool hybrid, int nthreads, int smem, int *blocks_per_sm)
+{
+    const void *fn = viscous ? (hybrid ? (const void *)stage_plane_persistent<true, true>
+                                       : (const void *)stage_plane_persistent<true, false>)
+                             : (hybrid ? (const void *)stage_plane_persistent<false, true>
+                                       : (const void *)stage_plane_persistent<false, false>);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kPlaneSmemMax);
+    if (e == cudaSuccess) {
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, nthreads, smem);
+    }
+    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "persistent batch occupancy");
 }
 #endif
 

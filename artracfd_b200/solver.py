@@ -69,6 +69,12 @@ class Solver:
         t = (ctypes.c_int * 3)(*[int(v) for v in tiles])
         check(self.lib.acfd_set_tiles(self.h, t), self.lib)
 
+    def set_wait_limit(self, polls: int):
+        """Polls of the plane-march kernels' bounded device waits before they
+        give up and report through the status word (acfd_set_wait_limit);
+        a negative value restores the default."""
+        check(self.lib.acfd_set_wait_limit(self.h, int(polls)), self.lib)
+
     # learned sensor -------------------------------------------------------
     def sensor_load(self, params: np.ndarray, threshold: float):
         """Trained sensor parameters and the probability threshold above which

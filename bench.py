@@ -433,9 +433,13 @@ def _form_block(torch, part, model, node, spec, form, nodes_pin, args, dist, str
     sec, launches, clk = _timed_steps(torch, s, spec, args.steps, args.warmup, dist, stream, local_rank, label)
     out = {"value": job_rate(int(os.environ.get("WORLD_SIZE", "1")), nodes_pin, args.steps, sec),
            "ms_per_step": sec / args.steps * 1e3, "tiles": tiles, "clocks": clk, "gpu_launches": launches}
+    if form == "hybrid":
+        out["flagged_fraction"] = s.sensor_update() / (3.0 * nodes_pin)
     if profile:
-        st, bc, by = _stage_profile(torch, s, spec, nodes_pin, stream)
-        out["stage_ms"] = {"sweep_mean": st, "ghost_fill_mean": bc}
+        per_axis = {}
+        st, bc, by = _stage_profile(torch, s, spec, nodes_pin, stream, per_axis)
+        out["stage_ms"] = {"sweep_mean": st, "ghost_fill_mean": bc,
+                           "per_axis": {str(ax): sum(d["ms"]) / len(d["ms"]) for ax, d in sorted(per_axis.items())}}
         if hbm_peak:
             out["hbm_frac"] = by / (st / 1e3) / 1e9 / hbm_peak
         out["_stage_mean_ms"] = st

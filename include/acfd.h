@@ -184,6 +184,14 @@ int acfd_autotune(acfd_case_t *cs, int tiles[3]);
 /* Select the stage-kernel variant of each sweep axis for the current
  * arithmetic form (tests and experiments; acfd_autotune picks by timing). */
 int acfd_set_tiles(acfd_case_t *cs, const int tiles[3]);
+/* Polls of the bounded device waits of the plane-march stage kernels (a TMA
+ * plane in the ring, a free ring slot) before they give up: the kernel then
+ * writes the case's status word and leaves, and the next call that reads the
+ * status (acfd_sync_to_host, acfd_cfl, ...) returns ACFD_ERR_DEVICE and clears
+ * it.  polls < 0 restores the default (4,194,304); 0 gives up at the first
+ * wait, which is how failure detection is tested without a GPU fault.  No
+ * counterpart in the reference (it has no device waits). */
+int acfd_set_wait_limit(acfd_case_t *cs, long long polls);
 /* Number of kernels this case has launched so far (graph replays count their
  * kernel nodes).  No reference counterpart: instrumentation (the reference
  * only times whole steps, timer.c:22-35). */
@@ -386,11 +394,18 @@ int acfd_batch_sensor_load(acfd_batch_t *b, const float *params, float threshold
  * c; dts (optional, steps x ncase doubles) receives the dt of every case and
  * step.  Returns after the work has finished. */
 int acfd_batch_advance(acfd_batch_t *b, const double *cfl, int steps, double *dts);
-/* Stage kernel of the batch: ACFD_BATCH_PLANE (the plane march; the default
- * when all cases are viscous or all inviscid) or ACFD_BATCH_BRICK (the
- * persistent brick kernel that pulls (case, tile) items from a counter). */
+/* Stage kernel of the batch:
+ *  ACFD_BATCH_PERSISTENT  every RK stage of a time step of every case in one
+ *                         persistent launch of plane-march blocks and ghost
+ *                         fills, linked by per-case counters (bounded waits;
+ *                         the default when all cases are viscous or all
+ *                         inviscid and every ghost fill is a copy);
+ *  ACFD_BATCH_PLANE       one plane-march launch per RK stage over all cases;
+ *  ACFD_BATCH_BRICK       the persistent brick kernel that pulls (case, tile)
+ *                         items from a counter, one launch per RK stage. */
 #define ACFD_BATCH_BRICK 0
 #define ACFD_BATCH_PLANE 1
+#define ACFD_BATCH_PERSISTENT 2
 int acfd_batch_set_kernel(acfd_batch_t *b, int kernel);
 /* Run the batch's work on the caller's CUDA stream (cudaStream_t as void*);
  * the library's own stream is released. */

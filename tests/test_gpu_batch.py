@@ -146,3 +146,50 @@ def test_batch_rejects_unsupported_cases():
     spec = configs.tgv(n=10, sScheme=0, stepN=0)  # WENO3
     with pytest.raises(abi.AcfdError):
         Batch([spec.descriptors()])
+
+
+def _copy_only_specs():
+    rng = np.random.default_rng(11)
+    return [configs.tgv(n=16, Re=800.0, Ma=0.2, stepN=0),
+            configs.riemann_viscous(n=16, Re=1000.0, Ma=0.3, rng=rng),
+            configs.tgv(n=24, Re=1200.0, Ma=0.4, stepN=0),
+            configs.riemann_viscous(n=20, Re=2000.0, Ma=0.2, rng=rng)]
+
+
+@pytest.mark.parametrize("form", ["fp32", "hybrid"])
+def test_batch_persistent_step_matches_single_cases(form):
+    """The persistent step (the default for all-viscous batches whose ghost
+    fills are copies): every RK stage of a time step of every case in one
+    launch, the plane-march blocks and the ghost fills linked by per-case
+    counters.  Each case agrees with the single-case plane kernels to FP32
+    round-off (the first dt bit for bit) and with the per-stage plane batch
+    to the same bound, and the launch count per step is the CFL, dt, sensor
+    and one persistent launch."""
+    specs = _copy_only_specs()
+    descs = [s.descriptors() for s in specs]
+    if form == "hybrid":
+        if not __import__("os").path.exists(sensor.WEIGHTS):
+            pytest.skip("no trained sensor weights")
+        params, thr, mode = (*sensor.load(sensor.WEIGHTS)[:2], abi.FP32_HYBRID)
+    else:
+        params, thr, mode = None, 0.5, abi.FP32_BULK
+    dts, outs, launches = _batch(specs, descs, mode, STEPS, params, thr, kernel=abi.BATCH_PERSISTENT)
+    pdts, pouts, _ = _batch(specs, descs, mode, STEPS, params, thr, kernel=abi.BATCH_PLANE)
+    for c, spec in enumerate(specs):
+        sdt, sout = _single(spec, *descs[c], mode, STEPS, params, thr, tiles=PLANE)
+        assert dts[0, c] == sdt[0], c
+        assert np.all(np.abs(dts[:, c] - sdt) <= 1e-6 * sdt), (c, dts[:, c], sdt)
+        assert rel_err(outs[c], sout) <= TOL_FP32_ORDER, (c, rel_err(outs[c], sout))
+        assert rel_err(outs[c], pouts[c]) <= TOL_FP32_ORDER, (c, rel_err(outs[c], pouts[c]))
+    per_case = 2 + (2 if form == "hybrid" else 0)
+    assert launches == STEPS * (len(specs) * per_case + 2), launches
+
+
+def test_batch_persistent_is_the_default_for_copy_only_viscous_cases():
+    specs = _copy_only_specs()
+    with Batch([s.descriptors() for s in specs]) as b:
+        b.set_kernel(abi.BATCH_PERSISTENT)  # accepted
+    specs = _specs(inviscid=False)  # the channel needs formulas in its fill
+    with Batch([s.descriptors() for s in specs]) as b:
+        with pytest.raises(abi.AcfdError):
+            b.set_kernel(abi.BATCH_PERSISTENT)
