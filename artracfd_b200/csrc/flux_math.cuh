@@ -360,6 +360,56 @@ __device__ __forceinline__ T weno5(T f0, T f1, T f2, T f3, T f4)
     return (a0 * q0 + a1 * q1 + a2 * q2) * rcp<T>(T(6) * (a0 + a1 + a2));
 }
 
+// hp + hn of one characteristic field, H+ from l+ * W[0..4] and H- from
+// l- * W[5..1], with the split eigenvalues factored out: every smoothness
+// indicator is quadratic in its stencil, so WENO5(l f) = l * sum_k w_k q_k(f)
+// / 6 with the weights taken from eps + l^2 IS_k(f).  The second differences
+// shared by the two sides are formed once and the two normalisations share
+// one reciprocal: G = (l+ N+ S- + l- N- S+) / (6 S+ S-), N the weighted sum
+// of the candidates and S the sum of the weights of a side.  For the FP64
+// form (the product of the two weight sums stays far inside the double
+// range); the same values as two weno5 calls up to rounding.
+template <typename T>
+__device__ __forceinline__ T weno5_pair(const T (&W)[6], T lp, T ln)
+{
+    const T eps = T(1.0e-6);
+    const T c1312 = T(13.0 / 12.0);
+    const T D0 = W[0] - T(2) * W[1] + W[2];
+    const T D1 = W[1] - T(2) * W[2] + W[3];
+    const T D2 = W[2] - T(2) * W[3] + W[4];
+    const T D3 = W[3] - T(2) * W[4] + W[5];
+    const T lp2 = lp * lp, ln2 = ln * ln;
+    // + side: stencil W0..W4
+    const T up0 = W[0] - T(4) * W[1] + T(3) * W[2];
+    const T up1 = W[1] - W[3];
+    const T up2 = T(3) * W[2] - T(4) * W[3] + W[4];
+    T p0 = eps + lp2 * (c1312 * D0 * D0 + T(0.25) * up0 * up0);
+    T p1 = eps + lp2 * (c1312 * D1 * D1 + T(0.25) * up1 * up1);
+    T p2 = eps + lp2 * (c1312 * D2 * D2 + T(0.25) * up2 * up2);
+    p0 = p0 * p0;
+    p1 = p1 * p1;
+    p2 = p2 * p2;
+    const T ap0 = T(0.1) * (p1 * p2), ap1 = T(0.6) * (p0 * p2), ap2 = T(0.3) * (p0 * p1);
+    const T Np = ap0 * (T(2) * W[0] - T(7) * W[1] + T(11) * W[2]) + ap1 * (-W[1] + T(5) * W[2] + T(2) * W[3]) +
+                 ap2 * (T(2) * W[2] + T(5) * W[3] - W[4]);
+    const T Sp = ap0 + ap1 + ap2;
+    // - side: stencil W5..W1 (second differences are symmetric)
+    const T un0 = W[5] - T(4) * W[4] + T(3) * W[3];
+    const T un1 = W[4] - W[2];
+    const T un2 = T(3) * W[3] - T(4) * W[2] + W[1];
+    T m0 = eps + ln2 * (c1312 * D3 * D3 + T(0.25) * un0 * un0);
+    T m1 = eps + ln2 * (c1312 * D2 * D2 + T(0.25) * un1 * un1);
+    T m2 = eps + ln2 * (c1312 * D1 * D1 + T(0.25) * un2 * un2);
+    m0 = m0 * m0;
+    m1 = m1 * m1;
+    m2 = m2 * m2;
+    const T an0 = T(0.1) * (m1 * m2), an1 = T(0.6) * (m0 * m2), an2 = T(0.3) * (m0 * m1);
+    const T Nn = an0 * (T(2) * W[5] - T(7) * W[4] + T(11) * W[3]) + an1 * (-W[4] + T(5) * W[3] + T(2) * W[2]) +
+                 an2 * (T(2) * W[3] + T(5) * W[2] - W[1]);
+    const T Sn = an0 + an1 + an2;
+    return (lp * Np * Sn + ln * Nn * Sp) * rcp<T>(T(6) * (Sp * Sn));
+}
+
 template <typename T>
 __device__ __forceinline__ T weno3(T f0, T f1, T f2)
 {

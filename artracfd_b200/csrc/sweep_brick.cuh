@@ -132,7 +132,10 @@ __device__ __forceinline__ void conv_weno(const IfaceState<Real> &is, const Real
         }
         const Real lp = is.lp[r], ln = is.ln[r];
         Real hp, hn;
-        if (NP == 6) {
+        if constexpr (NP == 6 && sizeof(Real) == sizeof(double)) {
+            hp = fast::weno5_pair<Real>(W, lp, ln);
+            hn = Real(0);
+        } else if constexpr (NP == 6) {
             hp = fast::weno5<Real>(lp * W[0], lp * W[1], lp * W[2], lp * W[3], lp * W[4]);
             hn = fast::weno5<Real>(ln * W[5], ln * W[4], ln * W[3], ln * W[2], ln * W[1]);
         } else {

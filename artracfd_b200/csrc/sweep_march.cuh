@@ -130,7 +130,10 @@ __device__ __forceinline__ void march_weno(const IfaceState<Real> &is, const Rea
         }
         const Real lp = is.lp[r], ln = is.ln[r];
         Real hp, hn;
-        if constexpr (NP == 6) {
+        if constexpr (NP == 6 && sizeof(Real) == sizeof(double)) {
+            hp = fast::weno5_pair<Real>(C, lp, ln);
+            hn = Real(0);
+        } else if constexpr (NP == 6) {
             hp = fast::weno5<Real>(lp * C[0], lp * C[1], lp * C[2], lp * C[3], lp * C[4]);
             hn = fast::weno5<Real>(ln * C[5], ln * C[4], ln * C[3], ln * C[2], ln * C[1]);
         } else {

@@ -243,6 +243,8 @@ def main():
     ap.add_argument("--n", type=int, default=48)
     ap.add_argument("--seeds", type=int, default=12)
     ap.add_argument("--epochs", type=int, default=6)
+    ap.add_argument("--uniform-margin", type=float, default=0.25,
+                    help="logit margin of the threshold above the output at zero features")
     ap.add_argument("--out", default=WEIGHTS)
     args = ap.parse_args()
     t0 = time.time()
@@ -261,12 +263,22 @@ def main():
     ps = torch.sort(prob[pos]).values
     k = int(math.floor((1.0 - args.recall) * ps.numel()))
     thr = float(ps[k].item()) if ps.numel() else 0.5
-    thr = min(max(thr, 1e-4), 0.5)
+    # a uniform stencil (all ten features zero) is smooth by construction: its
+    # WENO5 weights equal the linear weights exactly.  Positives whose own
+    # five-point features are flat (a jump just outside the stencil, which
+    # the neighbouring nodes' flags cover in the hybrid sweep) pull the
+    # recall threshold down onto the network's output at zero features; the
+    # threshold is kept a logit margin above it, so that uniform regions
+    # (the quiescent gas ahead of a shock) take the linear scheme
+    p0 = float(predict(params, torch.zeros((1, N_IN), dtype=torch.float32, device="cuda"))[0].item())
+    floor = 1.0 / (1.0 + math.exp(-(math.log(p0 / (1.0 - p0)) + args.uniform_margin)))
+    thr = min(max(thr, floor, 1e-4), 0.5)
     flag = prob > thr
     recall = float((flag & pos).sum().item() / max(pos.sum().item(), 1))
     flagged = float(flag.float().mean().item())
     meta = dict(tau=args.tau, samples=int(n), positives=float(y.sum().item()), pos_weight=pw, epochs=args.epochs,
-                loss=hist, threshold=thr, heldout_recall=recall, heldout_flagged_fraction=flagged,
+                loss=hist, threshold=thr, uniform_output=p0, uniform_margin=args.uniform_margin,
+                heldout_recall=recall, heldout_flagged_fraction=flagged,
                 heldout_positive_fraction=float(pos.float().mean().item()), seconds=time.time() - t0,
                 data=f"{args.seeds} seeds x (1D + 3D Riemann) at {args.n}^3 + 4 TGV (Re, Ma) at {args.n}^3 and "
                      f"{2 * args.n}^3, 25 steps, every 8th recorded")

@@ -566,6 +566,16 @@ def run_ours(args, rank, world, local_rank):
     e2e_sec = time.perf_counter() - t0
     e2e_sec = max_over_ranks(torch, dist, e2e_sec)
     node_bytes = host.nbytes
+    # the strictest drop-in use: the whole node array crosses PCIe both ways
+    # every step (a host that touches its nodes between steps)
+    rt_steps = max(1, min(args.steps, 5))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(rt_steps):
+        s.upload(host)
+        s.evolve(s.time_step(spec.cfl), graph=True)
+        s.download(host)
+    rt_sec = max_over_ranks(torch, dist, time.perf_counter() - t0)
     s.close()
     accuracy = None
     if args.mode in ("fp32", "hybrid") and args.accuracy_steps > 0:
@@ -573,6 +583,9 @@ def run_ours(args, rank, world, local_rank):
     shock_cyl = None
     if args.mode == "hybrid" and not args.no_shock_cylinder:
         shock_cyl = shock_cylinder_block(torch, args, dist, stream, local_rank)
+    batch = None
+    if args.mode == "hybrid" and args.batch_steps > 0:
+        batch = batch_block(args, args.batch_steps, local_rank)
     for blk in (plain, fp32):
         if blk:
             blk.pop("_stage_mean_ms", None)
@@ -602,6 +615,7 @@ def run_ours(args, rank, world, local_rank):
         "speedup_vs_fp32_bulk": (value / fp32["value"]) if fp32 else None,
         "accuracy": accuracy,
         "shock_cylinder": shock_cyl,
+        "batch": batch,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": traffic,
                      "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of an RK-stage-2 launch "
@@ -632,7 +646,12 @@ def run_ours(args, rank, world, local_rank):
                 "h2d_bytes_per_step": (node_bytes + 8 * args.steps) / args.steps,
                 "d2h_bytes_per_step": (node_bytes + 24 * args.steps) / args.steps,
                 "what": "C-ABI loop with host node arrays: acfd_sync_to_device, K x (acfd_cfl + host dt + "
-                        "acfd_evolve_fluid_graph), acfd_sync_to_host; wall clock"},
+                        "acfd_evolve_fluid_graph), acfd_sync_to_host; wall clock",
+                "node_array_every_step": {"value": job_rate(world, nodes_pin, rt_steps, rt_sec), "steps": rt_steps,
+                                          "h2d_bytes_per_step": node_bytes, "d2h_bytes_per_step": node_bytes,
+                                          "what": "each step uploads and downloads the whole node array "
+                                                  "(acfd_sync_to_device, acfd_cfl, acfd_evolve_fluid_graph, "
+                                                  "acfd_sync_to_host); wall clock"}},
         "gpu_launches": gpu_launches,
         "tiles": tiles,
         "sensor": sensor_info,
@@ -641,13 +660,16 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
-def run_batch(args, rank, world, local_rank):
+def batch_block(args, steps, local_rank):
     """The batched sweep: 48 independent viscous TGV and 3D Riemann cases
     (configs.batch_cases, seed 42) advanced together by the batch API in the
-    learned-sensor FP32 form, against the same cases run one at a time by the
-    single-case API on the plain FP64 path.  Both are device-timed with CUDA
-    events (the one-at-a-time runs include their per-step host dt, as a user
-    running cases one by one does); the batch's dt stays on the device."""
+    learned-sensor FP32 form -- every RK stage of a step of every case in one
+    persistent launch (ACFD_BATCH_PERSISTENT), and for comparison one
+    plane-march launch per RK stage (ACFD_BATCH_PLANE) -- against the same
+    cases run one at a time by the single-case API on the plain FP64 path.
+    All are device-timed with CUDA events (the one-at-a-time runs include
+    their per-step host dt, as a user running cases one by one does); the
+    batch's dt stays on the device.  `steps` timed steps of each."""
     import numpy as np
     import torch
     from concurrent.futures import ThreadPoolExecutor
@@ -660,7 +682,6 @@ def run_batch(args, rank, world, local_rank):
     specs = configs.batch_cases(count=args.batch_cases, seed=42)
     descs = [s.descriptors() for s in specs]
     pin = [int(np.prod(np.array(p.ns)[0, :, 1] - np.array(p.ns)[0, :, 0])) for p, _ in descs]
-    steps = args.steps
     stream = torch.cuda.Stream()
     b = Batch(descs)
     b.set_stream(stream.cuda_stream)
@@ -696,48 +717,77 @@ def run_batch(args, rank, world, local_rank):
     b.sensor_load(params, thr)
     b.set_precision(abi.FP32_HYBRID)
     cfl = [s.cfl for s in specs]
-    # the first advance captures the step graph; time the remaining steps
-    b.advance(cfl, 1)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    l0 = b.launches()
-    e0.record(stream)
-    b.advance(cfl, steps - 1)
-    e1.record(stream)
-    e1.synchronize()
-    secb = e0.elapsed_time(e1) / 1e3
-    launches = b.launches() - l0
-    errs = []
-    for c in range(len(specs)):
-        r = b.download(c)["U"][:, 0, 0]
-        m = np.array(descs[c][0].ns)[0]
-        n = list(descs[c][0].n)
-        mask = np.zeros((n[2], n[1], n[0]), dtype=bool)
-        mask[m[2, 0]:m[2, 1], m[1, 0]:m[1, 1], m[0, 0]:m[0, 1]] = True
-        mask = mask.ravel()
-        errs.append(float(np.abs(r[mask] - rho64[c][mask]).sum() / np.abs(rho64[c][mask]).sum()))
-    b.close()
     total = sum(pin)
-    line = {
-        "metric": METRIC, "workload": "batch", "value": total * (steps - 1) / secb / 1e6, "unit": UNIT,
-        "n_gpus": 1, "steps": steps - 1, "higher_is_better": True, "dtype": "f32/f64",
-        "data": "synthetic (seeded TGV and 3D Riemann initial fields)",
-        "config": {"workload": f"{len(specs)} independent viscous TGV / 3D Riemann cases, n^3 with n in "
-                               "{64..160 step 16}, Ma U[0.1,0.5], Re U[400,3200], seed 42; WENO5/RK3",
-                   "cases": len(specs), "pin_nodes": total,
-                   "kinds": {k: sum(1 for s in specs if s.kind == k) for k in ("tgv", "riemann")},
-                   "form": "hybrid (learned sensor, FP32 bulk)",
-                   "stage_kernel": "plane march: one launch per RK stage over the plane blocks of all cases",
-                   "stage_launches_per_step": 18},
-        "ms_per_step": secb / (steps - 1) * 1e3,
-        "one_at_a_time_fp64": {"value": total * steps / sec64 / 1e6, "ms_per_step_all_cases": sec64 / steps * 1e3,
+    kernels = {}
+    try:
+        b.set_kernel(abi.BATCH_PERSISTENT)
+        kernels["persistent"] = abi.BATCH_PERSISTENT
+    except abi.AcfdError:
+        pass
+    kernels["per_stage_plane"] = abi.BATCH_PLANE
+    timed = {}
+    errs = None
+    for name, kern in kernels.items():
+        b.set_kernel(kern)
+        # the first advance captures the step graph (after the first kernel's
+        # timed steps the cases continue from where they are: the rate of a
+        # step does not depend on the state's time)
+        b.advance(cfl, 1)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = b.launches()
+        e0.record(stream)
+        b.advance(cfl, steps)
+        e1.record(stream)
+        e1.synchronize()
+        secb = e0.elapsed_time(e1) / 1e3
+        timed[name] = {"value": total * steps / secb / 1e6, "ms_per_step": secb / steps * 1e3,
+                       "gpu_launches_per_step": (b.launches() - l0) / steps}
+        if errs is None:
+            # first kernel: 1 + steps steps from the start, against FP64 after `steps`
+            errs = []
+            for c in range(len(specs)):
+                r = b.download(c)["U"][:, 0, 0]
+                m = np.array(descs[c][0].ns)[0]
+                n = list(descs[c][0].n)
+                mask = np.zeros((n[2], n[1], n[0]), dtype=bool)
+                mask[m[2, 0]:m[2, 1], m[1, 0]:m[1, 1], m[0, 0]:m[0, 1]] = True
+                mask = mask.ravel()
+                errs.append(float(np.abs(r[mask] - rho64[c][mask]).sum() / np.abs(rho64[c][mask]).sum()))
+    b.close()
+    head = next(iter(timed))
+    v64 = total * steps / sec64 / 1e6
+    return {
+        "workload": f"{len(specs)} independent viscous TGV / 3D Riemann cases, n^3 with n in "
+                    "{64..160 step 16}, Ma U[0.1,0.5], Re U[400,3200], seed 42; WENO5/RK3",
+        "cases": len(specs), "pin_nodes": total,
+        "kinds": {k: sum(1 for s in specs if s.kind == k) for k in ("tgv", "riemann")},
+        "form": "hybrid (learned sensor, FP32 bulk)", "kernel": head,
+        "value": timed[head]["value"], "ms_per_step": timed[head]["ms_per_step"], "steps": steps,
+        "kernels": timed,
+        "one_at_a_time_fp64": {"value": v64, "ms_per_step_all_cases": sec64 / steps * 1e3,
                                "what": "each case alone through the single-case API, plain FP64 path, host dt "
                                        "per step, CUDA graph per step"},
-        "speedup_vs_one_at_a_time_fp64": (total * (steps - 1) / secb) / (total * steps / sec64),
+        "speedup_vs_one_at_a_time_fp64": timed[head]["value"] / v64,
         "accuracy": {"l1_rho_max_over_cases": max(errs), "l1_rho_mean": sum(errs) / len(errs),
-                     "against": "the same case on the plain FP64 path after the same number of steps "
-                                "(each with its own dt sequence)"},
-        "gpu_launches": launches,
+                     "against": "each case on the plain FP64 path (its own dt sequence); the batch has taken "
+                                "one step more"},
+    }
+
+
+def run_batch(args, rank, world, local_rank):
+    """--workload batch: the batched sweep as its own JSON line."""
+    blk = batch_block(args, args.steps, local_rank)
+    line = {
+        "metric": METRIC, "workload": "batch", "value": blk["value"], "unit": UNIT,
+        "n_gpus": 1, "steps": args.steps, "higher_is_better": True, "dtype": "f32/f64",
+        "data": "synthetic (seeded TGV and 3D Riemann initial fields)",
+        "config": {k: blk[k] for k in ("workload", "cases", "pin_nodes", "kinds", "form", "kernel")},
+        "ms_per_step": blk["ms_per_step"],
+        "kernels": blk["kernels"],
+        "one_at_a_time_fp64": blk["one_at_a_time_fp64"],
+        "speedup_vs_one_at_a_time_fp64": blk["speedup_vs_one_at_a_time_fp64"],
+        "accuracy": blk["accuracy"],
     }
     print(json.dumps(line), flush=True)
 
@@ -801,6 +851,8 @@ def main():
     ap.add_argument("--workload", default="tgv", choices=["tgv", "batch"],
                     help="tgv: the headline line (TGV 128^3); batch: the 48-case batched sweep")
     ap.add_argument("--batch-cases", type=int, default=48)
+    ap.add_argument("--batch-steps", type=int, default=10,
+                    help="timed steps of the batch block of the default line (0: leave it out)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
