@@ -372,41 +372,48 @@ __device__ __forceinline__ T weno5(T f0, T f1, T f2, T f3, T f4)
 template <typename T>
 __device__ __forceinline__ T weno5_pair(const T (&W)[6], T lp, T ln)
 {
+    // smoothness indicators as squares of scaled differences, so that each is
+    // one multiply and one fused multiply-add: IS = (s D)^2 + (u / 2)^2 with
+    // s = sqrt(13/12), D the second difference and u the first-difference
+    // term of the reference's indicator
     const T eps = T(1.0e-6);
-    const T c1312 = T(13.0 / 12.0);
-    const T D0 = W[0] - T(2) * W[1] + W[2];
-    const T D1 = W[1] - T(2) * W[2] + W[3];
-    const T D2 = W[2] - T(2) * W[3] + W[4];
-    const T D3 = W[3] - T(2) * W[4] + W[5];
+    const T s = T(1.0408329997330663);  // sqrt(13/12)
+    const T D0 = s * (W[0] - T(2) * W[1] + W[2]);
+    const T D1 = s * (W[1] - T(2) * W[2] + W[3]);
+    const T D2 = s * (W[2] - T(2) * W[3] + W[4]);
+    const T D3 = s * (W[3] - T(2) * W[4] + W[5]);
     const T lp2 = lp * lp, ln2 = ln * ln;
     // + side: stencil W0..W4
-    const T up0 = W[0] - T(4) * W[1] + T(3) * W[2];
-    const T up1 = W[1] - W[3];
-    const T up2 = T(3) * W[2] - T(4) * W[3] + W[4];
-    T p0 = eps + lp2 * (c1312 * D0 * D0 + T(0.25) * up0 * up0);
-    T p1 = eps + lp2 * (c1312 * D1 * D1 + T(0.25) * up1 * up1);
-    T p2 = eps + lp2 * (c1312 * D2 * D2 + T(0.25) * up2 * up2);
+    const T up0 = T(0.5) * W[0] - T(2) * W[1] + T(1.5) * W[2];
+    const T up1 = T(0.5) * (W[1] - W[3]);
+    const T up2 = T(1.5) * W[2] - T(2) * W[3] + T(0.5) * W[4];
+    T p0 = eps + lp2 * (D0 * D0 + up0 * up0);
+    T p1 = eps + lp2 * (D1 * D1 + up1 * up1);
+    T p2 = eps + lp2 * (D2 * D2 + up2 * up2);
     p0 = p0 * p0;
     p1 = p1 * p1;
     p2 = p2 * p2;
-    const T ap0 = T(0.1) * (p1 * p2), ap1 = T(0.6) * (p0 * p2), ap2 = T(0.3) * (p0 * p1);
-    const T Np = ap0 * (T(2) * W[0] - T(7) * W[1] + T(11) * W[2]) + ap1 * (-W[1] + T(5) * W[2] + T(2) * W[3]) +
-                 ap2 * (T(2) * W[2] + T(5) * W[3] - W[4]);
-    const T Sp = ap0 + ap1 + ap2;
+    // weights C_k prod_{j != k} p_j; the C_k folded into the candidates
+    const T P12 = p1 * p2, P02 = p0 * p2, P01 = p0 * p1;
+    const T Np = P12 * (T(0.2) * W[0] - T(0.7) * W[1] + T(1.1) * W[2]) +
+                 P02 * (T(-0.6) * W[1] + T(3.0) * W[2] + T(1.2) * W[3]) +
+                 P01 * (T(0.6) * W[2] + T(1.5) * W[3] - T(0.3) * W[4]);
+    const T Sp = T(0.1) * P12 + T(0.6) * P02 + T(0.3) * P01;
     // - side: stencil W5..W1 (second differences are symmetric)
-    const T un0 = W[5] - T(4) * W[4] + T(3) * W[3];
-    const T un1 = W[4] - W[2];
-    const T un2 = T(3) * W[3] - T(4) * W[2] + W[1];
-    T m0 = eps + ln2 * (c1312 * D3 * D3 + T(0.25) * un0 * un0);
-    T m1 = eps + ln2 * (c1312 * D2 * D2 + T(0.25) * un1 * un1);
-    T m2 = eps + ln2 * (c1312 * D1 * D1 + T(0.25) * un2 * un2);
+    const T un0 = T(0.5) * W[5] - T(2) * W[4] + T(1.5) * W[3];
+    const T un1 = T(0.5) * (W[4] - W[2]);
+    const T un2 = T(1.5) * W[3] - T(2) * W[2] + T(0.5) * W[1];
+    T m0 = eps + ln2 * (D3 * D3 + un0 * un0);
+    T m1 = eps + ln2 * (D2 * D2 + un1 * un1);
+    T m2 = eps + ln2 * (D1 * D1 + un2 * un2);
     m0 = m0 * m0;
     m1 = m1 * m1;
     m2 = m2 * m2;
-    const T an0 = T(0.1) * (m1 * m2), an1 = T(0.6) * (m0 * m2), an2 = T(0.3) * (m0 * m1);
-    const T Nn = an0 * (T(2) * W[5] - T(7) * W[4] + T(11) * W[3]) + an1 * (-W[4] + T(5) * W[3] + T(2) * W[2]) +
-                 an2 * (T(2) * W[3] + T(5) * W[2] - W[1]);
-    const T Sn = an0 + an1 + an2;
+    const T M12 = m1 * m2, M02 = m0 * m2, M01 = m0 * m1;
+    const T Nn = M12 * (T(0.2) * W[5] - T(0.7) * W[4] + T(1.1) * W[3]) +
+                 M02 * (T(-0.6) * W[4] + T(3.0) * W[3] + T(1.2) * W[2]) +
+                 M01 * (T(0.6) * W[3] + T(1.5) * W[2] - T(0.3) * W[1]);
+    const T Sn = T(0.1) * M12 + T(0.6) * M02 + T(0.3) * M01;
     return (lp * Np * Sn + ln * Nn * Sp) * rcp<T>(T(6) * (Sp * Sn));
 }
 

@@ -772,6 +772,16 @@ __device__ __noinline__ void persist_yz_item(const Grid &g, const ModelParams &m
     plane_yz_block<6, VISC, HYB>(g, mp, a, pt, mapp, blk, smem);
 }
 
+// the full/empty barriers of a plane block of sweep axis s (the layout of
+// plane_yz_block and plane_x_block)
+__device__ __forceinline__ uint64_t *plane_barriers(const PlaneTile &pt, int s, unsigned char *smem)
+{
+    const int slot_bytes = plane_slot_bytes(pt.BXp, pt.BC);
+    const int nflux = (s == 0) ? pt.TR * pt.NR : 0;
+    return reinterpret_cast<uint64_t *>(smem + (size_t)kPlaneSlots * slot_bytes + plane_flux_bytes(nflux) +
+                                        (size_t)pt.ncw * kCoopBytes);
+}
+
 template <bool VISC, bool HYB>
 __global__ void __launch_bounds__(kPlaneMaxThreads, 2)
 stage_plane_persistent(const BatchCase *__restrict__ cases, const BatchPlane *__restrict__ planes,
@@ -846,6 +856,12 @@ stage_plane_persistent(const BatchCase *__restrict__ cases, const BatchPlane *__
             }
             __syncthreads();
             if (threadIdx.x == 0) {
+                // the item's barriers are idle (its copies were waited for):
+                // invalidate them before the next item initialises its own
+                uint64_t *bars = plane_barriers(P.pt, s, smem);
+                for (int q = 0; q < 2 * kPlaneSlots; ++q) {
+                    tma::mbar_inval(bars + q);
+                }
                 __threadfence();
                 atomicAdd(done + (long long)k * ncase + c, 1u);
             }

@@ -28,6 +28,14 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
                  : "memory");
 }
 
+// invalidate a barrier that no thread or copy uses any more, so that its
+// memory may hold a new barrier (mbarrier.init on a valid barrier is
+// undefined)
+__device__ __forceinline__ void mbar_inval(uint64_t *bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 // plain arrival (count 1) on a barrier
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
 {

@@ -13,6 +13,7 @@ interfaces (|sum_k (omega_k - C_k) q_k| relative to the stencil values).  A
 node is labelled non-smooth when that change exceeds ``tau``.
 
     python -m artracfd_b200.sensor train [--tau 1e-3] [--out artracfd_b200/sensor_weights.npz]
+    python -m artracfd_b200.sensor calibrate [--uniform-margin 0.25]   # threshold floor only
 """
 from __future__ import annotations
 
@@ -233,11 +234,45 @@ def attach(solver: Solver, path=WEIGHTS, threshold=None):
     solver.set_precision(abi.FP32_HYBRID)
 
 
+def forward_cpu(params, X):
+    """The network on the CPU in float64 (for calibration; the GPU kernels
+    evaluate it in FP32 / FP16 tensor-core arithmetic)."""
+    p = np.asarray(params, dtype=np.float64)
+    o = 0
+    W1 = p[o:o + N_H * N_IN].reshape(N_H, N_IN); o += N_H * N_IN
+    b1 = p[o:o + N_H]; o += N_H
+    W2 = p[o:o + N_H * N_H].reshape(N_H, N_H); o += N_H * N_H
+    b2 = p[o:o + N_H]; o += N_H
+    w3 = p[o:o + N_H]; o += N_H
+    b3 = p[o]
+    h = np.maximum(0.0, np.atleast_2d(X) @ W1.T + b1)
+    h = np.maximum(0.0, h @ W2.T + b2)
+    return 1.0 / (1.0 + np.exp(-(h @ w3 + b3)))
+
+
+def uniform_floor(params, margin):
+    """The threshold floor of a trained network: its output on a uniform
+    stencil (all features zero), raised by `margin` in logit."""
+    p0 = float(forward_cpu(params, np.zeros(N_IN))[0])
+    return p0, 1.0 / (1.0 + math.exp(-(math.log(p0 / (1.0 - p0)) + margin)))
+
+
+def calibrate(path=WEIGHTS, margin=0.25):
+    """Raise the threshold of a weights file to the uniform-stencil floor
+    (parameters unchanged); rewrites the .npz and the .bin beside it."""
+    params, thr, meta = load(path)
+    p0, floor = uniform_floor(params, margin)
+    new = min(max(thr, floor), 0.5)
+    meta.update(threshold=new, threshold_before_calibration=thr, uniform_output=p0, uniform_margin=margin)
+    save(path, params, new, meta)
+    return thr, new, p0
+
+
 def main():
     import torch
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("cmd", choices=["train"])
+    ap.add_argument("cmd", choices=["train", "calibrate"])
     ap.add_argument("--tau", type=float, default=1e-3)
     ap.add_argument("--recall", type=float, default=0.999)
     ap.add_argument("--n", type=int, default=48)
@@ -247,6 +282,10 @@ def main():
                     help="logit margin of the threshold above the output at zero features")
     ap.add_argument("--out", default=WEIGHTS)
     args = ap.parse_args()
+    if args.cmd == "calibrate":
+        old, new, p0 = calibrate(args.out, args.uniform_margin)
+        print(json.dumps(dict(threshold_before=old, threshold=new, uniform_output=p0)))
+        return
     t0 = time.time()
     X, dep = collect(default_specs(range(args.seeds), args.n), verbose=True)
     y = (dep > args.tau).float()
@@ -270,8 +309,7 @@ def main():
     # recall threshold down onto the network's output at zero features; the
     # threshold is kept a logit margin above it, so that uniform regions
     # (the quiescent gas ahead of a shock) take the linear scheme
-    p0 = float(predict(params, torch.zeros((1, N_IN), dtype=torch.float32, device="cuda"))[0].item())
-    floor = 1.0 / (1.0 + math.exp(-(math.log(p0 / (1.0 - p0)) + args.uniform_margin)))
+    p0, floor = uniform_floor(params, args.uniform_margin)
     thr = min(max(thr, floor, 1e-4), 0.5)
     flag = prob > thr
     recall = float((flag & pos).sum().item() / max(pos.sum().item(), 1))

@@ -582,10 +582,16 @@ def run_ours(args, rank, world, local_rank):
         accuracy = _accuracy(part, model, node, spec, args.mode, args.accuracy_steps, stream)
     shock_cyl = None
     if args.mode == "hybrid" and not args.no_shock_cylinder:
-        shock_cyl = shock_cylinder_block(torch, args, dist, stream, local_rank)
+        try:
+            shock_cyl = shock_cylinder_block(torch, args, dist, stream, local_rank)
+        except Exception as exc:  # the headline line is printed regardless
+            shock_cyl = {"error": f"{type(exc).__name__}: {exc}"}
     batch = None
     if args.mode == "hybrid" and args.batch_steps > 0:
-        batch = batch_block(args, args.batch_steps, local_rank)
+        try:
+            batch = batch_block(args, args.batch_steps, local_rank)
+        except Exception as exc:
+            batch = {"error": f"{type(exc).__name__}: {exc}"}
     for blk in (plain, fp32):
         if blk:
             blk.pop("_stage_mean_ms", None)

@@ -3,12 +3,14 @@ at a time through the single-case API.
 
 Each RK stage of the batch is one launch over the tiles of all cases, with
 the plane-march kernel (the single-case plane variants) or the persistent
-brick kernel (the single-case brick variant 0); a case of the batch computes
-every interface exactly as the single-case kernel does, and its dt comes from
-its own CFL maximum in the reference's expression, so the batch reproduces
-the single-case runs bit for bit with the brick kernel (states, and dt at
-every step) and to FP32 round-off with the plane-march kernel (see its
-test).  The cases
+brick kernel (the single-case brick variant 0), or one persistent launch
+runs every stage of a step; a case of the batch computes every interface
+with the single-case kernel's block code, and its dt comes from its own CFL
+maximum in the reference's expression.  The batch kernels are other kernels
+than the single-case ones, in which the compiler may contract a different
+set of FP32 (and FP64) multiply-adds into FMAs, so a case agrees with its
+single-case run to FP32 round-off, its first dt (computed before any stage)
+bit for bit.  The cases
 mix periodic (TGV), outflow (Riemann), outflow + periodic (Sod) and
 inflow/outflow/wall/periodic boundaries (channel, the ordered ghost fill).
 """
@@ -77,6 +79,12 @@ def _batch(specs, descs, mode, steps, params=None, thr=0.5, kernel=None):
     return dts, outs, launches
 
 
+def _agree(dts, outs, c, sdt, sout):
+    assert dts[0, c] == sdt[0], (c, dts[0, c], sdt[0])
+    assert np.all(np.abs(dts[:, c] - sdt) <= 1e-6 * sdt), (c, dts[:, c], sdt)
+    assert rel_err(outs[c], sout) <= TOL_FP32_ORDER, (c, rel_err(outs[c], sout))
+
+
 def test_batch_equals_single_cases_fp32():
     specs = _specs()
     descs = [s.descriptors() for s in specs]
@@ -84,8 +92,7 @@ def test_batch_equals_single_cases_fp32():
     assert launches > 0
     for c, spec in enumerate(specs):
         sdt, sout = _single(spec, *descs[c], abi.FP32_BULK, STEPS)
-        assert np.array_equal(dts[:, c], sdt), (c, dts[:, c], sdt)
-        assert np.array_equal(outs[c], sout), (c, np.nanmax(np.abs(outs[c] - sout)))
+        _agree(dts, outs, c, sdt, sout)
 
 
 @pytest.mark.skipif(not __import__("os").path.exists(sensor.WEIGHTS), reason="no trained sensor weights")
@@ -96,8 +103,7 @@ def test_batch_equals_single_cases_hybrid():
     dts, outs, _ = _batch(specs, descs, abi.FP32_HYBRID, STEPS, params, thr)
     for c, spec in enumerate(specs):
         sdt, sout = _single(spec, *descs[c], abi.FP32_HYBRID, STEPS, params, thr)
-        assert np.array_equal(dts[:, c], sdt), c
-        assert np.array_equal(outs[c], sout), (c, np.nanmax(np.abs(outs[c] - sout)))
+        _agree(dts, outs, c, sdt, sout)
 
 
 def test_batch_brick_viscous_cases_equal_single_cases():
@@ -107,8 +113,7 @@ def test_batch_brick_viscous_cases_equal_single_cases():
     dts, outs, _ = _batch(specs, descs, abi.FP32_BULK, STEPS, kernel=abi.BATCH_BRICK)
     for c, spec in enumerate(specs):
         sdt, sout = _single(spec, *descs[c], abi.FP32_BULK, STEPS, tiles=BRICK)
-        assert np.array_equal(dts[:, c], sdt), c
-        assert np.array_equal(outs[c], sout), (c, np.nanmax(np.abs(outs[c] - sout)))
+        _agree(dts, outs, c, sdt, sout)
 
 
 @pytest.mark.parametrize("form", ["fp32", "hybrid"])

@@ -51,6 +51,20 @@ def test_shock_cylinder_body_fixture_belongs_to_the_named_case(tmp_path):
         assert np.array_equal(got, keep[0][key]), key
 
 
+def test_sensor_threshold_leaves_uniform_stencils_to_the_linear_scheme():
+    """A uniform stencil (all ten features zero) has WENO5 weights equal to the
+    linear weights: the shipped threshold lies above the network's output
+    there (by the stated logit margin), so uniform regions -- the quiescent
+    gas ahead of a shock -- are not flagged."""
+    import math
+    from artracfd_b200 import sensor
+    params, thr, meta = sensor.load(sensor.WEIGHTS)
+    p0 = float(sensor.forward_cpu(params, np.zeros(sensor.N_IN))[0])
+    assert thr > p0
+    margin = math.log(thr / (1 - thr)) - math.log(p0 / (1 - p0))
+    assert margin >= meta.get("uniform_margin", 0.25) - 1e-6, margin
+
+
 def test_node_record_layout():
     # acfd_node_t has the reference Node layout: 4 ints, U[3][5] doubles
     assert abi.NODE_DTYPE.itemsize == 136
