@@ -1850,6 +1850,8 @@ struct acfd_batch {
     unsigned *d_done = nullptr, *d_filled = nullptr;  // [kMaxStepStages][ncase]
     int *d_abort = nullptr;
     long long *d_pair_off = nullptr;                  // [ncase + 1]
+    long long *d_fill_pre = nullptr;                  // [ncase + 1] first fill item of each case
+    long long nfill = 0;                              // fill items of one stage
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int graph_mode = -1;
@@ -1911,6 +1913,7 @@ int batch_step(acfd_batch *b)
         for (int s = 0; s < 3; ++s) {
             ps.ntile[s] = b->pblocks[s];
         }
+        ps.nfill = b->nfill;
         for (int h = 0, k = 0; h < 6; ++h) {
             for (int q = 0; q < nstage; ++q, ++k) {
                 ps.s_of[k] = order[h];
@@ -1920,7 +1923,7 @@ int batch_step(acfd_batch *b)
                 ps.sc[k].to = rk[q].to;
                 ps.sc[k].tn = rk[q].tn;
                 ps.sc[k].tm = rk[q].tm;
-                ps.kbase[k + 1] = ps.kbase[k] + b->pblocks[order[h]] + ncase;
+                ps.kbase[k + 1] = ps.kbase[k] + b->pblocks[order[h]] + b->nfill;
             }
         }
         const size_t nflag = (size_t)kMaxStepStages * ncase;
@@ -1929,8 +1932,9 @@ int batch_step(acfd_batch *b)
         ACFD_CUDA(cudaMemsetAsync(b->d_filled, 0, sizeof(unsigned) * nflag, b->stream));
         ACFD_CUDA(cudaMemsetAsync(b->d_abort, 0, sizeof(int), b->stream));
         TRY(launch_stage_plane_persistent(b->d_cases, b->d_planes, b->d_pmaps, b->d_pprefix, ncase, ps, b->d_dts,
-                                          b->d_levels, b->d_pairs, b->d_pair_off, b->d_queue, b->d_done, b->d_filled,
-                                          b->d_abort, b->d_status, b->visc, hybrid, b->persist_blocks,
+                                          b->d_levels, b->d_pairs, b->d_pair_off, b->d_fill_pre, b->d_queue,
+                                          b->d_done, b->d_filled, b->d_abort, b->d_status, b->visc, hybrid,
+                                          b->persist_blocks,
                                           b->persist_threads, b->persist_smem, b->stream));
         ++b->launches;
         return ACFD_OK;
@@ -2170,6 +2174,12 @@ int acfd_batch_init(int ncase, const acfd_partition_t *parts, const acfd_model_t
         for (int c = 0; c < ncase; ++c) {
             off[(size_t)c + 1] += off[(size_t)c];
         }
+        // the copy pairs of a case's ghost fill in items of kFillChunk pairs
+        std::vector<long long> fpre((size_t)ncase + 1, 0);
+        for (int c = 0; c < ncase; ++c) {
+            const long long np = off[(size_t)c + 1] - off[(size_t)c];
+            fpre[(size_t)c + 1] = fpre[(size_t)c] + (np + kFillChunk - 1) / kFillChunk;
+        }
         b->persist_threads = std::max(b->pthreads[0], std::max(b->pthreads[1], b->pthreads[2]));
         b->persist_smem = std::max(b->psmem[0], std::max(b->psmem[1], b->psmem[2]));
         int bps = 0;
@@ -2181,7 +2191,11 @@ int acfd_batch_init(int ncase, const acfd_partition_t *parts, const acfd_model_t
             (e = cudaMalloc(&b->d_abort, sizeof(int))) == cudaSuccess &&
             (e = cudaMalloc(&b->d_pair_off, sizeof(long long) * off.size())) == cudaSuccess &&
             (e = cudaMemcpy(b->d_pair_off, off.data(), sizeof(long long) * off.size(), cudaMemcpyHostToDevice)) ==
+                cudaSuccess &&
+            (e = cudaMalloc(&b->d_fill_pre, sizeof(long long) * fpre.size())) == cudaSuccess &&
+            (e = cudaMemcpy(b->d_fill_pre, fpre.data(), sizeof(long long) * fpre.size(), cudaMemcpyHostToDevice)) ==
                 cudaSuccess) {
+            b->nfill = fpre[(size_t)ncase];
             b->persist_blocks = bps * b->sms;
             b->persist_ok = true;
             b->persist = true;
@@ -2229,6 +2243,7 @@ int acfd_batch_finalize(acfd_batch_t *b)
     cudaFree(b->d_filled);
     cudaFree(b->d_abort);
     cudaFree(b->d_pair_off);
+    cudaFree(b->d_fill_pre);
     if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
     delete b;
     return ACFD_OK;

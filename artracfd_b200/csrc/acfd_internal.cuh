@@ -215,30 +215,34 @@ int launch_stage_plane_batch(const BatchCase *cases, const BatchPlane *planes, c
 
 // Persistent batch step: every RK stage of one time step of every case in
 // one launch.  Work items, in order: for each stage k of the step, the plane
-// blocks of every case (case order) and then one ghost-fill item per case.
-// A plane block of stage k > 0 of case c waits until the fill of stage k-1
-// of case c is done; the fill of stage k of case c waits until all its plane
-// blocks of stage k are done (per-case counters, no grid-wide barrier).
+// blocks of every case (case order) and then the ghost-fill items of every
+// case (its copy pairs in chunks of kFillChunk).  A plane block of stage
+// k > 0 of case c waits until every fill item of stage k-1 of case c is
+// done; a fill item of stage k of case c waits until all plane blocks of
+// stage k of case c are done (per-case counters, no grid-wide barrier).
 // Items are taken from a queue in order, so every item a block waits for was
 // taken earlier by a running block.
 constexpr int kMaxStepStages = 18;
+constexpr long long kFillChunk = 16384;  // copy pairs of one ghost-fill item
 struct PersistStep {
     int nk;                               // stages of the step
     int s_of[kMaxStepStages];             // sweep axis of stage k
     StageCoefs sc[kMaxStepStages];
     long long kbase[kMaxStepStages + 1];  // first item of stage k
     long long ntile[3];                   // plane blocks of one stage along axis s, all cases
+    long long nfill;                      // ghost-fill items of one stage, all cases
 };
 // queue: one counter; done, filled: [nk][ncase] (zero at launch); abort: one
 // word set by a block whose wait gave up (status code 7), after which every
 // block leaves; pairs: (case, dst, src) copy pairs of the ghost fill, case
-// by case, pair_off[c] .. pair_off[c + 1] those of case c
+// by case, pair_off[c] .. pair_off[c + 1] those of case c; fill_pre[c]: the
+// first fill item of case c within a stage (fill_pre[ncase] = ps.nfill)
 int launch_stage_plane_persistent(const BatchCase *cases, const BatchPlane *planes, const CUtensorMap *pmaps,
                                   const long long *prefix, int ncase, const PersistStep &ps, const double *dts,
                                   const BatchLevel *levels, const int4 *pairs, const long long *pair_off,
-                                  unsigned long long *queue, unsigned *done, unsigned *filled, int *abort,
-                                  int *status, bool viscous, bool hybrid, int blocks, int nthreads, int smem,
-                                  cudaStream_t st);
+                                  const long long *fill_pre, unsigned long long *queue, unsigned *done,
+                                  unsigned *filled, int *abort, int *status, bool viscous, bool hybrid, int blocks,
+                                  int nthreads, int smem, cudaStream_t st);
 // resident blocks per SM of the persistent batch kernel
 int plane_persistent_occupancy(bool viscous, bool hybrid, int nthreads, int smem, int *blocks_per_sm);
 

@@ -95,13 +95,13 @@ int launch_stage_plane_batch(const BatchCase *cases, const BatchPlane *planes, c
 int launch_stage_plane_persistent(const BatchCase *cases, const BatchPlane *planes, const CUtensorMap *pmaps,
                                   const long long *prefix, int ncase, const PersistStep &ps, const double *dts,
                                   const BatchLevel *levels, const int4 *pairs, const long long *pair_off,
-                                  unsigned long long *queue, unsigned *done, unsigned *filled, int *abort,
-                                  int *status, bool viscous, bool hybrid, int blocks, int nthreads, int smem,
-                                  cudaStream_t st)
+                                  const long long *fill_pre, unsigned long long *queue, unsigned *done,
+                                  unsigned *filled, int *abort, int *status, bool viscous, bool hybrid, int blocks,
+                                  int nthreads, int smem, cudaStream_t st)
 {
     return form_fp32::launch_plane_persistent_impl(cases, planes, pmaps, prefix, ncase, ps, dts, levels, pairs,
-                                                   pair_off, queue, done, filled, abort, status, viscous, hybrid,
-                                                   blocks, nthreads, smem, st);
+                                                   pair_off, fill_pre, queue, done, filled, abort, status, viscous,
+                                                   hybrid, blocks, nthreads, smem, st);
 }
 
 int plane_persistent_occupancy(bool viscous, bool hybrid, int nthreads, int smem, int *blocks_per_sm)

@@ -787,8 +787,8 @@ __global__ void __launch_bounds__(kPlaneMaxThreads, 2)
 stage_plane_persistent(const BatchCase *__restrict__ cases, const BatchPlane *__restrict__ planes,
                        const CUtensorMap *pmaps, const long long *__restrict__ prefix, int ncase, PersistStep ps,
                        const double *dts, const BatchLevel *__restrict__ levels, const int4 *__restrict__ pairs,
-                       const long long *__restrict__ pair_off, unsigned long long *queue, unsigned *done,
-                       unsigned *filled, int *abort, int *status)
+                       const long long *__restrict__ pair_off, const long long *__restrict__ fill_pre,
+                       unsigned long long *queue, unsigned *done, unsigned *filled, int *abort, int *status)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ long long s_item;
@@ -816,7 +816,8 @@ stage_plane_persistent(const BatchCase *__restrict__ cases, const BatchPlane *__
             }
             const int c = lo;
             if (threadIdx.x == 0) {
-                s_ok = (k == 0) || persist_wait(filled + (long long)(k - 1) * ncase + c, 1u, abort, status);
+                s_ok = (k == 0) || persist_wait(filled + (long long)(k - 1) * ncase + c,
+                                                (unsigned)(fill_pre[c + 1] - fill_pre[c]), abort, status);
             }
             __syncthreads();
             if (!s_ok) {
@@ -866,7 +867,13 @@ stage_plane_persistent(const BatchCase *__restrict__ cases, const BatchPlane *__
                 atomicAdd(done + (long long)k * ncase + c, 1u);
             }
         } else {
-            const int c = (int)(local - ps.ntile[s]);
+            // fill item f: chunk f - fill_pre[c] of case c's copy pairs
+            const long long f = local - ps.ntile[s];
+            int c = 0, chi = ncase - 1;
+            while (c < chi) {
+                const int mid = (c + chi + 1) / 2;
+                if (fill_pre[mid] <= f) c = mid; else chi = mid - 1;
+            }
             if (threadIdx.x == 0) {
                 s_ok = persist_wait(done + (long long)k * ncase + c, (unsigned)(pre[c + 1] - pre[c]), abort, status);
             }
@@ -874,10 +881,12 @@ stage_plane_persistent(const BatchCase *__restrict__ cases, const BatchPlane *__
             if (!s_ok) {
                 break;
             }
-            // the ghost fill of case c (copy pairs), reading through L2
+            // the chunk's copy pairs, reading through L2
             const BatchLevel L = levels[c];
             double *U = L.U + (long long)ps.sc[k].tm * 5 * L.nn;
-            for (long long t = pair_off[c] + threadIdx.x; t < pair_off[c + 1]; t += blockDim.x) {
+            const long long t0 = pair_off[c] + (f - fill_pre[c]) * kFillChunk;
+            const long long t1 = min(pair_off[c + 1], t0 + kFillChunk);
+            for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
                 const int4 q = pairs[t];
                 double u[5];
 #pragma unroll
@@ -888,7 +897,7 @@ stage_plane_persistent(const BatchCase *__restrict__ cases, const BatchPlane *__
             __syncthreads();
             if (threadIdx.x == 0) {
                 __threadfence();
-                atomicExch(filled + (long long)k * ncase + c, 1u);
+                atomicAdd(filled + (long long)k * ncase + c, 1u);
             }
         }
     }
@@ -898,8 +907,9 @@ template <bool VISC, bool HYB>
 static int launch_plane_persistent_one(const BatchCase *cases, const BatchPlane *planes, const CUtensorMap *pmaps,
                                        const long long *prefix, int ncase, const PersistStep &ps, const double *dts,
                                        const BatchLevel *levels, const int4 *pairs, const long long *pair_off,
-                                       unsigned long long *queue, unsigned *done, unsigned *filled, int *abort,
-                                       int *status, int blocks, int nthreads, int smem, cudaStream_t st)
+                                       const long long *fill_pre, unsigned long long *queue, unsigned *done,
+                                       unsigned *filled, int *abort, int *status, int blocks, int nthreads, int smem,
+                                       cudaStream_t st)
 {
     static bool configured[64] = {false};
     int dev = 0;
@@ -911,17 +921,17 @@ static int launch_plane_persistent_one(const BatchCase *cases, const BatchPlane 
         configured[dev] = true;
     }
     cudaError_t e = launch_k(stage_plane_persistent<VISC, HYB>, dim3((unsigned)blocks), dim3(nthreads), smem, st,
-                             cases, planes, pmaps, prefix, ncase, ps, dts, levels, pairs, pair_off, queue, done, filled,
-                             abort, status);
+                             cases, planes, pmaps, prefix, ncase, ps, dts, levels, pairs, pair_off, fill_pre, queue,
+                             done, filled, abort, status);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "stage_plane_persistent launch");
 }
 
 static int launch_plane_persistent_impl(const BatchCase *cases, const BatchPlane *planes, const CUtensorMap *pmaps,
                                         const long long *prefix, int ncase, const PersistStep &ps, const double *dts,
                                         const BatchLevel *levels, const int4 *pairs, const long long *pair_off,
-                                        unsigned long long *queue, unsigned *done, unsigned *filled, int *abort,
-                                        int *status, bool viscous, bool hybrid, int blocks, int nthreads, int smem,
-                                        cudaStream_t st)
+                                        const long long *fill_pre, unsigned long long *queue, unsigned *done,
+                                        unsigned *filled, int *abort, int *status, bool viscous, bool hybrid,
+                                        int blocks, int nthreads, int smem, cudaStream_t st)
 {
     if (smem > kPlaneSmemMax || nthreads > kPlaneMaxThreads || ps.nk < 1 || ps.nk > kMaxStepStages) {
         set_error("persistent batch launch: %d threads, %d bytes of shared memory, %d stages", nthreads, smem, ps.nk);
@@ -929,7 +939,8 @@ static int launch_plane_persistent_impl(const BatchCase *cases, const BatchPlane
     }
 #define ACFD_PP(V_, H_)                                                                                           \
     return launch_plane_persistent_one<V_, H_>(cases, planes, pmaps, prefix, ncase, ps, dts, levels, pairs, pair_off, \
-                                               queue, done, filled, abort, status, blocks, nthreads, smem, st);
+                                               fill_pre, queue, done, filled, abort, status, blocks, nthreads, smem,  \
+                                               st);
     if (viscous) {
         if (hybrid) { ACFD_PP(true, true) } else { ACFD_PP(true, false) }
     } else {

@@ -175,11 +175,19 @@ def _run(b_part, b_model, node, mode, steps, dt, params=None, thr=0.5):
 
 
 def test_hybrid_all_flagged_is_the_fp32_form():
+    """Every node flagged: the hybrid form is the FP32-bulk form.  A warp whose
+    flagged lanes are few (tile edges) shares their WENO5 evaluations out over
+    the warp through shared memory, where the split eigenvalue times the
+    characteristic variable is rounded to FP32 before the reconstruction
+    (inline, the compiler may fuse it), so the two agree to FP32 rounding
+    relative to each variable's magnitude."""
+    from test_gpu_march import TOL_FP32_ORDER
+    from test_gpu_parity import rel_err
     b = golden_io.Bundle("tgv")
     node = b.initial_nodes()
     full = _run(b.part, b.model, node, abi.FP32_BULK, 3, b.dt[0])
     hyb = _run(b.part, b.model, node, None, 3, b.dt[0], params=_const_sensor(50.0))
-    assert np.allclose(hyb, full, rtol=1e-6, atol=0)
+    assert rel_err(hyb, full) <= TOL_FP32_ORDER / 10, rel_err(hyb, full)
 
 
 def test_hybrid_smooth_path_is_linear_weight_weno():
