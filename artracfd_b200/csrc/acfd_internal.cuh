@@ -316,9 +316,12 @@ constexpr int kGhostWall = 2;    // top := wall boundary node from the top (its 
 constexpr int kGhostImage = 3;   // (O, I) := image ghost of boundary point O and image node I
 constexpr int kGhostStack = 6;
 constexpr int kGhostMaxOps = 32;
-// pairs: (dst, src) copies; progs: (dst, first op, op count, 0); ops: (code | face << 3, node)
-int launch_ghost_program(const Grid &g, const ModelParams &m, const GhostFaces &F, const int2 *pairs, int npairs,
-                         const int4 *progs, int nprog, const int2 *ops, double *U, cudaStream_t st);
+// chunks: runs of copies (dst, src, length <= 256, 0), one block each;
+// pairs: the other (dst, src) copies; progs: (dst, first op, op count, 0);
+// ops: (code | face << 3, node)
+int launch_ghost_program(const Grid &g, const ModelParams &m, const GhostFaces &F, const int4 *chunks, int nchunk,
+                         const int2 *pairs, int npairs, const int4 *progs, int nprog, const int2 *ops, double *U,
+                         cudaStream_t st);
 // all groups of one TreatBoundary in one cooperative launch with grid barriers;
 // bar: two device words (arrival count, generation), zero at first use
 int launch_domain_boundary_fused(const Grid &g, const ModelParams &m, const acfd_partition_t &part,

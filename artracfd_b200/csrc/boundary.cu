@@ -509,69 +509,81 @@ int launch_ghost_gather(const Grid &g, const int2 *pairs, int count, double *U, 
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "ghost_gather launch");
 }
 
-// Ghost fill as one launch of formulas (see build_bc_program): threads
-// t < npairs copy U[src] to U[dst]; the others evaluate one postfix program
-// each -- LOAD pushes a node's five values, INFLOW the given inflow state,
+// Ghost fill as one launch of formulas (see build_bc_program): the first
+// nchunk blocks copy one run of nodes each; then a thread per remaining copy
+// (U[dst] = U[src]) and a thread per postfix program -- LOAD pushes a node's
+// five values, INFLOW the given inflow state,
 // WALL replaces the top with the wall formula of a boundary node, IMAGE
 // replaces the top two (boundary point O, image node I) with the image
 // ghost -- and store the result.  No node a program or pair reads is written
 // by the launch, so the threads need no ordering among themselves.
-__global__ void __launch_bounds__(256) ghost_program(long long nn, const int2 *__restrict__ pairs, int npairs,
+__global__ void __launch_bounds__(256) ghost_program(long long nn, const int4 *__restrict__ chunks, int nchunk,
+                                                     const int2 *__restrict__ pairs, int npairs,
                                                      const int4 *__restrict__ progs, int nprog,
                                                      const int2 *__restrict__ ops, GhostFaces F, ModelParams mp,
                                                      double *U)
 {
     pdl_wait();
-    const int total = npairs + nprog;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-        if (t < npairs) {
-            const int2 q = pairs[t];
-            copy_node(U, nn, q.x, q.y);
-            continue;
+    if ((int)blockIdx.x < nchunk) {
+        // a run of copies: consecutive destinations from consecutive sources
+        const int4 c = chunks[blockIdx.x];
+        if ((int)threadIdx.x < c.z) {
+            copy_node(U, nn, (long long)c.x + threadIdx.x, (long long)c.y + threadIdx.x);
         }
-        const int4 pr = progs[t - npairs];  // dst, first op, op count
-        double st[kGhostStack][5];
-        int sp = 0;
-        for (int o = 0; o < pr.z; ++o) {
-            const int2 op = ops[pr.y + o];
-            const int code = op.x & 7, face = op.x >> 3;
-            if (code == kGhostLoad) {
-                load5(U, nn, op.y, st[sp]);
-                ++sp;
-            } else if (code == kGhostInflow) {
-                to_conservative(mp.gamma, F.given[face], st[sp]);
-                ++sp;
-            } else if (code == kGhostWall) {
-                double Ut[5];
-                wall_node(mp, F.type[face], F.N[face], F.given[face][5], st[sp - 1], Ut);
+        return;
+    }
+    const int t = ((int)blockIdx.x - nchunk) * blockDim.x + threadIdx.x;
+    if (t < npairs) {
+        const int2 q = pairs[t];
+        copy_node(U, nn, q.x, q.y);
+        return;
+    }
+    if (t >= npairs + nprog) {
+        return;
+    }
+    const int4 pr = progs[t - npairs];  // dst, first op, op count
+    double st[kGhostStack][5];
+    int sp = 0;
+    for (int o = 0; o < pr.z; ++o) {
+        const int2 op = ops[pr.y + o];
+        const int code = op.x & 7, face = op.x >> 3;
+        if (code == kGhostLoad) {
+            load5(U, nn, op.y, st[sp]);
+            ++sp;
+        } else if (code == kGhostInflow) {
+            to_conservative(mp.gamma, F.given[face], st[sp]);
+            ++sp;
+        } else if (code == kGhostWall) {
+            double Ut[5];
+            wall_node(mp, F.type[face], F.N[face], F.given[face][5], st[sp - 1], Ut);
 #pragma unroll
-                for (int v = 0; v < 5; ++v) {
-                    st[sp - 1][v] = Ut[v];
-                }
-            } else {  // kGhostImage
-                double Ut[5];
-                image_ghost(mp, st[sp - 2], st[sp - 1], Ut);
-                --sp;
+            for (int v = 0; v < 5; ++v) {
+                st[sp - 1][v] = Ut[v];
+            }
+        } else {  // kGhostImage
+            double Ut[5];
+            image_ghost(mp, st[sp - 2], st[sp - 1], Ut);
+            --sp;
 #pragma unroll
-                for (int v = 0; v < 5; ++v) {
-                    st[sp - 1][v] = Ut[v];
-                }
+            for (int v = 0; v < 5; ++v) {
+                st[sp - 1][v] = Ut[v];
             }
         }
-        store5(U, nn, pr.x, st[0]);
     }
+    store5(U, nn, pr.x, st[0]);
 }
 
-int launch_ghost_program(const Grid &g, const ModelParams &m, const GhostFaces &F, const int2 *pairs, int npairs,
-                         const int4 *progs, int nprog, const int2 *ops, double *U, cudaStream_t st)
+int launch_ghost_program(const Grid &g, const ModelParams &m, const GhostFaces &F, const int4 *chunks, int nchunk,
+                         const int2 *pairs, int npairs, const int4 *progs, int nprog, const int2 *ops, double *U,
+                         cudaStream_t st)
 {
-    const int total = npairs + nprog;
-    if (total <= 0) {
+    const long long rest = (long long)npairs + nprog;
+    const long long blocks = nchunk + (rest + 255) / 256;
+    if (blocks <= 0) {
         return ACFD_OK;
     }
-    const int blocks = (int)blocks_for(total, 256);
-    cudaError_t e = launch_k(ghost_program, dim3(blocks), dim3(256), 0, st, g.nn, pairs, npairs, progs, nprog, ops,
-                             F, m, U);
+    cudaError_t e = launch_k(ghost_program, dim3((unsigned)blocks), dim3(256), 0, st, g.nn, chunks, nchunk, pairs,
+                             npairs, progs, nprog, ops, F, m, U);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "ghost_program launch");
 }
 
