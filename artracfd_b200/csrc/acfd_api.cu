@@ -1931,39 +1931,42 @@ int batch_step(acfd_batch *b)
     const Coef *rk = b->tScheme == 1 ? rk3 : rk2;
     const int nstage = b->tScheme == 1 ? 3 : 2;
     if (b->persist && b->plane) {
-        // every stage of the step in one launch, cases and stages linked by
-        // per-case counters
-        PersistStep ps;
-        memset(&ps, 0, sizeof(ps));
-        ps.nk = 6 * nstage;
-        ps.kbase[0] = 0;
-        for (int s = 0; s < 3; ++s) {
-            ps.ntile[s] = b->pblocks[s];
-        }
-        ps.nfill = b->nfill;
-        for (int h = 0, k = 0; h < 6; ++h) {
-            for (int q = 0; q < nstage; ++q, ++k) {
-                ps.s_of[k] = order[h];
-                ps.sc[k].coeA = rk[q].a;
-                ps.sc[k].coeB = rk[q].c;
-                ps.sc[k].dt_scale = 0.5;
-                ps.sc[k].to = rk[q].to;
-                ps.sc[k].tn = rk[q].tn;
-                ps.sc[k].tm = rk[q].tm;
-                ps.kbase[k + 1] = ps.kbase[k] + b->pblocks[order[h]] + b->nfill;
-            }
-        }
+        // one persistent launch per directional half step: its RK stages and
+        // ghost fills of every case, linked by per-case counters (indexed by
+        // the step-wide stage, cleared once per step)
         const size_t nflag = (size_t)kMaxStepStages * ncase;
-        ACFD_CUDA(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned long long), b->stream));
         ACFD_CUDA(cudaMemsetAsync(b->d_done, 0, sizeof(unsigned) * nflag, b->stream));
         ACFD_CUDA(cudaMemsetAsync(b->d_filled, 0, sizeof(unsigned) * nflag, b->stream));
         ACFD_CUDA(cudaMemsetAsync(b->d_abort, 0, sizeof(int), b->stream));
-        TRY(launch_stage_plane_persistent(b->d_cases, b->d_planes, b->d_pmaps, b->d_pprefix, ncase, ps, b->d_dts,
-                                          b->d_levels, b->d_pairs, b->d_pair_off, b->d_fill_pre, b->d_queue,
-                                          b->d_done, b->d_filled, b->d_abort, b->d_status, b->visc, hybrid,
-                                          b->persist_blocks,
-                                          b->persist_threads, b->persist_smem, b->stream));
-        ++b->launches;
+        for (int h = 0; h < 6; ++h) {
+            const int s = order[h];
+            PersistStep ps;
+            memset(&ps, 0, sizeof(ps));
+            ps.nk = nstage;
+            ps.k0 = h * nstage;
+            ps.kbase[0] = 0;
+            for (int a = 0; a < 3; ++a) {
+                ps.ntile[a] = b->pblocks[a];
+            }
+            ps.nfill = b->nfill;
+            for (int q = 0; q < nstage; ++q) {
+                ps.s_of[q] = s;
+                ps.sc[q].coeA = rk[q].a;
+                ps.sc[q].coeB = rk[q].c;
+                ps.sc[q].dt_scale = 0.5;
+                ps.sc[q].to = rk[q].to;
+                ps.sc[q].tn = rk[q].tn;
+                ps.sc[q].tm = rk[q].tm;
+                ps.kbase[q + 1] = ps.kbase[q] + b->pblocks[s] + b->nfill;
+            }
+            ACFD_CUDA(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned long long), b->stream));
+            TRY(launch_stage_plane_persistent(b->d_cases, b->d_planes, b->d_pmaps, b->d_pprefix, ncase, ps,
+                                              b->d_dts, b->d_levels, b->d_pairs, b->d_pair_off, b->d_fill_pre,
+                                              b->d_queue, b->d_done, b->d_filled, b->d_abort, b->d_status, b->visc,
+                                              hybrid, b->persist_blocks, b->persist_threads, b->persist_smem,
+                                              b->stream));
+            ++b->launches;
+        }
         return ACFD_OK;
     }
     ACFD_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long) * kBatchStagesPerStep, b->stream));

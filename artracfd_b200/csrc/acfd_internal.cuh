@@ -213,8 +213,10 @@ int launch_stage_plane_batch(const BatchCase *cases, const BatchPlane *planes, c
                              const double *dts, int *status, int s, bool viscous, bool hybrid, int nthreads, int smem,
                              cudaStream_t st);
 
-// Persistent batch step: every RK stage of one time step of every case in
-// one launch.  Work items, in order: for each stage k of the step, the plane
+// Persistent batch step: the RK stages of one directional half step of every
+// case in one launch (six launches per time step, one per sweep of the
+// Strang schedule, so that a kernel holds the block body of one sweep axis
+// only).  Work items, in order: for each stage k of the launch, the plane
 // blocks of every case (case order) and then the ghost-fill items of every
 // case (its copy pairs in chunks of kFillChunk).  A plane block of stage
 // k > 0 of case c waits until every fill item of stage k-1 of case c is
@@ -225,7 +227,8 @@ int launch_stage_plane_batch(const BatchCase *cases, const BatchPlane *planes, c
 constexpr int kMaxStepStages = 18;
 constexpr long long kFillChunk = 16384;  // copy pairs of one ghost-fill item
 struct PersistStep {
-    int nk;                               // stages of the step
+    int nk;                               // stages of this launch
+    int k0;                               // step-wide index of its first stage (counters are per step)
     int s_of[kMaxStepStages];             // sweep axis of stage k
     StageCoefs sc[kMaxStepStages];
     long long kbase[kMaxStepStages + 1];  // first item of stage k

@@ -756,22 +756,6 @@ __device__ __forceinline__ bool persist_wait(const unsigned *word, unsigned want
     return false;
 }
 
-// the block bodies as calls of their own, so that each keeps the register
-// allocation of its single-case kernel inside the persistent loop
-template <bool VISC, bool HYB>
-__device__ __noinline__ void persist_x_item(const Grid &g, const ModelParams &mp, const StageArgs &a,
-                                            const PlaneTile &pt, const CUtensorMap *mapp, int blk, unsigned char *smem)
-{
-    plane_x_block<6, VISC, HYB>(g, mp, a, pt, mapp, blk, smem);
-}
-
-template <bool VISC, bool HYB>
-__device__ __noinline__ void persist_yz_item(const Grid &g, const ModelParams &mp, const StageArgs &a,
-                                             const PlaneTile &pt, const CUtensorMap *mapp, int blk, unsigned char *smem)
-{
-    plane_yz_block<6, VISC, HYB>(g, mp, a, pt, mapp, blk, smem);
-}
-
 // the full/empty barriers of a plane block of sweep axis s (the layout of
 // plane_yz_block and plane_x_block)
 __device__ __forceinline__ uint64_t *plane_barriers(const PlaneTile &pt, int s, unsigned char *smem)
@@ -782,7 +766,7 @@ __device__ __forceinline__ uint64_t *plane_barriers(const PlaneTile &pt, int s, 
                                         (size_t)pt.ncw * kCoopBytes);
 }
 
-template <bool VISC, bool HYB>
+template <bool VISC, bool HYB, bool XS>
 __global__ void __launch_bounds__(kPlaneMaxThreads, 2)
 stage_plane_persistent(const BatchCase *__restrict__ cases, const BatchPlane *__restrict__ planes,
                        const CUtensorMap *pmaps, const long long *__restrict__ prefix, int ncase, PersistStep ps,
@@ -791,41 +775,60 @@ stage_plane_persistent(const BatchCase *__restrict__ cases, const BatchPlane *__
                        unsigned long long *queue, unsigned *done, unsigned *filled, int *abort, int *status)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ long long s_item;
-    __shared__ int s_ok;
-    const long long total = ps.kbase[ps.nk];
+    // the decoded item, shared by the block; nothing of the loop stays in
+    // registers across the item's block body (whose register budget is that
+    // of the single-case kernel)
+    __shared__ int s_k, s_c, s_blk, s_ok;  // s_blk < 0: fill chunk -s_blk-1 of case s_c
     for (;;) {
         if (threadIdx.x == 0) {
-            s_item = (*reinterpret_cast<volatile int *>(abort) != 0) ? total : (long long)atomicAdd(queue, 1ULL);
+            const long long total = ps.kbase[ps.nk];
+            const long long it = (*reinterpret_cast<volatile int *>(abort) != 0)
+                                     ? total : (long long)atomicAdd(queue, 1ULL);
+            int ok = it < total;
+            if (ok) {
+                int k = 0;
+                while (it >= ps.kbase[k + 1]) ++k;
+                const int s = ps.s_of[k];
+                const long long local = it - ps.kbase[k];
+                const long long *pre = prefix + (long long)s * (ncase + 1);
+                int c = 0;
+                if (local < ps.ntile[s]) {
+                    int hi = ncase - 1;  // the case whose blocks contain this one
+                    while (c < hi) {
+                        const int mid = (c + hi + 1) / 2;
+                        if (pre[mid] <= local) c = mid; else hi = mid - 1;
+                    }
+                    s_blk = (int)(local - pre[c]);
+                    // the fill of the stage before (step-wide index; the first
+                    // stage of a launch finds it done by the launch before)
+                    const int kg = ps.k0 + k;
+                    ok = (kg == 0) || persist_wait(filled + (long long)(kg - 1) * ncase + c,
+                                                   (unsigned)(fill_pre[c + 1] - fill_pre[c]), abort, status);
+                } else {
+                    const long long f = local - ps.ntile[s];
+                    int hi = ncase - 1;
+                    while (c < hi) {
+                        const int mid = (c + hi + 1) / 2;
+                        if (fill_pre[mid] <= f) c = mid; else hi = mid - 1;
+                    }
+                    s_blk = -(int)(f - fill_pre[c]) - 1;
+                    ok = persist_wait(done + (long long)(ps.k0 + k) * ncase + c, (unsigned)(pre[c + 1] - pre[c]),
+                                      abort, status);
+                }
+                s_k = k;
+                s_c = c;
+            }
+            s_ok = ok;
         }
         __syncthreads();
-        const long long it = s_item;
-        if (it >= total) {
+        if (!s_ok) {
             break;
         }
-        int k = 0;
-        while (it >= ps.kbase[k + 1]) ++k;
-        const int s = ps.s_of[k];
-        const long long local = it - ps.kbase[k];
-        const long long *pre = prefix + (long long)s * (ncase + 1);
-        if (local < ps.ntile[s]) {
-            int lo = 0, hi = ncase - 1;  // the case whose blocks contain this one
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) / 2;
-                if (pre[mid] <= local) lo = mid; else hi = mid - 1;
-            }
-            const int c = lo;
-            if (threadIdx.x == 0) {
-                s_ok = (k == 0) || persist_wait(filled + (long long)(k - 1) * ncase + c,
-                                                (unsigned)(fill_pre[c + 1] - fill_pre[c]), abort, status);
-            }
-            __syncthreads();
-            if (!s_ok) {
-                break;
-            }
+        if (s_blk >= 0) {
             // the planes this block's TMA copies read were written by other
             // blocks' ordinary stores
             asm volatile("fence.proxy.async.global;" ::: "memory");
+            const int k = s_k, c = s_c, s = ps.s_of[k];
             const BatchCase &C = cases[c];
             const BatchPlane &P = planes[3 * c + s];
             const StageCoefs &sc = ps.sc[k];
@@ -849,42 +852,29 @@ stage_plane_persistent(const BatchCase *__restrict__ cases, const BatchPlane *__
             a.status = status;
             a.flags = C.flags;
             a.wait_limit = kWaitLimitDefault;
-            const int blk = (int)(local - pre[c]);
-            if (s == 0) {
-                persist_x_item<VISC, HYB>(P.gk, C.mp, a, P.pt, pmaps + 3 * c + s, blk, smem);
+            if constexpr (XS) {
+                plane_x_block<6, VISC, HYB>(P.gk, C.mp, a, P.pt, pmaps + 3 * c + s, s_blk, smem);
             } else {
-                persist_yz_item<VISC, HYB>(P.gk, C.mp, a, P.pt, pmaps + 3 * c + s, blk, smem);
+                plane_yz_block<6, VISC, HYB>(P.gk, C.mp, a, P.pt, pmaps + 3 * c + s, s_blk, smem);
             }
             __syncthreads();
             if (threadIdx.x == 0) {
                 // the item's barriers are idle (its copies were waited for):
                 // invalidate them before the next item initialises its own
-                uint64_t *bars = plane_barriers(P.pt, s, smem);
+                const int c2 = s_c, s2 = ps.s_of[s_k];
+                uint64_t *bars = plane_barriers(planes[3 * c2 + s2].pt, s2, smem);
                 for (int q = 0; q < 2 * kPlaneSlots; ++q) {
                     tma::mbar_inval(bars + q);
                 }
                 __threadfence();
-                atomicAdd(done + (long long)k * ncase + c, 1u);
+                atomicAdd(done + (long long)(ps.k0 + s_k) * ncase + c2, 1u);
             }
         } else {
-            // fill item f: chunk f - fill_pre[c] of case c's copy pairs
-            const long long f = local - ps.ntile[s];
-            int c = 0, chi = ncase - 1;
-            while (c < chi) {
-                const int mid = (c + chi + 1) / 2;
-                if (fill_pre[mid] <= f) c = mid; else chi = mid - 1;
-            }
-            if (threadIdx.x == 0) {
-                s_ok = persist_wait(done + (long long)k * ncase + c, (unsigned)(pre[c + 1] - pre[c]), abort, status);
-            }
-            __syncthreads();
-            if (!s_ok) {
-                break;
-            }
-            // the chunk's copy pairs, reading through L2
+            // fill chunk of case c: its copy pairs, reading through L2
+            const int k = s_k, c = s_c;
             const BatchLevel L = levels[c];
             double *U = L.U + (long long)ps.sc[k].tm * 5 * L.nn;
-            const long long t0 = pair_off[c] + (f - fill_pre[c]) * kFillChunk;
+            const long long t0 = pair_off[c] + (long long)(-s_blk - 1) * kFillChunk;
             const long long t1 = min(pair_off[c + 1], t0 + kFillChunk);
             for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
                 const int4 q = pairs[t];
@@ -897,13 +887,14 @@ stage_plane_persistent(const BatchCase *__restrict__ cases, const BatchPlane *__
             __syncthreads();
             if (threadIdx.x == 0) {
                 __threadfence();
-                atomicAdd(filled + (long long)k * ncase + c, 1u);
+                atomicAdd(filled + (long long)(ps.k0 + s_k) * ncase + s_c, 1u);
             }
         }
+        __syncthreads();  // the shared item is read by all before thread 0 takes the next
     }
 }
 
-template <bool VISC, bool HYB>
+template <bool VISC, bool HYB, bool XS>
 static int launch_plane_persistent_one(const BatchCase *cases, const BatchPlane *planes, const CUtensorMap *pmaps,
                                        const long long *prefix, int ncase, const PersistStep &ps, const double *dts,
                                        const BatchLevel *levels, const int4 *pairs, const long long *pair_off,
@@ -915,12 +906,12 @@ static int launch_plane_persistent_one(const BatchCase *cases, const BatchPlane 
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !configured[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(stage_plane_persistent<VISC, HYB>,
+        cudaError_t e = cudaFuncSetAttribute(stage_plane_persistent<VISC, HYB, XS>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, kPlaneSmemMax);
         if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(stage_plane_persistent)");
         configured[dev] = true;
     }
-    cudaError_t e = launch_k(stage_plane_persistent<VISC, HYB>, dim3((unsigned)blocks), dim3(nthreads), smem, st,
+    cudaError_t e = launch_k(stage_plane_persistent<VISC, HYB, XS>, dim3((unsigned)blocks), dim3(nthreads), smem, st,
                              cases, planes, pmaps, prefix, ncase, ps, dts, levels, pairs, pair_off, fill_pre, queue,
                              done, filled, abort, status);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "stage_plane_persistent launch");
@@ -937,10 +928,14 @@ static int launch_plane_persistent_impl(const BatchCase *cases, const BatchPlane
         set_error("persistent batch launch: %d threads, %d bytes of shared memory, %d stages", nthreads, smem, ps.nk);
         return ACFD_ERR_ARG;
     }
-#define ACFD_PP(V_, H_)                                                                                           \
-    return launch_plane_persistent_one<V_, H_>(cases, planes, pmaps, prefix, ncase, ps, dts, levels, pairs, pair_off, \
-                                               fill_pre, queue, done, filled, abort, status, blocks, nthreads, smem,  \
-                                               st);
+#define ACFD_PP(V_, H_)                                                                                            \
+    return (ps.s_of[0] == 0)                                                                                       \
+               ? launch_plane_persistent_one<V_, H_, true>(cases, planes, pmaps, prefix, ncase, ps, dts, levels,     \
+                                                           pairs, pair_off, fill_pre, queue, done, filled, abort,    \
+                                                           status, blocks, nthreads, smem, st)                       \
+               : launch_plane_persistent_one<V_, H_, false>(cases, planes, pmaps, prefix, ncase, ps, dts, levels,    \
+                                                            pairs, pair_off, fill_pre, queue, done, filled, abort,   \
+                                                            status, blocks, nthreads, smem, st);
     if (viscous) {
         if (hybrid) { ACFD_PP(true, true) } else { ACFD_PP(true, false) }
     } else {
@@ -951,15 +946,28 @@ static int launch_plane_persistent_impl(const BatchCase *cases, const BatchPlane
 
 static int plane_persistent_occupancy_impl(bool viscous, bool hybrid, int nthreads, int smem, int *blocks_per_sm)
 {
-    const void *fn = viscous ? (hybrid ? (const void *)stage_plane_persistent<true, true>
-                                       : (const void *)stage_plane_persistent<true, false>)
-                             : (hybrid ? (const void *)stage_plane_persistent<false, true>
-                                       : (const void *)stage_plane_persistent<false, false>);
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kPlaneSmemMax);
-    if (e == cudaSuccess) {
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, nthreads, smem);
+    // the smaller of the X and Y/Z kernels' resident blocks
+    const void *fns[2] = {viscous ? (hybrid ? (const void *)stage_plane_persistent<true, true, true>
+                                            : (const void *)stage_plane_persistent<true, false, true>)
+                                  : (hybrid ? (const void *)stage_plane_persistent<false, true, true>
+                                            : (const void *)stage_plane_persistent<false, false, true>),
+                          viscous ? (hybrid ? (const void *)stage_plane_persistent<true, true, false>
+                                            : (const void *)stage_plane_persistent<true, false, false>)
+                                  : (hybrid ? (const void *)stage_plane_persistent<false, true, false>
+                                            : (const void *)stage_plane_persistent<false, false, false>)};
+    *blocks_per_sm = 1 << 30;
+    for (const void *fn : fns) {
+        int b = 0;
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kPlaneSmemMax);
+        if (e == cudaSuccess) {
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, nthreads, smem);
+        }
+        if (e != cudaSuccess) {
+            return cuda_status(e, "persistent batch occupancy");
+        }
+        *blocks_per_sm = std::min(*blocks_per_sm, b);
     }
-    return e == cudaSuccess ? ACFD_OK : cuda_status(e, "persistent batch occupancy");
+    return ACFD_OK;
 }
 #endif
 

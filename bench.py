@@ -586,6 +586,12 @@ def run_ours(args, rank, world, local_rank):
             shock_cyl = shock_cylinder_block(torch, args, dist, stream, local_rank)
         except Exception as exc:  # the headline line is printed regardless
             shock_cyl = {"error": f"{type(exc).__name__}: {exc}"}
+    ib = None
+    if args.mode == "hybrid" and args.ib_steps > 0:
+        try:
+            ib = ib_dropin_block(args)
+        except Exception as exc:
+            ib = {"error": f"{type(exc).__name__}: {exc}"}
     batch = None
     if args.mode == "hybrid" and args.batch_steps > 0:
         try:
@@ -622,6 +628,7 @@ def run_ours(args, rank, world, local_rank):
         "accuracy": accuracy,
         "shock_cylinder": shock_cyl,
         "batch": batch,
+        "ib_spheres_dropin": ib,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": traffic,
                      "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of an RK-stage-2 launch "
@@ -664,6 +671,46 @@ def run_ours(args, rank, world, local_rank):
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
+
+
+def ib_dropin_block(args):
+    """The immersed-boundary configuration through the drop-in program (the
+    reference's own host code -- case loading, rigid-body kinematics --
+    linked with libacfd_gpu): crossflow over eight moving 1280-facet spheres
+    in [0,4]^3 at 192^3 cells (191 x 193 x 193 = 7,114,559 computed nodes),
+    plain FP64 path, the rigid-body step's node scans, collisions and surface
+    motion on the device.  Rate from the program's own per-step timer
+    (host wall clock of a whole step, solid half steps included; the first
+    step, which captures the step graph, is left out)."""
+    import re
+    import shutil
+    from artracfd_b200 import configs
+    exe = os.path.join(ROOT, "artracfd_b200", "shim", "_build", "artracfd_gpu")
+    if not os.path.exists(exe):
+        return {"unavailable": "drop-in program not built (it needs the reference sources)"}
+    steps = max(2, args.ib_steps)
+    spec = configs.ib_spheres(n=192)
+    spec.stepN = steps
+    work = tempfile.mkdtemp(prefix="acfd_ib_")
+    case = os.path.join(work, "ib192")
+    spec.write(case)
+    env = dict(os.environ, ACFD_MODE="fp64")
+    t0 = time.perf_counter()
+    r = subprocess.run([exe, "-m", "gpu"], cwd=case, env=env, capture_output=True, text=True, timeout=900)
+    wall = time.perf_counter() - t0
+    shutil.rmtree(work, ignore_errors=True)
+    if r.returncode != 0:
+        return {"error": f"drop-in program exited {r.returncode}: {r.stdout[-300:]} {r.stderr[-300:]}"}
+    el = [float(x) for x in re.findall(r"elapsed: ([0-9.eE+-]+)s", r.stdout)]
+    if len(el) < 2:
+        return {"error": "no step timer lines in the drop-in program's output"}
+    per_step = sum(el[1:]) / len(el[1:])
+    pin = 191 * 193 * 193
+    return {"workload": "8 moving 1280-facet spheres in a Ma 0.3, Re 200 crossflow, 192^3 cells (7,114,559 "
+                        "computed nodes), WENO5/RK3, drop-in program, plain FP64 path, solid step on the device",
+            "value": pin / per_step / 1e6, "unit": UNIT, "ms_per_step": per_step * 1e3, "steps_timed": len(el) - 1,
+            "wall_s": wall, "timer": "the program's own per-step host timer (solve.c:89 restated), first step "
+                                     "(graph capture) left out"}
 
 
 def batch_block(args, steps, local_rank):
@@ -858,6 +905,8 @@ def main():
     ap.add_argument("--workload", default="tgv", choices=["tgv", "batch"],
                     help="tgv: the headline line (TGV 128^3); batch: the 48-case batched sweep")
     ap.add_argument("--batch-cases", type=int, default=48)
+    ap.add_argument("--ib-steps", type=int, default=6,
+                    help="steps of the 192^3 moving-spheres drop-in block (0: leave it out)")
     ap.add_argument("--batch-steps", type=int, default=10,
                     help="timed steps of the batch block of the default line (0: leave it out)")
     args = ap.parse_args()

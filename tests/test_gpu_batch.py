@@ -164,12 +164,12 @@ def _copy_only_specs():
 @pytest.mark.parametrize("form", ["fp32", "hybrid"])
 def test_batch_persistent_step_matches_single_cases(form):
     """The persistent step (the default for all-viscous batches whose ghost
-    fills are copies): every RK stage of a time step of every case in one
-    launch, the plane-march blocks and the ghost fills linked by per-case
-    counters.  Each case agrees with the single-case plane kernels to FP32
-    round-off (the first dt bit for bit) and with the per-stage plane batch
-    to the same bound, and the launch count per step is the CFL, dt, sensor
-    and one persistent launch."""
+    fills are copies): the RK stages of each directional half step of every
+    case in one launch (six per time step), the plane-march blocks and the
+    ghost fills linked by per-case counters.  Each case agrees with the
+    single-case plane kernels to FP32 round-off (the first dt bit for bit)
+    and with the per-stage plane batch to the same bound, and the launch
+    count per step is the CFL, dt, sensor and six persistent launches."""
     specs = _copy_only_specs()
     descs = [s.descriptors() for s in specs]
     if form == "hybrid":
@@ -187,7 +187,7 @@ def test_batch_persistent_step_matches_single_cases(form):
         assert rel_err(outs[c], sout) <= TOL_FP32_ORDER, (c, rel_err(outs[c], sout))
         assert rel_err(outs[c], pouts[c]) <= TOL_FP32_ORDER, (c, rel_err(outs[c], pouts[c]))
     per_case = 2 + (2 if form == "hybrid" else 0)
-    assert launches == STEPS * (len(specs) * per_case + 2), launches
+    assert launches == STEPS * (len(specs) * per_case + 1 + 6), launches
 
 
 def test_batch_persistent_is_the_default_for_copy_only_viscous_cases():
