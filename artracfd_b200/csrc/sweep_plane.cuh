@@ -876,13 +876,29 @@ stage_plane_persistent(const BatchCase *__restrict__ cases, const BatchPlane *__
             double *U = L.U + (long long)ps.sc[k].tm * 5 * L.nn;
             const long long t0 = pair_off[c] + (long long)(-s_blk - 1) * kFillChunk;
             const long long t1 = min(pair_off[c + 1], t0 + kFillChunk);
-            for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
-                const int4 q = pairs[t];
-                double u[5];
+            // four copies per thread per pass: twenty loads in flight
+            const long long stride = blockDim.x;
+            for (long long t = t0 + threadIdx.x; t < t1; t += 4 * stride) {
+                int4 q[4];
+                double u[4][5];
 #pragma unroll
-                for (int v = 0; v < 5; ++v) u[v] = __ldcg(U + v * L.nn + q.z);
+                for (int r = 0; r < 4; ++r) {
+                    q[r] = (t + r * stride < t1) ? pairs[t + r * stride] : make_int4(0, -1, -1, 0);
+                }
 #pragma unroll
-                for (int v = 0; v < 5; ++v) U[v * L.nn + q.y] = u[v];
+                for (int r = 0; r < 4; ++r) {
+                    if (q[r].y >= 0) {
+#pragma unroll
+                        for (int v = 0; v < 5; ++v) u[r][v] = __ldcg(U + v * L.nn + q[r].z);
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    if (q[r].y >= 0) {
+#pragma unroll
+                        for (int v = 0; v < 5; ++v) U[v * L.nn + q[r].y] = u[r][v];
+                    }
+                }
             }
             __syncthreads();
             if (threadIdx.x == 0) {

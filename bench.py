@@ -580,20 +580,23 @@ def run_ours(args, rank, world, local_rank):
     accuracy = None
     if args.mode in ("fp32", "hybrid") and args.accuracy_steps > 0:
         accuracy = _accuracy(part, model, node, spec, args.mode, args.accuracy_steps, stream)
+    # the blocks of the other configurations are single-GPU figures: at N > 1
+    # every rank times the headline replica only
+    extra = args.mode == "hybrid" and world == 1
     shock_cyl = None
-    if args.mode == "hybrid" and not args.no_shock_cylinder:
+    if extra and not args.no_shock_cylinder:
         try:
             shock_cyl = shock_cylinder_block(torch, args, dist, stream, local_rank)
         except Exception as exc:  # the headline line is printed regardless
             shock_cyl = {"error": f"{type(exc).__name__}: {exc}"}
     ib = None
-    if args.mode == "hybrid" and args.ib_steps > 0:
+    if extra and args.ib_steps > 0:
         try:
             ib = ib_dropin_block(args)
         except Exception as exc:
             ib = {"error": f"{type(exc).__name__}: {exc}"}
     batch = None
-    if args.mode == "hybrid" and args.batch_steps > 0:
+    if extra and args.batch_steps > 0:
         try:
             batch = batch_block(args, args.batch_steps, local_rank)
         except Exception as exc:
