@@ -106,9 +106,9 @@ class Batch:
         check(self.lib.acfd_batch_set_precision(self.h, mode), self.lib)
 
     def set_kernel(self, kernel: int):
-        """abi.BATCH_PERSISTENT (every RK stage of a step of every case in one
-        persistent launch; the default when the cases allow it),
-        abi.BATCH_PLANE (one plane-march launch per RK stage) or
+        """abi.BATCH_PLANE (one plane-march launch per RK stage; the default
+        when the cases allow it), abi.BATCH_PERSISTENT (the RK stages of each
+        directional half step of every case in one persistent launch) or
         abi.BATCH_BRICK (persistent brick kernel, one launch per RK stage)."""
         check(self.lib.acfd_batch_set_kernel(self.h, kernel), self.lib)
 

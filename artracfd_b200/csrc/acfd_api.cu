@@ -1865,9 +1865,6 @@ struct acfd_batch {
     // plane-march stage kernels (all cases viscous or all inviscid, plane maps present)
     bool plane_ok = false, plane = false, visc = false;
     BatchPlane *d_planes = nullptr;        // [ncase][3]
-    BatchPlane *d_pplanes = nullptr;       // [ncase][3] the persistent kernel's tiles (larger items)
-    long long *d_ppprefix = nullptr;       // [3][ncase + 1] their prefix sums
-    long long ppblocks[3] = {0, 0, 0};
     CUtensorMap *d_pmaps = nullptr;        // [ncase][3]
     long long *d_pprefix = nullptr;        // [3][ncase + 1] prefix sums of the plane blocks per sweep axis
     long long pblocks[3] = {0, 0, 0};
@@ -1949,7 +1946,7 @@ int batch_step(acfd_batch *b)
             ps.k0 = h * nstage;
             ps.kbase[0] = 0;
             for (int a = 0; a < 3; ++a) {
-                ps.ntile[a] = b->ppblocks[a];
+                ps.ntile[a] = b->pblocks[a];
             }
             ps.nfill = b->nfill;
             for (int q = 0; q < nstage; ++q) {
@@ -1960,10 +1957,10 @@ int batch_step(acfd_batch *b)
                 ps.sc[q].to = rk[q].to;
                 ps.sc[q].tn = rk[q].tn;
                 ps.sc[q].tm = rk[q].tm;
-                ps.kbase[q + 1] = ps.kbase[q] + b->ppblocks[s] + b->nfill;
+                ps.kbase[q + 1] = ps.kbase[q] + b->pblocks[s] + b->nfill;
             }
             ACFD_CUDA(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned long long), b->stream));
-            TRY(launch_stage_plane_persistent(b->d_cases, b->d_pplanes, b->d_pmaps, b->d_ppprefix, ncase, ps,
+            TRY(launch_stage_plane_persistent(b->d_cases, b->d_planes, b->d_pmaps, b->d_pprefix, ncase, ps,
                                               b->d_dts, b->d_levels, b->d_pairs, b->d_pair_off, b->d_fill_pre,
                                               b->d_queue, b->d_done, b->d_filled, b->d_abort, b->d_status, b->visc,
                                               hybrid, b->persist_blocks, b->persist_threads, b->persist_smem,
@@ -2111,9 +2108,9 @@ int acfd_batch_init(int ncase, const acfd_partition_t *parts, const acfd_model_t
     // persistent stage launch: two resident blocks of the viscous bricks per SM
     b->blocks = 2 * b->sms;
     // plane-march launches: one launch per stage over the plane blocks of all cases
-    std::vector<BatchPlane> hp((size_t)ncase * 3), hpp((size_t)ncase * 3);
+    std::vector<BatchPlane> hp((size_t)ncase * 3);
     std::vector<CUtensorMap> hpm((size_t)ncase * 3);
-    std::vector<long long> pprefix((size_t)3 * (ncase + 1), 0), ppprefix((size_t)3 * (ncase + 1), 0);
+    std::vector<long long> pprefix((size_t)3 * (ncase + 1), 0);
     if (st == ACFD_OK) {
         b->visc = viscous(b->cases[0]);
         b->plane_ok = true;
@@ -2148,22 +2145,13 @@ int acfd_batch_init(int ncase, const acfd_partition_t *parts, const acfd_model_t
                 hpm[(size_t)c * 3 + s] = cs->pmaps[s];
                 const long long nb = P.pt.nblk;
                 pprefix[(size_t)s * (ncase + 1) + c + 1] = pprefix[(size_t)s * (ncase + 1) + c] + nb;
-                // the persistent kernel's items: the same tile, its lines cut
-                // into a quarter of the segments (fewer, longer items; the
-                // cases of the batch keep the whole GPU busy)
-                BatchPlane &Q = hpp[(size_t)c * 3 + s];
-                Q = P;
-                const PlaneTile q4 = plane_tile(cs->grid, s, b->visc, 1, std::max(1, b->sms / 4));
-                Q.pt.nseg = q4.nseg;
-                Q.pt.nblk = q4.nblk;
-                ppprefix[(size_t)s * (ncase + 1) + c + 1] = ppprefix[(size_t)s * (ncase + 1) + c] + Q.pt.nblk;
+
                 b->pthreads[s] = std::max(b->pthreads[s], (P.pt.ncw + 1) * 32);
                 b->psmem[s] = std::max(b->psmem[s], plane_smem_bytes(P.pt, s));
             }
         }
         for (int s = 0; s < 3; ++s) {
             b->pblocks[s] = pprefix[(size_t)s * (ncase + 1) + ncase];
-            b->ppblocks[s] = ppprefix[(size_t)s * (ncase + 1) + ncase];
         }
         if (b->plane_ok) {
             if ((e = cudaMalloc(&b->d_planes, sizeof(BatchPlane) * hp.size())) != cudaSuccess ||
@@ -2174,12 +2162,6 @@ int acfd_batch_init(int ncase, const acfd_partition_t *parts, const acfd_model_t
                 (e = cudaMemcpy(b->d_pmaps, hpm.data(), sizeof(CUtensorMap) * hpm.size(), cudaMemcpyHostToDevice)) !=
                     cudaSuccess ||
                 (e = cudaMemcpy(b->d_pprefix, pprefix.data(), sizeof(long long) * pprefix.size(),
-                                cudaMemcpyHostToDevice)) != cudaSuccess ||
-                (e = cudaMalloc(&b->d_pplanes, sizeof(BatchPlane) * hpp.size())) != cudaSuccess ||
-                (e = cudaMalloc(&b->d_ppprefix, sizeof(long long) * ppprefix.size())) != cudaSuccess ||
-                (e = cudaMemcpy(b->d_pplanes, hpp.data(), sizeof(BatchPlane) * hpp.size(), cudaMemcpyHostToDevice)) !=
-                    cudaSuccess ||
-                (e = cudaMemcpy(b->d_ppprefix, ppprefix.data(), sizeof(long long) * ppprefix.size(),
                                 cudaMemcpyHostToDevice)) != cudaSuccess) {
                 st = cuda_status(e, "acfd_batch_init (plane maps)");
             }
@@ -2247,7 +2229,10 @@ int acfd_batch_init(int ncase, const acfd_partition_t *parts, const acfd_model_t
             b->nfill = fpre[(size_t)ncase];
             b->persist_blocks = bps * b->sms;
             b->persist_ok = true;
-            b->persist = true;
+            // available (acfd_batch_set_kernel), not the default: measured
+            // 811 against 878 Mcell-steps/s for one launch per RK stage on the
+            // 48-case batch
+            b->persist = false;
         } else {
             cudaGetLastError();  // keep the per-stage launches
         }
@@ -2293,8 +2278,6 @@ int acfd_batch_finalize(acfd_batch_t *b)
     cudaFree(b->d_abort);
     cudaFree(b->d_pair_off);
     cudaFree(b->d_fill_pre);
-    cudaFree(b->d_pplanes);
-    cudaFree(b->d_ppprefix);
     if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
     delete b;
     return ACFD_OK;

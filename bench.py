@@ -774,13 +774,14 @@ def batch_block(args, steps, local_rank):
     b.set_precision(abi.FP32_HYBRID)
     cfl = [s.cfl for s in specs]
     total = sum(pin)
-    kernels = {}
+    # the default (one plane-march launch per RK stage) first: its rate is
+    # the block's value; then the persistent step
+    kernels = {"per_stage_plane": abi.BATCH_PLANE}
     try:
         b.set_kernel(abi.BATCH_PERSISTENT)
         kernels["persistent"] = abi.BATCH_PERSISTENT
     except abi.AcfdError:
         pass
-    kernels["per_stage_plane"] = abi.BATCH_PLANE
     timed = {}
     errs = None
     for name, kern in kernels.items():

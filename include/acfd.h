@@ -395,13 +395,14 @@ int acfd_batch_sensor_load(acfd_batch_t *b, const float *params, float threshold
  * step.  Returns after the work has finished. */
 int acfd_batch_advance(acfd_batch_t *b, const double *cfl, int steps, double *dts);
 /* Stage kernel of the batch:
+ *  ACFD_BATCH_PLANE       one plane-march launch per RK stage over all cases
+ *                         (the default when all cases are viscous or all
+ *                         inviscid);
  *  ACFD_BATCH_PERSISTENT  the RK stages of each directional half step of
  *                         every case in one persistent launch (six per time
  *                         step) of plane-march blocks and ghost fills,
- *                         linked by per-case counters (bounded waits; the
- *                         default when all cases are viscous or all inviscid
- *                         and every ghost fill is a copy);
- *  ACFD_BATCH_PLANE       one plane-march launch per RK stage over all cases;
+ *                         linked by per-case counters (bounded waits); when
+ *                         every case's ghost fill is a copy;
  *  ACFD_BATCH_BRICK       the persistent brick kernel that pulls (case, tile)
  *                         items from a counter, one launch per RK stage. */
 #define ACFD_BATCH_BRICK 0

@@ -163,8 +163,8 @@ def _copy_only_specs():
 
 @pytest.mark.parametrize("form", ["fp32", "hybrid"])
 def test_batch_persistent_step_matches_single_cases(form):
-    """The persistent step (the default for all-viscous batches whose ghost
-    fills are copies): the RK stages of each directional half step of every
+    """The persistent step (for all-viscous batches whose ghost fills are
+    copies): the RK stages of each directional half step of every
     case in one launch (six per time step), the plane-march blocks and the
     ghost fills linked by per-case counters.  Each case agrees with the
     single-case plane kernels to FP32 round-off (the first dt bit for bit)
@@ -190,7 +190,7 @@ def test_batch_persistent_step_matches_single_cases(form):
     assert launches == STEPS * (len(specs) * per_case + 1 + 6), launches
 
 
-def test_batch_persistent_is_the_default_for_copy_only_viscous_cases():
+def test_batch_persistent_step_is_offered_for_copy_only_viscous_cases():
     specs = _copy_only_specs()
     with Batch([s.descriptors() for s in specs]) as b:
         b.set_kernel(abi.BATCH_PERSISTENT)  # accepted
