@@ -31,9 +31,9 @@ X, Y, Z, DIMS, PHI = 0, 1, 2, 3, 4
 FP64_EXACT, FP64, FP32_BULK, FP32_HYBRID = 0, 1, 2, 3
 # stage-kernel variants (acfd_set_tiles): bricks below BRICK_VARIANTS, then
 # the line-march kernels with 1, 2, 4 waves, then from PLANE_VARIANT the
-# plane-march kernels (Y/Z sweeps) with 1, 2, 4 waves
+# plane-march kernels with 1, 2, 4 waves (lines cut into segments per tile)
 BRICK_VARIANTS, PLANE_VARIANT, STAGE_VARIANTS = 2, 5, 11
-# the plane march with equal shares of all tiles' planes per block (Y/Z)
+# the plane march with equal shares of all tiles' planes per block
 PLANE_SHARE_VARIANT = PLANE_VARIANT + 3
 # stage kernel of a batch (acfd_batch_set_kernel)
 BATCH_BRICK, BATCH_PLANE, BATCH_PERSISTENT = 0, 1, 2

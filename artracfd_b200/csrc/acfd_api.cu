@@ -95,7 +95,7 @@ bool pdl_enabled()
 // Stage-kernel variants: the brick tile shapes (0 .. kTileVariants-1), the
 // line-march kernels and the plane-march kernels, each launched with 1, 2 or
 // 4 waves; the plane march twice: lines cut into equal segments per tile,
-// then (Y and Z sweeps) equal shares of all tiles' planes per block
+// then equal shares of all tiles' planes per block
 constexpr int kMarchVariants = 3;
 constexpr int kMarchWaves[kMarchVariants] = {1, 2, 4};
 constexpr int kPlaneVariants = 6;
@@ -2145,7 +2145,6 @@ int acfd_batch_init(int ncase, const acfd_partition_t *parts, const acfd_model_t
                 hpm[(size_t)c * 3 + s] = cs->pmaps[s];
                 const long long nb = P.pt.nblk;
                 pprefix[(size_t)s * (ncase + 1) + c + 1] = pprefix[(size_t)s * (ncase + 1) + c] + nb;
-
                 b->pthreads[s] = std::max(b->pthreads[s], (P.pt.ncw + 1) * 32);
                 b->psmem[s] = std::max(b->psmem[s], plane_smem_bytes(P.pt, s));
             }

@@ -132,8 +132,8 @@ struct PlaneTile {
     int TR;        // consumer threads per row (WX; WX + 1 interfaces on X sweeps)
     int ntx, ntc;  // tiles along x and along the rows
     int nseg;      // segments of each line (with shares: the chunks of the chunk-major plane order)
-    int nblk;      // blocks of a launch: tiles x segments, or (Y/Z, share) equal shares of all tiles' planes
-    int share;     // Y/Z kernel: 1 = a block marches an equal share of the tiles' planes, chunk-major
+    int nblk;      // blocks of a launch: tiles x segments, or (share) equal shares of all tiles' planes
+    int share;     // 1 = a block marches an equal share of the tiles' planes, chunk-major
     int BXp, BC;   // plane box: x extent (even, covers the x halo) and rows with halo
     int ncw;       // consumer warps (the producer is warp ncw)
     int swap;      // Y/Z kernel: 1 = a Z sweep run with axes 1 and 2 exchanged
@@ -176,7 +176,7 @@ inline PlaneTile plane_tile(const Grid &g, int s, bool visc, int waves, int sms,
     if (nseg > cap) nseg = cap;
     if (nseg < 1) nseg = 1;
     pt.nseg = (int)nseg;
-    pt.share = (share && s != 0) ? 1 : 0;
+    pt.share = share ? 1 : 0;
     if (!pt.share) {
         pt.nblk = (int)(tiles * nseg);
     } else {

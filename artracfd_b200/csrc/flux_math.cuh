@@ -307,6 +307,18 @@ __device__ __forceinline__ float rcp<float>(float x)
     return __fdividef(1.0f, x);
 }
 
+// a*b - c*d with one fused operation in a fixed form.  Left to the compiler,
+// the contraction of such an expression into a fused multiply-add may differ
+// between two inlined copies of the same code; where two copies compute the
+// same value for neighbouring blocks (the node left of a plane-march segment
+// and the same node carried inside the segment before it) they must round
+// alike, or the flux of the interface between the blocks differs by an ulp.
+template <typename T>
+__device__ __forceinline__ T diff_prod(T a, T b, T c, T d)
+{
+    return fma(a, b, -(c * d));
+}
+
 // Roe/arithmetic interface state: Uo[1..3] velocity, Uo[4] total enthalpy,
 // Uo[5] sound speed.
 template <typename T>

@@ -46,14 +46,16 @@ __device__ __forceinline__ void march_load(const double *__restrict__ U, long lo
     }
 }
 
-// velocity and temperature of a node
+// velocity and temperature of a node; the fused operations are written out
+// so that every inlined copy rounds alike (fast::diff_prod)
 __device__ __forceinline__ void march_prims(const Real w[5], Real cvinv, Real P[4])
 {
     const Real ir = fast::rcp<Real>(w[0]);
     P[0] = w[1] * ir;
     P[1] = w[2] * ir;
     P[2] = w[3] * ir;
-    P[3] = (w[4] * ir - Real(0.5) * (P[0] * P[0] + P[1] * P[1] + P[2] * P[2])) * cvinv;
+    const Real vv = fma(P[2], P[2], fma(P[1], P[1], P[0] * P[0]));
+    P[3] = fma(Real(-0.5), vv, w[4] * ir) * cvinv;
 }
 
 // the two transverse axes of sweep S, in increasing order
@@ -227,8 +229,8 @@ __device__ __forceinline__ void march_tdiff(const double *__restrict__ U, long l
     const Real rm = fast::rcp<Real>(Real(__ldg(U + qm)));
     const Real tp = Real(__ldg(U + (1 + t) * nn + qp)), tm = Real(__ldg(U + (1 + t) * nn + qm));
     const Real sp = Real(__ldg(U + (1 + S) * nn + qp)), sm = Real(__ldg(U + (1 + S) * nn + qm));
-    D[0] = tp * rp - tm * rm;
-    D[1] = sp * rp - sm * rm;
+    D[0] = fast::diff_prod(tp, rp, tm, rm);
+    D[1] = fast::diff_prod(sp, rp, sm, rm);
 }
 
 // interface flux (convective minus viscous is added by the caller)

@@ -31,6 +31,56 @@ namespace ACFD_NS {
 
 constexpr long long kPlaneWaitLimit = kWaitLimitDefault;
 
+// Items of a plane-march block (both kernels march along y, or along z with
+// the axes exchanged, over tiles of x by rows).  With shares (SHARE) a block
+// marches positions [w, r1) of the list of all tiles' lines in chunk-major
+// order: the lines are cut into pt.nseg chunks, and chunk c of every tile
+// comes before chunk c+1 of any tile, so that blocks of neighbouring tiles
+// march the same planes at the same time (their halo rows are shared in L2)
+// while every block of the launch gets the same number of planes.  A share
+// that crosses the end of a (chunk, tile) piece is two items, marched one
+// after the other through the same ring.  Without shares a block marches
+// segment blk / tiles of tile blk % tiles.  Returns false when the block has
+// no item left; otherwise the item's tile T and planes [p0, p1) counted from
+// the first computed node of the march axis, and w moves past the item.
+template <bool SHARE>
+__device__ __forceinline__ bool plane_next_item(const PlaneTile &pt, int Ls, long long tiles, int blk, long long r1,
+                                                long long &w, long long &T, int &p0, int &p1)
+{
+    if (w >= r1) return false;
+    const int nch = pt.nseg;
+    auto plo = [&](int c) { return (int)((long long)c * Ls / nch); };  // first plane of chunk c
+    if constexpr (SHARE) {
+        int c = (int)((w / tiles) * nch / Ls);
+        while (c + 1 < nch && tiles * plo(c + 1) <= w) ++c;
+        while (c > 0 && tiles * plo(c) > w) --c;
+        const int len = plo(c + 1) - plo(c);
+        const long long rel = w - tiles * plo(c);
+        T = rel / len;
+        const int o = (int)(rel - T * len);
+        const int n = (int)((r1 - w < (long long)(len - o)) ? r1 - w : (long long)(len - o));
+        p0 = plo(c) + o;
+        p1 = p0 + n;
+        w += n;
+    } else {
+        T = blk % tiles;
+        const int seg = (int)(blk / tiles);
+        p0 = plo(seg);
+        p1 = plo(seg + 1);
+        w = r1;
+    }
+    return true;
+}
+
+// the first and one past the last list position of block blk's share
+__device__ __forceinline__ void plane_share(const PlaneTile &pt, int Ls, long long tiles, int blk, long long &r0,
+                                           long long &r1)
+{
+    const long long work = tiles * Ls;
+    r0 = (long long)blk * work / pt.nblk;
+    r1 = (long long)(blk + 1) * work / pt.nblk;
+}
+
 // One instantiation serves both axes: the kernel is written for the Y sweep
 // (S = 1, rows along z).  A Z sweep runs it on a grid descriptor with axes 1
 // and 2 exchanged (pt.swap = 1): the line and row strides come from pt, the
@@ -73,49 +123,21 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
         return;
     }
 
-    // With shares (pt.share) a block marches planes [r0, r1) of the list of
-    // all tiles' lines in chunk-major order: the lines are cut into pt.nseg
-    // chunks, and chunk c of every tile comes before chunk c+1 of any tile, so
-    // that blocks of neighbouring tiles march the same planes at the same
-    // time (their halo rows are shared in L2) while every block of the launch
-    // gets the same number of planes.  A share that crosses the end of a
-    // (chunk, tile) piece is two items, marched one after the other through
-    // the same ring (the plane sequence q runs on).  Without shares
-    // (pt.share == 0) a block marches segment blk / tiles of tile blk % tiles.
+    // the items of the block (plane_next_item); the plane sequence q of the
+    // ring runs on from one item to the next
     const int Ls = g.hi[S] - g.lo[S];
     const long long tiles = (long long)pt.ntx * pt.ntc;
     long long r0 = 0, r1 = 1;
     if constexpr (SHARE) {
-        const long long work = tiles * Ls;
-        r0 = (long long)blk * work / pt.nblk;
-        r1 = (long long)(blk + 1) * work / pt.nblk;
+        plane_share(pt, Ls, tiles, blk, r0, r1);
         if (r1 <= r0) return;
     }
-    const int nch = pt.nseg;
-    auto plo = [&](int c) { return (int)((long long)c * Ls / nch); };  // first plane of chunk c
     // the item at list position w: tile origin, planes [p0, p1); w moves past it
     auto next_item = [&](long long &w, int &x0, int &c0, int &p0, int &p1) {
-        if (w >= r1) return false;
         long long T;
-        if constexpr (SHARE) {
-            int c = (int)((w / tiles) * nch / Ls);
-            while (c + 1 < nch && tiles * plo(c + 1) <= w) ++c;
-            while (c > 0 && tiles * plo(c) > w) --c;
-            const int len = plo(c + 1) - plo(c);
-            const long long rel = w - tiles * plo(c);
-            T = rel / len;
-            const int o = (int)(rel - T * len);
-            const int n = (int)((r1 - w < (long long)(len - o)) ? r1 - w : (long long)(len - o));
-            p0 = g.lo[S] + plo(c) + o;
-            p1 = p0 + n;
-            w += n;
-        } else {
-            T = blk % tiles;
-            const int seg = (int)(blk / tiles);
-            p0 = g.lo[S] + (int)((long long)seg * Ls / nch);
-            p1 = g.lo[S] + (int)((long long)(seg + 1) * Ls / nch);
-            w = r1;
-        }
+        if (!plane_next_item<SHARE>(pt, Ls, tiles, blk, r1, w, T, p0, p1)) return false;
+        p0 += g.lo[S];
+        p1 += g.lo[S];
         x0 = g.lo[0] + (int)(T % pt.ntx) * pt.WX;
         c0 = g.lo[T2] + (int)(T / pt.ntx) * pt.NR;
         return true;
@@ -208,8 +230,8 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
                 const int ot = vg(1 + tax) * pe, os = vg(1 + S) * pe;
                 const Real tp = Real(P[ot + ep]), tm = Real(P[ot + em]);
                 const Real sp = Real(P[os + ep]), sm = Real(P[os + em]);
-                D[q][0] = tp * rp - tm * rm;
-                D[q][1] = sp * rp - sm * rm;
+                D[q][0] = fast::diff_prod(tp, rp, tm, rm);
+                D[q][1] = fast::diff_prod(sp, rp, sm, rm);
             }
         };
 
@@ -336,7 +358,73 @@ stage_plane_yz(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_c
 // to the node on their right through a double-buffered shared array, one
 // named barrier of the consumer warps per plane.
 // ---------------------------------------------------------------------------
-template <int NP, bool VISC, bool HYB>
+
+// the item of an X-sweep block at list position w (plane_next_item): tile
+// origin (x0, c0) and rows [j0, j1) along y; w moves past it
+template <bool SHARE>
+__device__ __forceinline__ bool plane_x_item(const Grid &g, const PlaneTile &pt, long long tiles, int blk,
+                                             long long r1, long long &w, int &x0, int &c0, int &j0, int &j1)
+{
+    long long T;
+    if (!plane_next_item<SHARE>(pt, g.hi[1] - g.lo[1], tiles, blk, r1, w, T, j0, j1)) return false;
+    j0 += g.lo[1];
+    j1 += g.lo[1];
+    x0 = g.lo[0] + (int)(T % pt.ntx) * pt.WX;
+    c0 = g.lo[2] + (int)(T / pt.ntx) * pt.NR;
+    return true;
+}
+
+// producer lane of an X-sweep block: the planes of rows j0-hv .. j1-1+hv of
+// every item, plane q of the block's sequence into ring slot q % NS; the
+// block does not end with copies in flight
+template <int H, int hv, int NS, bool SHARE>
+__device__ __forceinline__ void plane_x_produce(const Grid &g, const StageArgs &a, const PlaneTile &pt,
+                                                const CUtensorMap *mapp, int blk, long long r0, long long r1,
+                                                double *ring, uint64_t *full, uint64_t *empty)
+{
+    const int plane_bytes = pt.BXp * pt.BC * 5 * 8;
+    const int slot_doubles = plane_slot_bytes(pt.BXp, pt.BC) / 8;
+    const long long tiles = (long long)pt.ntx * pt.ntc;
+    int q = 0, issued = 0;
+    bool ok = true;
+    long long w = r0;
+    int x0, c0, j0, j1;
+    while (ok && plane_x_item<SHARE>(g, pt, tiles, blk, r1, w, x0, c0, j0, j1)) {
+        const int xs = (x0 - H) & ~1, cs = c0 - hv;
+        const int NQ = j1 - j0 + 2 * hv;  // rows j0-hv .. j1-1+hv
+        for (int ql = 0; ql < NQ; ++ql, ++q) {
+            const int slot = q % NS;
+            if (q >= NS && !tma::mbar_wait_bounded(empty + slot, ((q / NS) - 1) & 1, a.status, 5, a.wait_limit)) {
+                ok = false;
+                break;
+            }
+            tma::mbar_expect_tx(full + slot, plane_bytes);
+            tma::load_5d(ring + (size_t)slot * slot_doubles, mapp, xs, j0 - hv + ql, cs, 0, a.tn, full + slot);
+            issued = q + 1;
+        }
+    }
+    for (int qq = issued - NS > 0 ? issued - NS : 0; qq < issued; ++qq) {
+        tma::mbar_wait_bounded(full + qq % NS, (qq / NS) & 1, a.status, 5, kPlaneWaitLimit);
+    }
+}
+
+// named barrier 1 of the nbar consumer threads, or-reducing `abort`: the
+// consumer warps leave together when a wait of one of them gave up
+__device__ __forceinline__ bool consumers_barrier_or(bool abort, unsigned nbar)
+{
+    unsigned any;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "bar.red.or.pred p, 1, %2, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(any)
+        : "r"((unsigned)abort), "r"(nbar)
+        : "memory");
+    return any != 0u;
+}
+
+template <int NP, bool VISC, bool HYB, bool SHARE = false>
 __device__ __forceinline__ void plane_x_block(const Grid &g, const ModelParams &mp, const StageArgs &a,
                                               const PlaneTile &pt, const CUtensorMap *mapp, int blk,
                                               unsigned char *smem)
@@ -346,7 +434,6 @@ __device__ __forceinline__ void plane_x_block(const Grid &g, const ModelParams &
     constexpr int NS = kPlaneSlots;
     constexpr unsigned kAll = 0xffffffffu;
     const int pe = pt.BXp * pt.BC;
-    const int plane_bytes = pe * 5 * 8;
     const int slot_doubles = plane_slot_bytes(pt.BXp, pt.BC) / 8;
     const int nflux = pt.TR * pt.NR;
     double *ring = reinterpret_cast<double *>(smem);
@@ -367,185 +454,167 @@ __device__ __forceinline__ void plane_x_block(const Grid &g, const ModelParams &
     if (warp > pt.ncw) {
         return;
     }
-
-    int b = blk;
-    const int tx = b % pt.ntx;
-    b /= pt.ntx;
-    const int tc = b % pt.ntc;
-    const int seg = b / pt.ntc;
-    const int Ly = g.hi[1] - g.lo[1];
-    const int x0 = g.lo[0] + tx * pt.WX;
-    const int c0 = g.lo[2] + tc * pt.NR;
-    const int j0 = g.lo[1] + (int)((long long)seg * Ly / pt.nseg);
-    const int j1 = g.lo[1] + (int)((long long)(seg + 1) * Ly / pt.nseg);
-    const int xs = (x0 - H) & ~1;
-    const int cs = c0 - hv;
-    const int NQ = j1 - j0 + 2 * hv;  // rows j0-hv .. j1-1+hv
-
+    // the items of the block (plane_x_item); the plane sequence q of the
+    // ring runs on from item to item
+    const long long tiles = (long long)pt.ntx * pt.ntc;
+    long long r0 = 0, r1 = 1;
+    if constexpr (SHARE) {
+        plane_share(pt, g.hi[1] - g.lo[1], tiles, blk, r0, r1);
+        if (r1 <= r0) return;
+    }
     if (warp == pt.ncw) {
-        if (lane == 0) {
-            int issued = 0;
-            for (int q = 0; q < NQ; ++q) {
-                const int slot = q % NS;
-                if (q >= NS && !tma::mbar_wait_bounded(empty + slot, ((q / NS) - 1) & 1, a.status, 5,
-                                                       a.wait_limit)) {
-                    break;
-                }
-                tma::mbar_expect_tx(full + slot, plane_bytes);
-                tma::load_5d(ring + (size_t)slot * slot_doubles, mapp, xs, j0 - hv + q, cs, 0, a.tn, full + slot);
-                issued = q + 1;
-            }
-            for (int q = issued - NS > 0 ? issued - NS : 0; q < issued; ++q) {
-                tma::mbar_wait_bounded(full + q % NS, (q / NS) & 1, a.status, 5, kPlaneWaitLimit);
-            }
-        }
+        if (lane == 0) plane_x_produce<H, hv, NS, SHARE>(g, a, pt, mapp, blk, r0, r1, ring, full, empty);
         return;
     }
 
-    // consumer thread: interface xi+1/2 of z-row c
-    const int t = threadIdx.x;
-    const int xl = t % pt.TR, rl = t / pt.TR;
-    const int xi = x0 - 1 + xl;
-    const int c = c0 + rl;
-    const bool row_ok = (rl < pt.NR) && (c < g.hi[2]);
-    const bool active = row_ok && (xi < g.hi[0]);          // interface computed
-    const bool upd = active && xl >= 1;                      // node xi updated
-    // element of node xi in a plane (inactive threads: the tile's first node)
-    const int e0 = active ? (rl + hv) * pt.BXp + (xi - xs) : hv * pt.BXp + (x0 - xs);
-    const long long nn = g.nn;
-    const long long sy = (long long)g.pitch, sz = (long long)g.pitch * g.n[1];
-    const long long xz = (long long)c * sz + xi;
-    const Real cvinv = Real(1.0 / mp.cv);
-    const bool same_o = (a.Uo == a.Un);
-    const double rdt = (a.dt_scale * a.dt[0]) * g.dd[0];
-    const uint8_t *__restrict__ fl = a.flags;  // sweep 0 flags
-    auto plane = [&](int q) { return ring + (size_t)(q % NS) * slot_doubles; };
-    auto wait_plane = [&](int q) {
-        const bool ok = tma::mbar_wait_bounded(full + q % NS, (q / NS) & 1, a.status, 5, a.wait_limit);
-        return __all_sync(kAll, ok);
-    };
-    auto release = [&](int q) {
-        __syncwarp();
-        if (lane == 0) tma::mbar_arrive(empty + q % NS);
-    };
     const unsigned nbar = (unsigned)pt.ncw * 32u;
-    // the consumer warps leave together: a wait that gave up is or-reduced
-    // over the named barrier of the flux exchange
-    auto exchange_barrier = [&](bool abort) {
-        unsigned any;
-        asm volatile(
-            "{\n\t.reg .pred p, q;\n\t"
-            "setp.ne.u32 q, %1, 0;\n\t"
-            "bar.red.or.pred p, 1, %2, q;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(any)
-            : "r"((unsigned)abort), "r"(nbar)
-            : "memory");
-        return any != 0u;
-    };
+    int qbase = 0;  // first plane of the item in the block's sequence
+    int buf = 0;    // flux buffer of the row
+    long long wi = r0;
+    int x0, c0, j0, j1;
+    while (plane_x_item<SHARE>(g, pt, tiles, blk, r1, wi, x0, c0, j0, j1)) {
+        const int xs = (x0 - H) & ~1;
+        const int NQ = j1 - j0 + 2 * hv;
 
-    bool ok = true;
-    for (int q = 0; q < 2 * hv; ++q) {
-        ok = ok && wait_plane(q);  // rows j0-1 and j0 (viscous)
-    }
-    // sensor flags of the interface's nodes xi-1 .. xi+2 and the did of node
-    // xi, loaded one row ahead of their use
-    auto row_flags = [&](long long idr) {
-        return (unsigned)(fl[idr - 1] | fl[idr] | fl[idr + 1] | fl[idr + 2]);
-    };
-    unsigned fl_n = (HYB && active) ? row_flags(xz + (long long)j0 * sy) : 1u;
-    int did_n = upd ? a.did[xz + (long long)j0 * sy] : 1;
-    int buf = 0;
-    for (int j = j0; j < j1; ++j) {
-        const int q = j - j0 + hv;  // plane of row j
-        const long long id = xz + (long long)j * sy;
-        const int did = did_n;
-        const unsigned fl_j = fl_n;
-        if (j + 1 < j1) {
-            if (upd) did_n = a.did[id + sy];
-            if (HYB && active) fl_n = row_flags(id + sy);
+        // consumer thread: interface xi+1/2 of z-row c
+        const int t = threadIdx.x;
+        const int xl = t % pt.TR, rl = t / pt.TR;
+        const int xi = x0 - 1 + xl;
+        const int c = c0 + rl;
+        const bool row_ok = (rl < pt.NR) && (c < g.hi[2]);
+        const bool active = row_ok && (xi < g.hi[0]);          // interface computed
+        const bool upd = active && xl >= 1;                      // node xi updated
+        // element of node xi in a plane (inactive threads: the tile's first node)
+        const int e0 = active ? (rl + hv) * pt.BXp + (xi - xs) : hv * pt.BXp + (x0 - xs);
+        const long long nn = g.nn;
+        const long long sy = (long long)g.pitch, sz = (long long)g.pitch * g.n[1];
+        const long long xz = (long long)c * sz + xi;
+        const Real cvinv = Real(1.0 / mp.cv);
+        const bool same_o = (a.Uo == a.Un);
+        const double rdt = (a.dt_scale * a.dt[0]) * g.dd[0];
+        const uint8_t *__restrict__ fl = a.flags;  // sweep 0 flags
+        // plane q of the item is plane qbase + q of the block's sequence
+        auto plane = [&](int q) { return ring + (size_t)((qbase + q) % NS) * slot_doubles; };
+        auto wait_plane = [&](int q) {
+            const int qq = qbase + q;
+            const bool ok = tma::mbar_wait_bounded(full + qq % NS, (qq / NS) & 1, a.status, 5, a.wait_limit);
+            return __all_sync(kAll, ok);
+        };
+        auto release = [&](int q) {
+            __syncwarp();
+            if (lane == 0) tma::mbar_arrive(empty + (qbase + q) % NS);
+        };
+        bool ok = true;
+        for (int q = 0; q < 2 * hv; ++q) {
+            ok = ok && wait_plane(q);  // rows j0-1 and j0 (viscous)
         }
-        double uo[5];
-        if (upd && !same_o && !a.accumulate) {
-#pragma unroll
-            for (int v = 0; v < 5; ++v) uo[v] = __ldcg(a.Uo + v * nn + id);
-        }
-        const bool full_w = !HYB || fl_j != 0u;
-        ok = ok && wait_plane(q + hv);  // row j+1 (viscous) or j
-        const double *P = plane(ok ? q : 0);
-        Real W[NP][5];
-#pragma unroll
-        for (int m = 0; m < NP; ++m) {
-#pragma unroll
-            for (int v = 0; v < 5; ++v) W[m][v] = Real(P[v * pe + e0 - (H - 1) + m]);
-        }
-        Real F[5];
-        if constexpr (HYB && NP == 6) {
-            march_flux_coop<0>(mp, W, full_w, F, coop + (size_t)warp * (kCoopBytes / sizeof(Real)));
-        } else {
-            march_flux<0, NP, HYB>(mp, W, full_w, F);
-        }
-        if (VISC) {
-            Real Pc[4], Pn[4], Dc[2][2], Dn[2][2];
-            march_prims(W[H - 1], cvinv, Pc);
-            march_prims(W[H], cvinv, Pn);
-            const double *Pm = plane(q - 1), *Pp = plane(q + 1);
-#pragma unroll
-            for (int side = 0; side < 2; ++side) {
-                const int e = e0 + side;
-                Real(&D)[2][2] = side ? Dn : Dc;
-                // y: planes j+1 and j-1 (v and u)
-                {
-                    const Real rp = fast::rcp<Real>(Real(Pp[e])), rm = fast::rcp<Real>(Real(Pm[e]));
-                    D[0][0] = Real(Pp[2 * pe + e]) * rp - Real(Pm[2 * pe + e]) * rm;
-                    D[0][1] = Real(Pp[pe + e]) * rp - Real(Pm[pe + e]) * rm;
+        // sensor flags of the interface's nodes xi-1 .. xi+2 and the did of node
+        // xi, loaded one row ahead of their use
+        auto row_flags = [&](long long idr) {
+            return (unsigned)(fl[idr - 1] | fl[idr] | fl[idr + 1] | fl[idr + 2]);
+        };
+        unsigned fl_n = (HYB && active) ? row_flags(xz + (long long)j0 * sy) : 1u;
+        int did_n = upd ? a.did[xz + (long long)j0 * sy] : 1;
+        for (int j = j0; j < j1; ++j) {
+            const int q = j - j0 + hv;  // plane of row j
+            const long long id = xz + (long long)j * sy;
+            const int did = did_n;
+            const unsigned fl_j = fl_n;
+            if (j + 1 < j1) {
+                if (upd) did_n = a.did[id + sy];
+                if (HYB && active) fl_n = row_flags(id + sy);
+            }
+            double uo[5];
+            if (upd && !same_o && !a.accumulate) {
+    #pragma unroll
+                for (int v = 0; v < 5; ++v) uo[v] = __ldcg(a.Uo + v * nn + id);
+            }
+            const bool full_w = !HYB || fl_j != 0u;
+            ok = ok && wait_plane(q + hv);  // row j+1 (viscous) or j
+            const double *P = plane(ok ? q : 0);
+            Real W[NP][5];
+    #pragma unroll
+            for (int m = 0; m < NP; ++m) {
+    #pragma unroll
+                for (int v = 0; v < 5; ++v) W[m][v] = Real(P[v * pe + e0 - (H - 1) + m]);
+            }
+            Real F[5];
+            if constexpr (HYB && NP == 6) {
+                march_flux_coop<0>(mp, W, full_w, F, coop + (size_t)warp * (kCoopBytes / sizeof(Real)));
+            } else {
+                march_flux<0, NP, HYB>(mp, W, full_w, F);
+            }
+            if (VISC) {
+                Real Pc[4], Pn[4], Dc[2][2], Dn[2][2];
+                march_prims(W[H - 1], cvinv, Pc);
+                march_prims(W[H], cvinv, Pn);
+                const double *Pm = plane(q - 1), *Pp = plane(q + 1);
+    #pragma unroll
+                for (int side = 0; side < 2; ++side) {
+                    const int e = e0 + side;
+                    Real(&D)[2][2] = side ? Dn : Dc;
+                    // y: planes j+1 and j-1 (v and u)
+                    {
+                        const Real rp = fast::rcp<Real>(Real(Pp[e])), rm = fast::rcp<Real>(Real(Pm[e]));
+                        D[0][0] = fast::diff_prod(Real(Pp[2 * pe + e]), rp, Real(Pm[2 * pe + e]), rm);
+                        D[0][1] = fast::diff_prod(Real(Pp[pe + e]), rp, Real(Pm[pe + e]), rm);
+                    }
+                    // z: rows c+1 and c-1 of plane j (w and u)
+                    {
+                        const int ep = e + pt.BXp, em = e - pt.BXp;
+                        const Real rp = fast::rcp<Real>(Real(P[ep])), rm = fast::rcp<Real>(Real(P[em]));
+                        D[1][0] = fast::diff_prod(Real(P[3 * pe + ep]), rp, Real(P[3 * pe + em]), rm);
+                        D[1][1] = fast::diff_prod(Real(P[pe + ep]), rp, Real(P[pe + em]), rm);
+                    }
                 }
-                // z: rows c+1 and c-1 of plane j (w and u)
-                {
-                    const int ep = e + pt.BXp, em = e - pt.BXp;
-                    const Real rp = fast::rcp<Real>(Real(P[ep])), rm = fast::rcp<Real>(Real(P[em]));
-                    D[1][0] = Real(P[3 * pe + ep]) * rp - Real(P[3 * pe + em]) * rm;
-                    D[1][1] = Real(P[pe + ep]) * rp - Real(P[pe + em]) * rm;
+                march_visc<0>(g, mp, Pc, Pn, Dc, Dn, F);
+            }
+            Real *sFb = sF + (size_t)buf * nflux * 5;
+            if (active) {
+    #pragma unroll
+                for (int v = 0; v < 5; ++v) sFb[v * nflux + t] = F[v];
+            }
+            if (consumers_barrier_or(!ok, nbar)) {
+                return;
+            }
+            if (upd && did == 0) {
+    #pragma unroll
+                for (int v = 0; v < 5; ++v) {
+                    const double phi = double(sFb[v * nflux + t - 1]) - double(F[v]);
+                    const long long qv = v * nn + id;
+                    const double un = P[v * pe + e0];
+                    if (a.accumulate) {
+                        a.Um[qv] = __ldcg(a.Um + qv) + a.coeB * rdt * phi;
+                    } else {
+                        a.Um[qv] = a.coeA * (same_o ? un : uo[v]) + a.coeB * (un + rdt * phi);
+                    }
                 }
             }
-            march_visc<0>(g, mp, Pc, Pn, Dc, Dn, F);
+            // the plane of row j-1 (viscous) or j is read for the last time
+            release(q - hv);
+            buf ^= 1;
         }
-        Real *sFb = sF + (size_t)buf * nflux * 5;
-        if (active) {
-#pragma unroll
-            for (int v = 0; v < 5; ++v) sFb[v * nflux + t] = F[v];
-        }
-        if (exchange_barrier(!ok)) {
-            break;
-        }
-        if (upd && did == 0) {
-#pragma unroll
-            for (int v = 0; v < 5; ++v) {
-                const double phi = double(sFb[v * nflux + t - 1]) - double(F[v]);
-                const long long qv = v * nn + id;
-                const double un = P[v * pe + e0];
-                if (a.accumulate) {
-                    a.Um[qv] = __ldcg(a.Um + qv) + a.coeB * rdt * phi;
-                } else {
-                    a.Um[qv] = a.coeA * (same_o ? un : uo[v]) + a.coeB * (un + rdt * phi);
-                }
+        if constexpr (SHARE) {
+            // rows j1-1 and j1 (viscous) were read for the last time: free their
+            // slots for the next item's planes
+            for (int q = NQ - 2 * hv; q < NQ; ++q) {
+                release(q);
             }
         }
-        // the plane of row j-1 (viscous) or j is read for the last time
-        release(q - hv);
-        buf ^= 1;
+        qbase += NQ;
     }
 }
 
-template <int NP, bool VISC, bool HYB>
+
+template <int NP, bool VISC, bool HYB, bool SHARE>
 __global__ void __launch_bounds__(kPlaneMaxThreads, sizeof(Real) == sizeof(float) ? 2 : 1)
 stage_plane_x(Grid g, ModelParams mp, StageArgs a, PlaneTile pt, const __grid_constant__ CUtensorMap map)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    plane_x_block<NP, VISC, HYB>(g, mp, a, pt, &map, (int)blockIdx.x, smem);
+    plane_x_block<NP, VISC, HYB, SHARE>(g, mp, a, pt, &map, (int)blockIdx.x, smem);
 }
 
-template <int NP, bool VISC, bool HYB>
+template <int NP, bool VISC, bool HYB, bool SHARE>
 static int launch_plane_x(const Grid &g, const ModelParams &m, const StageArgs &a, const PlaneTile &pt,
                           const CUtensorMap &map, cudaStream_t st)
 {
@@ -554,7 +623,7 @@ static int launch_plane_x(const Grid &g, const ModelParams &m, const StageArgs &
     cudaGetDevice(&dev);
     const int smem = plane_smem_bytes(pt, 0);
     if (dev >= 0 && dev < 64 && !configured[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(stage_plane_x<NP, VISC, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(stage_plane_x<NP, VISC, HYB, SHARE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              kPlaneSmemMax);
         if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(stage_plane_x)");
         configured[dev] = true;
@@ -564,7 +633,7 @@ static int launch_plane_x(const Grid &g, const ModelParams &m, const StageArgs &
         return ACFD_ERR_ARG;
     }
     const unsigned blocks = (unsigned)pt.nblk;
-    cudaError_t e = launch_k(stage_plane_x<NP, VISC, HYB>, dim3(blocks), dim3((pt.ncw + 1) * 32), smem, st, g, m, a,
+    cudaError_t e = launch_k(stage_plane_x<NP, VISC, HYB, SHARE>, dim3(blocks), dim3((pt.ncw + 1) * 32), smem, st, g, m, a,
                              pt, map);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "stage_plane_x launch");
 }
@@ -614,7 +683,10 @@ template <int NP, bool VISC, bool HYB>
 static int launch_plane_s(const Grid &g, const ModelParams &m, const StageArgs &a, int s, const PlaneTile &pt,
                           const CUtensorMap &map, cudaStream_t st)
 {
-    if (s == 0) return launch_plane_x<NP, VISC, HYB>(g, m, a, pt, map, st);
+    if (s == 0) {
+        return pt.share ? launch_plane_x<NP, VISC, HYB, true>(g, m, a, pt, map, st)
+                        : launch_plane_x<NP, VISC, HYB, false>(g, m, a, pt, map, st);
+    }
     return pt.share ? launch_plane_yz<NP, VISC, HYB, true>(g, m, a, s, pt, map, st)
                     : launch_plane_yz<NP, VISC, HYB, false>(g, m, a, s, pt, map, st);
 }
@@ -876,29 +948,13 @@ stage_plane_persistent(const BatchCase *__restrict__ cases, const BatchPlane *__
             double *U = L.U + (long long)ps.sc[k].tm * 5 * L.nn;
             const long long t0 = pair_off[c] + (long long)(-s_blk - 1) * kFillChunk;
             const long long t1 = min(pair_off[c + 1], t0 + kFillChunk);
-            // four copies per thread per pass: twenty loads in flight
-            const long long stride = blockDim.x;
-            for (long long t = t0 + threadIdx.x; t < t1; t += 4 * stride) {
-                int4 q[4];
-                double u[4][5];
+            for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                const int4 q = pairs[t];
+                double u[5];
 #pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    q[r] = (t + r * stride < t1) ? pairs[t + r * stride] : make_int4(0, -1, -1, 0);
-                }
+                for (int v = 0; v < 5; ++v) u[v] = __ldcg(U + v * L.nn + q.z);
 #pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    if (q[r].y >= 0) {
-#pragma unroll
-                        for (int v = 0; v < 5; ++v) u[r][v] = __ldcg(U + v * L.nn + q[r].z);
-                    }
-                }
-#pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    if (q[r].y >= 0) {
-#pragma unroll
-                        for (int v = 0; v < 5; ++v) U[v * L.nn + q[r].y] = u[r][v];
-                    }
-                }
+                for (int v = 0; v < 5; ++v) U[v * L.nn + q.y] = u[v];
             }
             __syncthreads();
             if (threadIdx.x == 0) {

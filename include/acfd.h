@@ -167,9 +167,8 @@ int acfd_synchronize(acfd_case_t *cs);
  * tile shapes; the next three the line-march kernels launched with 1, 2 or 4
  * waves of resident warps; ACFD_PLANE_VARIANT .. ACFD_STAGE_VARIANTS-1 the
  * plane-march kernels (a TMA ring of halo'd planes) with 1, 2 or 4 waves of
- * blocks, first with each tile's lines cut into equal segments, then (Y and
- * Z sweeps; X as the first three) with equal shares of all tiles' planes per
- * block.  The choice is kept per arithmetic form; the FP32 forms start on the
+ * blocks, first with each tile's lines cut into equal segments, then with
+ * equal shares of all tiles' planes per block.  The choice is kept per arithmetic form; the FP32 forms start on the
  * brick for X and the 4-wave plane march for Y and Z, the FP64 form on the
  * first brick; acfd_autotune replaces these with the measured fastest. */
 #define ACFD_BRICK_VARIANTS 2
