@@ -1041,7 +1041,8 @@ int acfd_init(const acfd_partition_t *part, const acfd_model_t *model, acfd_case
     if ((e = cudaMalloc(&cs->U, ubytes)) != cudaSuccess ||
         (e = cudaMalloc(&cs->flags, fbytes)) != cudaSuccess ||
         (e = cudaMalloc(&cs->d_dt, sizeof(double))) != cudaSuccess ||
-        (e = cudaMalloc(&cs->cfl_part, sizeof(double) * 4 * kCflBlocks)) != cudaSuccess ||
+        (e = cudaMalloc(&cs->cfl_part, sizeof(double) * kCflPartials)) != cudaSuccess ||
+        (e = cudaMemset(cs->cfl_part, 0, sizeof(double) * kCflPartials)) != cudaSuccess ||
         (e = cudaMalloc(&cs->cfl_out, sizeof(double) * 4)) != cudaSuccess ||
         (e = cudaMallocHost(&cs->h_cfl, sizeof(double) * 4)) != cudaSuccess ||
         (e = cudaMalloc(&cs->dstatus, sizeof(int))) != cudaSuccess ||
@@ -1229,7 +1230,7 @@ int acfd_cfl(acfd_case_t *cs, double vmax[3])
         return ACFD_ERR_ARG;
     }
     TRY(launch_cfl(cs->grid, cs->mp, cs->U, cs->flags, cs->cfl_part, cs->cfl_out, cs->stream));
-    cs->launches += 2;
+    ++cs->launches;
     ACFD_CUDA(cudaMemcpyAsync(cs->h_cfl, cs->cfl_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, cs->stream));
     ACFD_CUDA(cudaStreamSynchronize(cs->stream));
     for (int s = 0; s < 3; ++s) {
@@ -1907,7 +1908,7 @@ int batch_step(acfd_batch *b)
     const int ncase = (int)b->cases.size();
     for (acfd_case *cs : b->cases) {
         TRY(launch_cfl(cs->grid, cs->mp, cs->U, cs->flags, cs->cfl_part, cs->cfl_out, b->stream));
-        b->launches += 2;
+        ++b->launches;
     }
     TRY(launch_batch_dt(b->d_vmax, b->d_mesh, b->d_cfl, b->d_dts, ncase, b->stream));
     ++b->launches;

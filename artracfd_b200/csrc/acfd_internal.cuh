@@ -331,9 +331,12 @@ int launch_domain_boundary_fused(const Grid &g, const ModelParams &m, const acfd
                                  const FaceBox *const *groups, const int *sizes, int ngroups, double *U,
                                  unsigned *bar, int *status, cudaStream_t st);
 
-// CFL wave-speed maximum: partials (>= kCflBlocks*4 doubles) then out[4]: the
-// three maxima and the count of blocks that met a non-finite wave speed
+// CFL wave-speed maximum, one launch: partials (kCflPartials doubles: four
+// per block, then a completion counter that must be zero when the buffer is
+// allocated) and out[4]: the three maxima and the count of blocks that met a
+// non-finite wave speed
 constexpr int kCflBlocks = 1184;  // 148 SMs x 8 blocks of 256 threads: enough warps to hide the loads
+constexpr int kCflPartials = 4 * kCflBlocks + 1;
 int launch_cfl(const Grid &g, const ModelParams &m, const double *U, const int *did,
                double *partials, double *out, cudaStream_t st);
 

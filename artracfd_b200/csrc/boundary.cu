@@ -266,7 +266,14 @@ __device__ __forceinline__ double vmax_of(double a, double b)
     return (a < b) ? b : a;  // NaN in b never replaces a, as in solve.c:145
 }
 
-__global__ void cfl_partial(Grid g, ModelParams mp, const double *U, const int *did, double *part)
+// The maximum of the wave speeds over the computed fluid nodes, per sweep
+// direction, in one launch: each block reduces its nodes and writes its three
+// partial maxima and a non-finite flag; the last block to finish (a counter
+// after the partials, zero between launches) combines all blocks' partials
+// with the whole block and writes out[0..3].  Every partial maximum starts
+// from 0 and a NaN never replaces a value (vmax_of), so no NaN enters and the
+// maximum does not depend on the order of combination.
+__global__ void cfl_partial(Grid g, ModelParams mp, const double *U, const int *did, double *part, double *out)
 {
     pdl_wait();
     const int Lx = g.hi[0] - g.lo[0], Ly = g.hi[1] - g.lo[1], Lz = g.hi[2] - g.lo[2];
@@ -313,8 +320,9 @@ __global__ void cfl_partial(Grid g, ModelParams mp, const double *U, const int *
         m1 = vmax_of(m1, __shfl_xor_sync(0xffffffffu, m1, o));
         m2 = vmax_of(m2, __shfl_xor_sync(0xffffffffu, m2, o));
     }
-    __shared__ double sm[3][32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ double sm[4][32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (int)(blockDim.x >> 5);
     if (lane == 0) {
         sm[0][warp] = m0;
         sm[1][warp] = m1;
@@ -323,7 +331,7 @@ __global__ void cfl_partial(Grid g, ModelParams mp, const double *U, const int *
     const int any_bad = __syncthreads_or(bad);
     if (threadIdx.x < 3) {
         double m = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        for (int w = 0; w < nw; ++w) {
             m = vmax_of(m, sm[threadIdx.x][w]);
         }
         part[3 * blockIdx.x + threadIdx.x] = m;
@@ -331,40 +339,55 @@ __global__ void cfl_partial(Grid g, ModelParams mp, const double *U, const int *
     if (threadIdx.x == 3) {
         part[3 * gridDim.x + blockIdx.x] = any_bad ? 1.0 : 0.0;
     }
-}
-
-// One warp: each lane takes every 32nd block, then a shuffle tree.  Every
-// partial maximum starts from 0 and a NaN never replaces a value (vmax_of), so
-// no NaN enters and the maximum does not depend on the order of combination.
-__global__ void cfl_final(const double *part, int nblocks, double *out)
-{
-    pdl_wait();
-    const int lane = threadIdx.x & 31;
-    double m[3] = {0.0, 0.0, 0.0};
+    if (threadIdx.x < 4) {
+        __threadfence();  // the partials before the count
+    }
+    __syncthreads();
+    unsigned *count = reinterpret_cast<unsigned *>(part + 4 * gridDim.x);
+    if (threadIdx.x == 0) {
+        last = atomicAdd(count, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) {
+        return;
+    }
+    // the last block: every block's partials (written by other SMs: read
+    // through L2)
+    double r[3] = {0.0, 0.0, 0.0};
     double nbad = 0.0;
-    for (int b = lane; b < nblocks; b += 32) {
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
 #pragma unroll
-        for (int s = 0; s < 3; ++s) {
-            m[s] = vmax_of(m[s], part[3 * b + s]);
+        for (int q = 0; q < 3; ++q) {
+            r[q] = vmax_of(r[q], __ldcg(part + 3 * b + q));
         }
-        nbad += part[3 * nblocks + b];
+        nbad += __ldcg(part + 3 * gridDim.x + b);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            r[q] = vmax_of(r[q], __shfl_xor_sync(0xffffffffu, r[q], o));
+        }
         nbad += __shfl_xor_sync(0xffffffffu, nbad, o);
     }
+    __syncthreads();  // sm is reused
     if (lane == 0) {
-        out[3] = nbad;  // blocks that met a fluid node with a non-finite wave speed
+        sm[0][warp] = r[0];
+        sm[1][warp] = r[1];
+        sm[2][warp] = r[2];
+        sm[3][warp] = nbad;
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-        for (int s = 0; s < 3; ++s) {
-            m[s] = vmax_of(m[s], __shfl_xor_sync(0xffffffffu, m[s], o));
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double v = 0.0;
+        for (int w = 0; w < nw; ++w) {
+            v = threadIdx.x < 3 ? vmax_of(v, sm[threadIdx.x][w]) : v + sm[3][w];
         }
+        // out[3]: blocks that met a fluid node with a non-finite wave speed
+        out[threadIdx.x] = v;
     }
-    if (lane < 3) {
-        out[lane] = m[lane];
+    if (threadIdx.x == 0) {
+        *count = 0u;  // for the next launch (stream order)
     }
 }
 
@@ -763,8 +786,7 @@ int launch_domain_boundary_fused(const Grid &g, const ModelParams &m, const acfd
 int launch_cfl(const Grid &g, const ModelParams &m, const double *U, const int *did, double *partials,
                double *out, cudaStream_t st)
 {
-    cudaError_t e = launch_k(cfl_partial, dim3(kCflBlocks), dim3(256), 0, st, g, m, U, did, partials);
-    if (e == cudaSuccess) e = launch_k(cfl_final, dim3(1), dim3(32), 0, st, (const double *)partials, (int)kCflBlocks, out);
+    cudaError_t e = launch_k(cfl_partial, dim3(kCflBlocks), dim3(256), 0, st, g, m, U, did, partials, out);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "cfl launch");
 }
 

@@ -186,7 +186,7 @@ def test_batch_persistent_step_matches_single_cases(form):
         assert np.all(np.abs(dts[:, c] - sdt) <= 1e-6 * sdt), (c, dts[:, c], sdt)
         assert rel_err(outs[c], sout) <= TOL_FP32_ORDER, (c, rel_err(outs[c], sout))
         assert rel_err(outs[c], pouts[c]) <= TOL_FP32_ORDER, (c, rel_err(outs[c], pouts[c]))
-    per_case = 2 + (2 if form == "hybrid" else 0)
+    per_case = 1 + (2 if form == "hybrid" else 0)  # CFL; the sensor's two kernels
     assert launches == STEPS * (len(specs) * per_case + 1 + 6), launches
 
 
