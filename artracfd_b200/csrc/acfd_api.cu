@@ -16,6 +16,7 @@
 #include <cudaTypedefs.h>
 
 #include "acfd_internal.cuh"
+#include "ghost_tasks.h"
 #include "brick_geometry.cuh"
 
 namespace acfd {
@@ -166,10 +167,10 @@ struct acfd_case {
     int bc_npairs = 0;
     int4 *bc_progs = nullptr;      // ... and formula programs (dst, first op, op count)
     int bc_nprog = 0;
-    int4 *bc_chunks = nullptr;     // the copies as runs along x: (dst, src, length <= 256) ...
-    int bc_nchunk = 0;
-    int2 *bc_left = nullptr;       // ... and the copies outside runs
-    int bc_nleft = 0;
+    int4 *bc_tasks = nullptr;      // the copies in runs (launch_ghost_program) ...
+    int bc_ntask = 0;
+    int2 *bc_single = nullptr;     // ... and the others
+    int bc_nsingle = 0;
     int2 *bc_ops = nullptr;
     GhostFaces bc_faces;
     bool bc_gather = false;        // the one-launch fill replaces the ordered launches
@@ -522,29 +523,17 @@ bool build_bc_program(acfd_case *cs)
         for (int s = 0; s < 3; ++s) cs->bc_faces.N[f][s] = p.N[f][s];
         for (int v = 0; v < 6; ++v) cs->bc_faces.given[f][v] = p.varBC[f][v];
     }
-    // copies whose destinations and sources both advance by one node (rows of
-    // a periodic or outflow ghost plane) as runs, cut into chunks of at most
-    // 256: a block copies a chunk with no index loads
-    std::vector<int4> chunks;
-    std::vector<int2> left;
-    for (size_t i = 0; i < pairs.size();) {
-        size_t j = i + 1;
-        while (j < pairs.size() && pairs[j].x == pairs[j - 1].x + 1 && pairs[j].y == pairs[j - 1].y + 1) ++j;
-        if (j - i >= 32) {
-            for (size_t q = i; q < j; q += 256) {
-                chunks.push_back(make_int4(pairs[q].x, pairs[q].y, (int)std::min<size_t>(256, j - q), 0));
-            }
-        } else {
-            left.insert(left.end(), pairs.begin() + i, pairs.begin() + j);
-        }
-        i = j;
-    }
+    // the copies as tasks (runs, a block each, no index loads) and single
+    // copies (ghost_tasks.h)
+    std::vector<int4> tasks;
+    std::vector<int2> single;
+    ghost_copy_tasks(pairs, tasks, single);
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
     const size_t b_pairs = pairs.size() * sizeof(int2), b_progs = progs.size() * sizeof(int4);
-    const size_t b_ops = ops.size() * sizeof(int2), b_chunks = chunks.size() * sizeof(int4);
-    const size_t off_progs = al(b_pairs), off_ops = off_progs + al(b_progs), off_chunks = off_ops + al(b_ops);
-    const size_t off_left = off_chunks + al(b_chunks);
-    const size_t total = off_left + left.size() * sizeof(int2);
+    const size_t b_ops = ops.size() * sizeof(int2), b_tasks = tasks.size() * sizeof(int4);
+    const size_t off_progs = al(b_pairs), off_ops = off_progs + al(b_progs), off_tasks = off_ops + al(b_ops);
+    const size_t off_single = off_tasks + al(b_tasks);
+    const size_t total = off_single + single.size() * sizeof(int2);
     char *base = nullptr;
     if (cudaMalloc(&base, total) != cudaSuccess) {
         cudaGetLastError();
@@ -553,9 +542,9 @@ bool build_bc_program(acfd_case *cs)
     bool copied = cudaMemcpy(base, pairs.data(), b_pairs, cudaMemcpyHostToDevice) == cudaSuccess &&
                   cudaMemcpy(base + off_progs, progs.data(), b_progs, cudaMemcpyHostToDevice) == cudaSuccess &&
                   cudaMemcpy(base + off_ops, ops.data(), b_ops, cudaMemcpyHostToDevice) == cudaSuccess &&
-                  cudaMemcpy(base + off_chunks, chunks.data(), b_chunks, cudaMemcpyHostToDevice) == cudaSuccess &&
-                  cudaMemcpy(base + off_left, left.data(), left.size() * sizeof(int2), cudaMemcpyHostToDevice) ==
-                      cudaSuccess;
+                  cudaMemcpy(base + off_tasks, tasks.data(), b_tasks, cudaMemcpyHostToDevice) == cudaSuccess &&
+                  cudaMemcpy(base + off_single, single.data(), single.size() * sizeof(int2),
+                             cudaMemcpyHostToDevice) == cudaSuccess;
     if (!copied) {
         cudaGetLastError();
         cudaFree(base);
@@ -566,10 +555,10 @@ bool build_bc_program(acfd_case *cs)
     cs->bc_progs = reinterpret_cast<int4 *>(base + off_progs);
     cs->bc_nprog = (int)progs.size();
     cs->bc_ops = reinterpret_cast<int2 *>(base + off_ops);
-    cs->bc_chunks = reinterpret_cast<int4 *>(base + off_chunks);
-    cs->bc_nchunk = (int)chunks.size();
-    cs->bc_left = reinterpret_cast<int2 *>(base + off_left);
-    cs->bc_nleft = (int)left.size();
+    cs->bc_tasks = reinterpret_cast<int4 *>(base + off_tasks);
+    cs->bc_ntask = (int)tasks.size();
+    cs->bc_single = reinterpret_cast<int2 *>(base + off_single);
+    cs->bc_nsingle = (int)single.size();
     return true;
 }
 
@@ -596,8 +585,8 @@ static int treat_boundary_fill(acfd_case *cs, int tn)
     double *U = level(cs, tn);
     if (cs->bc_gather) {
         ++cs->launches;
-        return launch_ghost_program(cs->grid, cs->mp, cs->bc_faces, cs->bc_chunks, cs->bc_nchunk, cs->bc_left,
-                                    cs->bc_nleft, cs->bc_progs, cs->bc_nprog, cs->bc_ops, U, cs->stream);
+        return launch_ghost_program(cs->grid, cs->mp, cs->bc_faces, cs->bc_tasks, cs->bc_ntask, cs->bc_single,
+                                    cs->bc_nsingle, cs->bc_progs, cs->bc_nprog, cs->bc_ops, U, cs->stream);
     }
     if (!cs->bc_multi) {
         if (cs->bc_groups.empty()) {

@@ -319,11 +319,11 @@ constexpr int kGhostWall = 2;    // top := wall boundary node from the top (its 
 constexpr int kGhostImage = 3;   // (O, I) := image ghost of boundary point O and image node I
 constexpr int kGhostStack = 6;
 constexpr int kGhostMaxOps = 32;
-// chunks: runs of copies (dst, src, length <= 256, 0), one block each;
-// pairs: the other (dst, src) copies; progs: (dst, first op, op count, 0);
-// ops: (code | face << 3, node)
-int launch_ghost_program(const Grid &g, const ModelParams &m, const GhostFaces &F, const int4 *chunks, int nchunk,
-                         const int2 *pairs, int npairs, const int4 *progs, int nprog, const int2 *ops, double *U,
+// tasks: runs of copies, a block each -- (first destination, source offset,
+// length <= 2048, 0); single: the other copies (dst, src); progs: (dst,
+// first op, op count, 0); ops: (code | face << 3, node)
+int launch_ghost_program(const Grid &g, const ModelParams &m, const GhostFaces &F, const int4 *tasks, int ntask,
+                         const int2 *single, int nsingle, const int4 *progs, int nprog, const int2 *ops, double *U,
                          cudaStream_t st);
 // all groups of one TreatBoundary in one cooperative launch with grid barriers;
 // bar: two device words (arrival count, generation), zero at first use

@@ -540,31 +540,55 @@ int launch_ghost_gather(const Grid &g, const int2 *pairs, int count, double *U, 
 // replaces the top two (boundary point O, image node I) with the image
 // ghost -- and store the result.  No node a program or pair reads is written
 // by the launch, so the threads need no ordering among themselves.
-__global__ void __launch_bounds__(256) ghost_program(long long nn, const int4 *__restrict__ chunks, int nchunk,
-                                                     const int2 *__restrict__ pairs, int npairs,
+__global__ void __launch_bounds__(256) ghost_program(long long nn, const int4 *__restrict__ tasks, int ntask,
+                                                     const int2 *__restrict__ single, int nsingle,
                                                      const int4 *__restrict__ progs, int nprog,
                                                      const int2 *__restrict__ ops, GhostFaces F, ModelParams mp,
                                                      double *U)
 {
     pdl_wait();
-    if ((int)blockIdx.x < nchunk) {
-        // a run of copies: consecutive destinations from consecutive sources
-        const int4 c = chunks[blockIdx.x];
-        if ((int)threadIdx.x < c.z) {
-            copy_node(U, nn, (long long)c.x + threadIdx.x, (long long)c.y + threadIdx.x);
+    if ((int)blockIdx.x < ntask) {
+        // a run of copies, up to four per thread in flight: their twenty
+        // loads before their stores
+        const int4 c = tasks[blockIdx.x];
+        for (int q0 = threadIdx.x; q0 < c.z; q0 += 4 * blockDim.x) {
+            long long d[4];
+            double u[4][5];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int q = q0 + r * (int)blockDim.x;
+                d[r] = q < c.z ? (long long)c.x + q : -1;
+                // a copy outside the level is dropped (the tasks cover exactly
+                // the fill's copies: tests/test_host.py)
+                if (d[r] >= nn || d[r] + c.y < 0 || d[r] + c.y >= nn) d[r] = -1;
+            }
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                if (d[r] >= 0) {
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) u[r][v] = U[v * nn + d[r] + c.y];
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                if (d[r] >= 0) {
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) U[v * nn + d[r]] = u[r][v];
+                }
+            }
         }
         return;
     }
-    const int t = ((int)blockIdx.x - nchunk) * blockDim.x + threadIdx.x;
-    if (t < npairs) {
-        const int2 q = pairs[t];
+    const int t = ((int)blockIdx.x - ntask) * blockDim.x + threadIdx.x;
+    if (t < nsingle) {
+        const int2 q = single[t];
         copy_node(U, nn, q.x, q.y);
         return;
     }
-    if (t >= npairs + nprog) {
+    if (t >= nsingle + nprog) {
         return;
     }
-    const int4 pr = progs[t - npairs];  // dst, first op, op count
+    const int4 pr = progs[t - nsingle];  // dst, first op, op count
     double st[kGhostStack][5];
     int sp = 0;
     for (int o = 0; o < pr.z; ++o) {
@@ -596,17 +620,17 @@ __global__ void __launch_bounds__(256) ghost_program(long long nn, const int4 *_
     store5(U, nn, pr.x, st[0]);
 }
 
-int launch_ghost_program(const Grid &g, const ModelParams &m, const GhostFaces &F, const int4 *chunks, int nchunk,
-                         const int2 *pairs, int npairs, const int4 *progs, int nprog, const int2 *ops, double *U,
+int launch_ghost_program(const Grid &g, const ModelParams &m, const GhostFaces &F, const int4 *tasks, int ntask,
+                         const int2 *single, int nsingle, const int4 *progs, int nprog, const int2 *ops, double *U,
                          cudaStream_t st)
 {
-    const long long rest = (long long)npairs + nprog;
-    const long long blocks = nchunk + (rest + 255) / 256;
+    const long long rest = (long long)nsingle + nprog;
+    const long long blocks = ntask + (rest + 255) / 256;
     if (blocks <= 0) {
         return ACFD_OK;
     }
-    cudaError_t e = launch_k(ghost_program, dim3((unsigned)blocks), dim3(256), 0, st, g.nn, chunks, nchunk, pairs,
-                             npairs, progs, nprog, ops, F, m, U);
+    cudaError_t e = launch_k(ghost_program, dim3((unsigned)blocks), dim3(256), 0, st, g.nn, tasks, ntask, single,
+                             nsingle, progs, nprog, ops, F, m, U);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "ghost_program launch");
 }
 

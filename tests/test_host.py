@@ -329,3 +329,103 @@ def test_dropin_bad_case_file_stops_before_the_device(tmp_path):
     assert r.returncode != 0
     assert "mesh number should be positive" in r.stderr
     assert "Solving" not in r.stdout
+
+
+_TASKS_HARNESS = r"""
+#include <cstdio>
+#include <vector>
+struct int2 { int x, y; };
+struct int4 { int x, y, z, w; };
+#include "ghost_tasks.h"
+int main(int argc, char **argv)
+{
+    FILE *f = std::fopen(argv[1], "rb");
+    std::vector<int2> pairs;
+    int2 p;
+    while (std::fread(&p, sizeof p, 1, f) == 1) pairs.push_back(p);
+    std::fclose(f);
+    std::vector<int4> tasks;
+    std::vector<int2> single;
+    ghost_copy_tasks_of<int2, int4>(pairs, tasks, single);
+    FILE *o = std::fopen(argv[2], "wb");
+    long long in_tasks = 0;
+    for (const int4 &t : tasks) {
+        if (t.z < 1 || t.z > kGhostLong) return 3;
+        for (int q = 0; q < t.z; ++q) {
+            const int2 e = {t.x + q, t.x + q + t.y};
+            std::fwrite(&e, sizeof e, 1, o);
+        }
+        in_tasks += t.z;
+    }
+    for (const int2 &e : single) std::fwrite(&e, sizeof e, 1, o);
+    std::fclose(o);
+    std::printf("%zu %lld %zu\n", tasks.size(), in_tasks, single.size());
+    return 0;
+}
+"""
+
+
+def _periodic_fill_pairs(n, ng):
+    """(destination, source) node pairs of the one-launch fill of a grid whose
+    faces are all periodic: every ghost node takes the value of the computed
+    node one period away along each axis where it lies outside."""
+    nx, ny, nz = n
+    lo = [ng, ng, ng]
+    L = [nx - 2 * ng, ny - 2 * ng, nz - 2 * ng]
+    out = []
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                c = [i, j, k]
+                src = list(c)
+                for a in range(3):
+                    if c[a] < lo[a]:
+                        src[a] += L[a]
+                    elif c[a] >= lo[a] + L[a]:
+                        src[a] -= L[a]
+                if src != c:
+                    out.append(((k * ny + j) * nx + i, (src[2] * ny + src[1]) * nx + src[0]))
+    return np.array(out, dtype=np.int32)
+
+
+def test_ghost_copy_tasks_cover_exactly_the_copies(tmp_path):
+    """The copy tasks of the one-launch ghost fill (csrc/ghost_tasks.h,
+    compiled here for the host): the tasks expanded, with the single copies,
+    give back exactly the fill's (destination, source) copies -- periodic
+    grids whose x faces are three nodes wide, a plane far longer than one
+    task, the same copies in a random order, and an outflow-like list of
+    short runs."""
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no host C++ compiler")
+    src = tmp_path / "tasks.cpp"
+    src.write_text(_TASKS_HARNESS)
+    exe = tmp_path / "tasks"
+    csrc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "artracfd_b200", "csrc")
+    subprocess.run([gxx, "-O2", "-std=c++17", "-I" + csrc, str(src), "-o", str(exe)], check=True)
+    rng = np.random.default_rng(7)
+    cases_ = {
+        "periodic 19^3": _periodic_fill_pairs((19, 19, 19), 3),
+        "periodic thin z": _periodic_fill_pairs((70, 40, 11), 3),
+        "plane longer than a task": np.stack([np.arange(5000, 12000), np.arange(20000, 27000)], 1).astype(np.int32),
+    }
+    shuffled = cases_["periodic 19^3"].copy()
+    rng.shuffle(shuffled)
+    cases_["shuffled"] = shuffled
+    rows = [(r * 40 + c, r * 40 + c + 3) for r in range(60) for c in range(3)]
+    cases_["outflow-like"] = np.array(rows, dtype=np.int32)
+    for name, pairs in cases_.items():
+        pin, pout = tmp_path / "pairs.bin", tmp_path / "out.bin"
+        pairs.astype(np.int32).tofile(pin)
+        r = subprocess.run([str(exe), str(pin), str(pout)], capture_output=True, text=True, check=True)
+        got = np.fromfile(pout, dtype=np.int32).reshape(-1, 2)
+        want = pairs.reshape(-1, 2)
+        assert len(got) == len(want), name
+        assert np.array_equal(got[np.lexsort(got.T[::-1])], want[np.lexsort(want.T[::-1])]), name
+        ntask, in_tasks, nsingle = (int(x) for x in r.stdout.split())
+        if name == "plane longer than a task":
+            assert (ntask, in_tasks, nsingle) == (4, 7000, 0)  # three pieces of 2048 and the rest
+        if name == "outflow-like":
+            assert (ntask, nsingle) == (0, len(want))  # runs of three: single copies
