@@ -8,8 +8,12 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <atomic>
+#include <condition_variable>
 #include <mutex>
 #include <thread>
+
+#include <unistd.h>
 #include <unordered_map>
 #include <vector>
 
@@ -863,26 +867,94 @@ PinnedBounce &bounce()
     return b;
 }
 
+// Host threads for the bounce copies, created once per process and reused
+// (spawning threads for every chunk cost about as much as the copy): a copy
+// is cut into parts that the workers and the calling thread take in turn.
+// Used under the bounce lock, one copy at a time.  A process forked after
+// the pool started (whose child has no workers) builds its own pool.
+class CopyPool {
+public:
+    static CopyPool &get()
+    {
+        static std::mutex m;
+        static CopyPool *pool = nullptr;
+        std::lock_guard<std::mutex> g(m);
+        if (!pool || pool->pid_ != getpid()) {
+            pool = new CopyPool();  // a pool inherited across fork is left alone
+        }
+        return *pool;
+    }
+    void copy(void *dst, const void *src, size_t bytes)
+    {
+        const size_t kPart = (size_t)1 << 20;
+        const size_t nparts = (bytes + kPart - 1) / kPart;
+        if (workers_.empty() || nparts < 2) {
+            memcpy(dst, src, bytes);
+            return;
+        }
+        {
+            std::lock_guard<std::mutex> g(m_);
+            dst_ = (char *)dst;
+            src_ = (const char *)src;
+            bytes_ = bytes;
+            part_ = kPart;
+            nparts_ = nparts;
+            next_.store(0);
+            busy_ = (unsigned)workers_.size();
+            ++gen_;
+        }
+        cv_.notify_all();
+        work();
+        std::unique_lock<std::mutex> lk(m_);
+        done_.wait(lk, [&] { return busy_ == 0; });
+    }
+
+private:
+    CopyPool() : pid_(getpid())
+    {
+        unsigned T = std::thread::hardware_concurrency();
+        T = std::min<unsigned>(T == 0 ? 1u : T, 16u);
+        for (unsigned t = 1; t < T; ++t) {
+            workers_.emplace_back([this] { loop(); });
+            workers_.back().detach();  // the pool lives for the process
+        }
+    }
+    void work()
+    {
+        for (size_t p = next_.fetch_add(1); p < nparts_; p = next_.fetch_add(1)) {
+            const size_t off = p * part_;
+            memcpy(dst_ + off, src_ + off, std::min(part_, bytes_ - off));
+        }
+    }
+    void loop()
+    {
+        unsigned long long seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [&] { return gen_ != seen; });
+                seen = gen_;
+            }
+            work();
+            std::lock_guard<std::mutex> g(m_);
+            if (--busy_ == 0) done_.notify_one();
+        }
+    }
+    pid_t pid_;
+    std::vector<std::thread> workers_;
+    std::mutex m_;
+    std::condition_variable cv_, done_;
+    unsigned long long gen_ = 0;
+    unsigned busy_ = 0;
+    char *dst_ = nullptr;
+    const char *src_ = nullptr;
+    size_t bytes_ = 0, part_ = 0, nparts_ = 0;
+    std::atomic<size_t> next_{0};
+};
+
 void parallel_memcpy(void *dst, const void *src, size_t bytes)
 {
-    const size_t kPart = (size_t)4 << 20;
-    unsigned T = std::thread::hardware_concurrency();
-    T = std::min<unsigned>(T == 0 ? 1u : T, 8u);
-    T = (unsigned)std::min<size_t>(T, bytes / kPart);
-    if (T < 2) {
-        memcpy(dst, src, bytes);
-        return;
-    }
-    const size_t part = ((bytes + T - 1) / T + 63) & ~(size_t)63;
-    std::vector<std::thread> pool;
-    for (unsigned t = 1; t < T; ++t) {
-        const size_t off = t * part;
-        if (off >= bytes) break;
-        const size_t len = std::min(part, bytes - off);
-        pool.emplace_back([=] { memcpy((char *)dst + off, (const char *)src + off, len); });
-    }
-    memcpy(dst, src, std::min(part, bytes));
-    for (auto &th : pool) th.join();
+    CopyPool::get().copy(dst, src, bytes);
 }
 
 int ensure_bounce(PinnedBounce &b)
