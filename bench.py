@@ -59,10 +59,12 @@ def profiled_traffic(mode: str, tiles, axes=(0, 1, 2)):
         return None, f"no capture of the {mode} form"
     vals = []
     for a in axes:
-        ax = rec["axes"].get(str(a))
-        if ax is None or int(tiles[a]) not in [int(v) for v in ax["variants"]]:
+        caps = rec["axes"].get(str(a), [])
+        caps = caps if isinstance(caps, list) else [caps]
+        hit = [c for c in caps if int(tiles[a]) in [int(v) for v in c["variants"]]]
+        if not hit:
             return None, f"no capture of variant {tiles[a]} on axis {a}"
-        vals.append(float(ax["dram_bytes"]))
+        vals.append(float(hit[0]["dram_bytes"]))
     return sum(vals) / len(vals), rec["source"]
 
 
