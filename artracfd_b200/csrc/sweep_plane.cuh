@@ -235,17 +235,27 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
             }
         };
 
+        // A wait that gave up ends the block's march.  The FP64 form marks it
+        // and leaves at the end of the item, so that the march loop keeps a
+        // single exit (measured: FP64 stages 4% faster); the FP32 forms leave
+        // at once (measured: hybrid step 0.8% faster than with the mark).
+        constexpr bool kMarkFailure = sizeof(Real) == sizeof(double);
+        bool failed = false;
         Real W[NP][5];
     #pragma unroll
         for (int m = 0; m < NP - 1; ++m) {
-            if (!wait_plane(m)) return;
-            node_of_plane(plane(m), W[m]);
+            if constexpr (kMarkFailure) {
+                if (!failed && !wait_plane(m)) failed = true;
+            } else {
+                if (!wait_plane(m)) return;
+            }
+            node_of_plane(plane(failed ? 0 : m), W[m]);
         }
         Real Pc[4] = {Real(0), Real(0), Real(0), Real(0)};
         Real Dc[2][2] = {{Real(0), Real(0)}, {Real(0), Real(0)}};
         if (VISC) {
             march_prims(W[H - 1], cvinv, Pc);
-            tdiff(plane(H - 1), Dc);
+            tdiff(plane(failed ? 0 : H - 1), Dc);
         }
         for (int q = 0; q < H; ++q) {
             release(q);  // nodes p0-H .. p0-1 have no update
@@ -259,7 +269,7 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
             fl_ahead = fl[base + (long long)(p0 + 1) * st];
         }
         Real Fl[5];
-        for (int p = p0 - 1; p < p1; ++p) {
+        for (int p = p0 - 1; p < p1 && !failed; ++p) {
             const int qf = p - p0 + 2 * H;  // front node p+H
             const int q0 = p - p0 + H;      // node p
             const long long id = base + (long long)p * st;
@@ -278,7 +288,14 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
                 if (active) fl_ahead = fl[id + 3 * st];  // node p+3 <= p1+2, inside the march's planes
                 full_w = (fw != 0u);
             }
-            if (!wait_plane(qf)) return;
+            if (!wait_plane(qf)) {
+                if constexpr (kMarkFailure) {
+                    failed = true;
+                    break;
+                } else {
+                    return;
+                }
+            }
             node_of_plane(plane(qf), W[NP - 1]);
             Real Pn[4], Dn[2][2];
             if (VISC) {
@@ -332,10 +349,11 @@ __device__ __forceinline__ void plane_yz_block(const Grid &g, const ModelParams 
         if constexpr (SHARE) {
             // planes p1 .. p1+H-1 were read for the last time: free their slots
             // for the next item's planes
-            for (int q = NQ - H; q < NQ; ++q) {
+            for (int q = NQ - H; q < NQ && !failed; ++q) {
                 release(q);
             }
         }
+        if (failed) return;
         qbase += NQ;
     }
 }
