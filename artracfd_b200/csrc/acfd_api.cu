@@ -178,6 +178,23 @@ struct acfd_case {
     int2 *bc_ops = nullptr;
     GhostFaces bc_faces;
     bool bc_gather = false;        // the one-launch fill replaces the ordered launches
+    std::vector<int2> bc_copies;   // host copy of the copies of a copy-only fill
+    // The X half steps as Y sweeps of the transposed state (build_xt): xg is
+    // the grid with axes 0 and 1 exchanged, xU its three levels, xdid the
+    // node types on it, xfl the sensor's x flags as the flags of its axis 1
+    // ([2][xg.nn], slot 1), xmap the plane map of its Y sweep (box xbox), and
+    // the copy-only fill remapped to it (x_tasks, x_single).
+    bool xt_ok = false;
+    Grid xg = {};
+    double *xU = nullptr;
+    int *xdid = nullptr;
+    uint8_t *xfl = nullptr;
+    CUtensorMap xmap;
+    int xbox[2] = {0, 0};
+    int4 *x_tasks = nullptr;
+    int x_ntask = 0;
+    int2 *x_single = nullptr;
+    int x_nsingle = 0;
     long long wait_limit = kWaitLimitDefault;  // polls of a plane-march wait (acfd_set_wait_limit)
     // ACFD_DEBUG=1: every stage and ghost fill is followed by a scan of its
     // level for non-finite values, checked at once (no step graphs)
@@ -561,9 +578,91 @@ bool build_bc_program(acfd_case *cs)
     cs->bc_ops = reinterpret_cast<int2 *>(base + off_ops);
     cs->bc_tasks = reinterpret_cast<int4 *>(base + off_tasks);
     cs->bc_ntask = (int)tasks.size();
+    if (progs.empty()) {
+        cs->bc_copies = pairs;
+    }
     cs->bc_single = reinterpret_cast<int2 *>(base + off_single);
     cs->bc_nsingle = (int)single.size();
     return true;
+}
+
+// The X half steps of a step run as Y sweeps of the transposed state: the
+// plane march along y reaches a higher rate than the X sweep's (a stencil
+// window in registers instead of a stencil gathered from the plane, no
+// barrier per row), so U[TO] is transposed (x and y exchanged, with the x and
+// y momenta) before the first X half step of a run of them and back after the
+// last; the stages between run on the transposed levels with the copy-only
+// fill remapped to the transposed node indices.  Only for a fill of copies
+// (whose transpose is the fill of the transposed grid); ACFD_X_TRANSPOSE=0
+// keeps the X sweep.
+void build_xt(acfd_case *cs)
+{
+    const char *env = getenv("ACFD_X_TRANSPOSE");
+    if ((env && env[0] == '0') || !cs->bc_gather || cs->bc_nprog != 0 || cs->bc_copies.empty() || !cs->pmaps_ok ||
+        cs->model.multidim != 0) {
+        return;
+    }
+    const Grid &g = cs->grid;
+    Grid xg = g;
+    xg.n[0] = g.n[1];
+    xg.n[1] = g.n[0];
+    xg.lo[0] = g.lo[1];
+    xg.lo[1] = g.lo[0];
+    xg.hi[0] = g.hi[1];
+    xg.hi[1] = g.hi[0];
+    xg.dd[0] = g.dd[1];
+    xg.dd[1] = g.dd[0];
+    xg.pitch = (xg.n[0] + 7) & ~7;
+    xg.nn = (long long)xg.pitch * xg.n[1] * xg.n[2];
+    if (xg.nn * 5 > (long long)INT32_MAX || (long long)g.n[2] * 5 > 65535) return;
+    const PlaneTile pt = plane_tile(xg, 1, viscous(cs), 1, cs->sms);
+    if (pt.BXp > 256 || pt.BC > 256) return;
+    // the copies on the transposed node indices, in destination order
+    auto tr = [&](int q) {
+        const long long i = q % g.pitch, j = (q / g.pitch) % g.n[1], k = q / ((long long)g.pitch * g.n[1]);
+        return (int)((k * xg.n[1] + i) * xg.pitch + j);
+    };
+    std::vector<int2> xc(cs->bc_copies.size());
+    for (size_t q = 0; q < xc.size(); ++q) xc[q] = make_int2(tr(cs->bc_copies[q].x), tr(cs->bc_copies[q].y));
+    std::sort(xc.begin(), xc.end(), [](const int2 &a, const int2 &b) { return a.x < b.x; });
+    std::vector<int4> tasks;
+    std::vector<int2> single;
+    ghost_copy_tasks(xc, tasks, single);
+    const size_t b_tasks = (tasks.size() * sizeof(int4) + 255) / 256 * 256;
+    char *prog = nullptr;
+    if (cudaMalloc(&cs->xU, sizeof(double) * kLevels * kVars * (size_t)xg.nn) != cudaSuccess ||
+        cudaMalloc(&cs->xdid, sizeof(int) * (size_t)xg.nn) != cudaSuccess ||
+        cudaMalloc(&cs->xfl, 2 * (size_t)xg.nn) != cudaSuccess ||
+        cudaMemset(cs->xfl, 0, 2 * (size_t)xg.nn) != cudaSuccess ||
+        cudaMalloc(&prog, b_tasks + single.size() * sizeof(int2) + 16) != cudaSuccess ||
+        cudaMemcpy(prog, tasks.data(), tasks.size() * sizeof(int4), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(prog + b_tasks, single.data(), single.size() * sizeof(int2), cudaMemcpyHostToDevice) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(prog);
+        return;  // the X sweep stays (acfd_finalize frees what was allocated)
+    }
+    cs->x_tasks = reinterpret_cast<int4 *>(prog);
+    cs->x_ntask = (int)tasks.size();
+    cs->x_single = reinterpret_cast<int2 *>(prog + b_tasks);
+    cs->x_nsingle = (int)single.size();
+    PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (!encode) return;
+    const cuuint64_t dims[5] = {(cuuint64_t)xg.pitch, (cuuint64_t)xg.n[1], (cuuint64_t)xg.n[2], 5, 3};
+    const cuuint64_t strides[4] = {(cuuint64_t)xg.pitch * 8, (cuuint64_t)xg.pitch * xg.n[1] * 8,
+                                   (cuuint64_t)xg.nn * 8, (cuuint64_t)xg.nn * 5 * 8};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    const cuuint32_t box[5] = {(cuuint32_t)pt.BXp, 1, (cuuint32_t)pt.BC, 5, 1};
+    if (encode(&cs->xmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, cs->xU, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+        return;
+    }
+    cs->xbox[0] = pt.BXp;
+    cs->xbox[1] = pt.BC;
+    cs->xg = xg;
+    if (launch_transpose_int(cs->flags, g, cs->xdid, xg, cs->stream) != ACFD_OK) return;
+    cs->xt_ok = true;
 }
 
 int debug_scan(acfd_case *cs, int l, const char *what, int s);
@@ -764,6 +863,106 @@ int discretize(acfd_case *cs, double dt_scale, int s)
     return ACFD_OK;
 }
 
+// the X half steps may run as Y sweeps of the transposed state (build_xt):
+// the learned-sensor form (the FP64 and FP32-bulk X sweeps gain nothing by
+// it), no bodies (whose ghost values follow the fill), no debug scans
+bool xt_eligible(const acfd_case *cs)
+{
+    return cs->xt_ok && !cs->debug && !cs->plain_kernels && cs->mode == ACFD_FP32_HYBRID &&
+           !(cs->ib && ib_count(cs->ib) > 0);
+}
+
+// ... and do, when the X sweep's variant is a plane march (acfd_autotune
+// picks one for an eligible case); a brick or line variant keeps the X sweep
+bool use_xt(const acfd_case *cs)
+{
+    const int v = cs->tile_var[cs->mode][0];
+    return xt_eligible(cs) && v >= kPlaneFirst && v < kStageVariants;
+}
+
+// one LLLU stage along x on the transposed levels: the Y plane march of xg
+// with the X sweep's variant
+int stage_xt(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int tn, int tm)
+{
+    const long long lv = (long long)kVars * cs->xg.nn;
+    StageArgs a;
+    a.Uo = cs->xU + to * lv;
+    a.Un = cs->xU + tn * lv;
+    a.Um = cs->xU + tm * lv;
+    a.did = cs->xdid;
+    a.dt = cs->d_dt;
+    a.dt_scale = dt_scale;
+    a.coeA = coeA;
+    a.coeB = coeB;
+    a.accumulate = 0;
+    a.to = to;
+    a.tn = tn;
+    a.tm = tm;
+    a.maps = nullptr;
+    a.omaps = nullptr;
+    a.var[0] = a.var[1] = a.var[2] = 0;
+    a.status = cs->dstatus;
+    a.flags = cs->xfl;
+    a.wait_limit = cs->wait_limit;
+    const int var = cs->tile_var[cs->mode][0];
+    if (var < kPlaneFirst || var >= kStageVariants) {
+        set_error("transposed X sweep: variant %d is not a plane march", var);
+        return ACFD_ERR_STATE;
+    }
+    const int waves = kPlaneWaves[var - kPlaneFirst];
+    const bool share = kPlaneShare[var - kPlaneFirst];
+    const bool visc = viscous(cs);
+    const PlaneTile pt = plane_tile(cs->xg, 1, visc, waves, cs->sms, share);
+    if (pt.BXp != cs->xbox[0] || pt.BC != cs->xbox[1]) {
+        set_error("transposed plane tile (%d x %d) does not match its box (%d x %d)", pt.BXp, pt.BC, cs->xbox[0],
+                  cs->xbox[1]);
+        return ACFD_ERR_STATE;
+    }
+    int st;
+    switch (cs->mode) {
+        case ACFD_FP64: st = launch_stage_plane_fast(cs->xg, cs->mp, a, 1, visc, pt, cs->xmap, cs->stream); break;
+        case ACFD_FP32_HYBRID:
+            st = launch_stage_plane_fp32(cs->xg, cs->mp, a, 1, visc, true, pt, cs->xmap, cs->stream);
+            break;
+        default: st = launch_stage_plane_fp32(cs->xg, cs->mp, a, 1, visc, false, pt, cs->xmap, cs->stream); break;
+    }
+    ++cs->launches;
+    return st;
+}
+
+int fill_xt(acfd_case *cs, int tn)
+{
+    ++cs->launches;
+    return launch_ghost_program(cs->xg, cs->mp, cs->bc_faces, cs->x_tasks, cs->x_ntask, cs->x_single,
+                                cs->x_nsingle, nullptr, 0, nullptr, cs->xU + (long long)tn * kVars * cs->xg.nn,
+                                cs->stream);
+}
+
+// DiscretizeTime along x on the transposed levels (the stages of discretize)
+int discretize_xt(acfd_case *cs, double dt_scale)
+{
+    if (cs->model.tScheme == 0) {
+        TRY(stage_xt(cs, dt_scale, 0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN));
+        TRY(fill_xt(cs, ACFD_TN));
+        TRY(stage_xt(cs, dt_scale, 1.0 / 2.0, 1.0 / 2.0, ACFD_TO, ACFD_TN, ACFD_TO));
+        return fill_xt(cs, ACFD_TO);
+    }
+    TRY(stage_xt(cs, dt_scale, 0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN));
+    TRY(fill_xt(cs, ACFD_TN));
+    TRY(stage_xt(cs, dt_scale, 3.0 / 4.0, 1.0 / 4.0, ACFD_TO, ACFD_TN, ACFD_TM));
+    TRY(fill_xt(cs, ACFD_TM));
+    TRY(stage_xt(cs, dt_scale, 1.0 / 3.0, 2.0 / 3.0, ACFD_TO, ACFD_TM, ACFD_TO));
+    return fill_xt(cs, ACFD_TO);
+}
+
+// U[TO] (every node, ghosts included) to and from the transposed levels
+int xt_transpose(acfd_case *cs, bool into)
+{
+    ++cs->launches;
+    return into ? launch_transpose_state(level(cs, ACFD_TO), cs->grid, cs->xU, cs->xg, cs->stream)
+                : launch_transpose_state(cs->xU, cs->xg, level(cs, ACFD_TO), cs->grid, cs->stream);
+}
+
 // EvolveFluidDynamics (fluid_dynamics.c:55-116); the step dt is in d_dt
 int evolve(acfd_case *cs)
 {
@@ -779,6 +978,12 @@ int evolve(acfd_case *cs)
                                 cs->sensor_rp, cs->sensor_flags, nullptr, cs->stream));
         cs->launches += 2;
     }
+    const bool xt = use_xt(cs);
+    if (xt) {
+        // the x flags as the flags of the transposed grid's axis 1
+        TRY(launch_transpose_u8(cs->sensor_flags, cs->grid, cs->xfl + cs->xg.nn, cs->xg, cs->stream));
+        ++cs->launches;
+    }
     if (cs->model.sState != 0) {
         TRY(discretize(cs, 0.5, ACFD_PHI));
     }
@@ -786,7 +991,15 @@ int evolve(acfd_case *cs)
         const int c = cs->part.collapse;
         if (c >= 0 && c < 9) {
             for (int n = 0; n < 6 && kOrder[c][n] >= 0; ++n) {
-                TRY(discretize(cs, 0.5, kOrder[c][n]));
+                const int ax = kOrder[c][n];
+                if (ax == ACFD_X && xt) {
+                    // a run of X half steps on the transposed state
+                    if (n == 0 || kOrder[c][n - 1] != ACFD_X) TRY(xt_transpose(cs, true));
+                    TRY(discretize_xt(cs, 0.5));
+                    if (n + 1 >= 6 || kOrder[c][n + 1] != ACFD_X) TRY(xt_transpose(cs, false));
+                } else {
+                    TRY(discretize(cs, 0.5, ax));
+                }
             }
         }
     } else if (cs->model.multidim == 1) {
@@ -1153,6 +1366,7 @@ int acfd_init(const acfd_partition_t *part, const acfd_model_t *model, acfd_case
             return st;
         }
         cs->bc_gather = build_bc_program(cs);
+        build_xt(cs);
     }
     if ((e = cudaStreamSynchronize(cs->stream)) != cudaSuccess) {
         st = cuda_status(e, "acfd_init");
@@ -1181,6 +1395,10 @@ int acfd_finalize(acfd_case_t *cs)
     cudaFree(cs->dstatus);
     cudaFree(cs->bcbar);
     cudaFree(cs->bc_pairs);
+    cudaFree(cs->xU);
+    cudaFree(cs->xdid);
+    cudaFree(cs->xfl);
+    cudaFree(cs->x_tasks);
     cudaFree(cs->dbg_word);
     cudaFree(cs->sensor_params);
     cudaFree(cs->sensor_flags);
@@ -1248,6 +1466,9 @@ int acfd_sync_to_device(acfd_case_t *cs, const acfd_node_t *node, unsigned mask)
     TRY(launch_scatter_nodes(cs->grid, cs->staging, cs->U, cs->flags, mask, cs->stream));
     if (mask & ACFD_SYNC_FLAGS) {
         TRY(ib_flags_changed(cs->ib, cs->grid, cs->mp, cs->part, cs->flags, cs->stream));
+        if (cs->xt_ok) {
+            TRY(launch_transpose_int(cs->flags, cs->grid, cs->xdid, cs->xg, cs->stream));  // the node types
+        }
     }
     ACFD_CUDA(cudaStreamSynchronize(cs->stream));
     return ACFD_OK;
@@ -1371,19 +1592,33 @@ int acfd_autotune(acfd_case_t *cs, int tiles[3])
         if (g.lo[s] - half < 0 || g.hi[s] - 1 + half > g.n[s] - 1) {
             continue;  // no sweep along a collapsed axis
         }
+        // an X sweep that may run transposed is timed as it would run: the
+        // plane-march variants of the Y sweep over the transposed state
+        const bool xt = s == 0 && xt_eligible(cs);
+        if (xt) {
+            st = xt_transpose(cs, true);
+            if (st == ACFD_OK) {
+                st = launch_transpose_u8(cs->sensor_flags, cs->grid, cs->xfl + cs->xg.nn, cs->xg, cs->stream);
+            }
+        }
+        auto run = [&](double coeA, double coeB, int tn, int tm) {
+            return xt ? stage_xt(cs, 1.0, coeA, coeB, ACFD_TO, tn, tm)
+                      : stage(cs, 1.0, coeA, coeB, ACFD_TO, tn, tm, s);
+        };
         float best = 1e30f;
         int best_var = var_of[s];
-        for (int var = cs->maps_ok ? 0 : kTileVariants; var < kStageVariants && st == ACFD_OK; ++var) {
+        for (int var = xt ? kPlaneFirst : (cs->maps_ok ? 0 : kTileVariants); var < kStageVariants && st == ACFD_OK;
+             ++var) {
             var_of[s] = var;
             // RK stage 1 (U[TO] -> U[TN]) then the timed RK stage 2 (U[TO],
             // U[TN] -> U[TM]), which reads two levels like stages 2 and 3 of
             // every step; both levels written are overwritten by every step
-            st = stage(cs, 1.0, 0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN, s);
-            if (st == ACFD_OK) st = stage(cs, 1.0, 0.75, 0.25, ACFD_TO, ACFD_TN, ACFD_TM, s);  // warm-up
+            st = run(0.0, 1.0, ACFD_TO, ACFD_TN);
+            if (st == ACFD_OK) st = run(0.75, 0.25, ACFD_TN, ACFD_TM);  // warm-up
             float total = 0.0f;
             for (int rep = 0; rep < 3 && st == ACFD_OK; ++rep) {
                 cudaEventRecord(e0, cs->stream);
-                st = stage(cs, 1.0, 0.75, 0.25, ACFD_TO, ACFD_TN, ACFD_TM, s);
+                st = run(0.75, 0.25, ACFD_TN, ACFD_TM);
                 cudaEventRecord(e1, cs->stream);
                 cudaEventSynchronize(e1);
                 float ms = 0.0f;
@@ -1595,11 +1830,15 @@ int acfd_geo_upload(acfd_case_t *cs, const acfd_polyhedron_t *poly, int totN)
         set_error("acfd_geo_upload: bad body list");
         return ACFD_ERR_ARG;
     }
+    // bodies change the node types through their treatment: the X half steps
+    // stay on the X sweep from now on
+    const bool leave_xt = totN > 0 && cs->xt_ok;
+    if (totN > 0) cs->xt_ok = false;
     bool relayout = true;
     TRY(ib_upload(cs->ib, poly, totN, cs->part, cs->stream, &relayout));
     // bodies moved in place keep every device pointer and launch shape of a
     // captured step; a new body list does not
-    if (relayout) release_graph(cs);
+    if (relayout || leave_xt) release_graph(cs);
     return ACFD_OK;
 }
 

@@ -303,6 +303,12 @@ int launch_domain_boundary(const Grid &g, const ModelParams &m, const acfd_parti
 // ghost fill as one gather: U[dst] = U[src] for every (dst, src) pair, all
 // five variables of the level U
 int launch_ghost_gather(const Grid &g, const int2 *pairs, int count, double *U, cudaStream_t st);
+// one level of the state (five variables, the x and y momenta exchanged),
+// an int array or a byte array transposed from grid gs to grid gd, whose axes
+// 0 and 1 are those of gs exchanged (every node, ghosts included)
+int launch_transpose_state(const double *src, const Grid &gs, double *dst, const Grid &gd, cudaStream_t st);
+int launch_transpose_int(const int *src, const Grid &gs, int *dst, const Grid &gd, cudaStream_t st);
+int launch_transpose_u8(const uint8_t *src, const Grid &gs, uint8_t *dst, const Grid &gd, cudaStream_t st);
 // debug mode: add the count of non-finite values among U[0, count) to *word
 int launch_finite_scan(const double *U, long long count, int *word, cudaStream_t st);
 // ghost fill as one launch of formulas: per-face constants of the programs
