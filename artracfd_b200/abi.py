@@ -26,6 +26,8 @@ ACFD_ERR_NOT_FOUND = 6
 ACFD_ERR_IO = 7
 # levels / operators
 TO, TN, TM = 0, 1, 2
+# pieces of a profiled step (acfd_profile_step)
+PIECE_STAGE, PIECE_STAGE_XT, PIECE_FILL, PIECE_TRANSPOSE, PIECE_SENSOR = 0, 1, 2, 3, 4
 X, Y, Z, DIMS, PHI = 0, 1, 2, 3, 4
 # arithmetic forms
 FP64_EXACT, FP64, FP32_BULK, FP32_HYBRID = 0, 1, 2, 3
@@ -191,6 +193,8 @@ def load_library(path: str | None = None):
         "acfd_cfl_noalloc": [ctypes.POINTER(Partition), ctypes.POINTER(Model), vp, vp, i, vp, vp],
         "acfd_evolve_fluid": [vp, d],
         "acfd_evolve_fluid_graph": [vp, d],
+        "acfd_profile_step": [vp, d, i, ctypes.POINTER(i), ctypes.POINTER(i), ctypes.POINTER(i),
+                              ctypes.POINTER(ctypes.c_float), ctypes.POINTER(i)],
         "acfd_discretize_time": [vp, d, i],
         "acfd_lllu": [vp, d, d, d, i, i, i, i],
         "acfd_treat_boundary": [vp, i],

@@ -122,6 +122,12 @@ __global__ void set_scalar(double *p, double v)
 
 using namespace acfd;
 
+// one piece of a profiled step (acfd_profile_step)
+struct StepPiece {
+    int kind, axis, stage;
+    cudaEvent_t e0, e1;
+};
+
 struct acfd_case {
     acfd_partition_t part;
     acfd_model_t model;
@@ -185,6 +191,7 @@ struct acfd_case {
     // ([2][xg.nn], slot 1), xmap the plane map of its Y sweep (box xbox), and
     // the copy-only fill remapped to it (x_tasks, x_single).
     bool xt_ok = false;
+    bool xt_all_forms = false;     // the transposed X sweep for the fast FP64 form too
     Grid xg = {};
     double *xU = nullptr;
     int *xdid = nullptr;
@@ -196,6 +203,7 @@ struct acfd_case {
     int2 *x_single = nullptr;
     int x_nsingle = 0;
     long long wait_limit = kWaitLimitDefault;  // polls of a plane-march wait (acfd_set_wait_limit)
+    std::vector<StepPiece> *prof = nullptr;     // pieces of a step being profiled (acfd_profile_step)
     // ACFD_DEBUG=1: every stage and ghost fill is followed by a scan of its
     // level for non-finite values, checked at once (no step graphs)
     bool debug = false;
@@ -594,10 +602,12 @@ bool build_bc_program(acfd_case *cs)
 // last; the stages between run on the transposed levels with the copy-only
 // fill remapped to the transposed node indices.  Only for a fill of copies
 // (whose transpose is the fill of the transposed grid); ACFD_X_TRANSPOSE=0
-// keeps the X sweep.
+// keeps the X sweep, ACFD_X_TRANSPOSE=all offers the path to the fast FP64
+// form too.
 void build_xt(acfd_case *cs)
 {
     const char *env = getenv("ACFD_X_TRANSPOSE");
+    cs->xt_all_forms = env && strcmp(env, "all") == 0;
     if ((env && env[0] == '0') || !cs->bc_gather || cs->bc_nprog != 0 || cs->bc_copies.empty() || !cs->pmaps_ok ||
         cs->model.multidim != 0) {
         return;
@@ -845,31 +855,66 @@ int stage(acfd_case *cs, double dt_scale, double coeA, double coeB, int to, int 
     } while (0)
 
 // DiscretizeTime (fluid_dynamics.c:121-148) with dt = dt_scale * step dt
+// events around one piece of a step while a profile is taken (the end
+// event is recorded when the piece's scope closes)
+struct Piece {
+    acfd_case *cs;
+    cudaEvent_t e1 = nullptr;
+    Piece(acfd_case *c, int kind, int axis, int stage) : cs(c)
+    {
+        if (!cs->prof) return;
+        StepPiece p = {kind, axis, stage, nullptr, nullptr};
+        if (cudaEventCreate(&p.e0) != cudaSuccess) return;
+        if (cudaEventCreate(&p.e1) != cudaSuccess) {
+            cudaEventDestroy(p.e0);
+            return;
+        }
+        cudaEventRecord(p.e0, cs->stream);
+        cs->prof->push_back(p);
+        e1 = p.e1;
+    }
+    ~Piece()
+    {
+        if (e1) cudaEventRecord(e1, cs->stream);
+    }
+};
+
+// the RK stages of DiscretizeTime (fluid_dynamics.c:121-148): coefficients
+// of U[to] and of the updated U[tn], and the levels
+struct RkStage {
+    double coeA, coeB;
+    int to, tn, tm;
+};
+const RkStage kRk2[2] = {{0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN}, {1.0 / 2.0, 1.0 / 2.0, ACFD_TO, ACFD_TN, ACFD_TO}};
+const RkStage kRk3[3] = {{0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN},
+                         {3.0 / 4.0, 1.0 / 4.0, ACFD_TO, ACFD_TN, ACFD_TM},
+                         {1.0 / 3.0, 2.0 / 3.0, ACFD_TO, ACFD_TM, ACFD_TO}};
+
 int discretize(acfd_case *cs, double dt_scale, int s)
 {
-    if (cs->model.tScheme == 0) {
-        TRY(stage(cs, dt_scale, 0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN, s));
-        TRY(treat_boundary(cs, ACFD_TN));
-        TRY(stage(cs, dt_scale, 1.0 / 2.0, 1.0 / 2.0, ACFD_TO, ACFD_TN, ACFD_TO, s));
-        TRY(treat_boundary(cs, ACFD_TO));
-        return ACFD_OK;
+    const RkStage *rk = cs->model.tScheme == 0 ? kRk2 : kRk3;
+    const int n = cs->model.tScheme == 0 ? 2 : 3;
+    for (int q = 0; q < n; ++q) {
+        {
+            Piece p(cs, ACFD_PIECE_STAGE, s, q);
+            TRY(stage(cs, dt_scale, rk[q].coeA, rk[q].coeB, rk[q].to, rk[q].tn, rk[q].tm, s));
+        }
+        Piece p(cs, ACFD_PIECE_FILL, s, q);
+        TRY(treat_boundary(cs, rk[q].tm));
     }
-    TRY(stage(cs, dt_scale, 0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN, s));
-    TRY(treat_boundary(cs, ACFD_TN));
-    TRY(stage(cs, dt_scale, 3.0 / 4.0, 1.0 / 4.0, ACFD_TO, ACFD_TN, ACFD_TM, s));
-    TRY(treat_boundary(cs, ACFD_TM));
-    TRY(stage(cs, dt_scale, 1.0 / 3.0, 2.0 / 3.0, ACFD_TO, ACFD_TM, ACFD_TO, s));
-    TRY(treat_boundary(cs, ACFD_TO));
     return ACFD_OK;
 }
 
 // the X half steps may run as Y sweeps of the transposed state (build_xt):
-// the learned-sensor form (the FP64 and FP32-bulk X sweeps gain nothing by
-// it), no bodies (whose ghost values follow the fill), no debug scans
+// the FP32 forms, whose X sweep is slower than the Y sweep by more than the
+// two transposes of U[TO] cost (the fast FP64 form's is not: TGV 128^3, 12 us
+// a stage, 72 us a step, against 80 us of transposes), no bodies (whose ghost
+// values follow the fill), no debug scans
 bool xt_eligible(const acfd_case *cs)
 {
-    return cs->xt_ok && !cs->debug && !cs->plain_kernels && cs->mode == ACFD_FP32_HYBRID &&
-           !(cs->ib && ib_count(cs->ib) > 0);
+    const bool form = cs->mode == ACFD_FP32_HYBRID || cs->mode == ACFD_FP32_BULK ||
+                      (cs->xt_all_forms && cs->mode != ACFD_FP64_EXACT);
+    return cs->xt_ok && !cs->debug && !cs->plain_kernels && form && !(cs->ib && ib_count(cs->ib) > 0);
 }
 
 // ... and do, when the X sweep's variant is a plane march (acfd_autotune
@@ -941,23 +986,23 @@ int fill_xt(acfd_case *cs, int tn)
 // DiscretizeTime along x on the transposed levels (the stages of discretize)
 int discretize_xt(acfd_case *cs, double dt_scale)
 {
-    if (cs->model.tScheme == 0) {
-        TRY(stage_xt(cs, dt_scale, 0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN));
-        TRY(fill_xt(cs, ACFD_TN));
-        TRY(stage_xt(cs, dt_scale, 1.0 / 2.0, 1.0 / 2.0, ACFD_TO, ACFD_TN, ACFD_TO));
-        return fill_xt(cs, ACFD_TO);
+    const RkStage *rk = cs->model.tScheme == 0 ? kRk2 : kRk3;
+    const int n = cs->model.tScheme == 0 ? 2 : 3;
+    for (int q = 0; q < n; ++q) {
+        {
+            Piece p(cs, ACFD_PIECE_STAGE_XT, ACFD_X, q);
+            TRY(stage_xt(cs, dt_scale, rk[q].coeA, rk[q].coeB, rk[q].to, rk[q].tn, rk[q].tm));
+        }
+        Piece p(cs, ACFD_PIECE_FILL, ACFD_X, q);
+        TRY(fill_xt(cs, rk[q].tm));
     }
-    TRY(stage_xt(cs, dt_scale, 0.0, 1.0, ACFD_TO, ACFD_TO, ACFD_TN));
-    TRY(fill_xt(cs, ACFD_TN));
-    TRY(stage_xt(cs, dt_scale, 3.0 / 4.0, 1.0 / 4.0, ACFD_TO, ACFD_TN, ACFD_TM));
-    TRY(fill_xt(cs, ACFD_TM));
-    TRY(stage_xt(cs, dt_scale, 1.0 / 3.0, 2.0 / 3.0, ACFD_TO, ACFD_TM, ACFD_TO));
-    return fill_xt(cs, ACFD_TO);
+    return ACFD_OK;
 }
 
 // U[TO] (every node, ghosts included) to and from the transposed levels
 int xt_transpose(acfd_case *cs, bool into)
 {
+    Piece p(cs, ACFD_PIECE_TRANSPOSE, -1, 0);
     ++cs->launches;
     return into ? launch_transpose_state(level(cs, ACFD_TO), cs->grid, cs->xU, cs->xg, cs->stream)
                 : launch_transpose_state(cs->xU, cs->xg, level(cs, ACFD_TO), cs->grid, cs->stream);
@@ -974,13 +1019,15 @@ int evolve(acfd_case *cs)
         // sensor flags from U[TO], fixed for the whole step: the flags are
         // dilated by one node in the sweep, which covers the motion of a
         // feature during a step at CFL < 1
+        Piece p(cs, ACFD_PIECE_SENSOR, -1, 0);
         TRY(launch_sensor_flags(cs->grid, cs->mp, cs->U, cs->flags, cs->sensor_params, cs->sensor_logit,
                                 cs->sensor_rp, cs->sensor_flags, nullptr, cs->stream));
         cs->launches += 2;
     }
     const bool xt = use_xt(cs);
-    if (xt) {
+    if (xt && cs->mode == ACFD_FP32_HYBRID) {
         // the x flags as the flags of the transposed grid's axis 1
+        Piece p(cs, ACFD_PIECE_TRANSPOSE, -1, 0);
         TRY(launch_transpose_u8(cs->sensor_flags, cs->grid, cs->xfl + cs->xg.nn, cs->xg, cs->stream));
         ++cs->launches;
     }
@@ -1535,6 +1582,37 @@ int acfd_evolve_fluid(acfd_case_t *cs, double dt)
     return ACFD_OK;
 }
 
+int acfd_profile_step(acfd_case_t *cs, double dt, int cap, int *kind, int *axis, int *stage, float *ms, int *count)
+{
+    TRY(check_case(cs));
+    if (cap < 0 || !count || (cap > 0 && (!kind || !axis || !stage || !ms))) {
+        set_error("acfd_profile_step: bad output arrays");
+        return ACFD_ERR_ARG;
+    }
+    std::vector<StepPiece> pieces;
+    cs->prof = &pieces;
+    int st = set_dt(cs, dt);
+    if (st == ACFD_OK) st = evolve(cs);
+    cs->prof = nullptr;
+    const cudaError_t e = cudaStreamSynchronize(cs->stream);
+    *count = (int)pieces.size();
+    for (size_t i = 0; i < pieces.size(); ++i) {
+        float t = 0.0f;
+        if (st == ACFD_OK && e == cudaSuccess) cudaEventElapsedTime(&t, pieces[i].e0, pieces[i].e1);
+        if ((int)i < cap) {
+            kind[i] = pieces[i].kind;
+            axis[i] = pieces[i].axis;
+            stage[i] = pieces[i].stage;
+            ms[i] = t;
+        }
+        cudaEventDestroy(pieces[i].e0);
+        cudaEventDestroy(pieces[i].e1);
+    }
+    TRY(st);
+    if (e != cudaSuccess) return cuda_status(e, "acfd_profile_step");
+    return check_device_status(cs);
+}
+
 int acfd_evolve_fluid_graph(acfd_case_t *cs, double dt)
 {
     TRY(check_case(cs));
@@ -1597,7 +1675,7 @@ int acfd_autotune(acfd_case_t *cs, int tiles[3])
         const bool xt = s == 0 && xt_eligible(cs);
         if (xt) {
             st = xt_transpose(cs, true);
-            if (st == ACFD_OK) {
+            if (st == ACFD_OK && cs->mode == ACFD_FP32_HYBRID) {
                 st = launch_transpose_u8(cs->sensor_flags, cs->grid, cs->xfl + cs->xg.nn, cs->xg, cs->stream);
             }
         }

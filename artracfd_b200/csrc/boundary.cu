@@ -817,58 +817,71 @@ int launch_cfl(const Grid &g, const ModelParams &m, const double *U, const int *
 // Arrays transposed between two grids whose axes 0 and 1 are exchanged:
 // element (a, b, k) of src -- index (k * nb + b) * src_pitch + a, a < na the
 // fast axis -- goes to index (k * na + a) * dst_pitch + b of dst, for each of
-// nv variables; with swap_uv variables 1 and 2 (the x and y momenta) trade
+// NV variables; with swap_uv variables 1 and 2 (the x and y momenta) trade
 // places, so that a transposed state is the same flow with the axes renamed.
-// 32 x 32 tiles through shared memory: both sides coalesced.
-template <typename T>
+// 32 x 32 tiles through shared memory, both sides coalesced; one block moves
+// the tile of every variable, so that a thread has 4 * NV loads in flight
+// before the barrier (one variable per block leaves HBM half idle).
+template <typename T, int NV>
 __global__ void __launch_bounds__(256) transpose_xy(const T *__restrict__ src, long long src_nn, int src_pitch,
                                                     T *__restrict__ dst, long long dst_nn, int dst_pitch, int na,
-                                                    int nb, int nplanes, bool swap_uv)
+                                                    int nb, bool swap_uv)
 {
     pdl_wait();
-    __shared__ T tile[32][33];
-    const int k = (int)(blockIdx.z % (unsigned)nplanes), v = (int)(blockIdx.z / (unsigned)nplanes);
-    const int vd = swap_uv ? (v == 1 ? 2 : (v == 2 ? 1 : v)) : v;
+    __shared__ T tile[NV][32][33];
+    const int k = (int)blockIdx.z;
     const int a0 = blockIdx.x * 32, b0 = blockIdx.y * 32;
-    for (int r = threadIdx.y; r < 32; r += 8) {
-        const int a = a0 + threadIdx.x, b = b0 + r;
-        if (a < na && b < nb) tile[r][threadIdx.x] = src[v * src_nn + ((long long)k * nb + b) * src_pitch + a];
+    {
+        const int a = a0 + threadIdx.x;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int r = threadIdx.y + 8 * i, b = b0 + r;
+                if (a < na && b < nb) tile[v][r][threadIdx.x] = src[v * src_nn + ((long long)k * nb + b) * src_pitch + a];
+            }
+        }
     }
     __syncthreads();
-    for (int r = threadIdx.y; r < 32; r += 8) {
-        const int b = b0 + threadIdx.x, a = a0 + r;
-        if (a < na && b < nb) dst[vd * dst_nn + ((long long)k * na + a) * dst_pitch + b] = tile[threadIdx.x][r];
+    const int b = b0 + threadIdx.x;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        const int vd = swap_uv ? (v == 1 ? 2 : (v == 2 ? 1 : v)) : v;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int r = threadIdx.y + 8 * i, a = a0 + r;
+            if (a < na && b < nb) dst[vd * dst_nn + ((long long)k * na + a) * dst_pitch + b] = tile[v][threadIdx.x][r];
+        }
     }
 }
 
-template <typename T>
-static int launch_transpose(const T *src, const Grid &gs, T *dst, const Grid &gd, int nv, bool swap_uv,
-                            cudaStream_t st)
+template <typename T, int NV>
+static int launch_transpose(const T *src, const Grid &gs, T *dst, const Grid &gd, bool swap_uv, cudaStream_t st)
 {
-    if (gs.n[0] != gd.n[1] || gs.n[1] != gd.n[0] || gs.n[2] != gd.n[2] || (long long)gs.n[2] * nv > 65535) {
+    if (gs.n[0] != gd.n[1] || gs.n[1] != gd.n[0] || gs.n[2] != gd.n[2] || gs.n[2] > 65535) {
         set_error("transpose: grids (%d, %d, %d) and (%d, %d, %d) are not each other's transpose", gs.n[0], gs.n[1],
                   gs.n[2], gd.n[0], gd.n[1], gd.n[2]);
         return ACFD_ERR_ARG;
     }
-    const dim3 grid((unsigned)((gs.n[0] + 31) / 32), (unsigned)((gs.n[1] + 31) / 32), (unsigned)(gs.n[2] * nv));
-    cudaError_t e = launch_k(transpose_xy<T>, grid, dim3(32, 8), 0, st, src, gs.nn, gs.pitch, dst, gd.nn, gd.pitch,
-                             gs.n[0], gs.n[1], gs.n[2], swap_uv);
+    const dim3 grid((unsigned)((gs.n[0] + 31) / 32), (unsigned)((gs.n[1] + 31) / 32), (unsigned)gs.n[2]);
+    cudaError_t e = launch_k(transpose_xy<T, NV>, grid, dim3(32, 8), 0, st, src, gs.nn, gs.pitch, dst, gd.nn,
+                             gd.pitch, gs.n[0], gs.n[1], swap_uv);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "transpose launch");
 }
 
 int launch_transpose_state(const double *src, const Grid &gs, double *dst, const Grid &gd, cudaStream_t st)
 {
-    return launch_transpose<double>(src, gs, dst, gd, 5, true, st);
+    return launch_transpose<double, 5>(src, gs, dst, gd, true, st);
 }
 
 int launch_transpose_int(const int *src, const Grid &gs, int *dst, const Grid &gd, cudaStream_t st)
 {
-    return launch_transpose<int>(src, gs, dst, gd, 1, false, st);
+    return launch_transpose<int, 1>(src, gs, dst, gd, false, st);
 }
 
 int launch_transpose_u8(const uint8_t *src, const Grid &gs, uint8_t *dst, const Grid &gd, cudaStream_t st)
 {
-    return launch_transpose<uint8_t>(src, gs, dst, gd, 1, false, st);
+    return launch_transpose<uint8_t, 1>(src, gs, dst, gd, false, st);
 }
 
 int launch_finite_scan(const double *U, long long count, int *word, cudaStream_t st)

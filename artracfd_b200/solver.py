@@ -184,6 +184,17 @@ class Solver:
         fn = self.lib.acfd_evolve_fluid_graph if graph else self.lib.acfd_evolve_fluid
         check(fn(self.h, dt), self.lib)
 
+    def profile_step(self, dt: float):
+        """One time step (acfd_evolve_fluid) with CUDA events around each
+        piece (acfd_profile_step): a list of (kind, axis, stage, ms), kind
+        one of abi.PIECE_*."""
+        cap = 256
+        kind, axis, stage = ((ctypes.c_int * cap)() for _ in range(3))
+        ms = (ctypes.c_float * cap)()
+        n = ctypes.c_int()
+        check(self.lib.acfd_profile_step(self.h, dt, cap, kind, axis, stage, ms, ctypes.byref(n)), self.lib)
+        return [(kind[k], axis[k], stage[k], ms[k]) for k in range(min(n.value, cap))]
+
     def discretize_time(self, dt: float, s: int):
         check(self.lib.acfd_discretize_time(self.h, dt, s), self.lib)
 

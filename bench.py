@@ -331,38 +331,31 @@ def _timed_steps(torch, s, spec, steps, warmup, dist, stream, clock_index, label
     return sec, s.launches() - launches0, clk.summary()
 
 
-def _stage_profile(torch, s, spec, nodes_pin, stream, per_axis=None):
-    """One eager step with events around each LLLU stage and each ghost fill
-    on the solver's stream: mean stage and fill times (ms), and the
-    algorithmic bytes per stage launch.  per_axis (a dict, optional)
-    receives the stage times and algorithmic bytes of each sweep axis."""
+def _stage_profile(torch, s, spec, nodes_pin, stream, per_axis=None, other=None):
+    """One eager step through acfd_profile_step, with CUDA events around each
+    piece of the step on the solver's stream: mean stage-kernel and
+    ghost-fill times (ms), and the algorithmic bytes per stage launch.
+    per_axis (a dict, optional) receives the stage times and algorithmic
+    bytes of each sweep axis (the X half steps' stages whether they run on
+    the X sweep or transposed on the Y sweep), other (optional) the times of
+    the remaining pieces (the sensor's flags, transposes)."""
     from artracfd_b200 import abi
-    stage_ms, bc_ms = [], []
-    dt = s.time_step(spec.cfl)
-    order = [2, 1, 0, 0, 1, 2]
-    coefs = [(0.0, 1.0, abi.TO, abi.TO, abi.TN), (0.75, 0.25, abi.TO, abi.TN, abi.TM),
-             (1.0 / 3.0, 2.0 / 3.0, abi.TO, abi.TM, abi.TO)]
-    stage_bytes = 0.0
-    if s.mode == abi.FP32_HYBRID:
-        s.sensor_update()
-    with torch.cuda.stream(stream):
-        for sd in order:
-            for q, (a, b, to, tn, tm) in enumerate(coefs):
-                ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-                ev[0].record(stream)
-                s.lllu(0.5 * dt, a, b, to, tn, tm, sd)
-                ev[1].record(stream)
-                s.treat_boundary(tm)
-                ev[2].record(stream)
-                ev[2].synchronize()
-                stage_ms.append(ev[0].elapsed_time(ev[1]))
-                bc_ms.append(ev[1].elapsed_time(ev[2]))
-                stage_bytes += STAGE_BYTES[q] * nodes_pin
-                if per_axis is not None:
-                    ax = per_axis.setdefault(sd, {"ms": [], "bytes": []})
-                    ax["ms"].append(stage_ms[-1])
-                    ax["bytes"].append(STAGE_BYTES[q] * nodes_pin)
-    return sum(stage_ms) / len(stage_ms), sum(bc_ms) / len(bc_ms), stage_bytes / len(stage_ms)
+    names = {abi.PIECE_TRANSPOSE: "transpose", abi.PIECE_SENSOR: "sensor_flags"}
+    stage_ms, bc_ms, stage_bytes = [], [], []
+    for kind, ax, q, ms in s.profile_step(s.time_step(spec.cfl)):
+        if kind in (abi.PIECE_STAGE, abi.PIECE_STAGE_XT):
+            stage_ms.append(ms)
+            stage_bytes.append(STAGE_BYTES[q] * nodes_pin)
+            if per_axis is not None:
+                d = per_axis.setdefault(ax, {"ms": [], "bytes": [], "transposed": False})
+                d["ms"].append(ms)
+                d["bytes"].append(stage_bytes[-1])
+                d["transposed"] = kind == abi.PIECE_STAGE_XT
+        elif kind == abi.PIECE_FILL:
+            bc_ms.append(ms)
+        elif other is not None:
+            other.setdefault(names.get(kind, str(kind)), []).append(ms)
+    return sum(stage_ms) / len(stage_ms), sum(bc_ms) / len(bc_ms), sum(stage_bytes) / len(stage_bytes)
 
 
 def _pin_mask(part):
@@ -438,10 +431,12 @@ def _form_block(torch, part, model, node, spec, form, nodes_pin, args, dist, str
     if form == "hybrid":
         out["flagged_fraction"] = s.sensor_update() / (3.0 * nodes_pin)
     if profile:
-        per_axis = {}
-        st, bc, by = _stage_profile(torch, s, spec, nodes_pin, stream, per_axis)
+        per_axis, other = {}, {}
+        st, bc, by = _stage_profile(torch, s, spec, nodes_pin, stream, per_axis, other)
         out["stage_ms"] = {"sweep_mean": st, "ghost_fill_mean": bc,
-                           "per_axis": {str(ax): sum(d["ms"]) / len(d["ms"]) for ax, d in sorted(per_axis.items())}}
+                           "per_axis": {str(ax): sum(d["ms"]) / len(d["ms"]) for ax, d in sorted(per_axis.items())},
+                           "x_transposed": any(d["transposed"] for d in per_axis.values()),
+                           "other_per_step": {k: sum(v) for k, v in sorted(other.items())}}
         if hbm_peak:
             out["hbm_frac"] = by / (st / 1e3) / 1e9 / hbm_peak
         out["_stage_mean_ms"] = st
@@ -528,8 +523,8 @@ def run_ours(args, rank, world, local_rank):
     value = job_rate(world, nodes_pin, args.steps, sec)
     if args.mode == "hybrid":
         sensor_info["flagged_fraction_after_timed_steps"] = s.sensor_update() / (3.0 * nodes_pin)
-    per_axis = {}
-    stage_mean, bc_mean, bytes_per_stage = _stage_profile(torch, s, spec, nodes_pin, stream, per_axis)
+    per_axis, other = {}, {}
+    stage_mean, bc_mean, bytes_per_stage = _stage_profile(torch, s, spec, nodes_pin, stream, per_axis, other)
     # the dominant kernel: the stage-kernel family (tile variant class) with
     # the largest share of the stage time; its algorithmic bytes over its
     # mean launch duration
@@ -658,7 +653,9 @@ def run_ours(args, rank, world, local_rank):
                                "note": "the reference's flop count of the same stages over the FP32 form's stage time "
                                        "(reference-equivalent work: the hybrid computes fewer flops on smooth "
                                        "interfaces)"} if fp32_peak else None)},
-        "stage_ms": {"sweep_mean": stage_mean, "ghost_fill_mean": bc_mean},
+        "stage_ms": {"sweep_mean": stage_mean, "ghost_fill_mean": bc_mean,
+                     "x_transposed": any(d["transposed"] for d in per_axis.values()),
+                     "other_per_step": {k: sum(v) for k, v in sorted(other.items())}},
         "clocks": clocks,
         "e2e": {"value": job_rate(world, nodes_pin, args.steps, e2e_sec), "unit": UNIT,
                 "h2d_bytes_per_step": (node_bytes + 8 * args.steps) / args.steps,

@@ -253,6 +253,21 @@ int acfd_treat_boundary(acfd_case_t *cs, int tn);
 /* Capture one EvolveFluidDynamics into a CUDA graph keyed by dt and replay it
  * (same result as acfd_evolve_fluid). */
 int acfd_evolve_fluid_graph(acfd_case_t *cs, double dt);
+/* Pieces of a time step, as acfd_profile_step reports them. */
+#define ACFD_PIECE_STAGE 0     /* an LLLU stage kernel along sweep axis[i] */
+#define ACFD_PIECE_STAGE_XT 1  /* an LLLU stage along x, run as the Y sweep of the transposed state */
+#define ACFD_PIECE_FILL 2      /* the ghost fill (TreatBoundary) after a stage */
+#define ACFD_PIECE_TRANSPOSE 3 /* U[TO] or the x flags to or from the transposed state */
+#define ACFD_PIECE_SENSOR 4    /* the learned sensor's flags of U[TO] */
+/* acfd_evolve_fluid with CUDA events around each piece of the step on the
+ * case's stream: piece i has kind[i] (ACFD_PIECE_*), axis[i] (the sweep axis,
+ * -1 for none), stage[i] (RK stage 0..2 of a stage or fill, else 0) and its
+ * device time ms[i].  *count receives the number of pieces, of which the
+ * first cap are written.  The step is a real step (U[TO] advances); the call
+ * synchronizes.  Instrumentation with no reference counterpart (the
+ * reference times whole steps, timer.c:22-35). */
+int acfd_profile_step(acfd_case_t *cs, double dt, int cap, int *kind, int *axis, int *stage, float *ms,
+        int *count);
 
 /* ---- immersed boundaries ---------------------------------------------- */
 

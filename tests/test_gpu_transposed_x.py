@@ -1,7 +1,8 @@
-"""The learned-sensor form's X half steps as Y sweeps of the transposed state.
+"""The FP32 forms' X half steps as Y sweeps of the transposed state.
 
 For a case whose ghost fill is copies only (periodic and outflow faces) and
-that has no bodies, the hybrid form runs the X half steps of a time step on
+that has no bodies, the learned-sensor hybrid and the FP32-bulk forms run
+the X half steps of a time step on
 a copy of U[TO] with x and y exchanged (and the x and y momenta with them):
 the Y plane-march kernel sweeps it, the copy-only fill of the transposed grid
 fills its ghosts, and the state is transposed back after the last X half
@@ -27,8 +28,8 @@ pytestmark = [pytest.mark.gpu,
                                  reason="no trained sensor weights")]
 
 # transposes per time step: U[TO] in and out around the one run of X half
-# steps of a 3D step (sweep order z y x x y z), and the x flags
-XT_LAUNCHES = 3
+# steps of a 3D step (sweep order z y x x y z), and (hybrid) the x flags
+XT_LAUNCHES = {"all": 3, "none": 3, "fp32": 2}
 
 
 def _cases():
@@ -53,8 +54,11 @@ def _steps(spec, params, thr, tiles, steps, transpose, monkeypatch, dts=None, gr
             s.geo_upload(geo)
             s.compute_geometric_field()
         s.treat_boundary(abi.TO)
-        s.sensor_load(params, thr)
-        s.set_precision(abi.FP32_HYBRID)
+        if params is None:
+            s.set_precision(abi.FP32_BULK)
+        else:
+            s.sensor_load(params, thr)
+            s.set_precision(abi.FP32_HYBRID)
         s.set_tiles(tiles)
         for k in range(steps):
             dt = s.time_step(spec.cfl) if dts is None else dts[k]
@@ -66,18 +70,19 @@ def _steps(spec, params, thr, tiles, steps, transpose, monkeypatch, dts=None, gr
     return outs, used, per_step
 
 
-@pytest.mark.parametrize("flags", ["all", "none"])
+@pytest.mark.parametrize("flags", ["all", "none", "fp32"])
 @pytest.mark.parametrize("name", CASES)
 def test_transposed_x_matches_x_sweep(name, flags, monkeypatch):
-    """Every node flagged (WENO5) or none (linear weights): the flags do not
-    depend on the state, so three steps stay within FP32 round-off."""
+    """The hybrid form with every node flagged (WENO5) or none (linear
+    weights), and the FP32-bulk form: the flags do not depend on the state,
+    so three steps stay within FP32 round-off."""
     spec = CASES[name]
-    params = _const_sensor(50.0 if flags == "all" else -50.0)
+    params = None if flags == "fp32" else _const_sensor(50.0 if flags == "all" else -50.0)
     ref, dts, lref = _steps(spec, params, 0.5, PLANE, 3, False, monkeypatch)
     got, _, lgot = _steps(spec, params, 0.5, PLANE, 3, True, monkeypatch, dts=dts)
     for k in range(3):
         assert rel_err(got[k], ref[k]) <= TOL_FP32_ORDER, (k, rel_err(got[k], ref[k]))
-        assert lgot[k] == lref[k] + XT_LAUNCHES, (lgot, lref)
+        assert lgot[k] == lref[k] + XT_LAUNCHES[flags], (lgot, lref)
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -180,3 +185,49 @@ def test_bodies_keep_the_x_sweep(monkeypatch):
     nb, ub = graph_then_body(False)
     assert na == nb
     assert rel_err(ua, ub) <= TOL_FP32_ORDER
+
+
+@pytest.mark.parametrize("form", ["fp64", "fp32", "hybrid"])
+def test_profile_step_lists_the_pieces_of_a_step(form, monkeypatch):
+    """acfd_profile_step is acfd_evolve_fluid with events around its pieces:
+    the same bits, and the pieces in step order -- per half step (sweep
+    order z y x x y z) three RK stages each followed by its ghost fill; in
+    the FP32 forms the X half steps on the transposed state between the two
+    transposes of U[TO], and in the hybrid form first the sensor's flags and
+    the x flags' transpose."""
+    monkeypatch.setenv("ACFD_X_TRANSPOSE", "1")
+    spec = CASES["tgv_40x28x20"]
+    part, model = spec.descriptors()
+
+    def start(s):
+        s.upload(spec.initial_nodes(part, model))
+        s.treat_boundary(abi.TO)
+        if form == "hybrid":
+            s.sensor_load(_const_sensor(50.0), 0.5)
+            s.set_precision(abi.FP32_HYBRID)
+        elif form == "fp32":
+            s.set_precision(abi.FP32_BULK)
+        s.set_tiles(SHARE)
+
+    with Solver(part, model, abi.FP64) as a, Solver(part, model, abi.FP64) as b:
+        start(a)
+        start(b)
+        dt = a.time_step(spec.cfl)
+        pieces = a.profile_step(dt)
+        b.evolve(dt)
+        assert np.array_equal(a.download()["U"], b.download()["U"])
+    kinds = [p[0] for p in pieces]
+    half = []
+    for ax in (2, 1, 0, 0, 1, 2):
+        st = abi.PIECE_STAGE_XT if (form != "fp64" and ax == 0) else abi.PIECE_STAGE
+        for q in range(3):
+            half += [(st, ax, q), (abi.PIECE_FILL, ax, q)]
+    T = (abi.PIECE_TRANSPOSE, -1, 0)
+    if form == "hybrid":
+        want = [(abi.PIECE_SENSOR, -1, 0), T] + half[:12] + [T] + half[12:24] + [T] + half[24:]
+    elif form == "fp32":
+        want = half[:12] + [T] + half[12:24] + [T] + half[24:]
+    else:
+        want = half
+    assert [p[:3] for p in pieces] == want, kinds
+    assert all(p[3] > 0.0 for p in pieces)
