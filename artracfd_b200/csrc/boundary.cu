@@ -10,6 +10,7 @@
 #include <cstdlib>
 
 #include "acfd_internal.cuh"
+#include "fast_div.h"
 
 namespace acfd {
 
@@ -273,19 +274,24 @@ __device__ __forceinline__ double vmax_of(double a, double b)
 // with the whole block and writes out[0..3].  Every partial maximum starts
 // from 0 and a NaN never replaces a value (vmax_of), so no NaN enters and the
 // maximum does not depend on the order of combination.
-__global__ void cfl_partial(Grid g, ModelParams mp, const double *U, const int *did, double *part, double *out)
+// div_x, div_y: division by the PIN extents along x and y (32-bit path).
+__global__ void cfl_partial(Grid g, ModelParams mp, const double *U, const int *did, double *part, double *out,
+                            FastDiv div_x, FastDiv div_y)
 {
     pdl_wait();
     const int Lx = g.hi[0] - g.lo[0], Ly = g.hi[1] - g.lo[1], Lz = g.hi[2] - g.lo[2];
     const long long total = (long long)Lx * Ly * Lz;
     double m0 = 0.0, m1 = 0.0, m2 = 0.0;
     bool bad = false;  // a fluid node whose wave speed is not finite
+    // the node type and the state are loaded together (one memory round
+    // trip, not two); a node that is not a fluid node is passed over after
     auto visit = [&](long long id) {
-        if (did[id] != 0) {
-            return;
-        }
+        const int d = did[id];
         double Uc[5], Uo[6];
         load5(U, g.nn, id, Uc);
+        if (d != 0) {
+            return;
+        }
         to_primitive(mp.gamma, mp.gasR, Uc, Uo);
         const double c = sqrt(mp.gamma * mp.gasR * Uo[5]);
         const double v0 = fabs(Uo[1]) + c, v1 = fabs(Uo[2]) + c, v2 = fabs(Uo[3]) + c;
@@ -299,11 +305,20 @@ __global__ void cfl_partial(Grid g, ModelParams mp, const double *U, const int *
     if (total < (long long)INT32_MAX / 2 && g.nn < (long long)INT32_MAX) {
         // 32-bit work indices: 64-bit divisions would cost more than the loads
         const int tot = (int)total, sy = g.pitch, sz = g.pitch * g.n[1];
-        for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
-            const int rest = t / Lx;
-            const int kk = rest / Ly;
-            visit((long long)((g.lo[2] + kk) * sz + (g.lo[1] + rest - kk * Ly) * sy + g.lo[0] + t - rest * Lx));
+        const int stride = (int)(gridDim.x * blockDim.x);
+        auto node = [&](int t) {
+            const int rest = (int)fast_div((uint32_t)t, div_x);
+            const int kk = (int)fast_div((uint32_t)rest, div_y);
+            return (long long)((g.lo[2] + kk) * sz + (g.lo[1] + rest - kk * Ly) * sy + g.lo[0] + t - rest * Lx);
+        };
+        // two nodes an iteration: both nodes' loads in flight at once
+        int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+        for (; t + stride < tot; t += 2 * stride) {
+            const long long a = node(t), b = node(t + stride);
+            visit(a);
+            visit(b);
         }
+        if (t < tot) visit(node(t));
     } else {
         for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
              t += (long long)gridDim.x * blockDim.x) {
@@ -810,7 +825,10 @@ int launch_domain_boundary_fused(const Grid &g, const ModelParams &m, const acfd
 int launch_cfl(const Grid &g, const ModelParams &m, const double *U, const int *did, double *partials,
                double *out, cudaStream_t st)
 {
-    cudaError_t e = launch_k(cfl_partial, dim3(kCflBlocks), dim3(256), 0, st, g, m, U, did, partials, out);
+    const FastDiv div_x = make_fast_div((uint32_t)std::max(1, g.hi[0] - g.lo[0]));
+    const FastDiv div_y = make_fast_div((uint32_t)std::max(1, g.hi[1] - g.lo[1]));
+    cudaError_t e = launch_k(cfl_partial, dim3(kCflBlocks), dim3(256), 0, st, g, m, U, did, partials, out, div_x,
+                             div_y);
     return e == cudaSuccess ? ACFD_OK : cuda_status(e, "cfl launch");
 }
 

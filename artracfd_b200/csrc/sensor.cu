@@ -26,6 +26,7 @@
 #include <cuda_fp16.h>
 
 #include "acfd_internal.cuh"
+#include "fast_div.h"
 #include "flux_math.cuh"
 
 namespace acfd {
@@ -338,9 +339,11 @@ constexpr int kFlagWarps = 8;
 // Flags: flags[s][node] = 1 where the network's logit exceeds the threshold
 // or the node is not a fluid node, 0 elsewhere; nodes outside PIN keep the 1
 // written when the sensor was loaded.  count (optional) accumulates the flags set.
+// div_x, div_y: division by the PIN extents along x and y.
 __global__ void __launch_bounds__(kFlagWarps * 32) flags_mma_kernel(Grid g, const float2 *rp, const int *did,
                                                                     const float *params, float logit_threshold,
-                                                                    uint8_t *flags, unsigned long long *count)
+                                                                    uint8_t *flags, unsigned long long *count,
+                                                                    FastDiv div_x, FastDiv div_y)
 {
     pdl_wait();
     // one 32 x 16 f16 feature tile per warp, rows padded to 12 words so that
@@ -391,9 +394,9 @@ __global__ void __launch_bounds__(kFlagWarps * 32) flags_mma_kernel(Grid g, cons
 #pragma unroll
         for (int m = 0; m < kIn; ++m) f[m] = 0.0f;
         if (valid) {
-            const int rest = q / Lx;
+            const int rest = (int)fast_div((uint32_t)q, div_x);
             const int i = g.lo[0] + (q - rest * Lx);
-            const int kk = rest / Ly;
+            const int kk = (int)fast_div((uint32_t)rest, div_y);
             const int j = g.lo[1] + (rest - kk * Ly);
             const int k = g.lo[2] + kk;
             id = (long long)(k * sz + j * sy + i);
@@ -406,7 +409,9 @@ __global__ void __launch_bounds__(kFlagWarps * 32) flags_mma_kernel(Grid g, cons
                 mr += v[m].x;
                 mp += v[m].y;
             }
-            const float ir = 5.0f / mr, ip = 5.0f / mp;
+            // 5 / mean, with the approximate division (2 ulp): the features
+            // go to f16 next
+            const float ir = __fdividef(5.0f, mr), ip = __fdividef(5.0f, mp);
 #pragma unroll
             for (int m = 0; m < 5; ++m) {
                 f[m] = 10.0f * (v[m].x * ir - 1.0f);
@@ -499,8 +504,10 @@ int launch_sensor_flags(const Grid &g, const ModelParams &m, const double *U, co
                        m.gamma - 1.0, U, rho_p));
     const long long groups = ((pin + 31) / 32) * 3;
     const long long blocks = std::min<long long>((groups + sensor::kFlagWarps - 1) / sensor::kFlagWarps, 148LL * 8);
+    const FastDiv div_x = make_fast_div((uint32_t)(g.hi[0] - g.lo[0]));
+    const FastDiv div_y = make_fast_div((uint32_t)(g.hi[1] - g.lo[1]));
     ACFD_CUDA(launch_k(sensor::flags_mma_kernel, dim3((unsigned)blocks), dim3(sensor::kFlagWarps * 32), 0, st, g,
-                       (const float2 *)rho_p, did, params, logit_threshold, flags, count));
+                       (const float2 *)rho_p, did, params, logit_threshold, flags, count, div_x, div_y));
     return ACFD_OK;
 }
 

@@ -43,13 +43,14 @@ FLOP_PER_NODE_STAGE_VISCOUS = 1535.0  # ComputeFhat 1380 + ComputeFvhat 115 + LU
 STAGE_BYTES = (80.0, 120.0, 120.0)
 
 
-def profiled_traffic(mode: str, tiles, axes=(0, 1, 2)):
+def profiled_traffic(mode: str, tiles, axes=(0, 1, 2), transposed=()):
     """DRAM bytes per RK-stage-2 launch of this form's stage kernels, mean over
     the given sweep axes, from the committed ncu record profiles/dram_traffic.json
     (dram__bytes_read.sum + dram__bytes_write.sum of one capture per axis, the
-    stage-kernel variant of each axis recorded beside it).  Returns (bytes,
-    source) or (None, reason) when the record does not hold this form with
-    these variants."""
+    stage-kernel variant of each axis recorded beside it, and whether the X
+    half step ran on the X sweep or as the Y sweep of the transposed state).
+    Returns (bytes, source) or (None, reason) when the record does not hold
+    this form with these variants."""
     p = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if not os.path.exists(p):
         return None, "no profiles/dram_traffic.json"
@@ -61,9 +62,11 @@ def profiled_traffic(mode: str, tiles, axes=(0, 1, 2)):
     for a in axes:
         caps = rec["axes"].get(str(a), [])
         caps = caps if isinstance(caps, list) else [caps]
-        hit = [c for c in caps if int(tiles[a]) in [int(v) for v in c["variants"]]]
+        tr = a in transposed
+        hit = [c for c in caps if int(tiles[a]) in [int(v) for v in c["variants"]]
+               and bool(c.get("transposed", False)) == tr]
         if not hit:
-            return None, f"no capture of variant {tiles[a]} on axis {a}"
+            return None, f"no capture of variant {tiles[a]} on axis {a}" + (" (transposed)" if tr else "")
         vals.append(float(hit[0]["dram_bytes"]))
     return sum(vals) / len(vals), rec["source"]
 
@@ -542,7 +545,8 @@ def run_ours(args, rank, world, local_rank):
     dom_share = sum(dom["ms"]) / sum(sum(d["ms"]) for d in fams.values())
     # ncu traffic of RK stage 2 (120 B algorithmic per node), scaled to the
     # mean RK-stage mix of one step (106.7 B per node)
-    tr2, tr_src = profiled_traffic(args.mode, tiles, tuple(sorted(dom["axes"])))
+    tr2, tr_src = profiled_traffic(args.mode, tiles, tuple(sorted(dom["axes"])),
+                                   tuple(ax for ax, d in per_axis.items() if d["transposed"]))
     traffic = tr2 * (dom_bytes / (STAGE_BYTES[1] * nodes_pin)) if tr2 else None
     flop_rate = FLOP_PER_NODE_STAGE_VISCOUS * nodes_pin / (stage_mean / 1e3) / 1e12
     fp64_peak = fp64_peak_tflops(torch) if rank == 0 else None

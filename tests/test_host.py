@@ -429,3 +429,68 @@ def test_ghost_copy_tasks_cover_exactly_the_copies(tmp_path):
             assert (ntask, in_tasks, nsingle) == (4, 7000, 0)  # three pieces of 2048 and the rest
         if name == "outflow-like":
             assert (ntask, nsingle) == (0, len(want))  # runs of three: single copies
+
+
+_DIV_HARNESS = r"""
+#include <cstdio>
+#include <cstdint>
+#include <initializer_list>
+#include "fast_div.h"
+// every divisor 1..4096 against numerators at and around its multiples and
+// at random across the range the kernels use (n < 2^31), then random divisors
+static uint64_t state = 88172645463325252ull;
+static uint32_t rnd() { state ^= state << 13; state ^= state >> 7; state ^= state << 17; return (uint32_t)state; }
+static int check(uint32_t d, uint32_t n)
+{
+    if (n >= (1u << 31)) return 0;
+    return fast_div(n, make_fast_div(d)) != n / d;
+}
+int main()
+{
+    long long bad = 0, tried = 0;
+    for (uint32_t d = 1; d <= 4096; ++d) {
+        for (uint32_t q = 0; q < 2000; ++q) {
+            for (int e = -1; e <= 1; ++e) {
+                const long long n = (long long)q * d + e;
+                if (n < 0) continue;
+                bad += check(d, (uint32_t)n);
+                ++tried;
+            }
+        }
+        for (int r = 0; r < 2000; ++r) {
+            bad += check(d, rnd() >> 1);
+            ++tried;
+        }
+    }
+    for (int r = 0; r < 200000; ++r) {
+        const uint32_t d = (rnd() >> 1) | 1u, n = rnd() >> 1;
+        bad += check(d, n) + check(d, n - n % d) + check(d, n - n % d - 1u * (n >= d));
+        tried += 3;
+    }
+    const uint32_t edge[] = {0u, 1u, 2147483647u, 2147483646u, 1073741824u, 1073741823u};
+    for (uint32_t d : {1u, 2u, 3u, 7u, 129u, 1023u, 65537u, 2147483647u})
+        for (uint32_t n : edge) { bad += check(d, n); ++tried; }
+    std::printf("%lld %lld\n", tried, bad);
+    return bad != 0;
+}
+"""
+
+
+def test_fast_division_matches_integer_division(tmp_path):
+    """The multiply-high division of csrc/fast_div.h (the node index of the
+    sensor and CFL kernels), compiled here for the host: equal to n / d for
+    every divisor up to 4096 at and around its multiples and at random
+    numerators below 2^31, and for random divisors up to 2^31."""
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no host C++ compiler")
+    src = tmp_path / "div.cpp"
+    src.write_text(_DIV_HARNESS)
+    exe = tmp_path / "div"
+    csrc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "artracfd_b200", "csrc")
+    subprocess.run([gxx, "-O2", "-std=c++17", "-I" + csrc, str(src), "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    tried, bad = (int(x) for x in r.stdout.split())
+    assert tried > 20_000_000 and bad == 0 and r.returncode == 0, (tried, bad)
