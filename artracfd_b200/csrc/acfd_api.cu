@@ -604,6 +604,25 @@ bool build_bc_program(acfd_case *cs)
 // (whose transpose is the fill of the transposed grid); ACFD_X_TRANSPOSE=0
 // keeps the X sweep, ACFD_X_TRANSPOSE=all offers the path to the fast FP64
 // form too.
+void build_xt(acfd_case *cs);
+
+// the transposed levels and their fill freed; the X half steps stay on the
+// X sweep
+void release_xt(acfd_case *cs)
+{
+    cudaFree(cs->xU);
+    cudaFree(cs->xdid);
+    cudaFree(cs->xfl);
+    cudaFree(cs->x_tasks);
+    cs->xU = nullptr;
+    cs->xdid = nullptr;
+    cs->xfl = nullptr;
+    cs->x_tasks = nullptr;
+    cs->x_single = nullptr;
+    cs->x_ntask = cs->x_nsingle = 0;
+    cs->xt_ok = false;
+}
+
 void build_xt(acfd_case *cs)
 {
     const char *env = getenv("ACFD_X_TRANSPOSE");
@@ -1442,10 +1461,7 @@ int acfd_finalize(acfd_case_t *cs)
     cudaFree(cs->dstatus);
     cudaFree(cs->bcbar);
     cudaFree(cs->bc_pairs);
-    cudaFree(cs->xU);
-    cudaFree(cs->xdid);
-    cudaFree(cs->xfl);
-    cudaFree(cs->x_tasks);
+    release_xt(cs);
     cudaFree(cs->dbg_word);
     cudaFree(cs->sensor_params);
     cudaFree(cs->sensor_flags);
@@ -2434,6 +2450,9 @@ int acfd_batch_init(int ncase, const acfd_partition_t *parts, const acfd_model_t
         acfd_case *cs = nullptr;
         st = acfd_init(&parts[c], &models[c], &cs);
         if (st == ACFD_OK) {
+            // the batch kernels sweep x directly: a batch case holds no
+            // transposed levels
+            release_xt(cs);
             b->cases.push_back(cs);
         }
     }
