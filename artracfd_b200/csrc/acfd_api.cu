@@ -647,13 +647,7 @@ void build_xt(acfd_case *cs)
     const PlaneTile pt = plane_tile(xg, 1, viscous(cs), 1, cs->sms);
     if (pt.BXp > 256 || pt.BC > 256) return;
     // the copies on the transposed node indices, in destination order
-    auto tr = [&](int q) {
-        const long long i = q % g.pitch, j = (q / g.pitch) % g.n[1], k = q / ((long long)g.pitch * g.n[1]);
-        return (int)((k * xg.n[1] + i) * xg.pitch + j);
-    };
-    std::vector<int2> xc(cs->bc_copies.size());
-    for (size_t q = 0; q < xc.size(); ++q) xc[q] = make_int2(tr(cs->bc_copies[q].x), tr(cs->bc_copies[q].y));
-    std::sort(xc.begin(), xc.end(), [](const int2 &a, const int2 &b) { return a.x < b.x; });
+    const std::vector<int2> xc = transposed_copies_of(cs->bc_copies, g.pitch, g.n[0], g.n[1], xg.pitch);
     std::vector<int4> tasks;
     std::vector<int2> single;
     ghost_copy_tasks(xc, tasks, single);

@@ -43,6 +43,27 @@ void ghost_copy_tasks_of(const std::vector<Int2> &pairs, std::vector<Int4> &task
     }
 }
 
+// The copies of a fill on the grid whose axes 0 and 1 are exchanged: node
+// (i, j, k) of a grid with n1 nodes along axis 1 and row pitch `pitch` is
+// node (j, i, k) of the transposed grid (n0 rows of pitch `xpitch`); the
+// copies come back in destination order.  For a fill of copies (periodic and
+// outflow faces) this is the same fill of the transposed grid.
+template <class Int2>
+std::vector<Int2> transposed_copies_of(const std::vector<Int2> &pairs, int pitch, int n0, int n1, int xpitch)
+{
+    auto tr = [&](int q) {
+        const long long i = q % pitch, j = (q / pitch) % n1, k = q / ((long long)pitch * n1);
+        return (int)((k * n0 + i) * xpitch + j);
+    };
+    std::vector<Int2> xc(pairs.size());
+    for (size_t q = 0; q < xc.size(); ++q) {
+        xc[q].x = tr(pairs[q].x);
+        xc[q].y = tr(pairs[q].y);
+    }
+    std::sort(xc.begin(), xc.end(), [](const Int2 &a, const Int2 &b) { return a.x < b.x; });
+    return xc;
+}
+
 #ifdef __CUDACC__
 inline void ghost_copy_tasks(const std::vector<int2> &pairs, std::vector<int4> &tasks, std::vector<int2> &single)
 {

@@ -365,11 +365,13 @@ int main(int argc, char **argv)
 """
 
 
-def _periodic_fill_pairs(n, ng):
+def _periodic_fill_pairs(n, ng, pitch=None):
     """(destination, source) node pairs of the one-launch fill of a grid whose
     faces are all periodic: every ghost node takes the value of the computed
-    node one period away along each axis where it lies outside."""
+    node one period away along each axis where it lies outside (rows of
+    `pitch` nodes, by default nx)."""
     nx, ny, nz = n
+    px = nx if pitch is None else pitch
     lo = [ng, ng, ng]
     L = [nx - 2 * ng, ny - 2 * ng, nz - 2 * ng]
     out = []
@@ -384,7 +386,7 @@ def _periodic_fill_pairs(n, ng):
                     elif c[a] >= lo[a] + L[a]:
                         src[a] -= L[a]
                 if src != c:
-                    out.append(((k * ny + j) * nx + i, (src[2] * ny + src[1]) * nx + src[0]))
+                    out.append(((k * ny + j) * px + i, (src[2] * ny + src[1]) * px + src[0]))
     return np.array(out, dtype=np.int32)
 
 
@@ -494,3 +496,56 @@ def test_fast_division_matches_integer_division(tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     tried, bad = (int(x) for x in r.stdout.split())
     assert tried > 20_000_000 and bad == 0 and r.returncode == 0, (tried, bad)
+
+
+_TRANSPOSE_HARNESS = r"""
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+struct int2 { int x, y; };
+struct int4 { int x, y, z, w; };
+#include "ghost_tasks.h"
+int main(int argc, char **argv)
+{
+    FILE *f = std::fopen(argv[1], "rb");
+    std::vector<int2> pairs;
+    int2 p;
+    while (std::fread(&p, sizeof p, 1, f) == 1) pairs.push_back(p);
+    std::fclose(f);
+    const std::vector<int2> xc = transposed_copies_of(pairs, std::atoi(argv[3]), std::atoi(argv[4]),
+                                                      std::atoi(argv[5]), std::atoi(argv[6]));
+    for (size_t q = 1; q < xc.size(); ++q)
+        if (xc[q].x < xc[q - 1].x) return 3;  // destination order
+    FILE *o = std::fopen(argv[2], "wb");
+    std::fwrite(xc.data(), sizeof(int2), xc.size(), o);
+    std::fclose(o);
+    return 0;
+}
+"""
+
+
+def test_transposed_fill_is_the_fill_of_the_transposed_grid(tmp_path):
+    """The copies of a periodic fill remapped to the grid with axes 0 and 1
+    exchanged (csrc/ghost_tasks.h, the fill of the transposed state that the
+    FP32 forms' X half steps run on), compiled here for the host: exactly the
+    periodic fill of the transposed grid, with padded rows on both sides."""
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no host C++ compiler")
+    src = tmp_path / "tr.cpp"
+    src.write_text(_TRANSPOSE_HARNESS)
+    exe = tmp_path / "tr"
+    csrc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "artracfd_b200", "csrc")
+    subprocess.run([gxx, "-O2", "-std=c++17", "-I" + csrc, str(src), "-o", str(exe)], check=True)
+    for (n0, n1, n2) in ((19, 13, 11), (25, 9, 10), (16, 16, 9)):
+        pitch, xpitch = (n0 + 7) // 8 * 8, (n1 + 7) // 8 * 8
+        pairs = _periodic_fill_pairs((n0, n1, n2), 3, pitch)
+        pin, pout = tmp_path / "pairs.bin", tmp_path / "out.bin"
+        pairs.astype(np.int32).tofile(pin)
+        subprocess.run([str(exe), str(pin), str(pout), str(pitch), str(n0), str(n1), str(xpitch)], check=True)
+        got = np.fromfile(pout, dtype=np.int32).reshape(-1, 2)
+        want = _periodic_fill_pairs((n1, n0, n2), 3, xpitch)
+        want = want[np.argsort(want[:, 0], kind="stable")]
+        assert np.array_equal(got, want), (n0, n1, n2)
